@@ -1,0 +1,225 @@
+/*
+ * whir_b200 — C ABI of the B200 (sm_100a) implementation of the WHIR prover
+ * hot path of tcoratger/whir-p3 (KoalaBear base field, degree-4 binomial
+ * extension, Poseidon2 Merkle commitments, duplex-sponge Fiat-Shamir).
+ *
+ * Conventions
+ *   - Every function returns an int status: WHIR_OK (0) or a negative
+ *     WHIR_ERR_* code; whir_last_error() describes the last failure of the
+ *     calling thread. No C++ exception crosses this boundary.
+ *   - Field elements passed through HOST pointers are canonical uint32 values
+ *     in [0, p), p = 2^31 - 2^24 + 1. An extension element is 4 consecutive
+ *     words (coefficients of 1, X, X^2, X^3 with X^4 = 3).
+ *   - Field elements in DEVICE buffers are in Montgomery form (x * 2^32 mod p).
+ *     whir_monty_encode / whir_monty_decode convert device buffers in place.
+ *   - A whir_ctx owns one CUDA stream on one device; calls on a context are
+ *     ordered on its stream and must come from one host thread at a time.
+ *     Functions that return values to the host synchronize that stream.
+ *
+ * Each entry point cites the reference interface it replaces (paths are
+ * inside the reference project; Plonky3 items are at git rev c38eb05).
+ */
+#ifndef WHIR_B200_H
+#define WHIR_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum {
+  WHIR_OK = 0,
+  WHIR_ERR_INVALID = -1,     /* bad argument or unsupported shape */
+  WHIR_ERR_CUDA = -2,        /* a CUDA runtime call failed */
+  WHIR_ERR_NOMEM = -3,       /* device or host allocation failed */
+  WHIR_ERR_NOT_FOUND = -4,   /* proof-of-work search exhausted its limit */
+  WHIR_ERR_BUFFER = -5,      /* caller buffer too small; required size reported */
+  WHIR_ERR_NO_DEVICE = -6    /* no CUDA device available */
+};
+
+typedef struct whir_ctx whir_ctx;
+typedef struct whir_witness whir_witness;
+
+/* Poseidon2 permutation data (canonical values). Supported shapes: width 16
+ * with 8 full + 20 partial rounds, width 24 with 8 full + 23 partial rounds.
+ * Replaces p3-koala-bear Poseidon2KoalaBear<16>/<24> (src/bin/main.rs:31-32). */
+typedef struct {
+  uint32_t width;
+  uint32_t rounds_f;
+  uint32_t rounds_p;
+  uint32_t ext_rc[8 * 24]; /* rounds_f rows of `width`: first half before, second half after the partial rounds */
+  uint32_t int_rc[32];     /* one per partial round, added to lane 0 */
+  uint32_t diag[24];       /* internal matrix = all-ones + diag(diag) */
+} whir_poseidon2_params;
+
+/* ProtocolParameters (src/parameters/mod.rs:147-166) plus the hash and
+ * domain-separator choices of the caller's set-up (src/bin/main.rs:34-39,178-180). */
+typedef struct {
+  int32_t security_level;
+  int32_t pow_bits;
+  int32_t folding_factor_0;      /* FoldingFactor::ConstantFromSecondRound(f0, f); Constant(f) has f0 == f */
+  int32_t folding_factor;
+  int32_t soundness;             /* 0 UniqueDecoding, 1 JohnsonBound, 2 CapacityBound */
+  int32_t starting_log_inv_rate;
+  int32_t rs_reduction;          /* rs_domain_initial_reduction_factor */
+  int32_t leaf_hash;             /* 0: PaddingFreeSponge<P24,24,16,8>; 1: PaddingFreeSponge<P16,16,8,8> */
+  int32_t ds_digest_elems;       /* DIGEST_ELEMS constant given to DomainSeparator::commit_statement */
+} whir_protocol_params;
+
+#define WHIR_MAX_ROUNDS 32
+/* RoundConfig (src/whir/parameters.rs:31-40); folded_domain_gen canonical */
+typedef struct {
+  int32_t pow_bits, folding_pow_bits, num_queries, ood_samples, num_variables, folding_factor;
+  uint64_t domain_size;
+  uint32_t folded_domain_gen;
+} whir_round_config;
+
+/* WhirConfig (src/whir/parameters.rs:43-68) */
+typedef struct {
+  int32_t num_variables, security_level, max_pow_bits, commitment_ood_samples;
+  int32_t starting_log_inv_rate, starting_folding_pow_bits;
+  int32_t folding_factor_0, folding_factor, rs_reduction, soundness;
+  int32_t n_rounds;
+  whir_round_config rounds[WHIR_MAX_ROUNDS];
+  int32_t final_queries, final_pow_bits, final_sumcheck_rounds, final_folding_pow_bits;
+} whir_config;
+
+/* DuplexChallenger<KoalaBear, Poseidon2-16, 16, 8> state (canonical values):
+ * sponge_state, input_buffer and output_buffer of p3-challenger. */
+typedef struct {
+  uint32_t state[16];
+  uint32_t input[8];
+  int32_t input_len;
+  uint32_t output[8];
+  int32_t output_len;
+} whir_challenger;
+
+/* ---- library / context ---------------------------------------------------- */
+const char* whir_last_error(void);
+/* Number of CUDA kernels this library has enqueued in this process. */
+uint64_t whir_kernel_launches(void);
+/* The library's default Poseidon2 data (seeded stand-in, not Plonky3's). */
+int whir_poseidon2_default_params(whir_poseidon2_params* p16, whir_poseidon2_params* p24);
+int whir_ctx_create(int32_t device, const whir_poseidon2_params* p16, const whir_poseidon2_params* p24,
+                    whir_ctx** out);
+int whir_ctx_destroy(whir_ctx* ctx);
+/* Enqueue on a caller-owned cudaStream_t instead of the context's own stream. */
+int whir_ctx_set_stream(whir_ctx* ctx, void* cuda_stream);
+int whir_ctx_synchronize(whir_ctx* ctx);
+/* Host permutation with the context's data (width taken from the state length 16 or 24). */
+int whir_poseidon2_permute(const whir_ctx* ctx, uint32_t* state, int32_t width);
+
+/* ---- parameters (WhirConfig::new, src/whir/parameters.rs:81-234) ----------- */
+int whir_config_new(const whir_protocol_params* params, int32_t num_variables, whir_config* out);
+/* DomainSeparator::commit_statement + add_whir_proof pattern
+ * (src/fiat_shamir/domain_separator.rs:95-213); returns the pattern length
+ * (>= 0) and writes min(length, cap) words. */
+int whir_domain_separator(const whir_config* cfg, int32_t digest_elems, uint32_t* out, int32_t cap);
+
+/* ---- challenger (p3-challenger DuplexChallenger + GrindingChallenger) ------- */
+void whir_challenger_init(whir_challenger* ch);
+int whir_challenger_observe(const whir_ctx* ctx, whir_challenger* ch, const uint32_t* values, size_t n);
+int whir_challenger_sample(const whir_ctx* ctx, whir_challenger* ch, uint32_t* out, size_t n);
+int whir_challenger_sample_bits(const whir_ctx* ctx, whir_challenger* ch, int32_t bits, uint64_t* out);
+/* GrindingChallenger::grind (called at src/whir/proof.rs:188,
+ * src/whir/prover/mod.rs:224,363): searches on the GPU and returns the
+ * smallest witness; absorbs it into `ch` like the reference. */
+int whir_challenger_grind(whir_ctx* ctx, whir_challenger* ch, int32_t bits, uint32_t* witness);
+/* GrindingChallenger::check_witness: 1 valid, 0 invalid, < 0 error */
+int whir_challenger_check_witness(const whir_ctx* ctx, whir_challenger* ch, int32_t bits, uint32_t witness);
+
+/* ---- device buffers ------------------------------------------------------- */
+int whir_device_alloc(whir_ctx* ctx, size_t bytes, void** d_ptr);
+int whir_device_free(whir_ctx* ctx, void* d_ptr);
+int whir_memcpy_h2d(whir_ctx* ctx, void* d_dst, const void* h_src, size_t bytes);
+int whir_memcpy_d2h(whir_ctx* ctx, void* h_dst, const void* d_src, size_t bytes);
+int whir_monty_encode(whir_ctx* ctx, uint32_t* d_words, size_t n);
+int whir_monty_decode(whir_ctx* ctx, uint32_t* d_words, size_t n);
+
+/* ---- Plonky3 trait kernels (device buffers, Montgomery form) -------------- */
+/* transpose & pad & TwoAdicSubgroupDft::dft_batch / dft_algebra_batch
+ * (src/whir/committer/writer.rs:70-86, src/whir/prover/mod.rs:166-180):
+ * 2^log_width contiguous chunks of 2^log_chunk elements (ext: 4 words each) ->
+ * row-major matrix of 2^(log_chunk+log_blowup) rows x 2^log_width elements. */
+int whir_dft_batch(whir_ctx* ctx, const uint32_t* d_chunks, int32_t log_chunk, int32_t log_width,
+                   int32_t log_blowup, int32_t ext, uint32_t* d_out);
+/* Mmcs::commit_matrix (MerkleTreeMmcs, writer.rs:89, prover/mod.rs:182-184).
+ * d_digests: (2 * 2^log_height - 1) * 8 words, leaf digests first; root (host) canonical. */
+int whir_merkle_commit(whir_ctx* ctx, const uint32_t* d_rows, int32_t log_height, int32_t row_words,
+                       int32_t leaf_hash, uint32_t* d_digests, uint32_t* root);
+/* Mmcs::open_batch (prover/mod.rs:248-300): row (row_words) and sibling path
+ * (log_height digests, leaf level first) for `index`, canonical, to host. */
+int whir_merkle_open(whir_ctx* ctx, const uint32_t* d_rows, const uint32_t* d_digests, int32_t log_height,
+                     int32_t row_words, uint64_t index, uint32_t* row_out, uint32_t* path_out);
+
+/* ---- multilinear kernels (src/poly/evals.rs); points/challenges on host ---- */
+/* EvaluationsList::new_from_point (evals.rs:312-320): d_out[x] = scale*eq(point, x) */
+int whir_eq_table(whir_ctx* ctx, const uint32_t* point, int32_t n, const uint32_t* scale, uint32_t* d_out);
+/* evaluate_hypercube_base / evaluate_hypercube_ext (evals.rs:334-366) */
+int whir_eval_base(whir_ctx* ctx, const uint32_t* d_evals, int32_t n, const uint32_t* point, uint32_t* out);
+int whir_eval_ext(whir_ctx* ctx, const uint32_t* d_evals, int32_t n, const uint32_t* point, uint32_t* out);
+/* compress (evals.rs:127-148), in place: keeps the first 2^(n-1) entries */
+int whir_fold_ext(whir_ctx* ctx, uint32_t* d_evals, int32_t n, const uint32_t* r);
+/* compress_ext (evals.rs:382-400): base -> extension */
+int whir_fold_base(whir_ctx* ctx, const uint32_t* d_evals, int32_t n, const uint32_t* r, uint32_t* d_out);
+/* compress_multi_into_packed (evals.rs:422-447), k <= 6 */
+int whir_fold_multi_base(whir_ctx* ctx, const uint32_t* d_evals, int32_t n, const uint32_t* rs, int32_t k,
+                         uint32_t* d_out);
+/* sumcheck_coefficients (evals.rs:493-526) on extension f, w */
+int whir_sumcheck_coeffs(whir_ctx* ctx, const uint32_t* d_f, const uint32_t* d_w, int32_t n, uint32_t* c0,
+                         uint32_t* c2);
+/* EqStatement::combine_hypercube with INITIALIZED (statement/eq.rs:182-246):
+ * d_w[x] += sum_i gamma_pows[i] * eq(points_i, x); m <= 16 */
+int whir_combine_eq(whir_ctx* ctx, uint32_t* d_w, int32_t n, const uint32_t* points, int32_t m,
+                    const uint32_t* gamma_pows);
+/* SelectStatement::combine (statement/select.rs:296-380): d_w[x] += sum_j gamma_pows[j] * vars_j^x */
+int whir_combine_select(whir_ctx* ctx, uint32_t* d_w, int32_t n, const uint32_t* vars, int32_t m,
+                        const uint32_t* gamma_pows);
+/* SplitEqInner::partial_evals (src/sumcheck/svo.rs:465-502): out[y] =
+ * sum_x poly[y*2^(n-l) + x] * eq(point[l..], x) for y < 2^l, and the full
+ * evaluation poly(point) in eval_out (may be NULL). */
+int whir_svo_partial_evals(whir_ctx* ctx, const uint32_t* d_poly, int32_t n, int32_t l, const uint32_t* point,
+                           uint32_t* out, uint32_t* eval_out);
+
+/* ---- protocol entry points -------------------------------------------------
+ * Proof encoding (uint32 words, canonical values):
+ *   0x50524857 'WHRP', 1,
+ *   root[8], n_ood, ood[4*n_ood],                                  (commit)
+ *   sumcheck, n_rounds,
+ *   per round: root[8], n_ood, ood[4*n_ood], pow_witness, n_queries,
+ *              queries, sumcheck,
+ *   n_final, final_poly[4*n_final], final_pow_witness, n_final_queries,
+ *   queries, has_final_sumcheck, [sumcheck]
+ * sumcheck = n_polys, (c0[4], c2[4]) * n_polys, n_pow, pow[n_pow]
+ * query    = kind (0 base, 1 ext), n_values, values, path_len, path[8*path_len]
+ * This mirrors WhirProof (src/whir/proof.rs:17-121) field by field.
+ */
+/* InitialStatement::evaluate for each user point (src/whir/constraints/statement/initial.rs:143-152)
+ * followed by CommitmentWriter::commit (src/whir/committer/writer.rs:56-109).
+ * poly: 2^n values, host canonical (poly_on_device = 0) or device Montgomery
+ * (poly_on_device = 1, borrowed until whir_witness_free). user_points: num_points
+ * * n extension elements; user_evals_out receives num_points evaluations (may
+ * be NULL). The challenger must already have observed the domain separator. */
+int whir_commit(whir_ctx* ctx, const whir_protocol_params* params, int32_t n, const uint32_t* poly,
+                int32_t poly_on_device, const uint32_t* user_points, int32_t num_points, uint32_t* user_evals_out,
+                whir_challenger* ch, whir_witness** out);
+/* Prover::prove (src/whir/prover/mod.rs:97-128); writes the whole proof
+ * (commit part included). proof_words receives the length; WHIR_ERR_BUFFER if
+ * cap_words is too small (the witness stays usable for a retry only before proving). */
+int whir_prove(whir_ctx* ctx, whir_witness* w, whir_challenger* ch, uint32_t* proof_out, size_t cap_words,
+               size_t* proof_words);
+int whir_witness_free(whir_witness* w);
+
+/* Convenience: domain separator + commit + prove + one checkpoint sample
+ * (the sequence of src/whir/mod.rs:103-141). checkpoint may be NULL. */
+int whir_commit_and_prove(whir_ctx* ctx, const whir_protocol_params* params, int32_t n, const uint32_t* poly,
+                          int32_t poly_on_device, const uint32_t* user_points, int32_t num_points,
+                          uint32_t* user_evals_out, uint32_t* proof_out, size_t cap_words, size_t* proof_words,
+                          uint32_t* checkpoint);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -19,3 +19,26 @@ def oracle():
     from oracle.oracle import Oracle
 
     return Oracle()
+
+
+@pytest.fixture(scope="session")
+def pkg():
+    import __graft_entry__
+
+    mod = __graft_entry__.load_package()
+    mod.lib()
+    return mod
+
+
+@pytest.fixture(scope="session")
+def host_ctx(pkg):
+    ctx = pkg.Context(-1)
+    yield ctx
+    ctx.close()
+
+
+@pytest.fixture(scope="session")
+def gpu_ctx(pkg):
+    ctx = pkg.Context(0)
+    yield ctx
+    ctx.close()

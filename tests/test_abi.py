@@ -1,0 +1,118 @@
+"""C-ABI boundary checks that need no GPU: the library loads, exports every
+symbol declared in include/whir_b200.h, and its host-side logic (Poseidon2
+data and permutation, WhirConfig derivation, domain separator, duplex
+challenger) agrees with the oracle word for word."""
+import re
+
+import numpy as np
+import pytest
+
+from conftest import ROOT
+from oracle.oracle import Chal, P, make_params
+
+
+def header_functions():
+    text = (ROOT / "include" / "whir_b200.h").read_text()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b(whir_[a-z0-9_]+)\s*\(", text)))
+
+
+def test_library_exports_every_header_symbol(pkg):
+    lib = pkg.lib()
+    names = header_functions()
+    assert len(names) >= 35
+    missing = [n for n in names if not hasattr(lib, n)]
+    assert not missing, missing
+
+
+def test_host_only_context_rejects_device_work(pkg, host_ctx):
+    arr_ptr = None
+    with pytest.raises(pkg.WhirError) as e:
+        pkg.lib()
+        pkg._check(pkg.lib().whir_monty_encode(host_ctx.handle, arr_ptr, 0))
+    assert e.value.code == -6
+
+
+def test_default_poseidon2_matches_oracle(pkg, oracle):
+    p16, p24 = pkg.default_poseidon2()
+    for a, b in ((p16, oracle.p16), (p24, oracle.p24)):
+        assert (a.width, a.rounds_f, a.rounds_p) == (b.width, b.rounds_f, b.rounds_p)
+        assert list(a.ext_rc) == list(b.ext_rc)
+        assert list(a.int_rc) == list(b.int_rc)
+        assert list(a.diag) == list(b.diag)
+
+
+@pytest.mark.parametrize("width", [16, 24])
+def test_permutation_matches_oracle(host_ctx, oracle, width):
+    rng = np.random.default_rng(width)
+    for _ in range(20):
+        s = rng.integers(0, P, width, dtype=np.uint64).astype(np.uint32)
+        assert np.array_equal(host_ctx.permute(s), oracle.permute(s))
+    # edge values
+    for v in (0, 1, P - 1):
+        s = np.full(width, v, dtype=np.uint32)
+        assert np.array_equal(host_ctx.permute(s), oracle.permute(s))
+
+
+def _cfg_tuple(c):
+    rounds = [(r.pow_bits, r.folding_pow_bits, r.num_queries, r.ood_samples, r.num_variables, r.folding_factor,
+               r.domain_size, r.folded_domain_gen) for r in list(c.rounds)[: c.n_rounds]]
+    return (c.num_variables, c.commitment_ood_samples, c.starting_folding_pow_bits, c.n_rounds, rounds,
+            c.final_queries, c.final_pow_bits, c.final_sumcheck_rounds, c.final_folding_pow_bits)
+
+
+CONFIG_GRID = [(n, sec, pw, f0, f, snd, r, rs) for n in (1, 4, 7, 10, 16, 18, 20, 24, 26)
+               for sec in (32, 90, 100, 128) for pw in (0, 16, 20) for (f0, f) in ((1, 1), (2, 2), (3, 2), (4, 4), (5, 2))
+               for snd in (0, 1, 2) for r in (1, 2) for rs in (1, 2, 3)
+               if f0 <= n and f <= n and rs <= f0 and n + r - f0 <= 24]
+
+
+def test_config_matches_oracle(pkg, oracle):
+    checked = 0
+    for (n, sec, pw, f0, f, snd, r, rs) in CONFIG_GRID:
+        params = pkg.ProtocolParameters(sec, pw, pkg.FoldingFactor(f0, f), pkg.SecurityAssumption(snd), r, rs)
+        mine = pkg.WhirConfig(n, params)
+        ref = oracle.config(make_params(sec, pw, f, f0, snd, r, rs), n)
+        assert _cfg_tuple(mine._c) == _cfg_tuple(ref), (n, sec, pw, f0, f, snd, r, rs)
+        for dig in (8, 32):
+            assert np.array_equal(pkg.DomainSeparator(mine, dig).pattern, oracle.domain_separator(ref, dig))
+        checked += 1
+    assert checked > 1000
+
+
+def test_config_rejects_invalid(pkg):
+    with pytest.raises(pkg.WhirError):
+        pkg.WhirConfig(3, pkg.ProtocolParameters(folding_factor=pkg.FoldingFactor.constant(5)))
+    with pytest.raises(pkg.WhirError):
+        pkg.WhirConfig(10, pkg.ProtocolParameters(folding_factor=pkg.FoldingFactor.constant(2),
+                                                  rs_domain_initial_reduction_factor=3))
+    with pytest.raises(pkg.WhirError):
+        pkg.WhirConfig(10, pkg.ProtocolParameters(folding_factor=pkg.FoldingFactor.constant(0)))
+
+
+def test_challenger_matches_oracle(pkg, host_ctx, oracle):
+    import ctypes as C
+
+    rng = np.random.default_rng(3)
+    ch = pkg.DuplexChallenger(host_ctx)
+    oc = Chal()
+    oracle.lib.or_chal_init(C.byref(oc))
+    for step in range(300):
+        op = rng.integers(0, 4)
+        if op == 0:
+            vals = rng.integers(0, P, rng.integers(1, 20), dtype=np.uint64).astype(np.uint32)
+            ch.observe_slice(vals)
+            for v in vals:
+                oracle.lib.or_chal_observe(C.byref(oc), C.byref(oracle.p16), int(v))
+        elif op == 1:
+            assert ch.sample() == oracle.lib.or_chal_sample(C.byref(oc), C.byref(oracle.p16))
+        elif op == 2:
+            bits = int(rng.integers(0, 31))
+            assert ch.sample_bits(bits) == oracle.lib.or_chal_sample_bits(C.byref(oc), C.byref(oracle.p16), bits)
+        else:
+            bits = int(rng.integers(1, 4))
+            w = int(rng.integers(0, 64))
+            a = ch.check_witness(bits, w)
+            b = bool(oracle.lib.or_chal_check_witness(C.byref(oc), C.byref(oracle.p16), bits, w))
+            assert a == b
+    assert list(ch.c.state) == list(oc.state)

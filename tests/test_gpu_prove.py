@@ -1,0 +1,98 @@
+"""End-to-end parity of the GPU prover: for the same seeded polynomial,
+constraints and parameters the proof words and the post-proof transcript
+checkpoint equal the oracle's exactly, and the oracle's verifier accepts."""
+import numpy as np
+import pytest
+
+from oracle.oracle import P, make_params
+
+pytestmark = pytest.mark.gpu
+
+
+def rnd(rng, n):
+    return rng.integers(0, P, n, dtype=np.uint64).astype(np.uint32)
+
+
+def run_both(pkg, ctx, oracle, n, sec, pw, f0, f, snd, rate, rs, leaf, dig, npts, seed):
+    rng = np.random.default_rng(seed)
+    poly = rnd(rng, 1 << n)
+    pts = rnd(rng, 4 * n * npts)
+    params = pkg.ProtocolParameters(sec, pw, pkg.FoldingFactor(f0, f), pkg.SecurityAssumption(snd), rate, rs,
+                                    "poseidon2_24" if leaf == 0 else "poseidon2_16", dig)
+    proof, cp, evals = pkg.commit_and_prove(ctx, params, n, poly, pts if npts else None)
+    oprm = make_params(sec, pw, f, f0, snd, rate, rs, leaf, dig)
+    ref, ref_cp = oracle.prove(oprm, n, poly, pts if npts else None)
+    assert proof.size == ref.size
+    if not np.array_equal(proof, ref):
+        first = int(np.nonzero(proof != ref)[0][0])
+        raise AssertionError(f"proof differs at word {first} of {proof.size}")
+    assert np.array_equal(cp, ref_cp)
+    rc, vcp = oracle.verify(oprm, n, pts if npts else None, evals if npts else None, proof)
+    assert rc == 0 and np.array_equal(vcp, cp)
+    return proof
+
+
+def grid():
+    cases = []
+    for rs in (1, 2, 3):
+        for f0, f in [(1, 1), (2, 2), (3, 3), (4, 4), (2, 1), (3, 1), (3, 2), (5, 2)]:
+            if f0 < rs:
+                continue
+            for n in range(f0, 3 * f0 + 1):
+                cases.append((rs, f0, f, n))
+    return cases
+
+
+@pytest.mark.parametrize("rs,f0,f,n", grid())
+def test_e2e_grid(pkg, gpu_ctx, oracle, rs, f0, f, n):
+    """The parameter grid of the reference's test_whir_end_to_end1
+    (src/whir/mod.rs:177-232), with a rotating subset of (points, soundness, pow)."""
+    for j in range(3):
+        npts = (n + j) % 3
+        snd = (n + f0 + j) % 3
+        pw = (0, 5, 10)[(f + j) % 3]
+        run_both(pkg, gpu_ctx, oracle, n, 32, pw, f0, f, snd, 1, rs, 1, 8, npts, 1000 * rs + 100 * f0 + 10 * f + n + j)
+
+
+@pytest.mark.parametrize("leaf,dig", [(0, 32), (1, 8), (0, 8)])
+def test_e2e_hash_and_separator_choices(pkg, gpu_ctx, oracle, leaf, dig):
+    run_both(pkg, gpu_ctx, oracle, 14, 64, 8, 4, 4, 2, 1, 2, leaf, dig, 2, 77 + leaf + dig)
+
+
+def test_e2e_cli_default_shape_n18(pkg, gpu_ctx, oracle):
+    """n = 18, k = 4, rate 1/2, 90-bit CapacityBound, pow_bits 16, rs reduction
+    3 (the reference CLI defaults, src/bin/main.rs:41-67), one constraint."""
+    run_both(pkg, gpu_ctx, oracle, 18, 90, 16, 4, 4, 2, 1, 3, 0, 32, 1, 18)
+
+
+def test_e2e_n20_rs1_four_constraints(pkg, gpu_ctx, oracle):
+    run_both(pkg, gpu_ctx, oracle, 20, 100, 16, 4, 4, 2, 1, 1, 0, 32, 4, 20)
+
+
+def test_split_commit_then_prove_matches(pkg, gpu_ctx):
+    """CommitmentWriter::commit then Prover::prove (two calls, device-resident
+    polynomial) gives the same proof as the one-call path."""
+    rng = np.random.default_rng(5)
+    n = 16
+    poly = rnd(rng, 1 << n)
+    pt = rnd(rng, 4 * n)
+    params = pkg.ProtocolParameters(80, 10, pkg.FoldingFactor.constant(4), pkg.SecurityAssumption.CapacityBound, 1, 2)
+    one, cp1, _ = pkg.commit_and_prove(gpu_ctx, params, n, poly, pt)
+    cfg = pkg.WhirConfig(n, params)
+    ch = pkg.DuplexChallenger(gpu_ctx)
+    pkg.DomainSeparator(cfg).observe_domain_separator(ch)
+    dpoly = pkg.DeviceArray.from_host(gpu_ctx, poly)
+    st = pkg.InitialStatement(dpoly, n)
+    st.evaluate(pt)
+    wit = pkg.CommitmentWriter(cfg).commit(gpu_ctx, ch, st)
+    two = pkg.Prover(cfg).prove(gpu_ctx, ch, wit)
+    wit.free()
+    assert np.array_equal(one, two)
+    assert np.array_equal(ch.sample_algebra_element(), cp1)
+
+
+def test_e2e_headline_n24(pkg, gpu_ctx, oracle):
+    """The reference's benchmark configuration (benches/whir.rs:34-120): n = 24,
+    k = 4, rate 1/2, 100-bit CapacityBound, pow_bits 16, rs reduction 3, one
+    constraint, Poseidon2-24 leaves, DIGEST_ELEMS 32."""
+    run_both(pkg, gpu_ctx, oracle, 24, 100, 16, 4, 4, 2, 1, 3, 0, 32, 1, 24)

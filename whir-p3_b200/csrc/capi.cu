@@ -1,0 +1,649 @@
+// extern "C" entry points: context, parameters, challenger and the
+// Plonky3-trait / multilinear kernels on caller-owned device buffers.
+#include <string.h>
+
+#include <algorithm>
+
+#include "host.h"
+
+namespace wh {
+const char* last_error();
+}
+
+using kb::ef;
+
+namespace {
+
+constexpr size_t kArenaBytes = 64ull << 20;
+constexpr size_t kPinnedBytes = 8ull << 20;
+
+int check_ctx(const whir_ctx* ctx) {
+  if (!ctx) {
+    wh::set_error("null context");
+    return WHIR_ERR_INVALID;
+  }
+  return WHIR_OK;
+}
+
+// device work needs a context created on a device (not a host-only one)
+int check_gpu(const whir_ctx* ctx) {
+  WH_TRY(check_ctx(ctx));
+  if (ctx->device < 0) {
+    wh::set_error("host-only context (device -1) cannot run device work");
+    return WHIR_ERR_NO_DEVICE;
+  }
+  cudaSetDevice(ctx->device);
+  return WHIR_OK;
+}
+
+ef load_ef_canon(const uint32_t* p) {
+  return ef{{kb::to_mont(p[0]), kb::to_mont(p[1]), kb::to_mont(p[2]), kb::to_mont(p[3])}};
+}
+void store_ef_canon(uint32_t* p, const ef& v) {
+  for (int i = 0; i < 4; i++) p[i] = kb::from_mont(v.c[i]);
+}
+bool canon_ok(const uint32_t* p, size_t n) {
+  for (size_t i = 0; i < n; i++)
+    if (p[i] >= kb::P) return false;
+  return true;
+}
+
+int sync(whir_ctx* ctx) {
+  WH_TRY_CUDA(cudaStreamSynchronize(ctx->stream));
+  return WHIR_OK;
+}
+
+}  // namespace
+
+// shared with prover.cu
+namespace wh {
+
+int ensure_dft_tables(whir_ctx* ctx, int log_h, wk::DftTables* t) {
+  auto it = ctx->dft.find(log_h);
+  if (it == ctx->dft.end()) {
+    DftCache c;
+    WH_TRY_CUDA(cudaMalloc(&c.tw_lo, 4096 * 4));
+    WH_TRY_CUDA(cudaMalloc(&c.tw_hi, 4096 * 4));
+    WH_TRY_CUDA(wk::build_dft_tables(ctx->tw_stage, c.tw_lo, c.tw_hi, log_h, ctx->stream));
+    it = ctx->dft.emplace(log_h, c).first;
+  }
+  t->tw_stage = ctx->tw_stage;
+  t->tw_lo = it->second.tw_lo;
+  t->tw_hi = it->second.tw_hi;
+  return WHIR_OK;
+}
+
+// Split-eq tables of a point with `n` coordinates into the arena at `at`:
+// hi (2^(n-lo)) scaled by `scale`, then lo (2^lo); returns the lo bit count.
+int split_eq_tables(whir_ctx* ctx, const ef* z, int n, const ef& scale, int lo_bits, ef* hi, ef* lo) {
+  wk::EqPoint a;
+  memset(&a, 0, sizeof(a));
+  a.h = n - lo_bits;
+  for (int i = 0; i < a.h; i++) a.z[i] = z[i];
+  a.scale = scale;
+  WH_TRY_CUDA(wk::eq_table_small(a, hi, ctx->stream));
+  wk::EqPoint b;
+  memset(&b, 0, sizeof(b));
+  b.h = lo_bits;
+  for (int i = 0; i < lo_bits; i++) b.z[i] = z[n - lo_bits + i];
+  b.scale = kb::ef_one();
+  WH_TRY_CUDA(wk::eq_table_small(b, lo, ctx->stream));
+  return WHIR_OK;
+}
+
+// sum_x f[x] eq(z, x) for extension (ext=1) or base f of 2^n entries, split
+// into 2^seg_bits segments of 2^(n - seg_bits) (the point covers one segment).
+// Results (Montgomery) land in ctx->d_small[0 .. 2^seg_bits).
+int dot_eq(whir_ctx* ctx, const uint32_t* d_f, int ext, int seg_bits, const ef* z, int m_bits) {
+  if (m_bits > 40) return set_error("dot_eq: size"), WHIR_ERR_INVALID;
+  const int lo_bits = std::min(m_bits, 8);
+  ef* hi = reinterpret_cast<ef*>(ctx->d_arena);
+  ef* lo = hi + ((size_t)1 << (m_bits - lo_bits));
+  WH_TRY(split_eq_tables(ctx, z, m_bits, kb::ef_one(), lo_bits, hi, lo));
+  WH_TRY_CUDA(wk::dot_split(d_f, ext, seg_bits, m_bits, hi, lo, lo_bits, ctx->d_partials, ctx->d_small, ctx->stream));
+  return WHIR_OK;
+}
+
+int fetch(whir_ctx* ctx, void* host, const void* dev, size_t bytes) {
+  if (bytes <= ctx->pinned_bytes) {
+    WH_TRY_CUDA(cudaMemcpyAsync(ctx->h_pinned, dev, bytes, cudaMemcpyDeviceToHost, ctx->stream));
+    WH_TRY(sync(ctx));
+    memcpy(host, ctx->h_pinned, bytes);
+  } else {
+    WH_TRY_CUDA(cudaMemcpyAsync(host, dev, bytes, cudaMemcpyDeviceToHost, ctx->stream));
+    WH_TRY(sync(ctx));
+  }
+  return WHIR_OK;
+}
+
+int upload(whir_ctx* ctx, void* dev, const void* host, size_t bytes) {
+  if (bytes <= ctx->pinned_bytes) {
+    // the staging buffer may still feed an earlier copy: wait for the stream first
+    WH_TRY(sync(ctx));
+    memcpy(ctx->h_pinned, host, bytes);
+    WH_TRY_CUDA(cudaMemcpyAsync(dev, ctx->h_pinned, bytes, cudaMemcpyHostToDevice, ctx->stream));
+  } else {
+    WH_TRY_CUDA(cudaMemcpyAsync(dev, host, bytes, cudaMemcpyHostToDevice, ctx->stream));
+    WH_TRY(sync(ctx));
+  }
+  return WHIR_OK;
+}
+
+// GrindingChallenger::grind on the device, then check_witness on the host
+// state (absorbing the witness exactly as the reference does).
+int grind(whir_ctx* ctx, Chal& ch, int bits, uint32_t* witness) {
+  if (bits <= 0) {
+    *witness = 0;
+    return WHIR_OK;
+  }
+  WH_CHECK(bits <= 30, "grinding bits above 30");
+  // inputs pending beyond 7 never occur (8 inputs trigger a duplexing)
+  WH_TRY_CUDA(wk::grind(ch.st, ch.in, ch.in_len, bits, kb::P, ctx->d_words, ctx->d_words + 1, ctx->p16, ctx->stream));
+  uint32_t w = 0;
+  WH_TRY(fetch(ctx, &w, ctx->d_words, 4));
+  if (w >= kb::P) {
+    set_error("proof-of-work search found no witness");
+    return WHIR_ERR_NOT_FOUND;
+  }
+  ch.observe(ctx->p16, kb::to_mont(w));
+  if (ch.sample_bits(ctx->p16, bits) != 0) {
+    set_error("device grinding returned an invalid witness");
+    return WHIR_ERR_CUDA;
+  }
+  *witness = w;
+  return WHIR_OK;
+}
+
+}  // namespace wh
+
+namespace wh {
+// eq table of k <= 6 challenge coordinates on the host (Montgomery)
+wk::EqSmall eq_small_host(const ef* rs, int k) {
+  wk::EqSmall e;
+  memset(&e, 0, sizeof(e));
+  e.v[0] = kb::ef_one();
+  for (int i = 0; i < k; i++) {
+    // bit i (from the bottom) of y <-> rs[k-1-i]
+    const ef z = rs[k - 1 - i];
+    const int half = 1 << i;
+    for (int y = 0; y < half; y++) {
+      ef lo = e.v[y];
+      ef hi = kb::ef_mul(lo, z);
+      e.v[y + half] = hi;
+      e.v[y] = kb::ef_sub(lo, hi);
+    }
+  }
+  return e;
+}
+}  // namespace wh
+
+namespace wh {
+// W += sum_i scale_i * eq(z_i, .) over 2^n entries (Montgomery inputs)
+int add_eq_points(whir_ctx* ctx, ef* d_w, int n, const std::vector<std::vector<ef>>& pts, const std::vector<ef>& scales,
+                  int accumulate) {
+  const int m = (int)pts.size();
+  if (m == 0) {
+    if (!accumulate) WH_TRY_CUDA(cudaMemsetAsync(d_w, 0, ((size_t)1 << n) * sizeof(ef), ctx->stream));
+    return WHIR_OK;
+  }
+  const int lo_bits = std::min(n, 10);
+  const size_t H = (size_t)1 << (n - lo_bits), Lc = (size_t)1 << lo_bits;
+  WH_CHECK((H + Lc) * (size_t)m * sizeof(ef) <= ctx->arena_bytes, "too many constraints for the scratch arena");
+  ef* hi = reinterpret_cast<ef*>(ctx->d_arena);
+  ef* lo = hi + H * m;
+  for (int c = 0; c < m; c++) WH_TRY(split_eq_tables(ctx, pts[c].data(), n, scales[c], lo_bits, hi + H * c, lo + Lc * c));
+  for (int c0 = 0; c0 < m; c0 += 16) {
+    const int cnt = std::min(16, m - c0);
+    WH_TRY_CUDA(wk::add_eq_batch(d_w, n, hi + H * c0, lo + Lc * c0, lo_bits, cnt, accumulate || c0 > 0, ctx->stream));
+  }
+  return WHIR_OK;
+}
+
+// W += sum_j g_j * vars_j^x (vars base field, Montgomery)
+int add_select_vars(whir_ctx* ctx, ef* d_w, int n, const std::vector<uint32_t>& vars, const std::vector<ef>& g) {
+  const int m = (int)vars.size();
+  if (m == 0) return WHIR_OK;
+  const int lo_bits = std::min(n, 10);
+  const size_t Lc = (size_t)1 << lo_bits, H = (size_t)1 << (n - lo_bits);
+  const size_t need = (size_t)m * 4 + (size_t)m * sizeof(ef) + (size_t)m * (Lc + H) * 4 + 64;
+  WH_CHECK(need <= ctx->arena_bytes, "too many select constraints for the scratch arena");
+  uint8_t* base = reinterpret_cast<uint8_t*>(ctx->d_arena);
+  ef* d_g = reinterpret_cast<ef*>(base);
+  uint32_t* d_vars = reinterpret_cast<uint32_t*>(d_g + m);
+  uint32_t* pow_lo = d_vars + ((m + 3) & ~3);
+  uint32_t* pow_hi = pow_lo + (size_t)m * Lc;
+  std::vector<uint8_t> host((size_t)m * sizeof(ef) + (size_t)m * 4);
+  memcpy(host.data(), g.data(), (size_t)m * sizeof(ef));
+  memcpy(host.data() + (size_t)m * sizeof(ef), vars.data(), (size_t)m * 4);
+  WH_TRY(upload(ctx, d_g, host.data(), host.size()));
+  WH_TRY_CUDA(wk::select_tables(d_vars, m, n, lo_bits, pow_lo, pow_hi, ctx->stream));
+  WH_TRY_CUDA(wk::add_select(d_w, n, pow_lo, pow_hi, lo_bits, d_g, m, ctx->stream));
+  return WHIR_OK;
+}
+}  // namespace wh
+
+extern "C" {
+
+const char* whir_last_error(void) { return wh::last_error(); }
+uint64_t whir_kernel_launches(void) { return wk::launches(); }
+
+int whir_poseidon2_default_params(whir_poseidon2_params* p16, whir_poseidon2_params* p24) {
+  wh::default_params(p16, p24);
+  return WHIR_OK;
+}
+
+int whir_ctx_create(int32_t device, const whir_poseidon2_params* p16, const whir_poseidon2_params* p24,
+                    whir_ctx** out) {
+  if (!out) return wh::set_error("null output"), WHIR_ERR_INVALID;
+  *out = nullptr;
+  if (device == -1) {
+    // host-only context: Poseidon2 data, parameters and transcript, no device
+    whir_poseidon2_params d16, d24;
+    wh::default_params(&d16, &d24);
+    if (!p16) p16 = &d16;
+    if (!p24) p24 = &d24;
+    WH_TRY(wh::validate_params(*p16, 16));
+    WH_TRY(wh::validate_params(*p24, 24));
+    whir_ctx* c = new whir_ctx();
+    c->device = -1;
+    c->p16_params = *p16;
+    c->p24_params = *p24;
+    c->p16 = wh::to_consts(*p16);
+    c->p24 = wh::to_consts(*p24);
+    *out = c;
+    return WHIR_OK;
+  }
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+    cudaGetLastError();
+    wh::set_error("no CUDA device");
+    return WHIR_ERR_NO_DEVICE;
+  }
+  if (device < 0 || device >= ndev) return wh::set_error("device index out of range"), WHIR_ERR_INVALID;
+  whir_poseidon2_params d16, d24;
+  wh::default_params(&d16, &d24);
+  if (!p16) p16 = &d16;
+  if (!p24) p24 = &d24;
+  WH_TRY(wh::validate_params(*p16, 16));
+  WH_TRY(wh::validate_params(*p24, 24));
+  whir_ctx* c = new whir_ctx();
+  c->device = device;
+  c->p16_params = *p16;
+  c->p24_params = *p24;
+  c->p16 = wh::to_consts(*p16);
+  c->p24 = wh::to_consts(*p24);
+  auto fail = [&](int code) {
+    whir_ctx_destroy(c);
+    return code;
+  };
+  if (cudaSetDevice(device) != cudaSuccess) return wh::set_error("cudaSetDevice failed"), fail(WHIR_ERR_CUDA);
+  if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess)
+    return wh::set_error("stream creation failed"), fail(WHIR_ERR_CUDA);
+  c->own_stream = true;
+  if (cudaMalloc(&c->tw_stage, 2048 * 4) != cudaSuccess || cudaMalloc(&c->d_partials, 8192 * sizeof(ef)) != cudaSuccess ||
+      cudaMalloc(&c->d_small, 256 * sizeof(ef)) != cudaSuccess || cudaMalloc(&c->d_words, 64) != cudaSuccess ||
+      cudaMalloc(&c->d_arena, kArenaBytes) != cudaSuccess)
+    return wh::set_error("device allocation failed"), fail(WHIR_ERR_NOMEM);
+  c->arena_bytes = kArenaBytes;
+  if (cudaHostAlloc(&c->h_pinned, kPinnedBytes, cudaHostAllocDefault) != cudaSuccess)
+    return wh::set_error("pinned allocation failed"), fail(WHIR_ERR_NOMEM);
+  c->pinned_bytes = kPinnedBytes;
+  // stage twiddles omega_{2^12}^k come with the first table build
+  wk::DftTables t;
+  int s = wh::ensure_dft_tables(c, 12, &t);
+  if (s != WHIR_OK) return fail(s);
+  if (cudaStreamSynchronize(c->stream) != cudaSuccess) return wh::set_error("initial sync failed"), fail(WHIR_ERR_CUDA);
+  // keep stream-ordered allocations cached between proofs
+  cudaMemPool_t pool;
+  if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) {
+    uint64_t thr = UINT64_MAX;
+    cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr);
+  }
+  *out = c;
+  return WHIR_OK;
+}
+
+int whir_ctx_destroy(whir_ctx* c) {
+  if (!c) return WHIR_OK;
+  if (c->device < 0) {
+    delete c;
+    return WHIR_OK;
+  }
+  cudaSetDevice(c->device);
+  if (c->stream) cudaStreamSynchronize(c->stream);
+  for (auto& kv : c->dft) {
+    cudaFree(kv.second.tw_lo);
+    cudaFree(kv.second.tw_hi);
+  }
+  cudaFree(c->tw_stage);
+  cudaFree(c->d_partials);
+  cudaFree(c->d_small);
+  cudaFree(c->d_words);
+  cudaFree(c->d_arena);
+  if (c->h_pinned) cudaFreeHost(c->h_pinned);
+  if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);
+  delete c;
+  return WHIR_OK;
+}
+
+int whir_ctx_set_stream(whir_ctx* ctx, void* stream) {
+  WH_TRY(check_gpu(ctx));
+  WH_TRY(sync(ctx));
+  if (ctx->own_stream && ctx->stream) cudaStreamDestroy(ctx->stream);
+  ctx->stream = (cudaStream_t)stream;
+  ctx->own_stream = false;
+  return WHIR_OK;
+}
+
+int whir_ctx_synchronize(whir_ctx* ctx) {
+  WH_TRY(check_gpu(ctx));
+  return sync(ctx);
+}
+
+int whir_poseidon2_permute(const whir_ctx* ctx, uint32_t* state, int32_t width) {
+  WH_TRY(check_ctx(ctx));
+  WH_CHECK(state && (width == 16 || width == 24), "width must be 16 or 24");
+  WH_CHECK(canon_ok(state, (size_t)width), "state value out of range");
+  if (width == 16) {
+    uint32_t s[16];
+    for (int i = 0; i < 16; i++) s[i] = kb::to_mont(state[i]);
+    p2::permute<16, p2::RP16>(s, ctx->p16);
+    for (int i = 0; i < 16; i++) state[i] = kb::from_mont(s[i]);
+  } else {
+    uint32_t s[24];
+    for (int i = 0; i < 24; i++) s[i] = kb::to_mont(state[i]);
+    p2::permute<24, p2::RP24>(s, ctx->p24);
+    for (int i = 0; i < 24; i++) state[i] = kb::from_mont(s[i]);
+  }
+  return WHIR_OK;
+}
+
+int whir_config_new(const whir_protocol_params* params, int32_t n, whir_config* out) {
+  WH_CHECK(params && out, "null argument");
+  return wh::config_new(*params, n, out);
+}
+
+int whir_domain_separator(const whir_config* cfg, int32_t digest_elems, uint32_t* out, int32_t cap) {
+  WH_CHECK(cfg, "null config");
+  std::vector<uint32_t> v = wh::domain_separator(*cfg, digest_elems);
+  if (out)
+    for (int32_t i = 0; i < cap && i < (int32_t)v.size(); i++) out[i] = v[i];
+  return (int)v.size();
+}
+
+void whir_challenger_init(whir_challenger* ch) {
+  if (ch) memset(ch, 0, sizeof(*ch));
+}
+
+int whir_challenger_observe(const whir_ctx* ctx, whir_challenger* ch, const uint32_t* values, size_t n) {
+  WH_TRY(check_ctx(ctx));
+  WH_CHECK(ch && (values || n == 0), "null argument");
+  WH_CHECK(canon_ok(values, n), "value out of range");
+  wh::Chal c;
+  c.load(*ch);
+  for (size_t i = 0; i < n; i++) c.observe(ctx->p16, kb::to_mont(values[i]));
+  c.store(*ch);
+  return WHIR_OK;
+}
+
+int whir_challenger_sample(const whir_ctx* ctx, whir_challenger* ch, uint32_t* out, size_t n) {
+  WH_TRY(check_ctx(ctx));
+  WH_CHECK(ch && (out || n == 0), "null argument");
+  wh::Chal c;
+  c.load(*ch);
+  for (size_t i = 0; i < n; i++) out[i] = kb::from_mont(c.sample(ctx->p16));
+  c.store(*ch);
+  return WHIR_OK;
+}
+
+int whir_challenger_sample_bits(const whir_ctx* ctx, whir_challenger* ch, int32_t bits, uint64_t* out) {
+  WH_TRY(check_ctx(ctx));
+  WH_CHECK(ch && out && bits >= 0 && bits < 31, "bad argument");
+  wh::Chal c;
+  c.load(*ch);
+  *out = c.sample_bits(ctx->p16, bits);
+  c.store(*ch);
+  return WHIR_OK;
+}
+
+int whir_challenger_grind(whir_ctx* ctx, whir_challenger* ch, int32_t bits, uint32_t* witness) {
+  WH_TRY(check_gpu(ctx));
+  WH_CHECK(ch && witness && bits >= 0, "bad argument");
+  cudaSetDevice(ctx->device);
+  wh::Chal c;
+  c.load(*ch);
+  if (bits == 0) {
+    *witness = 0;
+    return WHIR_OK;
+  }
+  WH_TRY(wh::grind(ctx, c, bits, witness));
+  c.store(*ch);
+  return WHIR_OK;
+}
+
+int whir_challenger_check_witness(const whir_ctx* ctx, whir_challenger* ch, int32_t bits, uint32_t witness) {
+  WH_TRY(check_ctx(ctx));
+  WH_CHECK(ch && bits >= 0 && bits < 31 && witness < kb::P, "bad argument");
+  if (bits == 0) return 1;
+  wh::Chal c;
+  c.load(*ch);
+  c.observe(ctx->p16, kb::to_mont(witness));
+  const int ok = c.sample_bits(ctx->p16, bits) == 0;
+  c.store(*ch);
+  return ok;
+}
+
+int whir_device_alloc(whir_ctx* ctx, size_t bytes, void** d_ptr) {
+  WH_TRY(check_gpu(ctx));
+  WH_CHECK(d_ptr, "null argument");
+  cudaSetDevice(ctx->device);
+  WH_TRY_CUDA(cudaMalloc(d_ptr, bytes ? bytes : 1));
+  return WHIR_OK;
+}
+int whir_device_free(whir_ctx* ctx, void* d_ptr) {
+  WH_TRY(check_gpu(ctx));
+  WH_TRY(sync(ctx));
+  WH_TRY_CUDA(cudaFree(d_ptr));
+  return WHIR_OK;
+}
+int whir_memcpy_h2d(whir_ctx* ctx, void* d_dst, const void* h_src, size_t bytes) {
+  WH_TRY(check_gpu(ctx));
+  WH_TRY_CUDA(cudaMemcpyAsync(d_dst, h_src, bytes, cudaMemcpyHostToDevice, ctx->stream));
+  return sync(ctx);
+}
+int whir_memcpy_d2h(whir_ctx* ctx, void* h_dst, const void* d_src, size_t bytes) {
+  WH_TRY(check_gpu(ctx));
+  WH_TRY_CUDA(cudaMemcpyAsync(h_dst, d_src, bytes, cudaMemcpyDeviceToHost, ctx->stream));
+  return sync(ctx);
+}
+int whir_monty_encode(whir_ctx* ctx, uint32_t* d, size_t n) {
+  WH_TRY(check_gpu(ctx));
+  WH_TRY_CUDA(wk::encode(d, n, ctx->stream));
+  return WHIR_OK;
+}
+int whir_monty_decode(whir_ctx* ctx, uint32_t* d, size_t n) {
+  WH_TRY(check_gpu(ctx));
+  WH_TRY_CUDA(wk::decode(d, n, ctx->stream));
+  return WHIR_OK;
+}
+
+int whir_dft_batch(whir_ctx* ctx, const uint32_t* d_chunks, int32_t log_chunk, int32_t log_width, int32_t log_blowup,
+                   int32_t ext, uint32_t* d_out) {
+  WH_TRY(check_gpu(ctx));
+  WH_CHECK(d_chunks && d_out && log_chunk >= 0 && log_width >= 0 && log_width <= 12 && log_blowup >= 0 &&
+               log_chunk + log_blowup <= 24,
+           "bad DFT shape");
+  const int lanes = ext ? 4 : 1;
+  const int log_h = log_chunk + log_blowup;
+  wk::DftTables t;
+  WH_TRY(wh::ensure_dft_tables(ctx, log_h, &t));
+  uint32_t* scratch = nullptr;
+  const size_t bytes = ((size_t)1 << (log_h + log_width)) * 4 * lanes;
+  WH_TRY_CUDA(cudaMallocAsync(&scratch, bytes, ctx->stream));
+  cudaError_t e = wk::dft_batch(d_chunks, d_out, scratch, log_chunk, log_width, log_blowup, lanes, t, ctx->stream);
+  cudaFreeAsync(scratch, ctx->stream);
+  if (e == cudaErrorInvalidValue) return wh::set_error("unsupported DFT shape"), WHIR_ERR_INVALID;
+  WH_TRY_CUDA(e);
+  return WHIR_OK;
+}
+
+int whir_merkle_commit(whir_ctx* ctx, const uint32_t* d_rows, int32_t log_height, int32_t row_words,
+                       int32_t leaf_hash, uint32_t* d_digests, uint32_t* root) {
+  WH_TRY(check_gpu(ctx));
+  WH_CHECK(d_rows && d_digests && log_height >= 0 && log_height <= 30 && row_words > 0 &&
+               (leaf_hash == 0 || leaf_hash == 1),
+           "bad Merkle arguments");
+  WH_TRY_CUDA(wk::merkle_build(d_rows, log_height, row_words, leaf_hash, d_digests, ctx->p16, ctx->p24, ctx->stream));
+  if (root) {
+    const size_t h = (size_t)1 << log_height;
+    uint32_t r[8];
+    WH_TRY(wh::fetch(ctx, r, d_digests + (2 * h - 2) * 8, 32));
+    for (int i = 0; i < 8; i++) root[i] = kb::from_mont(r[i]);
+  }
+  return WHIR_OK;
+}
+
+int whir_merkle_open(whir_ctx* ctx, const uint32_t* d_rows, const uint32_t* d_digests, int32_t log_height,
+                     int32_t row_words, uint64_t index, uint32_t* row_out, uint32_t* path_out) {
+  WH_TRY(check_gpu(ctx));
+  WH_CHECK(d_rows && d_digests && row_out && path_out && index < (1ull << log_height) && row_words > 0,
+           "bad opening arguments");
+  uint64_t* d_idx = reinterpret_cast<uint64_t*>(ctx->d_arena);
+  uint32_t* d_row = reinterpret_cast<uint32_t*>(d_idx + 8);
+  uint32_t* d_path = d_row + row_words;
+  WH_TRY(wh::upload(ctx, d_idx, &index, 8));
+  WH_TRY_CUDA(wk::merkle_open(d_rows, d_digests, log_height, row_words, d_idx, 1, d_row, d_path, ctx->stream));
+  std::vector<uint32_t> tmp((size_t)row_words + (size_t)log_height * 8);
+  WH_TRY(wh::fetch(ctx, tmp.data(), d_row, tmp.size() * 4));
+  for (int i = 0; i < row_words; i++) row_out[i] = kb::from_mont(tmp[i]);
+  for (int i = 0; i < log_height * 8; i++) path_out[i] = kb::from_mont(tmp[row_words + i]);
+  return WHIR_OK;
+}
+
+int whir_eq_table(whir_ctx* ctx, const uint32_t* point, int32_t n, const uint32_t* scale, uint32_t* d_out) {
+  WH_TRY(check_gpu(ctx));
+  WH_CHECK((point || n == 0) && scale && d_out && n >= 0 && n <= 30, "bad eq-table arguments");
+  WH_CHECK(canon_ok(point, 4 * (size_t)n) && canon_ok(scale, 4), "value out of range");
+  std::vector<ef> z(n);
+  for (int i = 0; i < n; i++) z[i] = load_ef_canon(point + 4 * i);
+  const int lo_bits = std::min(n, 10);
+  ef* hi = reinterpret_cast<ef*>(ctx->d_arena);
+  ef* lo = hi + ((size_t)1 << (n - lo_bits));
+  WH_TRY(wh::split_eq_tables(ctx, z.data(), n, load_ef_canon(scale), lo_bits, hi, lo));
+  WH_TRY_CUDA(wk::eq_outer(hi, lo, lo_bits, (size_t)1 << n, reinterpret_cast<ef*>(d_out), ctx->stream));
+  return WHIR_OK;
+}
+
+static int eval_common(whir_ctx* ctx, const uint32_t* d_evals, int32_t n, const uint32_t* point, uint32_t* out,
+                       int ext) {
+  WH_TRY(check_gpu(ctx));
+  WH_CHECK(d_evals && (point || n == 0) && out && n >= 0 && n <= 30, "bad evaluation arguments");
+  WH_CHECK(canon_ok(point, 4 * (size_t)n), "value out of range");
+  std::vector<ef> z(n > 0 ? n : 1);
+  for (int i = 0; i < n; i++) z[i] = load_ef_canon(point + 4 * i);
+  WH_TRY(wh::dot_eq(ctx, d_evals, ext, 0, z.data(), n));
+  ef r;
+  WH_TRY(wh::fetch(ctx, &r, ctx->d_small, sizeof(ef)));
+  store_ef_canon(out, r);
+  return WHIR_OK;
+}
+
+int whir_eval_base(whir_ctx* ctx, const uint32_t* d_evals, int32_t n, const uint32_t* point, uint32_t* out) {
+  return eval_common(ctx, d_evals, n, point, out, 0);
+}
+int whir_eval_ext(whir_ctx* ctx, const uint32_t* d_evals, int32_t n, const uint32_t* point, uint32_t* out) {
+  return eval_common(ctx, d_evals, n, point, out, 1);
+}
+
+int whir_fold_ext(whir_ctx* ctx, uint32_t* d_evals, int32_t n, const uint32_t* r) {
+  WH_TRY(check_gpu(ctx));
+  WH_CHECK(d_evals && r && n >= 1 && n <= 30 && canon_ok(r, 4), "bad fold arguments");
+  WH_TRY_CUDA(wk::fold_ext(reinterpret_cast<ef*>(d_evals), nullptr, (size_t)1 << (n - 1), load_ef_canon(r), ctx->stream));
+  return WHIR_OK;
+}
+
+int whir_fold_base(whir_ctx* ctx, const uint32_t* d_evals, int32_t n, const uint32_t* r, uint32_t* d_out) {
+  WH_TRY(check_gpu(ctx));
+  WH_CHECK(d_evals && d_out && r && n >= 1 && n <= 30 && canon_ok(r, 4), "bad fold arguments");
+  WH_TRY_CUDA(wk::fold_base(d_evals, (size_t)1 << (n - 1), load_ef_canon(r), reinterpret_cast<ef*>(d_out), ctx->stream));
+  return WHIR_OK;
+}
+
+
+
+int whir_fold_multi_base(whir_ctx* ctx, const uint32_t* d_evals, int32_t n, const uint32_t* rs, int32_t k,
+                         uint32_t* d_out) {
+  WH_TRY(check_gpu(ctx));
+  WH_CHECK(d_evals && d_out && (rs || k == 0) && k >= 0 && k <= 6 && k <= n && n <= 30 && canon_ok(rs, 4 * (size_t)k),
+           "bad fold arguments");
+  std::vector<ef> r(k > 0 ? k : 1);
+  for (int i = 0; i < k; i++) r[i] = load_ef_canon(rs + 4 * i);
+  wk::EqSmall e = wh::eq_small_host(r.data(), k);
+  WH_TRY_CUDA(wk::fold_multi_base(d_evals, k, (size_t)1 << (n - k), e, reinterpret_cast<ef*>(d_out), ctx->stream));
+  return WHIR_OK;
+}
+
+int whir_sumcheck_coeffs(whir_ctx* ctx, const uint32_t* d_f, const uint32_t* d_w, int32_t n, uint32_t* c0,
+                         uint32_t* c2) {
+  WH_TRY(check_gpu(ctx));
+  WH_CHECK(d_f && d_w && c0 && c2 && n >= 1 && n <= 30, "bad sumcheck arguments");
+  WH_TRY_CUDA(wk::sumcheck_coeffs(reinterpret_cast<const ef*>(d_f), reinterpret_cast<const ef*>(d_w),
+                                  (size_t)1 << (n - 1), ctx->d_partials, ctx->d_small, ctx->stream));
+  ef r[2];
+  WH_TRY(wh::fetch(ctx, r, ctx->d_small, sizeof(r)));
+  store_ef_canon(c0, r[0]);
+  store_ef_canon(c2, r[1]);
+  return WHIR_OK;
+}
+
+
+
+int whir_combine_eq(whir_ctx* ctx, uint32_t* d_w, int32_t n, const uint32_t* points, int32_t m,
+                    const uint32_t* gamma_pows) {
+  WH_TRY(check_gpu(ctx));
+  WH_CHECK(d_w && n >= 0 && n <= 30 && m >= 0 && (m == 0 || (points && gamma_pows)), "bad combine arguments");
+  WH_CHECK(canon_ok(points, 4 * (size_t)n * m) && canon_ok(gamma_pows, 4 * (size_t)m), "value out of range");
+  std::vector<std::vector<ef>> pts(m, std::vector<ef>(n));
+  std::vector<ef> sc(m);
+  for (int c = 0; c < m; c++) {
+    for (int i = 0; i < n; i++) pts[c][i] = load_ef_canon(points + 4 * ((size_t)c * n + i));
+    sc[c] = load_ef_canon(gamma_pows + 4 * c);
+  }
+  return wh::add_eq_points(ctx, reinterpret_cast<ef*>(d_w), n, pts, sc, 1);
+}
+
+int whir_combine_select(whir_ctx* ctx, uint32_t* d_w, int32_t n, const uint32_t* vars, int32_t m,
+                        const uint32_t* gamma_pows) {
+  WH_TRY(check_gpu(ctx));
+  WH_CHECK(d_w && n >= 0 && n <= 30 && m >= 0 && (m == 0 || (vars && gamma_pows)), "bad combine arguments");
+  WH_CHECK(canon_ok(vars, (size_t)m) && canon_ok(gamma_pows, 4 * (size_t)m), "value out of range");
+  std::vector<uint32_t> v(m);
+  std::vector<ef> g(m);
+  for (int j = 0; j < m; j++) {
+    v[j] = kb::to_mont(vars[j]);
+    g[j] = load_ef_canon(gamma_pows + 4 * j);
+  }
+  return wh::add_select_vars(ctx, reinterpret_cast<ef*>(d_w), n, v, g);
+}
+
+int whir_svo_partial_evals(whir_ctx* ctx, const uint32_t* d_poly, int32_t n, int32_t l, const uint32_t* point,
+                           uint32_t* out, uint32_t* eval_out) {
+  WH_TRY(check_gpu(ctx));
+  WH_CHECK(d_poly && point && out && l >= 0 && l <= 8 && l <= n && n <= 30, "bad partial-evaluation arguments");
+  WH_CHECK(canon_ok(point, 4 * (size_t)n), "value out of range");
+  std::vector<ef> z(n > 0 ? n : 1);
+  for (int i = 0; i < n; i++) z[i] = load_ef_canon(point + 4 * i);
+  WH_TRY(wh::dot_eq(ctx, d_poly, 0, l, z.data() + l, n - l));
+  std::vector<ef> g((size_t)1 << l);
+  WH_TRY(wh::fetch(ctx, g.data(), ctx->d_small, g.size() * sizeof(ef)));
+  ef eval = kb::ef_zero();
+  wk::EqSmall e = wh::eq_small_host(z.data(), l);
+  for (size_t y = 0; y < g.size(); y++) {
+    store_ef_canon(out + 4 * y, g[y]);
+    eval = kb::ef_add(eval, kb::ef_mul(e.v[y], g[y]));
+  }
+  if (eval_out) store_ef_canon(eval_out, eval);
+  return WHIR_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,93 @@
+// Host-side pieces of the WHIR prover: context, parameter derivation, the
+// duplex-sponge challenger and the proof writer. Internal to the library.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <map>
+#include <string>
+#include <vector>
+
+#include "../../include/whir_b200.h"
+#include "kb.cuh"
+#include "kernels.h"
+#include "poseidon2.cuh"
+
+namespace wh {
+
+void set_error(const std::string& msg);
+
+// status helpers
+#define WH_TRY_CUDA(expr)                                                   \
+  do {                                                                      \
+    cudaError_t _e = (expr);                                                \
+    if (_e != cudaSuccess) {                                                \
+      ::wh::set_error(std::string(#expr) + ": " + cudaGetErrorString(_e)); \
+      return _e == cudaErrorMemoryAllocation ? WHIR_ERR_NOMEM : WHIR_ERR_CUDA; \
+    }                                                                       \
+  } while (0)
+#define WH_TRY(expr)        \
+  do {                      \
+    int _s = (expr);        \
+    if (_s != WHIR_OK) return _s; \
+  } while (0)
+#define WH_CHECK(cond, msg)                 \
+  do {                                      \
+    if (!(cond)) {                          \
+      ::wh::set_error(msg);                 \
+      return WHIR_ERR_INVALID;              \
+    }                                       \
+  } while (0)
+
+p2::P2Consts to_consts(const whir_poseidon2_params& p);  // canonical -> Montgomery
+void default_params(whir_poseidon2_params* p16, whir_poseidon2_params* p24);
+int validate_params(const whir_poseidon2_params& p, uint32_t width);
+
+// WhirConfig::new restated (src/whir/parameters.rs:81-234); returns WHIR_OK or an error
+int config_new(const whir_protocol_params& prm, int n, whir_config* out);
+whir_round_config final_round_config(const whir_config& c);
+int ff_at(const whir_config& c, int round);
+int rsr_at(const whir_config& c, int round);
+std::vector<uint32_t> domain_separator(const whir_config& c, int digest_elems);  // canonical
+
+// DuplexChallenger with Montgomery-form state
+struct Chal {
+  uint32_t st[16];
+  uint32_t in[8];
+  int in_len;
+  uint32_t out[8];
+  int out_len;
+  void init();
+  void duplex(const p2::P2Consts& k);
+  void observe(const p2::P2Consts& k, uint32_t v);  // Montgomery value
+  uint32_t sample(const p2::P2Consts& k);           // Montgomery value
+  uint64_t sample_bits(const p2::P2Consts& k, int bits);
+  kb::ef sample_ef(const p2::P2Consts& k);
+  void observe_ef(const p2::P2Consts& k, const kb::ef& v);
+  void load(const whir_challenger& c);   // canonical -> internal
+  void store(whir_challenger& c) const;  // internal -> canonical
+};
+
+struct DftCache {
+  uint32_t* tw_lo = nullptr;
+  uint32_t* tw_hi = nullptr;
+};
+
+}  // namespace wh
+
+struct whir_ctx {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  bool own_stream = false;
+  whir_poseidon2_params p16_params, p24_params;
+  p2::P2Consts p16, p24;  // Montgomery form
+  uint32_t* tw_stage = nullptr;
+  std::map<int, wh::DftCache> dft;  // per log2(height)
+  // scratch
+  kb::ef* d_partials = nullptr;  // 8192 ef
+  kb::ef* d_small = nullptr;     // 256 ef
+  uint32_t* d_words = nullptr;   // 4 words (grind result, counter)
+  void* d_arena = nullptr;       // general scratch (tables, gathers)
+  size_t arena_bytes = 0;
+  void* h_pinned = nullptr;      // staging for small transfers
+  size_t pinned_bytes = 0;
+};

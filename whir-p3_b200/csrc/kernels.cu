@@ -1,0 +1,898 @@
+// Device kernels of the WHIR prover hot path for sm_100a.
+//
+// Every kernel here is a data-parallel replacement for an O(2^n) loop of the
+// reference prover (tcoratger/whir-p3) or of the Plonky3 code it calls; the
+// sequential Fiat-Shamir spine stays on the host (host.cu). Each kernel names
+// the reference function whose result it reproduces bit for bit.
+//
+// Memory-bound kernels use coalesced 16-byte element accesses and grid-stride
+// loops sized to the SM count; the Poseidon2 kernels keep the permutation state
+// in registers with every round constant an immediate (kernel parameters live
+// in the constant bank).
+#include <atomic>
+
+#include "kernels.h"
+
+using kb::ef;
+using p2::P2Consts;
+
+namespace wk {
+
+static std::atomic<unsigned long long> g_launches{0};
+unsigned long long launches() { return g_launches.load(); }
+void count_launch() { g_launches.fetch_add(1); }
+
+static int g_sms = 0;
+static int sm_count() {
+  if (!g_sms) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&g_sms, cudaDevAttrMultiProcessorCount, dev);
+    if (g_sms <= 0) g_sms = 148;
+  }
+  return g_sms;
+}
+
+static inline unsigned grid_for(size_t work, int threads, int per_sm = 8) {
+  size_t b = (work + threads - 1) / threads;
+  size_t cap = (size_t)sm_count() * per_sm;
+  if (b > cap) b = cap;
+  if (b < 1) b = 1;
+  return (unsigned)b;
+}
+
+#define LAUNCH_DONE() \
+  do {                \
+    count_launch();   \
+    return cudaGetLastError(); \
+  } while (0)
+
+__device__ __forceinline__ ef ld_ef(const ef* p) {
+  uint4 v = __ldg(reinterpret_cast<const uint4*>(p));
+  return ef{{v.x, v.y, v.z, v.w}};
+}
+__device__ __forceinline__ void st_ef(ef* p, const ef& v) {
+  *reinterpret_cast<uint4*>(p) = make_uint4(v.c[0], v.c[1], v.c[2], v.c[3]);
+}
+
+// ---------------------------------------------------------------------------
+// Representation conversion
+// ---------------------------------------------------------------------------
+
+__global__ void k_encode(uint32_t* p, size_t n) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+    p[i] = kb::to_mont(p[i]);
+}
+__global__ void k_decode(uint32_t* p, size_t n) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+    p[i] = kb::from_mont(p[i]);
+}
+cudaError_t encode(uint32_t* p, size_t n, cudaStream_t st) {
+  if (!n) return cudaSuccess;
+  k_encode<<<grid_for(n, 256), 256, 0, st>>>(p, n);
+  LAUNCH_DONE();
+}
+cudaError_t decode(uint32_t* p, size_t n, cudaStream_t st) {
+  if (!n) return cudaSuccess;
+  k_decode<<<grid_for(n, 256), 256, 0, st>>>(p, n);
+  LAUNCH_DONE();
+}
+
+// ---------------------------------------------------------------------------
+// Reductions
+// ---------------------------------------------------------------------------
+
+__device__ __forceinline__ ef warp_sum(ef v) {
+#pragma unroll
+  for (int off = 16; off; off >>= 1) {
+#pragma unroll
+    for (int c = 0; c < 4; c++) v.c[c] = kb::add(v.c[c], __shfl_down_sync(0xffffffffu, v.c[c], off));
+  }
+  return v;
+}
+
+// Block-wide sum of K extension values; thread 0 gets the result.
+template <int K>
+__device__ __forceinline__ void block_sum(ef (&v)[K], ef (&sh)[K][32]) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
+#pragma unroll
+  for (int k = 0; k < K; k++) v[k] = warp_sum(v[k]);
+  if (lane == 0)
+#pragma unroll
+    for (int k = 0; k < K; k++) sh[k][warp] = v[k];
+  __syncthreads();
+  if (warp == 0) {
+#pragma unroll
+    for (int k = 0; k < K; k++) {
+      v[k] = lane < nw ? sh[k][lane] : kb::ef_zero();
+      v[k] = warp_sum(v[k]);
+    }
+  }
+}
+
+// out[i] = sum_{b < nparts} partials[i * nparts + b]
+__global__ void k_sum_partials(const ef* partials, int nparts, ef* out) {
+  __shared__ ef sh[1][32];
+  ef v[1] = {kb::ef_zero()};
+  const ef* p = partials + (size_t)blockIdx.x * nparts;
+  for (int b = threadIdx.x; b < nparts; b += blockDim.x) v[0] = kb::ef_add(v[0], p[b]);
+  block_sum<1>(v, sh);
+  if (threadIdx.x == 0) out[blockIdx.x] = v[0];
+}
+
+// ---------------------------------------------------------------------------
+// DFT (TwoAdicSubgroupDft::dft_batch / dft_algebra_batch as called at
+// src/whir/committer/writer.rs:86 and src/whir/prover/mod.rs:180, including
+// the transpose & pad of writer.rs:70-82 and prover/mod.rs:166-176).
+//
+// Output row r, column j: sum_{i < L} x_j[i] * omega_H^(i*r). With H = H1*H2,
+// i = i1*H2 + i2 and r = r1 + H1*r2:
+//   pass 1 (columns): Y_j[r1][i2] = omega_H^(i2*r1) * DFT_H1(x_j[i1*H2 + i2])[r1]
+//                     (only i1 < L/H2 are nonzero: the zero padding is free)
+//   pass 2 (rows):    out[r1 + H1*r2][j] = DFT_H2(Y_j[r1][.])[r2]
+// Both passes run radix-2 DFTs of <= 2^12 points in shared memory; pass 2
+// writes whole output rows (all columns j of the CTA) contiguously.
+// ---------------------------------------------------------------------------
+
+__global__ void k_dft_tables(uint32_t* tw_stage, uint32_t* tw_lo, uint32_t* tw_hi, uint32_t w12, uint32_t wh,
+                             uint32_t wh_hi) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < 2048) tw_stage[i] = kb::pow(w12, (uint64_t)i);
+  if (i < 4096) {
+    tw_lo[i] = kb::pow(wh, (uint64_t)i);
+    tw_hi[i] = kb::pow(wh_hi, (uint64_t)i);
+  }
+}
+
+cudaError_t build_dft_tables(uint32_t* tw_stage, uint32_t* tw_lo, uint32_t* tw_hi, int log_h, cudaStream_t st) {
+  uint32_t w12 = kb::two_adic_generator(12);
+  uint32_t wh = kb::two_adic_generator(log_h);
+  uint32_t wh_hi = kb::pow(wh, 4096);
+  k_dft_tables<<<16, 256, 0, st>>>(tw_stage, tw_lo, tw_hi, w12, wh, wh_hi);
+  LAUNCH_DONE();
+}
+
+template <int LANES>
+struct Elem;
+template <>
+struct Elem<1> {
+  using T = uint32_t;
+  __device__ static T zero() { return 0u; }
+  __device__ static T add(T a, T b) { return kb::add(a, b); }
+  __device__ static T sub(T a, T b) { return kb::sub(a, b); }
+  __device__ static T mulb(T a, uint32_t w) { return kb::mul(a, w); }
+};
+template <>
+struct Elem<4> {
+  using T = uint4;
+  __device__ static T zero() { return make_uint4(0, 0, 0, 0); }
+  __device__ static T add(T a, T b) {
+    return make_uint4(kb::add(a.x, b.x), kb::add(a.y, b.y), kb::add(a.z, b.z), kb::add(a.w, b.w));
+  }
+  __device__ static T sub(T a, T b) {
+    return make_uint4(kb::sub(a.x, b.x), kb::sub(a.y, b.y), kb::sub(a.z, b.z), kb::sub(a.w, b.w));
+  }
+  __device__ static T mulb(T a, uint32_t w) {
+    return make_uint4(kb::mul(a.x, w), kb::mul(a.y, w), kb::mul(a.z, w), kb::mul(a.w, w));
+  }
+};
+
+__device__ __forceinline__ uint32_t bitrev(uint32_t x, int bits) { return bits ? (__brev(x) >> (32 - bits)) : 0u; }
+
+__device__ __forceinline__ uint32_t tw_pow(const uint32_t* tw_lo, const uint32_t* tw_hi, uint64_t e) {
+  // omega_H^e for e < H <= 2^24
+  return kb::mul(__ldg(tw_lo + (e & 4095)), __ldg(tw_hi + (e >> 12)));
+}
+
+// In-place radix-2 DIT over `nv` vectors of S = 2^log_s points stored
+// contiguously (vector v at a[v*S]); inputs already in bit-reversed order.
+template <int LANES>
+__device__ __forceinline__ void smem_dft(typename Elem<LANES>::T* a, int nv, int log_s, const uint32_t* tw) {
+  using E = Elem<LANES>;
+  const int S = 1 << log_s;
+  const int total = nv * (S >> 1);
+  for (int s = 1; s <= log_s; s++) {
+    const int half = 1 << (s - 1);
+    const int tshift = 12 - s;
+    for (int b = threadIdx.x; b < total; b += blockDim.x) {
+      const int v = b >> (log_s - 1);
+      const int k = b & ((S >> 1) - 1);
+      const int grp = k >> (s - 1), pos = k & (half - 1);
+      const int i0 = v * S + grp * (half << 1) + pos;
+      typename E::T u = a[i0];
+      typename E::T w = E::mulb(a[i0 + half], tw[pos << tshift]);
+      a[i0] = E::add(u, w);
+      a[i0 + half] = E::sub(u, w);
+    }
+    __syncthreads();
+  }
+}
+
+template <int LANES>
+__global__ void k_dft_cols(const typename Elem<LANES>::T* __restrict__ x, typename Elem<LANES>::T* __restrict__ y,
+                           int log_l, int log_h1, int log_h2, int log_h, int tile,
+                           const uint32_t* __restrict__ tw_stage, const uint32_t* __restrict__ tw_lo,
+                           const uint32_t* __restrict__ tw_hi) {
+  using E = Elem<LANES>;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  uint32_t* tw = reinterpret_cast<uint32_t*>(smem_raw);
+  typename E::T* a = reinterpret_cast<typename E::T*>(smem_raw + 2048 * sizeof(uint32_t));
+  const int H1 = 1 << log_h1, H2 = 1 << log_h2;
+  const size_t L = (size_t)1 << log_l;
+  const int L1 = (int)(L >> log_h2);  // nonzero rows of each column vector
+  const int j = blockIdx.y;
+  const int i2_0 = blockIdx.x * tile;
+  const typename E::T* xj = x + (size_t)j * L;
+  typename E::T* yj = y + ((size_t)j << log_h);
+  for (int i = threadIdx.x; i < 2048; i += blockDim.x) tw[i] = __ldg(tw_stage + i);
+  for (int idx = threadIdx.x; idx < tile * H1; idx += blockDim.x) {
+    const int t = idx % tile, i1 = idx / tile;
+    typename E::T v = E::zero();
+    if (i1 < L1) v = xj[(size_t)i1 * H2 + i2_0 + t];
+    a[t * H1 + bitrev((uint32_t)i1, log_h1)] = v;
+  }
+  __syncthreads();
+  smem_dft<LANES>(a, tile, log_h1, tw);
+  for (int idx = threadIdx.x; idx < tile * H1; idx += blockDim.x) {
+    const int t = idx % tile, r1 = idx / tile;
+    const uint64_t e = (uint64_t)(i2_0 + t) * (uint64_t)r1;
+    typename E::T v = a[t * H1 + r1];
+    if (e) v = E::mulb(v, tw_pow(tw_lo, tw_hi, e));
+    yj[((size_t)r1 << log_h2) + i2_0 + t] = v;
+  }
+}
+
+// pass 2: out[r1 + H1*r2][j] = DFT_H2(Y_j[r1][.])[r2], jt columns per CTA
+template <int LANES>
+__global__ void k_dft_rows(const typename Elem<LANES>::T* __restrict__ y, typename Elem<LANES>::T* __restrict__ out,
+                           int log_h1, int log_h2, int log_h, int log_w, int jt,
+                           const uint32_t* __restrict__ tw_stage) {
+  using E = Elem<LANES>;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  uint32_t* tw = reinterpret_cast<uint32_t*>(smem_raw);
+  typename E::T* a = reinterpret_cast<typename E::T*>(smem_raw + 2048 * sizeof(uint32_t));
+  const int H2 = 1 << log_h2;
+  const int r1 = blockIdx.x;
+  const int j0 = blockIdx.y * jt;
+  for (int i = threadIdx.x; i < 2048; i += blockDim.x) tw[i] = __ldg(tw_stage + i);
+  for (int idx = threadIdx.x; idx < jt * H2; idx += blockDim.x) {
+    const int jj = idx >> log_h2, i2 = idx & (H2 - 1);
+    a[jj * H2 + bitrev((uint32_t)i2, log_h2)] = y[((size_t)(j0 + jj) << log_h) + ((size_t)r1 << log_h2) + i2];
+  }
+  __syncthreads();
+  smem_dft<LANES>(a, jt, log_h2, tw);
+  for (int idx = threadIdx.x; idx < jt * H2; idx += blockDim.x) {
+    const int jj = idx % jt, r2 = idx / jt;
+    const size_t row = (size_t)r1 + ((size_t)r2 << log_h1);
+    out[(row << log_w) + j0 + jj] = a[jj * H2 + r2];
+  }
+}
+
+// Small chunks (L <= 2^12): out[a*B + b][j] = DFT_L(x_j[i] * omega_H^(i*b))[a];
+// one CTA per twist b and column group, H = L*B.
+template <int LANES>
+__global__ void k_dft_coset(const typename Elem<LANES>::T* __restrict__ x, typename Elem<LANES>::T* __restrict__ out,
+                            int log_l, int log_b, int log_w, int jt, const uint32_t* __restrict__ tw_stage,
+                            const uint32_t* __restrict__ tw_lo, const uint32_t* __restrict__ tw_hi) {
+  using E = Elem<LANES>;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  uint32_t* tw = reinterpret_cast<uint32_t*>(smem_raw);
+  typename E::T* a = reinterpret_cast<typename E::T*>(smem_raw + 2048 * sizeof(uint32_t));
+  const int L = 1 << log_l;
+  const uint32_t b = blockIdx.x;
+  const int j0 = blockIdx.y * jt;
+  for (int i = threadIdx.x; i < 2048; i += blockDim.x) tw[i] = __ldg(tw_stage + i);
+  for (int idx = threadIdx.x; idx < jt * L; idx += blockDim.x) {
+    const int jj = idx >> log_l, i = idx & (L - 1);
+    typename E::T v = x[(size_t)(j0 + jj) * L + i];
+    const uint64_t e = (uint64_t)i * b;
+    if (e) v = E::mulb(v, tw_pow(tw_lo, tw_hi, e));
+    a[jj * L + bitrev((uint32_t)i, log_l)] = v;
+  }
+  __syncthreads();
+  smem_dft<LANES>(a, jt, log_l, tw);
+  for (int idx = threadIdx.x; idx < jt * L; idx += blockDim.x) {
+    const int jj = idx % jt, r = idx / jt;
+    const size_t row = ((size_t)r << log_b) + b;
+    out[(row << log_w) + j0 + jj] = a[jj * L + r];
+  }
+}
+
+static int pow2_clamp(long v, int lo, int hi) {
+  int r = lo;
+  while ((long)r * 2 <= v && r * 2 <= hi) r *= 2;
+  return r;
+}
+
+template <typename K>
+static void set_smem(K kernel, size_t bytes) {
+  cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+}
+
+cudaError_t dft_batch(const uint32_t* in, uint32_t* out, uint32_t* scratch, int log_chunk, int log_w,
+                      int log_blowup, int lanes, const DftTables& t, cudaStream_t st) {
+  const int log_h = log_chunk + log_blowup;
+  if (log_h > 24 || log_chunk < 0 || log_blowup < 0 || (lanes != 1 && lanes != 4)) return cudaErrorInvalidValue;
+  const int W = 1 << log_w;
+  const long ebytes = 4 * lanes;
+  const long budget = 64 * 1024;
+  const size_t tw_bytes = 2048 * 4;
+  const int max_single = lanes == 1 ? 12 : 11;
+  if (log_chunk <= max_single) {
+    const int L = 1 << log_chunk;
+    const int jt = pow2_clamp(budget / (L * ebytes), 1, W);
+    const size_t smem = tw_bytes + (size_t)jt * L * ebytes;
+    dim3 grid(1u << log_blowup, W / jt);
+    if (lanes == 1) {
+      set_smem(k_dft_coset<1>, smem);
+      k_dft_coset<1><<<grid, 256, smem, st>>>(in, out, log_chunk, log_blowup, log_w, jt, t.tw_stage, t.tw_lo, t.tw_hi);
+    } else {
+      set_smem(k_dft_coset<4>, smem);
+      k_dft_coset<4><<<grid, 256, smem, st>>>(reinterpret_cast<const uint4*>(in), reinterpret_cast<uint4*>(out),
+                                              log_chunk, log_blowup, log_w, jt, t.tw_stage, t.tw_lo, t.tw_hi);
+    }
+    LAUNCH_DONE();
+  }
+  int log_h2 = lanes == 1 ? 11 : 10;
+  if (log_h - log_h2 > 12) log_h2 = log_h - 12;
+  int log_h1 = log_h - log_h2;
+  if (log_h2 > max_single || log_h1 > 12 || log_h1 < log_blowup || log_h2 > log_chunk) return cudaErrorInvalidValue;
+  const int H1 = 1 << log_h1, H2 = 1 << log_h2;
+  {
+    int tile = pow2_clamp(budget / ((long)H1 * ebytes), 1, lanes == 1 ? 16 : 8);
+    if (tile > H2) tile = H2;
+    const size_t smem = tw_bytes + (size_t)tile * H1 * ebytes;
+    dim3 grid(H2 / tile, W);
+    if (lanes == 1) {
+      set_smem(k_dft_cols<1>, smem);
+      k_dft_cols<1><<<grid, 512, smem, st>>>(in, scratch, log_chunk, log_h1, log_h2, log_h, tile, t.tw_stage,
+                                             t.tw_lo, t.tw_hi);
+    } else {
+      set_smem(k_dft_cols<4>, smem);
+      k_dft_cols<4><<<grid, 512, smem, st>>>(reinterpret_cast<const uint4*>(in), reinterpret_cast<uint4*>(scratch),
+                                             log_chunk, log_h1, log_h2, log_h, tile, t.tw_stage, t.tw_lo, t.tw_hi);
+    }
+    count_launch();
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+  }
+  const int jt = pow2_clamp(budget / ((long)H2 * ebytes), 1, W);
+  const size_t smem = tw_bytes + (size_t)jt * H2 * ebytes;
+  dim3 grid(H1, W / jt);
+  if (lanes == 1) {
+    set_smem(k_dft_rows<1>, smem);
+    k_dft_rows<1><<<grid, 512, smem, st>>>(scratch, out, log_h1, log_h2, log_h, log_w, jt, t.tw_stage);
+  } else {
+    set_smem(k_dft_rows<4>, smem);
+    k_dft_rows<4><<<grid, 512, smem, st>>>(reinterpret_cast<const uint4*>(scratch), reinterpret_cast<uint4*>(out),
+                                           log_h1, log_h2, log_h, log_w, jt, t.tw_stage);
+  }
+  LAUNCH_DONE();
+}
+
+// ---------------------------------------------------------------------------
+// Merkle tree (MerkleTreeMmcs::commit_matrix, src/whir/committer/writer.rs:89
+// and src/whir/prover/mod.rs:182-184): one thread hashes one row with the
+// PaddingFreeSponge (overwrite mode), then the CTA compresses its subtree
+// level by level in shared memory with TruncatedPermutation<P16>.
+// ---------------------------------------------------------------------------
+
+constexpr int MERKLE_CTA = 128;
+
+__device__ __forceinline__ void compress16(const uint32_t* l, const uint32_t* r, uint32_t* out,
+                                           const P2Consts& k) {
+  uint32_t s[16];
+#pragma unroll
+  for (int i = 0; i < 8; i++) {
+    s[i] = l[i];
+    s[i + 8] = r[i];
+  }
+  p2::permute<16, p2::RP16>(s, k);
+#pragma unroll
+  for (int i = 0; i < 8; i++) out[i] = s[i];
+}
+
+// Compress `levels` levels above the digests in sh[0 .. count*8), writing each
+// level to global; `node0` is this CTA's first node index at the input level.
+__device__ __forceinline__ void subtree_up(uint32_t* sh, int count, int levels, size_t node0, uint32_t* level_base,
+                                           size_t level_size, const P2Consts& comp) {
+  size_t off = 0;
+  size_t lsz = level_size;
+  for (int l = 1; l <= levels; l++) {
+    const int act = count >> l;
+    uint32_t d[8];
+    const int t = threadIdx.x;
+    if (t < act) compress16(sh + 2 * t * 8, sh + (2 * t + 1) * 8, d, comp);
+    __syncthreads();
+    off += lsz;
+    lsz >>= 1;
+    if (t < act) {
+      const size_t node = (node0 >> l) + t;
+#pragma unroll
+      for (int i = 0; i < 8; i++) {
+        sh[t * 8 + i] = d[i];
+        level_base[(off + node) * 8 + i] = d[i];
+      }
+    }
+    __syncthreads();
+  }
+}
+
+template <int T, int RP, int RATE>
+__global__ void __launch_bounds__(MERKLE_CTA) k_merkle_leaves(const uint32_t* __restrict__ rows, int row_words,
+                                                               size_t h, int levels, uint32_t* __restrict__ digests,
+                                                               const __grid_constant__ P2Consts leaf,
+                                                               const __grid_constant__ P2Consts comp) {
+  __shared__ uint32_t sh[MERKLE_CTA * 8];
+  const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < h) {
+    uint32_t s[T];
+#pragma unroll
+    for (int k = 0; k < T; k++) s[k] = 0u;
+    const uint32_t* row = rows + i * (size_t)row_words;
+    for (int pos = 0; pos < row_words; pos += RATE) {
+      const int take = row_words - pos < RATE ? row_words - pos : RATE;
+      if (take == RATE && (row_words & 3) == 0) {
+#pragma unroll
+        for (int k = 0; k < RATE; k += 4) {
+          uint4 v = __ldg(reinterpret_cast<const uint4*>(row + pos + k));
+          s[k] = v.x;
+          s[k + 1] = v.y;
+          s[k + 2] = v.z;
+          s[k + 3] = v.w;
+        }
+      } else {
+#pragma unroll
+        for (int k = 0; k < RATE; k++)
+          if (k < take) s[k] = row[pos + k];
+      }
+      p2::permute<T, RP>(s, leaf);
+    }
+#pragma unroll
+    for (int k = 0; k < 8; k++) {
+      sh[threadIdx.x * 8 + k] = s[k];
+      digests[i * 8 + k] = s[k];
+    }
+  }
+  __syncthreads();
+  subtree_up(sh, blockDim.x, levels, (size_t)blockIdx.x * blockDim.x, digests, h, comp);
+}
+
+// One CTA consumes `blockDim.x*2` nodes of the input level (offset in_off, in words/8).
+__global__ void __launch_bounds__(MERKLE_CTA) k_merkle_nodes(uint32_t* __restrict__ digests, size_t in_off,
+                                                              size_t in_count, int levels,
+                                                              const __grid_constant__ P2Consts comp) {
+  __shared__ uint32_t sh[2 * MERKLE_CTA * 8];
+  const int t = threadIdx.x;
+  const size_t base = (size_t)blockIdx.x * blockDim.x * 2;
+  const int cnt = (int)min((size_t)blockDim.x * 2, in_count - base);
+  for (int k = t; k < cnt * 8; k += blockDim.x) sh[k] = digests[(in_off + base) * 8 + k];
+  __syncthreads();
+  // subtree_up expects `count` digests in sh and writes levels above in_off
+  size_t off = in_off, lsz = in_count;
+  for (int l = 1; l <= levels; l++) {
+    const int act = cnt >> l;
+    uint32_t d[8];
+    if (t < act) compress16(sh + 2 * t * 8, sh + (2 * t + 1) * 8, d, comp);
+    __syncthreads();
+    off += lsz;
+    lsz >>= 1;
+    if (t < act) {
+      const size_t node = (base >> l) + t;
+#pragma unroll
+      for (int i = 0; i < 8; i++) {
+        sh[t * 8 + i] = d[i];
+        digests[(off + node) * 8 + i] = d[i];
+      }
+    }
+    __syncthreads();
+  }
+}
+
+static int ilog2i(size_t v) {
+  int r = -1;
+  while (v) {
+    r++;
+    v >>= 1;
+  }
+  return r;
+}
+
+cudaError_t merkle_build(const uint32_t* rows, int log_h, int row_words, int leaf_hash, uint32_t* digests,
+                         const P2Consts& p16, const P2Consts& p24, cudaStream_t st) {
+  const size_t h = (size_t)1 << log_h;
+  const int cta = (int)(h < (size_t)MERKLE_CTA ? h : (size_t)MERKLE_CTA);
+  const int lv = ilog2i((size_t)cta);
+  const unsigned blocks = (unsigned)(h / cta);
+  if (leaf_hash == 0)
+    k_merkle_leaves<24, p2::RP24, 16><<<blocks, cta, 0, st>>>(rows, row_words, h, lv, digests, p24, p16);
+  else
+    k_merkle_leaves<16, p2::RP16, 8><<<blocks, cta, 0, st>>>(rows, row_words, h, lv, digests, p16, p16);
+  count_launch();
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  size_t off = 0, cnt = h;
+  for (int l = 0; l < lv; l++) {
+    off += cnt;
+    cnt >>= 1;
+  }
+  while (cnt > 1) {
+    const int c2 = (int)(cnt < (size_t)(2 * MERKLE_CTA) ? cnt : (size_t)(2 * MERKLE_CTA));
+    const int levels = ilog2i((size_t)c2);
+    const unsigned blocks2 = (unsigned)(cnt / c2);
+    k_merkle_nodes<<<blocks2, c2 / 2, 0, st>>>(digests, off, cnt, levels, p16);
+    count_launch();
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    for (int l = 0; l < levels; l++) {
+      off += cnt;
+      cnt >>= 1;
+    }
+  }
+  return cudaSuccess;
+}
+
+// Mmcs::open_batch gather (src/whir/prover/mod.rs:248-300, 378-401)
+__global__ void k_merkle_open(const uint32_t* __restrict__ rows, const uint32_t* __restrict__ digests, int log_h,
+                              int row_words, const uint64_t* __restrict__ idx, uint32_t* __restrict__ rows_out,
+                              uint32_t* __restrict__ paths_out) {
+  const int q = blockIdx.x;
+  const uint64_t i = idx[q];
+  for (int w = threadIdx.x; w < row_words; w += blockDim.x)
+    rows_out[(size_t)q * row_words + w] = rows[i * row_words + w];
+  for (int k = threadIdx.x; k < log_h * 8; k += blockDim.x) {
+    const int l = k >> 3, c = k & 7;
+    size_t off = 0, n = (size_t)1 << log_h;
+    for (int m = 0; m < l; m++) {
+      off += n;
+      n >>= 1;
+    }
+    const size_t sib = (size_t)((i >> l) ^ 1u);
+    paths_out[((size_t)q * log_h + l) * 8 + c] = digests[(off + sib) * 8 + c];
+  }
+}
+
+cudaError_t merkle_open(const uint32_t* rows, const uint32_t* digests, int log_h, int row_words,
+                        const uint64_t* d_idx, int count, uint32_t* d_rows_out, uint32_t* d_paths_out,
+                        cudaStream_t st) {
+  if (count <= 0) return cudaSuccess;
+  k_merkle_open<<<count, 128, 0, st>>>(rows, digests, log_h, row_words, d_idx, d_rows_out, d_paths_out);
+  LAUNCH_DONE();
+}
+
+// ---------------------------------------------------------------------------
+// Proof of work (GrindingChallenger::grind on DuplexChallenger, called at
+// src/whir/proof.rs:188 and src/whir/prover/mod.rs:224,363). Candidates are
+// claimed in increasing chunks; a CTA stops once every remaining chunk starts
+// above the best witness found, so the result is the smallest valid witness.
+// The loop is bounded by `limit` candidates.
+// ---------------------------------------------------------------------------
+
+constexpr int GRIND_CTA = 256;
+constexpr int GRIND_PER_THREAD = 16;
+
+__global__ void __launch_bounds__(GRIND_CTA) k_grind(const __grid_constant__ P2Consts p16, uint4 st0, uint4 st1,
+                                                      uint4 st2, uint4 st3, int slot, int bits, uint64_t limit,
+                                                      uint32_t* result, uint32_t* counter) {
+  __shared__ uint64_t s_start;
+  __shared__ int s_go;
+  const uint32_t mask = (1u << bits) - 1u;
+  const uint64_t chunk_size = (uint64_t)GRIND_CTA * GRIND_PER_THREAD;
+  const uint32_t base_state[16] = {st0.x, st0.y, st0.z, st0.w, st1.x, st1.y, st1.z, st1.w,
+                                   st2.x, st2.y, st2.z, st2.w, st3.x, st3.y, st3.z, st3.w};
+  for (;;) {
+    if (threadIdx.x == 0) {
+      const uint64_t start = (uint64_t)atomicAdd(counter, 1u) * chunk_size;
+      s_start = start;
+      s_go = start < limit && start < (uint64_t)*(volatile uint32_t*)result;
+    }
+    __syncthreads();
+    const uint64_t start = s_start;
+    const int go = s_go;
+    __syncthreads();
+    if (!go) return;
+    for (int k = 0; k < GRIND_PER_THREAD; k++) {
+      const uint64_t w = start + (uint64_t)k * GRIND_CTA + threadIdx.x;
+      if (w >= limit) break;
+      uint32_t s[16];
+      const uint32_t wm = kb::to_mont((uint32_t)w);
+#pragma unroll
+      for (int i = 0; i < 16; i++) s[i] = i == slot ? wm : base_state[i];
+      p2::permute<16, p2::RP16>(s, p16);
+      if ((kb::from_mont(s[7]) & mask) == 0u) atomicMin(result, (uint32_t)w);
+    }
+  }
+}
+
+__global__ void k_grind_init(uint32_t* result, uint32_t* counter) {
+  *result = kb::P;
+  *counter = 0u;
+}
+
+cudaError_t grind(const uint32_t* state, const uint32_t* in, int in_len, int bits, uint64_t limit,
+                  uint32_t* result, uint32_t* counter, const P2Consts& p16, cudaStream_t st) {
+  if (in_len < 0 || in_len > 7 || bits < 0 || bits > 30) return cudaErrorInvalidValue;
+  if (limit > kb::P) limit = kb::P;
+  uint32_t s[16];
+  for (int i = 0; i < 16; i++) s[i] = state[i];
+  for (int i = 0; i < in_len; i++) s[i] = in[i];
+  k_grind_init<<<1, 1, 0, st>>>(result, counter);
+  count_launch();
+  uint4 a = make_uint4(s[0], s[1], s[2], s[3]), b = make_uint4(s[4], s[5], s[6], s[7]);
+  uint4 c = make_uint4(s[8], s[9], s[10], s[11]), d = make_uint4(s[12], s[13], s[14], s[15]);
+  k_grind<<<sm_count() * 4, GRIND_CTA, 0, st>>>(p16, a, b, c, d, in_len, bits, limit, result, counter);
+  LAUNCH_DONE();
+}
+
+// ---------------------------------------------------------------------------
+// eq tables (EvaluationsList::new_from_point, src/poly/evals.rs:312-320, and
+// the split tables of evals.rs:254-295 / svo.rs:387-403)
+// ---------------------------------------------------------------------------
+
+__global__ void k_eq_small(const __grid_constant__ EqPoint pt, ef* out) {
+  const size_t n = (size_t)1 << pt.h;
+  for (size_t x = blockIdx.x * (size_t)blockDim.x + threadIdx.x; x < n; x += (size_t)gridDim.x * blockDim.x) {
+    ef acc = pt.scale;
+    for (int j = 0; j < pt.h; j++) {
+      const ef& z = pt.z[j];
+      const bool bit = (x >> (pt.h - 1 - j)) & 1;
+      acc = kb::ef_mul(acc, bit ? z : kb::ef_sub(kb::ef_one(), z));
+    }
+    st_ef(out + x, acc);
+  }
+}
+
+cudaError_t eq_table_small(const EqPoint& pt, ef* out, cudaStream_t st) {
+  if (pt.h < 0 || pt.h > 20) return cudaErrorInvalidValue;
+  const size_t n = (size_t)1 << pt.h;
+  k_eq_small<<<grid_for(n, 256), 256, 0, st>>>(pt, out);
+  LAUNCH_DONE();
+}
+
+__global__ void k_eq_outer(const ef* __restrict__ hi, const ef* __restrict__ lo, int lo_bits, size_t n,
+                           ef* __restrict__ out) {
+  const size_t mask = ((size_t)1 << lo_bits) - 1;
+  for (size_t x = blockIdx.x * (size_t)blockDim.x + threadIdx.x; x < n; x += (size_t)gridDim.x * blockDim.x)
+    st_ef(out + x, kb::ef_mul(ld_ef(hi + (x >> lo_bits)), ld_ef(lo + (x & mask))));
+}
+
+cudaError_t eq_outer(const ef* hi, const ef* lo, int lo_bits, size_t n, ef* out, cudaStream_t st) {
+  k_eq_outer<<<grid_for(n, 256), 256, 0, st>>>(hi, lo, lo_bits, n, out);
+  LAUNCH_DONE();
+}
+
+// ---------------------------------------------------------------------------
+// Split-eq dot products: multilinear evaluation (evaluate_hypercube_base/_ext,
+// src/poly/evals.rs:334-366, 648-738) and the SVO partial evaluations
+// (SplitEqInner::partial_evals, src/sumcheck/svo.rs:465-502). Each thread
+// keeps one low index xl and accumulates f * hi[xh] over its xh, multiplying
+// by lo[xl] once at the end.
+// ---------------------------------------------------------------------------
+
+constexpr int DOT_CTA = 256;
+
+template <int EXT>
+__global__ void __launch_bounds__(DOT_CTA) k_dot_split(const uint32_t* __restrict__ f, int m_bits,
+                                                        const ef* __restrict__ hi, const ef* __restrict__ lo,
+                                                        int lo_bits, ef* __restrict__ partials) {
+  __shared__ ef sh[1][32];
+  const size_t M = (size_t)1 << m_bits;
+  const int seg = blockIdx.y;
+  const uint32_t lomask = (1u << lo_bits) - 1;
+  ef total = kb::ef_zero();
+  if ((size_t)threadIdx.x < M || M >= DOT_CTA) {
+    const uint32_t xl = threadIdx.x & lomask;
+    ef acc = kb::ef_zero();
+    kb::ef_acc lazy;
+    lazy.clear();
+    for (size_t x = (size_t)blockIdx.x * DOT_CTA + threadIdx.x; x < M; x += (size_t)gridDim.x * DOT_CTA) {
+      const ef h = ld_ef(hi + (x >> lo_bits));
+      if (EXT) {
+        const ef v = ld_ef(reinterpret_cast<const ef*>(f) + (size_t)seg * M + x);
+        acc = kb::ef_add(acc, kb::ef_mul(v, h));
+      } else {
+        lazy.mac(h, __ldg(f + (size_t)seg * M + x), acc);
+      }
+    }
+    if (!EXT) lazy.fold(acc);
+    total = kb::ef_mul(acc, ld_ef(lo + xl));
+  }
+  ef v[1] = {total};
+  block_sum<1>(v, sh);
+  if (threadIdx.x == 0) partials[(size_t)seg * gridDim.x + blockIdx.x] = v[0];
+}
+
+cudaError_t dot_split(const uint32_t* f, int ext, int seg_bits, int m_bits, const ef* hi, const ef* lo, int lo_bits,
+                      ef* partials, ef* out, cudaStream_t st) {
+  if (lo_bits > 8 || lo_bits > m_bits) return cudaErrorInvalidValue;
+  const size_t M = (size_t)1 << m_bits;
+  const int segs = 1 << seg_bits;
+  unsigned bx = grid_for(M, DOT_CTA, 8);
+  unsigned cap = (unsigned)((sm_count() * 8 + segs - 1) / segs);
+  if (bx > cap) bx = cap;
+  if (bx < 1) bx = 1;
+  dim3 grid(bx, segs);
+  if (ext)
+    k_dot_split<1><<<grid, DOT_CTA, 0, st>>>(f, m_bits, hi, lo, lo_bits, partials);
+  else
+    k_dot_split<0><<<grid, DOT_CTA, 0, st>>>(f, m_bits, hi, lo, lo_bits, partials);
+  count_launch();
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  k_sum_partials<<<segs, 256, 0, st>>>(partials, (int)bx, out);
+  LAUNCH_DONE();
+}
+
+// ---------------------------------------------------------------------------
+// Folding (EvaluationsList::compress / compress_ext / compress_multi_into_packed,
+// src/poly/evals.rs:127-148, 382-400, 422-447)
+// ---------------------------------------------------------------------------
+
+__global__ void k_fold_ext(ef* __restrict__ a, ef* __restrict__ b, size_t half, ef r) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < half; i += (size_t)gridDim.x * blockDim.x) {
+    ef lo = ld_ef(a + i), hi = ld_ef(a + i + half);
+    st_ef(a + i, kb::ef_add(lo, kb::ef_mul(kb::ef_sub(hi, lo), r)));
+    if (b) {
+      ef lo2 = ld_ef(b + i), hi2 = ld_ef(b + i + half);
+      st_ef(b + i, kb::ef_add(lo2, kb::ef_mul(kb::ef_sub(hi2, lo2), r)));
+    }
+  }
+}
+
+cudaError_t fold_ext(ef* a, ef* b, size_t half, ef r, cudaStream_t st) {
+  k_fold_ext<<<grid_for(half, 256), 256, 0, st>>>(a, b, half, r);
+  LAUNCH_DONE();
+}
+
+__global__ void k_fold_base(const uint32_t* __restrict__ f, size_t half, ef r, ef* __restrict__ out) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < half; i += (size_t)gridDim.x * blockDim.x) {
+    const uint32_t lo = __ldg(f + i), hi = __ldg(f + i + half);
+    ef v = kb::ef_mul_base(r, kb::sub(hi, lo));
+    v.c[0] = kb::add(v.c[0], lo);
+    st_ef(out + i, v);
+  }
+}
+
+cudaError_t fold_base(const uint32_t* f, size_t half, ef r, ef* out, cudaStream_t st) {
+  k_fold_base<<<grid_for(half, 256), 256, 0, st>>>(f, half, r, out);
+  LAUNCH_DONE();
+}
+
+__global__ void k_fold_multi_base(const uint32_t* __restrict__ f, int k, size_t m,
+                                  const __grid_constant__ EqSmall eqrs, ef* __restrict__ out) {
+  const int K = 1 << k;
+  for (size_t x = blockIdx.x * (size_t)blockDim.x + threadIdx.x; x < m; x += (size_t)gridDim.x * blockDim.x) {
+    ef acc = kb::ef_zero();
+    kb::ef_acc lazy;
+    lazy.clear();
+    for (int y = 0; y < K; y++) lazy.mac(eqrs.v[y], __ldg(f + (size_t)y * m + x), acc);
+    lazy.fold(acc);
+    st_ef(out + x, acc);
+  }
+}
+
+cudaError_t fold_multi_base(const uint32_t* f, int k, size_t m, const EqSmall& eqrs, ef* out, cudaStream_t st) {
+  if (k < 0 || k > 6) return cudaErrorInvalidValue;
+  k_fold_multi_base<<<grid_for(m, 256), 256, 0, st>>>(f, k, m, eqrs, out);
+  LAUNCH_DONE();
+}
+
+// ---------------------------------------------------------------------------
+// Sumcheck round coefficients (EvaluationsList::sumcheck_coefficients,
+// src/poly/evals.rs:493-526): c0 = sum e_lo*w_lo, c2 = sum (2e_hi-e_lo)(2w_hi-w_lo)
+// ---------------------------------------------------------------------------
+
+__global__ void __launch_bounds__(256) k_sumcheck_coeffs(const ef* __restrict__ f, const ef* __restrict__ w,
+                                                          size_t half, ef* __restrict__ partials) {
+  __shared__ ef sh[2][32];
+  ef v[2] = {kb::ef_zero(), kb::ef_zero()};
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < half; i += (size_t)gridDim.x * blockDim.x) {
+    const ef el = ld_ef(f + i), eh = ld_ef(f + i + half);
+    const ef wl = ld_ef(w + i), wh = ld_ef(w + i + half);
+    v[0] = kb::ef_add(v[0], kb::ef_mul(el, wl));
+    v[1] = kb::ef_add(v[1], kb::ef_mul(kb::ef_sub(kb::ef_dbl(eh), el), kb::ef_sub(kb::ef_dbl(wh), wl)));
+  }
+  block_sum<2>(v, sh);
+  if (threadIdx.x == 0) {
+    partials[blockIdx.x] = v[0];
+    partials[gridDim.x + blockIdx.x] = v[1];
+  }
+}
+
+cudaError_t sumcheck_coeffs(const ef* f, const ef* w, size_t half, ef* partials, ef* out, cudaStream_t st) {
+  const unsigned b = grid_for(half, 256, 8);
+  k_sumcheck_coeffs<<<b, 256, 0, st>>>(f, w, half, partials);
+  count_launch();
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  k_sum_partials<<<2, 256, 0, st>>>(partials, (int)b, out);
+  LAUNCH_DONE();
+}
+
+// ---------------------------------------------------------------------------
+// Constraint weights (Constraint::combine, src/whir/constraints/mod.rs:197-248)
+//   eq part:     EqStatement::combine_hypercube(_packed), statement/eq.rs:182-312
+//   select part: SelectStatement::combine(_packed), statement/select.rs:296-496
+// ---------------------------------------------------------------------------
+
+__global__ void k_add_eq_batch(ef* __restrict__ w, size_t N, int hi_count_bits, const ef* __restrict__ hi,
+                               const ef* __restrict__ lo, int lo_bits, int m, int accumulate) {
+  const size_t lomask = ((size_t)1 << lo_bits) - 1;
+  const size_t H = (size_t)1 << hi_count_bits, Lc = (size_t)1 << lo_bits;
+  for (size_t x = blockIdx.x * (size_t)blockDim.x + threadIdx.x; x < N; x += (size_t)gridDim.x * blockDim.x) {
+    ef acc = accumulate ? ld_ef(w + x) : kb::ef_zero();
+    for (int c = 0; c < m; c++)
+      acc = kb::ef_add(acc, kb::ef_mul(ld_ef(hi + c * H + (x >> lo_bits)), ld_ef(lo + c * Lc + (x & lomask))));
+    st_ef(w + x, acc);
+  }
+}
+
+cudaError_t add_eq_batch(ef* w, int n, const ef* hi, const ef* lo, int lo_bits, int m, int accumulate,
+                         cudaStream_t st) {
+  const size_t N = (size_t)1 << n;
+  k_add_eq_batch<<<grid_for(N, 256), 256, 0, st>>>(w, N, n - lo_bits, hi, lo, lo_bits, m, accumulate);
+  LAUNCH_DONE();
+}
+
+__global__ void k_select_tables(const uint32_t* __restrict__ vars, int m, int n, int lo_bits,
+                                uint32_t* __restrict__ pow_lo, uint32_t* __restrict__ pow_hi) {
+  const size_t Lc = (size_t)1 << lo_bits, Hc = (size_t)1 << (n - lo_bits);
+  const size_t per = Lc + Hc;
+  for (size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x; t < (size_t)m * per;
+       t += (size_t)gridDim.x * blockDim.x) {
+    const size_t s = t / per, r = t % per;
+    const uint32_t v = vars[s];
+    if (r < Lc)
+      pow_lo[s * Lc + r] = kb::pow(v, r);
+    else
+      pow_hi[s * Hc + (r - Lc)] = kb::pow(v, (r - Lc) << lo_bits);
+  }
+}
+
+cudaError_t select_tables(const uint32_t* vars, int m, int n, int lo_bits, uint32_t* pow_lo, uint32_t* pow_hi,
+                          cudaStream_t st) {
+  if (m <= 0) return cudaSuccess;
+  const size_t work = (size_t)m * (((size_t)1 << lo_bits) + ((size_t)1 << (n - lo_bits)));
+  k_select_tables<<<grid_for(work, 256), 256, 0, st>>>(vars, m, n, lo_bits, pow_lo, pow_hi);
+  LAUNCH_DONE();
+}
+
+// Each CTA covers whole runs of 2^lo_bits >= blockDim consecutive x, so all its
+// threads share xh and the per-constraint factor g[s]*pow_hi[s][xh] is formed
+// once per CTA in shared memory.
+__global__ void k_add_select(ef* __restrict__ w, size_t N, int lo_bits, const uint32_t* __restrict__ pow_lo,
+                             const uint32_t* __restrict__ pow_hi, const ef* __restrict__ g, int m, int hi_bits) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  ef* cs = reinterpret_cast<ef*>(smem_raw);
+  const size_t Lc = (size_t)1 << lo_bits, Hc = (size_t)1 << hi_bits;
+  for (size_t x0 = (size_t)blockIdx.x * blockDim.x; x0 < N; x0 += (size_t)gridDim.x * blockDim.x) {
+    const size_t xh = x0 >> lo_bits;
+    __syncthreads();
+    for (int s = threadIdx.x; s < m; s += blockDim.x)
+      cs[s] = kb::ef_mul_base(ld_ef(g + s), __ldg(pow_hi + s * Hc + xh));
+    __syncthreads();
+    const size_t x = x0 + threadIdx.x;
+    const size_t xl = x & (Lc - 1);
+    ef acc = ld_ef(w + x);
+    kb::ef_acc lazy;
+    lazy.clear();
+    for (int s = 0; s < m; s++) lazy.mac(cs[s], __ldg(pow_lo + s * Lc + xl), acc);
+    lazy.fold(acc);
+    st_ef(w + x, acc);
+  }
+}
+
+cudaError_t add_select(ef* w, int n, const uint32_t* pow_lo, const uint32_t* pow_hi, int lo_bits, const ef* g, int m,
+                       cudaStream_t st) {
+  if (m <= 0) return cudaSuccess;
+  const size_t N = (size_t)1 << n;
+  const int threads = (int)(N < 256 ? N : 256);
+  if (((size_t)1 << lo_bits) < (size_t)threads) return cudaErrorInvalidValue;
+  const size_t smem = (size_t)m * sizeof(ef);
+  if (smem > 160 * 1024) return cudaErrorInvalidValue;
+  cudaFuncSetAttribute(k_add_select, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  k_add_select<<<grid_for(N, threads), threads, smem, st>>>(w, N, lo_bits, pow_lo, pow_hi, g, m, n - lo_bits);
+  LAUNCH_DONE();
+}
+
+}  // namespace wk

@@ -1,0 +1,96 @@
+// Launchers for the device kernels of the WHIR prover hot path. All device
+// arrays hold field elements in Montgomery form (see kb.cuh); an extension
+// element is 4 consecutive words. Every launcher enqueues on `st` and returns
+// the launch status; none of them synchronizes.
+#pragma once
+#include <cuda_runtime.h>
+#include <stddef.h>
+#include <stdint.h>
+
+#include "kb.cuh"
+#include "poseidon2.cuh"
+
+namespace wk {
+
+// Kernel launch counter (the number of kernels this library enqueued).
+unsigned long long launches();
+void count_launch();
+
+// small device-side tables owned by the caller
+struct DftTables {
+  const uint32_t* tw_stage;  // omega_{2^12}^k, k < 2^11
+  const uint32_t* tw_lo;     // omega_H^e, e < 2^12
+  const uint32_t* tw_hi;     // omega_H^(e * 2^12), e < 2^12
+};
+
+cudaError_t encode(uint32_t* p, size_t n, cudaStream_t st);
+cudaError_t decode(uint32_t* p, size_t n, cudaStream_t st);
+
+// tables: tw_stage needs 2^11 words, tw_lo/tw_hi 2^12 words each
+cudaError_t build_dft_tables(uint32_t* tw_stage, uint32_t* tw_lo, uint32_t* tw_hi, int log_h, cudaStream_t st);
+
+// transpose & pad & DFT: 2^log_w chunks of 2^log_chunk elements -> row-major
+// (2^(log_chunk+log_blowup)) x 2^log_w; `scratch` needs out-size elements.
+cudaError_t dft_batch(const uint32_t* in, uint32_t* out, uint32_t* scratch, int log_chunk, int log_w,
+                      int log_blowup, int lanes, const DftTables& t, cudaStream_t st);
+
+// Merkle tree: digests has (2h-1)*8 words, leaves first. leaf_hash 0: sponge
+// over Poseidon2-24 rate 16; 1: Poseidon2-16 rate 8. Compression: Poseidon2-16.
+cudaError_t merkle_build(const uint32_t* rows, int log_h, int row_words, int leaf_hash, uint32_t* digests,
+                         const p2::P2Consts& p16, const p2::P2Consts& p24, cudaStream_t st);
+// gather opened rows and sibling paths for `count` indices
+cudaError_t merkle_open(const uint32_t* rows, const uint32_t* digests, int log_h, int row_words,
+                        const uint64_t* d_idx, int count, uint32_t* d_rows_out, uint32_t* d_paths_out,
+                        cudaStream_t st);
+
+// PoW search: smallest w in [0, limit) such that the duplex challenger whose
+// sponge state is `state` (16 words) with pending inputs in[0..in_len) samples
+// `bits` zero low bits after observing w. `result` (device, 1 word) receives
+// the witness or p if none; `counter` (device, 1 word) is scratch.
+cudaError_t grind(const uint32_t* state, const uint32_t* in, int in_len, int bits, uint64_t limit,
+                  uint32_t* result, uint32_t* counter, const p2::P2Consts& p16, cudaStream_t st);
+
+// eq table of `h` coordinates scaled by `scale`: out[x] = scale * prod eq(z_j, bit_j(x)), MSB <-> z[0].
+struct EqPoint {
+  kb::ef z[32];
+  int h;
+  kb::ef scale;
+};
+cudaError_t eq_table_small(const EqPoint& pt, kb::ef* out, cudaStream_t st);
+// out[x] = hi[x >> lo_bits] * lo[x & (2^lo_bits - 1)]
+cudaError_t eq_outer(const kb::ef* hi, const kb::ef* lo, int lo_bits, size_t n, kb::ef* out, cudaStream_t st);
+
+// segmented split-eq dot products:
+//   out[s] = sum_{x < M} f[s*M + x] * hi[x >> lo_bits] * lo[x & mask],  M = 2^m_bits, s < 2^seg_bits
+// f is base (ext=0) or extension (ext=1). partials needs blocks*2^seg_bits ef.
+cudaError_t dot_split(const uint32_t* f, int ext, int seg_bits, int m_bits, const kb::ef* hi, const kb::ef* lo,
+                      int lo_bits, kb::ef* partials, kb::ef* out, cudaStream_t st);
+
+// compress (fold the first variable) on one or two extension arrays in place
+cudaError_t fold_ext(kb::ef* a, kb::ef* b, size_t half, kb::ef r, cudaStream_t st);
+// compress_ext: base evals of 2*half entries -> extension evals of half entries
+cudaError_t fold_base(const uint32_t* f, size_t half, kb::ef r, kb::ef* out, cudaStream_t st);
+// compress_multi: out[x] = sum_{y < 2^k} eqrs[y] * f[y*M + x]
+struct EqSmall {
+  kb::ef v[64];
+};
+cudaError_t fold_multi_base(const uint32_t* f, int k, size_t m, const EqSmall& eqrs, kb::ef* out,
+                            cudaStream_t st);
+// sumcheck coefficients over extension f, w of 2*half entries: out[0] = c0, out[1] = c2
+cudaError_t sumcheck_coeffs(const kb::ef* f, const kb::ef* w, size_t half, kb::ef* partials, kb::ef* out,
+                            cudaStream_t st);
+
+// W[x] (+)= sum_c hi_c[x >> lo_bits] * lo_c[x & mask] for c < m constraints (the
+// scale of each constraint is folded into its hi table); tables are laid out
+// constraint-major (hi: m * 2^(n-lo_bits), lo: m * 2^lo_bits).
+cudaError_t add_eq_batch(kb::ef* w, int n, const kb::ef* hi, const kb::ef* lo, int lo_bits, int m, int accumulate,
+                         cudaStream_t st);
+
+// select weights: W[x] += sum_s g[s] * v_s^x. Tables: pow_lo[s*2^lo + xl] = v_s^xl,
+// pow_hi[s*2^(n-lo) + xh] = v_s^(xh * 2^lo); built by select_tables.
+cudaError_t select_tables(const uint32_t* vars, int m, int n, int lo_bits, uint32_t* pow_lo, uint32_t* pow_hi,
+                          cudaStream_t st);
+cudaError_t add_select(kb::ef* w, int n, const uint32_t* pow_lo, const uint32_t* pow_hi, int lo_bits,
+                       const kb::ef* g, int m, cudaStream_t st);
+
+}  // namespace wk

@@ -1,0 +1,101 @@
+// Poseidon2 permutation over KoalaBear, width 16 and 24, S-box x^3.
+//
+// Structure from the Poseidon2 paper (Grassi, Khovratovich, Schofnegger,
+// eprint 2023/323): an initial external linear layer, R_F/2 full rounds,
+// R_P partial rounds, R_F/2 full rounds. The external layer is
+// circ(2*M4, M4, ..., M4) with the paper's 4x4 matrix M4, evaluated with its
+// published 8-addition chain; the internal layer is 1*1^T + diag(mu).
+//
+// Reference types this replaces: p3-koala-bear `Poseidon2KoalaBear<16>` and
+// `<24>` (src/bin/main.rs:31-32), used by PaddingFreeSponge (leaf hashing),
+// TruncatedPermutation (2-to-1 compression) and DuplexChallenger.
+//
+// The round constants and diagonal are run-time data (`P2Consts`, Montgomery
+// form) so a caller can supply the exact permutation of its deployment; the
+// shapes (8 full rounds; 20 partial rounds at width 16, 23 at width 24) are
+// compile-time so that every constant becomes an immediate operand.
+#pragma once
+#include "kb.cuh"
+
+namespace p2 {
+
+constexpr int RF = 8;
+constexpr int RP16 = 20;
+constexpr int RP24 = 23;
+
+struct P2Consts {
+  uint32_t width, rounds_f, rounds_p;
+  uint32_t ext_rc[8 * 24];
+  uint32_t int_rc[32];
+  uint32_t diag[24];
+};
+
+// M4 = [[5,7,1,3],[4,6,1,1],[1,3,5,7],[1,1,4,6]] via the paper's addition chain.
+KB_HD void m4(uint32_t& x0, uint32_t& x1, uint32_t& x2, uint32_t& x3) {
+  using namespace kb;
+  uint32_t t0 = add(x0, x1);
+  uint32_t t1 = add(x2, x3);
+  uint32_t t2 = add(dbl(x1), t1);
+  uint32_t t3 = add(dbl(x3), t0);
+  uint32_t t4 = add(dbl(dbl(t1)), t3);
+  uint32_t t5 = add(dbl(dbl(t0)), t2);
+  uint32_t t6 = add(t3, t5);
+  uint32_t t7 = add(t2, t4);
+  x0 = t6;
+  x1 = t5;
+  x2 = t7;
+  x3 = t4;
+}
+
+template <int T>
+KB_HD void ext_layer(uint32_t (&x)[T]) {
+  using namespace kb;
+#pragma unroll
+  for (int c = 0; c < T; c += 4) m4(x[c], x[c + 1], x[c + 2], x[c + 3]);
+  uint32_t s0 = x[0], s1 = x[1], s2 = x[2], s3 = x[3];
+#pragma unroll
+  for (int c = 4; c < T; c += 4) {
+    s0 = add(s0, x[c]);
+    s1 = add(s1, x[c + 1]);
+    s2 = add(s2, x[c + 2]);
+    s3 = add(s3, x[c + 3]);
+  }
+#pragma unroll
+  for (int c = 0; c < T; c += 4) {
+    x[c] = add(x[c], s0);
+    x[c + 1] = add(x[c + 1], s1);
+    x[c + 2] = add(x[c + 2], s2);
+    x[c + 3] = add(x[c + 3], s3);
+  }
+}
+
+KB_HD uint32_t cube(uint32_t v) { return kb::mul(kb::sqr(v), v); }
+
+template <int T, int RP>
+KB_HD void permute(uint32_t (&x)[T], const P2Consts& k) {
+  using namespace kb;
+  ext_layer<T>(x);
+#pragma unroll
+  for (int r = 0; r < RF / 2; r++) {
+#pragma unroll
+    for (int i = 0; i < T; i++) x[i] = cube(add(x[i], k.ext_rc[r * T + i]));
+    ext_layer<T>(x);
+  }
+#pragma unroll
+  for (int r = 0; r < RP; r++) {
+    x[0] = cube(add(x[0], k.int_rc[r]));
+    uint32_t s = x[0];
+#pragma unroll
+    for (int i = 1; i < T; i++) s = add(s, x[i]);
+#pragma unroll
+    for (int i = 0; i < T; i++) x[i] = add(s, mul(k.diag[i], x[i]));
+  }
+#pragma unroll
+  for (int r = RF / 2; r < RF; r++) {
+#pragma unroll
+    for (int i = 0; i < T; i++) x[i] = cube(add(x[i], k.ext_rc[r * T + i]));
+    ext_layer<T>(x);
+  }
+}
+
+}  // namespace p2

@@ -1,0 +1,613 @@
+// WHIR commit and prove on one GPU (CommitmentWriter::commit,
+// src/whir/committer/writer.rs:56-109, and Prover::prove/round/final_round,
+// src/whir/prover/mod.rs:97-417).
+//
+// The polynomial, codewords, Merkle trees and sumcheck arrays stay in HBM for
+// the whole proof; the host runs the Fiat-Shamir transcript and reads back
+// only transcript values (digests, OOD answers, sumcheck coefficients, opened
+// rows). The initial sumcheck uses split-eq partial evaluations (the
+// reference's SVO strategy, src/sumcheck/svo.rs): one pass over the base
+// polynomial per constraint yields 2^k values from which all k first-round
+// sumcheck polynomials follow exactly, so no 2^n extension weight table is
+// materialised. Classic and SVO give identical transcripts in the reference
+// (src/sumcheck/tests.rs:459-490), and so does this path.
+#include <string.h>
+
+#include <algorithm>
+
+#include "host.h"
+
+using kb::ef;
+
+namespace wh {
+int ensure_dft_tables(whir_ctx* ctx, int log_h, wk::DftTables* t);
+int dot_eq(whir_ctx* ctx, const uint32_t* d_f, int ext, int seg_bits, const ef* z, int m_bits);
+int fetch(whir_ctx* ctx, void* host, const void* dev, size_t bytes);
+int upload(whir_ctx* ctx, void* dev, const void* host, size_t bytes);
+int grind(whir_ctx* ctx, Chal& ch, int bits, uint32_t* witness);
+wk::EqSmall eq_small_host(const ef* rs, int k);
+int add_eq_points(whir_ctx* ctx, ef* d_w, int n, const std::vector<std::vector<ef>>& pts, const std::vector<ef>& scales,
+                  int accumulate);
+int add_select_vars(whir_ctx* ctx, ef* d_w, int n, const std::vector<uint32_t>& vars, const std::vector<ef>& g);
+}  // namespace wh
+
+namespace {
+
+struct Tree {
+  uint32_t* rows = nullptr;     // codeword, row-major (Montgomery)
+  uint32_t* digests = nullptr;  // (2h - 1) * 8 words
+  int log_h = 0;
+  int row_words = 0;
+  int ext = 0;
+};
+
+struct Constraint {
+  std::vector<ef> point;  // n coordinates (Montgomery)
+  ef eval;
+  std::vector<ef> partial;  // 2^k0 split partial evaluations
+};
+
+void put_ef(std::vector<uint32_t>& out, const ef& v) {
+  for (int i = 0; i < 4; i++) out.push_back(kb::from_mont(v.c[i]));
+}
+
+std::vector<ef> expand_from_univariate(const ef& z, int n) {
+  std::vector<ef> r(n);
+  ef cur = z;
+  for (int i = n - 1; i >= 0; i--) {
+    r[i] = cur;
+    cur = kb::ef_sqr(cur);
+  }
+  return r;
+}
+
+// extrapolate_012 (src/sumcheck/lagrange.rs:141-147)
+ef extrapolate_012(const ef& e0, const ef& e1, const ef& e2, const ef& r) {
+  const uint32_t inv2 = kb::to_mont((kb::P + 1) / 2);
+  const ef one = kb::ef_one(), two = kb::ef_dbl(kb::ef_one());
+  const ef l0 = kb::ef_mul_base(kb::ef_mul(kb::ef_sub(r, one), kb::ef_sub(r, two)), inv2);
+  const ef l1 = kb::ef_mul(r, kb::ef_sub(two, r));
+  const ef l2 = kb::ef_mul_base(kb::ef_mul(r, kb::ef_sub(r, one)), inv2);
+  return kb::ef_add(kb::ef_add(kb::ef_mul(e0, l0), kb::ef_mul(e1, l1)), kb::ef_mul(e2, l2));
+}
+
+// in-place first-variable fold of a host table
+void host_fold(std::vector<ef>& t, const ef& r) {
+  const size_t half = t.size() / 2;
+  for (size_t i = 0; i < half; i++) t[i] = kb::ef_add(t[i], kb::ef_mul(kb::ef_sub(t[i + half], t[i]), r));
+  t.resize(half);
+}
+
+// multilinear evaluation of 2^k host values at k coordinates (MSB first)
+ef host_eval(std::vector<ef> t, const ef* pt, int k) {
+  for (int i = 0; i < k; i++) host_fold(t, pt[i]);
+  return t[0];
+}
+
+struct Sumcheck {
+  std::vector<uint32_t> words;  // sumcheck section of the proof
+  int npolys = 0;
+  std::vector<ef> polys;
+  std::vector<uint32_t> pows;
+  void emit(std::vector<uint32_t>& out) const {
+    out.push_back((uint32_t)npolys);
+    for (const ef& v : polys) put_ef(out, v);
+    out.push_back((uint32_t)pows.size());
+    for (uint32_t w : pows) out.push_back(w);
+  }
+};
+
+// SumcheckData::observe_and_sample (src/whir/proof.rs:163-193)
+int observe_and_sample(whir_ctx* ctx, wh::Chal& ch, Sumcheck& sd, const ef& c0, const ef& c2, int pow_bits, ef* r) {
+  sd.polys.push_back(c0);
+  sd.polys.push_back(c2);
+  sd.npolys++;
+  ch.observe_ef(ctx->p16, c0);
+  ch.observe_ef(ctx->p16, c2);
+  if (pow_bits > 0) {
+    uint32_t w;
+    WH_TRY(wh::grind(ctx, ch, pow_bits, &w));
+    sd.pows.push_back(w);
+  }
+  *r = ch.sample_ef(ctx->p16);
+  return WHIR_OK;
+}
+
+int ilog2u(uint64_t v) {
+  int r = -1;
+  while (v) {
+    r++;
+    v >>= 1;
+  }
+  return r;
+}
+
+// get_challenge_stir_queries (src/whir/utils.rs:24-145)
+std::vector<uint64_t> stir_queries(whir_ctx* ctx, wh::Chal& ch, uint64_t domain_size, int ff, int nq) {
+  const uint64_t folded = domain_size >> ff;
+  const int bits = ilog2u(folded);
+  const int max_bits = 20;  // min(F::bits() - 1, 20)
+  const int total = nq * bits;
+  std::vector<uint64_t> q;
+  q.reserve(nq);
+  if (total <= max_bits) {
+    uint64_t all = ch.sample_bits(ctx->p16, total);
+    const uint64_t mask = (1ull << bits) - 1;
+    for (int i = 0; i < nq; i++) {
+      q.push_back((all & mask) % folded);
+      all >>= bits;
+    }
+  } else {
+    const int per = max_bits / bits;
+    if (per >= 2) {
+      const uint64_t mask = (1ull << bits) - 1;
+      int rem = nq;
+      while (rem > 0) {
+        const int b = std::min(rem, per);
+        uint64_t all = ch.sample_bits(ctx->p16, b * bits);
+        for (int i = 0; i < b; i++) {
+          q.push_back((all & mask) % folded);
+          all >>= bits;
+        }
+        rem -= b;
+      }
+    } else {
+      for (int i = 0; i < nq; i++) q.push_back(ch.sample_bits(ctx->p16, bits));
+    }
+  }
+  std::sort(q.begin(), q.end());
+  q.erase(std::unique(q.begin(), q.end()), q.end());
+  return q;
+}
+
+}  // namespace
+
+struct whir_witness {
+  whir_ctx* ctx = nullptr;
+  whir_protocol_params params;
+  whir_config cfg;
+  int n = 0;
+  uint32_t* d_poly = nullptr;
+  bool own_poly = false;
+  Tree commit_tree;
+  std::vector<Constraint> cons;
+  std::vector<uint32_t> proof;
+  bool proved = false;
+};
+
+namespace {
+
+void free_tree(whir_ctx* ctx, Tree& t) {
+  if (t.rows) cudaFreeAsync(t.rows, ctx->stream);
+  if (t.digests) cudaFreeAsync(t.digests, ctx->stream);
+  t.rows = nullptr;
+  t.digests = nullptr;
+}
+
+// DFT + Merkle commitment of 2^log_w contiguous chunks of 2^log_chunk elements
+int commit_matrix(whir_ctx* ctx, const uint32_t* d_src, int log_chunk, int log_w, int log_blowup, int ext,
+                  int leaf_hash, Tree* t, uint32_t* root_canon) {
+  const int lanes = ext ? 4 : 1;
+  t->log_h = log_chunk + log_blowup;
+  t->row_words = lanes << log_w;
+  t->ext = ext;
+  const size_t h = (size_t)1 << t->log_h;
+  const size_t words = h * (size_t)t->row_words;
+  WH_TRY_CUDA(cudaMallocAsync(&t->rows, words * 4, ctx->stream));
+  WH_TRY_CUDA(cudaMallocAsync(&t->digests, (2 * h - 1) * 8 * 4, ctx->stream));
+  wk::DftTables tab;
+  WH_TRY(wh::ensure_dft_tables(ctx, t->log_h, &tab));
+  uint32_t* scratch = nullptr;
+  WH_TRY_CUDA(cudaMallocAsync(&scratch, words * 4, ctx->stream));
+  cudaError_t e = wk::dft_batch(d_src, t->rows, scratch, log_chunk, log_w, log_blowup, lanes, tab, ctx->stream);
+  cudaFreeAsync(scratch, ctx->stream);
+  if (e == cudaErrorInvalidValue) return wh::set_error("unsupported DFT shape"), WHIR_ERR_INVALID;
+  WH_TRY_CUDA(e);
+  WH_TRY_CUDA(wk::merkle_build(t->rows, t->log_h, t->row_words, leaf_hash, t->digests, ctx->p16, ctx->p24, ctx->stream));
+  uint32_t r[8];
+  WH_TRY(wh::fetch(ctx, r, t->digests + (2 * h - 2) * 8, 32));
+  for (int i = 0; i < 8; i++) root_canon[i] = kb::from_mont(r[i]);
+  return WHIR_OK;
+}
+
+// Open `idx` on tree t: appends the query records to the proof and returns
+// the opened rows (Montgomery) in `rows`.
+int open_queries(whir_ctx* ctx, const Tree& t, const std::vector<uint64_t>& idx, std::vector<uint32_t>& proof,
+                 std::vector<uint32_t>& rows) {
+  const int q = (int)idx.size();
+  const size_t per = (size_t)t.row_words + (size_t)t.log_h * 8;
+  WH_CHECK((size_t)q * 8 + (size_t)q * per * 4 + 64 <= ctx->arena_bytes, "too many queries for the scratch arena");
+  uint64_t* d_idx = reinterpret_cast<uint64_t*>(ctx->d_arena);
+  uint32_t* d_rows = reinterpret_cast<uint32_t*>(d_idx + q + 1);
+  uint32_t* d_paths = d_rows + (size_t)q * t.row_words;
+  if (q == 0) return WHIR_OK;
+  WH_TRY(wh::upload(ctx, d_idx, idx.data(), (size_t)q * 8));
+  WH_TRY_CUDA(wk::merkle_open(t.rows, t.digests, t.log_h, t.row_words, d_idx, q, d_rows, d_paths, ctx->stream));
+  std::vector<uint32_t> tmp((size_t)q * per);
+  WH_TRY(wh::fetch(ctx, tmp.data(), d_rows, tmp.size() * 4));
+  rows.assign(tmp.begin(), tmp.begin() + (size_t)q * t.row_words);
+  const uint32_t* paths = tmp.data() + (size_t)q * t.row_words;
+  const int nvals = t.ext ? t.row_words / 4 : t.row_words;
+  for (int k = 0; k < q; k++) {
+    proof.push_back((uint32_t)t.ext);
+    proof.push_back((uint32_t)nvals);
+    for (int i = 0; i < t.row_words; i++) proof.push_back(kb::from_mont(rows[(size_t)k * t.row_words + i]));
+    proof.push_back((uint32_t)t.log_h);
+    for (int i = 0; i < t.log_h * 8; i++) proof.push_back(kb::from_mont(paths[(size_t)k * t.log_h * 8 + i]));
+  }
+  return WHIR_OK;
+}
+
+// One ProductPolynomial::round on the device arrays f, w of 2^m entries
+int sumcheck_round(whir_ctx* ctx, wh::Chal& ch, Sumcheck& sd, ef* d_f, ef* d_w, int m, ef* sum, int pow_bits,
+                   ef* r_out) {
+  const size_t half = (size_t)1 << (m - 1);
+  WH_TRY_CUDA(wk::sumcheck_coeffs(d_f, d_w, half, ctx->d_partials, ctx->d_small, ctx->stream));
+  ef c[2];
+  WH_TRY(wh::fetch(ctx, c, ctx->d_small, sizeof(c)));
+  ef r;
+  WH_TRY(observe_and_sample(ctx, ch, sd, c[0], c[1], pow_bits, &r));
+  WH_TRY_CUDA(wk::fold_ext(d_f, d_w, half, r, ctx->stream));
+  *sum = extrapolate_012(c[0], kb::ef_sub(*sum, c[0]), c[1], r);
+  *r_out = r;
+  return WHIR_OK;
+}
+
+// InitialStatement::evaluate for the split strategy: partial evaluations over
+// the first k0 variables, then the full evaluation.
+int evaluate_constraint(whir_ctx* ctx, whir_witness* w, const std::vector<ef>& point, Constraint* out) {
+  const int n = w->n, k0 = w->cfg.folding_factor_0;
+  WH_TRY(wh::dot_eq(ctx, w->d_poly, 0, k0, point.data() + k0, n - k0));
+  out->point = point;
+  out->partial.resize((size_t)1 << k0);
+  WH_TRY(wh::fetch(ctx, out->partial.data(), ctx->d_small, out->partial.size() * sizeof(ef)));
+  wk::EqSmall e = wh::eq_small_host(point.data(), k0);
+  ef eval = kb::ef_zero();
+  for (size_t y = 0; y < out->partial.size(); y++) eval = kb::ef_add(eval, kb::ef_mul(e.v[y], out->partial[y]));
+  out->eval = eval;
+  return WHIR_OK;
+}
+
+int do_commit(whir_ctx* ctx, whir_witness* w, wh::Chal& ch, const uint32_t* user_points, int num_points,
+              uint32_t* user_evals_out) {
+  const whir_config& c = w->cfg;
+  const int n = w->n, k0 = c.folding_factor_0;
+  for (int i = 0; i < num_points; i++) {
+    std::vector<ef> pt(n);
+    for (int j = 0; j < n; j++)
+      for (int l = 0; l < 4; l++) {
+        const uint32_t v = user_points[4 * ((size_t)i * n + j) + l];
+        WH_CHECK(v < kb::P, "point value out of range");
+        pt[j].c[l] = kb::to_mont(v);
+      }
+    Constraint con;
+    WH_TRY(evaluate_constraint(ctx, w, pt, &con));
+    if (user_evals_out)
+      for (int l = 0; l < 4; l++) user_evals_out[4 * i + l] = kb::from_mont(con.eval.c[l]);
+    w->cons.push_back(std::move(con));
+  }
+  std::vector<uint32_t>& pf = w->proof;
+  pf.push_back(0x50524857u);
+  pf.push_back(1u);
+  uint32_t root[8];
+  WH_TRY(commit_matrix(ctx, w->d_poly, n - k0, k0, c.starting_log_inv_rate, 0, w->params.leaf_hash, &w->commit_tree,
+                       root));
+  for (int i = 0; i < 8; i++) pf.push_back(root[i]);
+  for (int i = 0; i < 8; i++) ch.observe(ctx->p16, kb::to_mont(root[i]));
+  pf.push_back((uint32_t)c.commitment_ood_samples);
+  for (int i = 0; i < c.commitment_ood_samples; i++) {
+    const ef z = ch.sample_ef(ctx->p16);
+    Constraint con;
+    WH_TRY(evaluate_constraint(ctx, w, expand_from_univariate(z, n), &con));
+    put_ef(pf, con.eval);
+    ch.observe_ef(ctx->p16, con.eval);
+    w->cons.push_back(std::move(con));
+  }
+  return WHIR_OK;
+}
+
+int do_prove(whir_ctx* ctx, whir_witness* wit, wh::Chal& ch) {
+  const whir_config& c = wit->cfg;
+  const int n = wit->n, k0 = c.folding_factor_0;
+  std::vector<uint32_t>& pf = wit->proof;
+  const int m = (int)wit->cons.size();
+
+  // ---- initial sumcheck (Sumcheck::from_base_evals, sumcheck_prover.rs:237-292)
+  const ef alpha = ch.sample_ef(ctx->p16);
+  std::vector<ef> apow(m > 0 ? m : 1);
+  ef sum = kb::ef_zero();
+  {
+    ef a = kb::ef_one();
+    for (int i = 0; i < m; i++) {
+      apow[i] = a;
+      sum = kb::ef_add(sum, kb::ef_mul(a, wit->cons[i].eval));
+      a = kb::ef_mul(a, alpha);
+    }
+  }
+  std::vector<std::vector<ef>> G(m), E(m);
+  for (int i = 0; i < m; i++) {
+    G[i] = wit->cons[i].partial;
+    wk::EqSmall e = wh::eq_small_host(wit->cons[i].point.data(), k0);
+    E[i].assign(e.v, e.v + ((size_t)1 << (k0 & 7)));
+  }
+  Sumcheck sd0;
+  std::vector<ef> rs;
+  for (int j = 0; j < k0; j++) {
+    ef c0 = kb::ef_zero(), c2 = kb::ef_zero();
+    for (int i = 0; i < m; i++) {
+      const size_t half = G[i].size() / 2;
+      ef a0 = kb::ef_zero(), a2 = kb::ef_zero();
+      for (size_t y = 0; y < half; y++) {
+        a0 = kb::ef_add(a0, kb::ef_mul(G[i][y], E[i][y]));
+        a2 = kb::ef_add(a2, kb::ef_mul(kb::ef_sub(kb::ef_dbl(G[i][y + half]), G[i][y]),
+                                       kb::ef_sub(kb::ef_dbl(E[i][y + half]), E[i][y])));
+      }
+      c0 = kb::ef_add(c0, kb::ef_mul(apow[i], a0));
+      c2 = kb::ef_add(c2, kb::ef_mul(apow[i], a2));
+    }
+    ef r;
+    WH_TRY(observe_and_sample(ctx, ch, sd0, c0, c2, c.starting_folding_pow_bits, &r));
+    sum = extrapolate_012(c0, kb::ef_sub(sum, c0), c2, r);
+    for (int i = 0; i < m; i++) {
+      host_fold(G[i], r);
+      host_fold(E[i], r);
+    }
+    rs.push_back(r);
+  }
+  sd0.emit(pf);
+
+  // fold the polynomial by the k0 challenges and build the weights
+  int nv = n - k0;
+  const size_t N = (size_t)1 << nv;
+  ef *d_f = nullptr, *d_w = nullptr;
+  WH_TRY_CUDA(cudaMallocAsync(&d_f, N * sizeof(ef), ctx->stream));
+  WH_TRY_CUDA(cudaMallocAsync(&d_w, N * sizeof(ef), ctx->stream));
+  struct Guard {
+    whir_ctx* ctx;
+    ef** a;
+    ef** b;
+    ~Guard() {
+      cudaFreeAsync(*a, ctx->stream);
+      cudaFreeAsync(*b, ctx->stream);
+    }
+  } guard{ctx, &d_f, &d_w};
+  {
+    wk::EqSmall e = wh::eq_small_host(rs.data(), k0);
+    WH_TRY_CUDA(wk::fold_multi_base(wit->d_poly, k0, N, e, d_f, ctx->stream));
+    std::vector<std::vector<ef>> tails(m);
+    std::vector<ef> scales(m);
+    for (int i = 0; i < m; i++) {
+      tails[i].assign(wit->cons[i].point.begin() + k0, wit->cons[i].point.end());
+      scales[i] = kb::ef_mul(apow[i], E[i][0]);  // alpha^i * eq(z_i[0:k0], rs)
+    }
+    WH_TRY(wh::add_eq_points(ctx, d_w, nv, tails, scales, 0));
+  }
+
+  pf.push_back((uint32_t)c.n_rounds);
+  Tree prev = wit->commit_tree;
+  bool prev_owned = false;  // the commit tree belongs to the witness
+  std::vector<ef> fold_rs = rs;
+  std::vector<uint32_t> rows;
+  for (int round = 0; round < c.n_rounds; round++) {
+    const whir_round_config& rc = c.rounds[round];
+    const int ffn = wh::ff_at(c, round + 1);
+    const uint64_t new_dom = rc.domain_size >> wh::rsr_at(c, round);
+    const int log_blowup = ilog2u(new_dom) - nv;
+    Tree nt;
+    uint32_t root[8];
+    WH_TRY(commit_matrix(ctx, reinterpret_cast<const uint32_t*>(d_f), nv - ffn, ffn, log_blowup, 1,
+                         wit->params.leaf_hash, &nt, root));
+    for (int i = 0; i < 8; i++) ch.observe(ctx->p16, kb::to_mont(root[i]));
+    for (int i = 0; i < 8; i++) pf.push_back(root[i]);
+    // OOD samples
+    std::vector<std::vector<ef>> opts;
+    std::vector<ef> oevs;
+    pf.push_back((uint32_t)rc.ood_samples);
+    for (int i = 0; i < rc.ood_samples; i++) {
+      const ef z = ch.sample_ef(ctx->p16);
+      std::vector<ef> pt = expand_from_univariate(z, nv);
+      WH_TRY(wh::dot_eq(ctx, reinterpret_cast<const uint32_t*>(d_f), 1, 0, pt.data(), nv));
+      ef ev;
+      WH_TRY(wh::fetch(ctx, &ev, ctx->d_small, sizeof(ef)));
+      ch.observe_ef(ctx->p16, ev);
+      put_ef(pf, ev);
+      opts.push_back(std::move(pt));
+      oevs.push_back(ev);
+    }
+    uint32_t pw = 0;
+    if (rc.pow_bits > 0) WH_TRY(wh::grind(ctx, ch, rc.pow_bits, &pw));
+    pf.push_back(pw);
+    (void)ch.sample(ctx->p16);
+    const std::vector<uint64_t> idx = stir_queries(ctx, ch, rc.domain_size, wh::ff_at(c, round), rc.num_queries);
+    pf.push_back((uint32_t)idx.size());
+    WH_TRY(open_queries(ctx, prev, idx, pf, rows));
+    const int kprev = wh::ff_at(c, round);
+    const ef* frs = fold_rs.data() + fold_rs.size() - kprev;
+    std::vector<uint32_t> svars(idx.size());
+    std::vector<ef> sevs(idx.size());
+    const uint32_t gen = kb::to_mont(rc.folded_domain_gen);
+    for (size_t q = 0; q < idx.size(); q++) {
+      std::vector<ef> vals((size_t)1 << kprev);
+      for (size_t v = 0; v < vals.size(); v++) {
+        if (prev.ext)
+          for (int l = 0; l < 4; l++) vals[v].c[l] = rows[q * prev.row_words + 4 * v + l];
+        else
+          vals[v] = kb::ef_from_base(rows[q * prev.row_words + v]);
+      }
+      sevs[q] = host_eval(vals, frs, kprev);
+      svars[q] = kb::pow(gen, idx[q]);
+    }
+    // Constraint::combine (constraints/mod.rs:234-248) then the sumcheck rounds
+    const ef gamma = ch.sample_ef(ctx->p16);
+    std::vector<ef> gpow(opts.size());
+    ef g = kb::ef_one();
+    for (size_t i = 0; i < opts.size(); i++) {
+      gpow[i] = g;
+      sum = kb::ef_add(sum, kb::ef_mul(g, oevs[i]));
+      g = kb::ef_mul(g, gamma);
+    }
+    WH_TRY(wh::add_eq_points(ctx, d_w, nv, opts, gpow, 1));
+    std::vector<ef> spow(idx.size());
+    for (size_t q = 0; q < idx.size(); q++) {
+      spow[q] = g;
+      sum = kb::ef_add(sum, kb::ef_mul(g, sevs[q]));
+      g = kb::ef_mul(g, gamma);
+    }
+    WH_TRY(wh::add_select_vars(ctx, d_w, nv, svars, spow));
+    Sumcheck sd;
+    fold_rs.clear();
+    for (int j = 0; j < ffn; j++) {
+      ef r;
+      WH_TRY(sumcheck_round(ctx, ch, sd, d_f, d_w, nv - j, &sum, rc.folding_pow_bits, &r));
+      fold_rs.push_back(r);
+    }
+    sd.emit(pf);
+    nv -= ffn;
+    if (prev_owned) free_tree(ctx, prev);
+    prev = nt;
+    prev_owned = true;
+  }
+
+  // ---- final round (prover/mod.rs:330-417)
+  {
+    const size_t fn = (size_t)1 << nv;
+    std::vector<ef> fin(fn);
+    WH_TRY(wh::fetch(ctx, fin.data(), d_f, fn * sizeof(ef)));
+    pf.push_back((uint32_t)fn);
+    for (size_t i = 0; i < fn; i++) {
+      ch.observe_ef(ctx->p16, fin[i]);
+      put_ef(pf, fin[i]);
+    }
+    uint32_t pw = 0;
+    if (c.final_pow_bits > 0) WH_TRY(wh::grind(ctx, ch, c.final_pow_bits, &pw));
+    pf.push_back(pw);
+    const whir_round_config fc = wh::final_round_config(c);
+    const std::vector<uint64_t> idx = stir_queries(ctx, ch, fc.domain_size, wh::ff_at(c, c.n_rounds), c.final_queries);
+    pf.push_back((uint32_t)idx.size());
+    WH_TRY(open_queries(ctx, prev, idx, pf, rows));
+    if (c.final_sumcheck_rounds > 0) {
+      Sumcheck sd;
+      for (int j = 0; j < c.final_sumcheck_rounds; j++) {
+        ef r;
+        WH_TRY(sumcheck_round(ctx, ch, sd, d_f, d_w, nv - j, &sum, c.final_folding_pow_bits, &r));
+      }
+      pf.push_back(1u);
+      sd.emit(pf);
+    } else {
+      pf.push_back(0u);
+    }
+  }
+  if (prev_owned) free_tree(ctx, prev);
+  return WHIR_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int whir_commit(whir_ctx* ctx, const whir_protocol_params* params, int32_t n, const uint32_t* poly,
+                int32_t poly_on_device, const uint32_t* user_points, int32_t num_points, uint32_t* user_evals_out,
+                whir_challenger* chs, whir_witness** out) {
+  WH_CHECK(ctx && params && poly && chs && out && num_points >= 0 && (num_points == 0 || user_points),
+           "null argument");
+  *out = nullptr;
+  whir_witness* w = new whir_witness();
+  w->ctx = ctx;
+  w->params = *params;
+  w->n = n;
+  int s = wh::config_new(*params, n, &w->cfg);
+  if (s != WHIR_OK) {
+    delete w;
+    return s;
+  }
+  if (ctx->device < 0) {
+    delete w;
+    wh::set_error("host-only context (device -1) cannot run device work");
+    return WHIR_ERR_NO_DEVICE;
+  }
+  if (w->cfg.folding_factor_0 > 6) {
+    delete w;
+    wh::set_error("folding factor above 6 is not supported");
+    return WHIR_ERR_INVALID;
+  }
+  cudaSetDevice(ctx->device);
+  const size_t N = (size_t)1 << n;
+  if (poly_on_device) {
+    w->d_poly = const_cast<uint32_t*>(poly);
+  } else {
+    // values are KoalaBear elements, canonical by type as in the reference
+    if (cudaMallocAsync(&w->d_poly, N * 4, ctx->stream) != cudaSuccess) {
+      delete w;
+      wh::set_error("polynomial allocation failed");
+      return WHIR_ERR_NOMEM;
+    }
+    w->own_poly = true;
+    if (cudaMemcpyAsync(w->d_poly, poly, N * 4, cudaMemcpyHostToDevice, ctx->stream) != cudaSuccess ||
+        wk::encode(w->d_poly, N, ctx->stream) != cudaSuccess) {
+      whir_witness_free(w);
+      wh::set_error("polynomial upload failed");
+      return WHIR_ERR_CUDA;
+    }
+  }
+  wh::Chal ch;
+  ch.load(*chs);
+  s = do_commit(ctx, w, ch, user_points, num_points, user_evals_out);
+  if (s != WHIR_OK) {
+    whir_witness_free(w);
+    return s;
+  }
+  ch.store(*chs);
+  *out = w;
+  return WHIR_OK;
+}
+
+int whir_prove(whir_ctx* ctx, whir_witness* w, whir_challenger* chs, uint32_t* proof_out, size_t cap_words,
+               size_t* proof_words) {
+  WH_CHECK(ctx && w && chs && proof_words && w->ctx == ctx, "bad argument");
+  WH_CHECK(!w->proved, "witness already proved");
+  cudaSetDevice(ctx->device);
+  wh::Chal ch;
+  ch.load(*chs);
+  WH_TRY(do_prove(ctx, w, ch));
+  w->proved = true;
+  ch.store(*chs);
+  *proof_words = w->proof.size();
+  if (!proof_out || cap_words < w->proof.size()) {
+    wh::set_error("proof buffer too small");
+    return WHIR_ERR_BUFFER;
+  }
+  memcpy(proof_out, w->proof.data(), w->proof.size() * 4);
+  return WHIR_OK;
+}
+
+int whir_witness_free(whir_witness* w) {
+  if (!w) return WHIR_OK;
+  whir_ctx* ctx = w->ctx;
+  free_tree(ctx, w->commit_tree);
+  if (w->own_poly && w->d_poly) cudaFreeAsync(w->d_poly, ctx->stream);
+  cudaStreamSynchronize(ctx->stream);
+  delete w;
+  return WHIR_OK;
+}
+
+int whir_commit_and_prove(whir_ctx* ctx, const whir_protocol_params* params, int32_t n, const uint32_t* poly,
+                          int32_t poly_on_device, const uint32_t* user_points, int32_t num_points,
+                          uint32_t* user_evals_out, uint32_t* proof_out, size_t cap_words, size_t* proof_words,
+                          uint32_t* checkpoint) {
+  WH_CHECK(ctx && params && proof_words, "null argument");
+  whir_config cfg;
+  WH_TRY(wh::config_new(*params, n, &cfg));
+  whir_challenger chs;
+  whir_challenger_init(&chs);
+  const std::vector<uint32_t> ds = wh::domain_separator(cfg, params->ds_digest_elems);
+  WH_TRY(whir_challenger_observe(ctx, &chs, ds.data(), ds.size()));
+  whir_witness* w = nullptr;
+  WH_TRY(whir_commit(ctx, params, n, poly, poly_on_device, user_points, num_points, user_evals_out, &chs, &w));
+  int s = whir_prove(ctx, w, &chs, proof_out, cap_words, proof_words);
+  whir_witness_free(w);
+  if (s != WHIR_OK) return s;
+  if (checkpoint) WH_TRY(whir_challenger_sample(ctx, &chs, checkpoint, 4));
+  return WHIR_OK;
+}
+
+}  // extern "C"
