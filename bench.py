@@ -1,0 +1,279 @@
+#!/usr/bin/env python
+"""WHIR commit + prove at 2^24 variables on B200.
+
+Workload (the reference's own benchmark, benches/whir.rs:34-120 "prove"):
+KoalaBear / quartic extension, num_variables = 24, folding factor 4, rate 1/2,
+100-bit CapacityBound, pow_bits 16, rs_domain_initial_reduction_factor 3, one
+evaluation constraint, Poseidon2-24 leaf hashing, Poseidon2-16 compression and
+duplex challenger, DIGEST_ELEMS 32. Inputs are seeded synthetic data.
+
+One step = one full commit + prove of one polynomial on each GPU (replicas:
+one independent proof per rank, no collective on the data path). Rank 0 prints
+one JSON line; `value` is milliseconds per proof for the whole job (the max
+over ranks of the timed region divided by the proofs all ranks produced).
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import pathlib
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = pathlib.Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+N_VARS = 24
+CONFIG = dict(workload="whir_commit_prove", num_variables=N_VARS, folding_factor=4, starting_log_inv_rate=1,
+              security_level=100, soundness="CapacityBound", pow_bits=16, rs_domain_initial_reduction_factor=3,
+              constraints=1, leaf_hash="poseidon2_24", compress="poseidon2_16", challenger="duplex_poseidon2_16",
+              ds_digest_elems=32, l2="flushed between timed steps (256 MiB write)")
+METRIC = "WHIR prove ms @2^24 vars"
+UNIT = "ms/proof"
+P = 0x7F000001
+
+
+def inputs(rank: int, n: int):
+    rng = np.random.default_rng(1000 + rank)
+    poly = rng.integers(0, P, 1 << n, dtype=np.uint64).astype(np.uint32)
+    point = rng.integers(0, P, 4 * n, dtype=np.uint64).astype(np.uint32)
+    return poly, point
+
+
+def oracle_params():
+    from oracle.oracle import make_params
+
+    return make_params(100, 16, 4, None, 2, 1, 3, 0, 32)
+
+
+class Clocks:
+    """nvidia-smi sampling during the timed region."""
+
+    def __init__(self, index: int):
+        self.proc = None
+        self.path = ROOT / "gpurun_out" / f"clocks_rank{index}.csv"
+        try:
+            self.path.parent.mkdir(exist_ok=True)
+            q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+                 "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+                 "clocks_event_reasons.sw_power_cap")
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(index), f"--query-gpu={q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        self.proc.wait()
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.path.read_text().splitlines():
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 8:
+                continue
+            try:
+                sm.append(float(f[0]))
+                mx = float(f[1])
+            except ValueError:
+                continue
+            for name, v in zip(names, f[4:8]):
+                if v.lower().startswith("active"):
+                    reasons.add(name)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def run_reference(args) -> None:
+    """The reference's CPU prover cannot be built here (Rust, no cargo); the
+    CPU arm runs the oracle port of the same algorithm on all host cores."""
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    from oracle.oracle import Oracle
+
+    o = Oracle()
+    prm = oracle_params()
+    poly, point = inputs(0, N_VARS)
+    cores = os.cpu_count() or 1
+    for _ in range(max(args.warmup, 0)):
+        o.prove(prm, N_VARS, poly, point)
+    times = []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        o.prove(prm, N_VARS, poly, point)
+        times.append((time.perf_counter() - t0) * 1e3)
+    ms = float(np.mean(times))
+    line = {"metric": METRIC, "value": ms, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": False, "scaling": "weak",
+            "vs_baseline": None, "dtype": "u32 (KoalaBear mod p)", "data": "synthetic (seeded)",
+            "config": dict(CONFIG, parallelism="cpu"), "impl": "reference",
+            "cpu_baseline": {"value": ms, "unit": UNIT, "cores": cores, "kind": "port",
+                             "sample": f"{args.steps} full n=24 commit+prove runs of the oracle port (OpenMP)"},
+            "e2e": {"value": ms, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def cpu_baseline_sample() -> dict:
+    from oracle.oracle import Oracle
+
+    o = Oracle()
+    poly, point = inputs(0, N_VARS)
+    t0 = time.perf_counter()
+    o.prove(oracle_params(), N_VARS, poly, point)
+    ms = (time.perf_counter() - t0) * 1e3
+    return {"value": ms, "unit": UNIT, "cores": os.cpu_count() or 1, "kind": "port",
+            "sample": "one full n=24 commit+prove of the oracle port on all host cores (OpenMP)"}
+
+
+def main() -> None:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        run_reference(args)
+        return
+
+    import torch
+
+    import __graft_entry__
+
+    pkg = __graft_entry__.load_package()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    ctx = pkg.Context(local)
+    stream = torch.cuda.current_stream()
+    ctx.set_stream(stream.cuda_stream)
+    params = pkg.ProtocolParameters(100, 16, pkg.FoldingFactor.constant(4), pkg.SecurityAssumption.CapacityBound, 1, 3,
+                                    "poseidon2_24", 32)
+    poly, point = inputs(rank, N_VARS)
+    d_poly = pkg.DeviceArray.from_host(ctx, poly)  # resident in HBM, Montgomery form
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+
+    def barrier():
+        torch.cuda.synchronize()
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    def step(poly_arg):
+        return pkg.commit_and_prove(ctx, params, N_VARS, poly_arg, point)
+
+    for _ in range(max(args.warmup, 3)):
+        step(d_poly)
+    ref_proof = step(d_poly)[0]
+
+    # ---- device-resident timing (value) ----
+    clocks = Clocks(local)
+    barrier()
+    l0 = pkg.kernel_launches()
+    total_ms = 0.0
+    for _ in range(args.steps):
+        flush.zero_()
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record(stream)
+        proof = step(d_poly)[0]
+        e.record(stream)
+        e.synchronize()
+        total_ms += s.elapsed_time(e)
+        assert np.array_equal(proof, ref_proof)
+    barrier()
+    launches = pkg.kernel_launches() - l0
+    clk = clocks.stop()
+    t = torch.tensor([total_ms], dtype=torch.float64, device="cuda")
+    if dist is not None:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    step_ms = float(t.item()) / args.steps
+    value = step_ms / world
+
+    # ---- end to end through the public API with host buffers ----
+    host_poly = torch.from_numpy(poly).pin_memory()
+    host_np = host_poly.numpy()
+    barrier()
+    e2e_ms = 0.0
+    for _ in range(args.steps):
+        flush.zero_()
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record(stream)
+        proof = step(host_np)[0]
+        e.record(stream)
+        e.synchronize()
+        e2e_ms += s.elapsed_time(e)
+    barrier()
+    t = torch.tensor([e2e_ms], dtype=torch.float64, device="cuda")
+    if dist is not None:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    e2e_value = float(t.item()) / args.steps / world
+    h2d = poly.nbytes + point.nbytes
+    d2h = int(proof.size) * 4
+
+    # ---- dominant HBM kernel: the commit DFT (16 columns x 2^21 rows), timed alone ----
+    k = 4
+    log_chunk, log_h = N_VARS - k, N_VARS + 1 - k
+    d_out = pkg.DeviceArray(ctx, (1 << log_h) << k)
+    for _ in range(3):
+        pkg.dft_batch(ctx, d_poly, log_chunk, k, 1, False, d_out)
+    reps = 20
+    torch.cuda.synchronize()
+    s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    dft_ms = 0.0
+    for _ in range(reps):
+        flush.zero_()
+        s.record(stream)
+        pkg.dft_batch(ctx, d_poly, log_chunk, k, 1, False, d_out)
+        e.record(stream)
+        e.synchronize()
+        dft_ms += s.elapsed_time(e)
+    dft_ms /= reps
+    alg_bytes = (1 << N_VARS) * 4 + (1 << (log_h + k)) * 4
+    peaks = json.loads((ROOT / "MEASURED_PEAKS.json").read_text()) if (ROOT / "MEASURED_PEAKS.json").exists() else {}
+    peak = float(peaks.get("hbm_gbs", 6650.0))
+    achieved = alg_bytes / (dft_ms * 1e-3) / 1e9
+    roofline = {"kernel": "dft_batch (k_dft_cols + k_dft_rows), commit LDE 16 x 2^20 -> 16 x 2^21",
+                "bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                "frac": round(achieved / peak, 4), "traffic": None,
+                "peak_source": "MEASURED_PEAKS.json hbm_gbs (burst copy)" if peaks else "fallback 6650 GB/s",
+                "ms_per_launch": round(dft_ms, 4), "algorithmic_bytes": alg_bytes}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline_sample()
+    if rank == 0:
+        line = {"metric": METRIC, "value": round(value, 4), "unit": UNIT, "n_gpus": world, "steps": args.steps,
+                "warmup": max(args.warmup, 3), "ms_per_step": round(step_ms, 4), "higher_is_better": False,
+                "scaling": "weak", "vs_baseline": None, "dtype": "u32 (KoalaBear mod p, exact)",
+                "data": "synthetic (seeded)",
+                "config": dict(CONFIG, parallelism=f"replicas x{world} (one proof per GPU per step)"),
+                "proofs_per_s": round(1e3 / value, 3), "proof_words": int(ref_proof.size),
+                "e2e": {"value": round(e2e_value, 4), "unit": UNIT, "h2d_bytes_per_step": h2d * world,
+                        "d2h_bytes_per_step": d2h * world},
+                "gpu_launches": int(launches), "roofline": roofline, "cpu_baseline": cpu, "clocks": clk}
+        print(json.dumps(line), flush=True)
+    ctx.close()
+    if dist is not None:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -56,13 +56,15 @@ KB_HD uint32_t reduce(uint64_t t) {
   uint32_t r = hi - mulhi(m, P);
   return umin32(r, r + P);
 }
-// Montgomery reduction of T < 2^64 (any sum of up to four products < p^2).
+// Montgomery reduction of T < 2p * 2^32 (any sum of up to four products < p^2).
+// Here hi - mulhi(m, p) lies in (-p, 2p); the two ranges overlap as unsigned
+// 32-bit values, so the sign comes from the borrow, not from the value.
 KB_HD uint32_t reduce_wide(uint64_t t) {
   uint32_t lo = (uint32_t)t, hi = (uint32_t)(t >> 32);
   uint32_t m = lo * P_INV;
-  uint32_t r = hi - mulhi(m, P);   // in (-p, 2p) as a signed value
-  r = umin32(r, r + P);            // -> [0, 2p)
-  return umin32(r, r - P);         // -> [0, p)
+  uint32_t mh = mulhi(m, P);
+  uint32_t r = hi - mh + (hi < mh ? P : 0u);  // -> [0, 2p)
+  return umin32(r, r - P);                    // -> [0, p)
 }
 
 KB_HD uint32_t mul(uint32_t a, uint32_t b) { return reduce((uint64_t)a * b); }
