@@ -170,6 +170,22 @@ int whir_fold_multi_base(whir_ctx* ctx, const uint32_t* d_evals, int32_t n, cons
 /* sumcheck_coefficients (evals.rs:493-526) on extension f, w */
 int whir_sumcheck_coeffs(whir_ctx* ctx, const uint32_t* d_f, const uint32_t* d_w, int32_t n, uint32_t* c0,
                          uint32_t* c2);
+/* Allocation-free variant of whir_sumcheck_coeffs. It has no counterpart in
+ * the reference: it exists for callers that cannot allocate device memory on
+ * this path (a host application that owns all device memory through its own
+ * pool, or a latency-critical loop where allocation is not allowed). It takes
+ * no context: inputs d_f, d_w (2^n extension elements each, Montgomery form),
+ * output d_out (8 words: c0 then c2, Montgomery form), all device pointers
+ * owned by the caller, and an optional cudaStream_t (NULL = default stream).
+ * The per-block partial sums live in a fixed 64 KiB array inside the library
+ * (2048 blocks at most), present on every device that loads the library until
+ * the process exits. The first call on a device looks up that array's device
+ * address; make that first call before any stream capture. Calls that overlap
+ * on the GPU share the array and race: run them on one stream at a time.
+ * n must be in [1, 30]. Nothing is allocated or freed. Asynchronous: results
+ * are ready when the stream reaches this point. */
+int whir_sumcheck_coeffs_noalloc(const uint32_t* d_f, const uint32_t* d_w, int32_t n, uint32_t* d_out,
+                                 void* cuda_stream);
 /* EqStatement::combine_hypercube with INITIALIZED (statement/eq.rs:182-246):
  * d_w[x] += sum_i gamma_pows[i] * eq(points_i, x); m <= 16 */
 int whir_combine_eq(whir_ctx* ctx, uint32_t* d_w, int32_t n, const uint32_t* points, int32_t m,

@@ -809,6 +809,18 @@ cudaError_t sumcheck_coeffs(const ef* f, const ef* w, size_t half, ef* partials,
   LAUNCH_DONE();
 }
 
+cudaError_t sumcheck_coeffs_capped(const ef* f, const ef* w, size_t half, ef* partials, unsigned max_blocks, ef* out,
+                                   cudaStream_t st) {
+  unsigned b = grid_for(half, 256, 8);
+  if (b > max_blocks) b = max_blocks;
+  k_sumcheck_coeffs<<<b, 256, 0, st>>>(f, w, half, partials);
+  count_launch();
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  k_sum_partials<<<2, 256, 0, st>>>(partials, (int)b, out);
+  LAUNCH_DONE();
+}
+
 // ---------------------------------------------------------------------------
 // Constraint weights (Constraint::combine, src/whir/constraints/mod.rs:197-248)
 //   eq part:     EqStatement::combine_hypercube(_packed), statement/eq.rs:182-312

@@ -80,6 +80,11 @@ cudaError_t fold_multi_base(const uint32_t* f, int k, size_t m, const EqSmall& e
 cudaError_t sumcheck_coeffs(const kb::ef* f, const kb::ef* w, size_t half, kb::ef* partials, kb::ef* out,
                             cudaStream_t st);
 
+// The same reduction with the block count capped at max_blocks, so that the
+// partials fit a fixed-size buffer (2 * max_blocks entries).
+cudaError_t sumcheck_coeffs_capped(const kb::ef* f, const kb::ef* w, size_t half, kb::ef* partials,
+                                   unsigned max_blocks, kb::ef* out, cudaStream_t st);
+
 // W[x] (+)= sum_c hi_c[x >> lo_bits] * lo_c[x & mask] for c < m constraints (the
 // scale of each constraint is folded into its hi table); tables are laid out
 // constraint-major (hi: m * 2^(n-lo_bits), lo: m * 2^lo_bits).
