@@ -13,6 +13,14 @@ one JSON line; `value` is milliseconds per proof for the whole job (the max
 over ranks of the timed region divided by the proofs all ranks produced).
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+
+Kernel-level microbenchmarks (the kernel configuration of the benchmark
+suite: eq expansion / evaluation / fold over 2^24 extension elements, the
+2^24 -> 2^25 LDE, a Poseidon2 Merkle tree over 2^21 leaves of 16 elements, and
+proof-of-work grinding), each timed alone with CUDA events on the context's
+stream and printed as one JSON line per kernel:
+
+  python bench.py --micro all|eq|eval|fold|dft|merkle|grind [--steps K]
 """
 from __future__ import annotations
 
@@ -134,6 +142,91 @@ def cpu_baseline_sample() -> dict:
             "sample": "one full n=24 commit+prove of the oracle port on all host cores (OpenMP)"}
 
 
+def run_micro(args) -> None:
+    import torch
+
+    import __graft_entry__
+
+    pkg = __graft_entry__.load_package()
+    torch.cuda.set_device(0)
+    ctx = pkg.Context(0)
+    stream = torch.cuda.current_stream()
+    ctx.set_stream(stream.cuda_stream)
+    peaks = json.loads((ROOT / "MEASURED_PEAKS.json").read_text()) if (ROOT / "MEASURED_PEAKS.json").exists() else {}
+    hbm = float(peaks.get("hbm_gbs", 6650.0))
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+    rng = np.random.default_rng(7)
+    reps = max(args.steps, 1)
+
+    def timed(fn):
+        for _ in range(max(args.warmup, 1)):
+            fn()
+        total = 0.0
+        for _ in range(reps):
+            flush.zero_()
+            s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            s.record(stream)
+            fn()
+            e.record(stream)
+            e.synchronize()
+            total += s.elapsed_time(e)
+        return total / reps
+
+    def emit(name, ms, alg_bytes=None, units=None, unit_name=None, extra=None):
+        line = {"micro": name, "ms": round(ms, 5)}
+        if alg_bytes is not None:
+            gbs = alg_bytes / (ms * 1e-3) / 1e9
+            line.update({"algorithmic_bytes": alg_bytes, "GB/s": round(gbs, 1), "hbm_frac": round(gbs / hbm, 4)})
+        if units is not None:
+            line[unit_name] = round(units / (ms * 1e-3), 1)
+        line.update(extra or {})
+        print(json.dumps(line), flush=True)
+
+    kinds = ["eq", "eval", "fold", "dft", "merkle", "grind"] if args.micro == "all" else [args.micro]
+    n = 24
+    N = 1 << n
+    if any(k in kinds for k in ("eq", "eval", "fold")):
+        f = pkg.DeviceArray(ctx, 4 * N)
+        point = rng.integers(0, P, 4 * n, dtype=np.uint64).astype(np.uint32)
+        scale = np.array([1, 0, 0, 0], dtype=np.uint32)
+        pkg.eq_table(ctx, point, scale, f)  # also initialises f with data
+    if "eq" in kinds:
+        emit("eq_table 2^24 ext", timed(lambda: pkg.eq_table(ctx, point, scale, f)), alg_bytes=16 * N)
+    if "eval" in kinds:
+        emit("eval_ext 2^24 ext", timed(lambda: pkg.eval_ext(ctx, f, point)), alg_bytes=16 * N)
+    if "fold" in kinds:
+        r = rng.integers(0, P, 4, dtype=np.uint64).astype(np.uint32)
+        # in-place compress of the first variable: reads 2^24, writes 2^23 elements
+        emit("fold_ext 2^24 -> 2^23 ext", timed(lambda: pkg.fold_ext(ctx, f, n, r)), alg_bytes=16 * N + 8 * N)
+    if "dft" in kinds:
+        x = pkg.DeviceArray.from_host(ctx, rng.integers(0, P, N, dtype=np.uint64).astype(np.uint32))
+        out = pkg.DeviceArray(ctx, 2 * N)
+        emit("dft 1 x 2^24 -> 2^25 (rate 1/2)", timed(lambda: pkg.dft_batch(ctx, x, n, 0, 1, False, out)),
+             alg_bytes=4 * N + 8 * N)
+        emit("dft 16 x 2^20 -> 16 x 2^21 (commit LDE)", timed(lambda: pkg.dft_batch(ctx, x, n - 4, 4, 1, False, out)),
+             alg_bytes=4 * N + 8 * N)
+    if "merkle" in kinds:
+        log_h, words = 21, 16
+        rows = pkg.DeviceArray.from_host(ctx, rng.integers(0, P, words << log_h, dtype=np.uint64).astype(np.uint32))
+        dig = pkg.DeviceArray(ctx, (2 * (1 << log_h) - 1) * 8)
+        ms = timed(lambda: pkg.merkle_commit(ctx, rows, log_h, words, 0, dig))
+        emit("merkle 2^21 leaves x 16 (P24 leaves, P16 nodes)", ms, alg_bytes=4 * words << log_h,
+             units=2 * (1 << log_h) - 1, unit_name="permutations/s")
+    if "grind" in kinds:
+        bits = 18
+        ch = pkg.DuplexChallenger(ctx)
+        seq = iter(range(1 << 30))
+
+        def grind():
+            ch.observe(next(seq))
+            ch.grind(bits)
+
+        ms = timed(grind)
+        emit(f"grind {bits} bits", ms, units=float(1 << bits), unit_name="expected permutations/s",
+             extra={"note": "expected work 2^bits Poseidon2-16 permutations per grind"})
+    ctx.close()
+
+
 def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -141,7 +234,11 @@ def main() -> None:
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--micro", default=None, choices=["all", "eq", "eval", "fold", "dft", "merkle", "grind"])
     args = ap.parse_args()
+    if args.micro:
+        run_micro(args)
+        return
     if args.impl == "reference":
         run_reference(args)
         return

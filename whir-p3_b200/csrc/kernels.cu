@@ -179,6 +179,13 @@ struct Elem<4> {
 
 __device__ __forceinline__ uint32_t bitrev(uint32_t x, int bits) { return bits ? (__brev(x) >> (32 - bits)) : 0u; }
 
+// Shared-memory swizzle for the DFT tiles: XOR the bank bits with bits 5-9 and
+// 10-14 of the index. It is a bijection (it only changes bits 0-4, as a
+// function of higher bits), keeps any aligned run of 32 words conflict-free,
+// and spreads the bit-reversed scatter (indices k * 2^(L-5), L <= 12) and the
+// column-strided accesses of several vectors over all 32 banks.
+__device__ __forceinline__ int swz(int i) { return i ^ (((i >> 5) ^ (i >> 10)) & 31); }
+
 __device__ __forceinline__ uint32_t tw_pow(const uint32_t* tw_lo, const uint32_t* tw_hi, uint64_t e) {
   // omega_H^e for e < H <= 2^24
   return kb::mul(__ldg(tw_lo + (e & 4095)), __ldg(tw_hi + (e >> 12)));
@@ -199,10 +206,11 @@ __device__ __forceinline__ void smem_dft(typename Elem<LANES>::T* a, int nv, int
       const int k = b & ((S >> 1) - 1);
       const int grp = k >> (s - 1), pos = k & (half - 1);
       const int i0 = v * S + grp * (half << 1) + pos;
-      typename E::T u = a[i0];
-      typename E::T w = E::mulb(a[i0 + half], tw[pos << tshift]);
-      a[i0] = E::add(u, w);
-      a[i0 + half] = E::sub(u, w);
+      const int p0 = swz(i0), p1 = swz(i0 + half);
+      typename E::T u = a[p0];
+      typename E::T w = E::mulb(a[p1], tw[pos << tshift]);
+      a[p0] = E::add(u, w);
+      a[p1] = E::sub(u, w);
     }
     __syncthreads();
   }
@@ -210,7 +218,7 @@ __device__ __forceinline__ void smem_dft(typename Elem<LANES>::T* a, int nv, int
 
 template <int LANES>
 __global__ void k_dft_cols(const typename Elem<LANES>::T* __restrict__ x, typename Elem<LANES>::T* __restrict__ y,
-                           int log_l, int log_h1, int log_h2, int log_h, int tile,
+                           int log_l, int log_h1, int log_h2, int log_h, int log_tile,
                            const uint32_t* __restrict__ tw_stage, const uint32_t* __restrict__ tw_lo,
                            const uint32_t* __restrict__ tw_hi) {
   using E = Elem<LANES>;
@@ -221,22 +229,24 @@ __global__ void k_dft_cols(const typename Elem<LANES>::T* __restrict__ x, typena
   const size_t L = (size_t)1 << log_l;
   const int L1 = (int)(L >> log_h2);  // nonzero rows of each column vector
   const int j = blockIdx.y;
+  const int tile = 1 << log_tile;
+  const int tmask = tile - 1;
   const int i2_0 = blockIdx.x * tile;
   const typename E::T* xj = x + (size_t)j * L;
   typename E::T* yj = y + ((size_t)j << log_h);
   for (int i = threadIdx.x; i < 2048; i += blockDim.x) tw[i] = __ldg(tw_stage + i);
   for (int idx = threadIdx.x; idx < tile * H1; idx += blockDim.x) {
-    const int t = idx % tile, i1 = idx / tile;
+    const int t = idx & tmask, i1 = idx >> log_tile;
     typename E::T v = E::zero();
     if (i1 < L1) v = xj[(size_t)i1 * H2 + i2_0 + t];
-    a[t * H1 + bitrev((uint32_t)i1, log_h1)] = v;
+    a[swz(t * H1 + bitrev((uint32_t)i1, log_h1))] = v;
   }
   __syncthreads();
   smem_dft<LANES>(a, tile, log_h1, tw);
   for (int idx = threadIdx.x; idx < tile * H1; idx += blockDim.x) {
-    const int t = idx % tile, r1 = idx / tile;
+    const int t = idx & tmask, r1 = idx >> log_tile;
     const uint64_t e = (uint64_t)(i2_0 + t) * (uint64_t)r1;
-    typename E::T v = a[t * H1 + r1];
+    typename E::T v = a[swz(t * H1 + r1)];
     if (e) v = E::mulb(v, tw_pow(tw_lo, tw_hi, e));
     yj[((size_t)r1 << log_h2) + i2_0 + t] = v;
   }
@@ -245,7 +255,7 @@ __global__ void k_dft_cols(const typename Elem<LANES>::T* __restrict__ x, typena
 // pass 2: out[r1 + H1*r2][j] = DFT_H2(Y_j[r1][.])[r2], jt columns per CTA
 template <int LANES>
 __global__ void k_dft_rows(const typename Elem<LANES>::T* __restrict__ y, typename Elem<LANES>::T* __restrict__ out,
-                           int log_h1, int log_h2, int log_h, int log_w, int jt,
+                           int log_h1, int log_h2, int log_h, int log_w, int log_jt,
                            const uint32_t* __restrict__ tw_stage) {
   using E = Elem<LANES>;
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -253,18 +263,19 @@ __global__ void k_dft_rows(const typename Elem<LANES>::T* __restrict__ y, typena
   typename E::T* a = reinterpret_cast<typename E::T*>(smem_raw + 2048 * sizeof(uint32_t));
   const int H2 = 1 << log_h2;
   const int r1 = blockIdx.x;
+  const int jt = 1 << log_jt;
   const int j0 = blockIdx.y * jt;
   for (int i = threadIdx.x; i < 2048; i += blockDim.x) tw[i] = __ldg(tw_stage + i);
   for (int idx = threadIdx.x; idx < jt * H2; idx += blockDim.x) {
     const int jj = idx >> log_h2, i2 = idx & (H2 - 1);
-    a[jj * H2 + bitrev((uint32_t)i2, log_h2)] = y[((size_t)(j0 + jj) << log_h) + ((size_t)r1 << log_h2) + i2];
+    a[swz(jj * H2 + bitrev((uint32_t)i2, log_h2))] = y[((size_t)(j0 + jj) << log_h) + ((size_t)r1 << log_h2) + i2];
   }
   __syncthreads();
   smem_dft<LANES>(a, jt, log_h2, tw);
   for (int idx = threadIdx.x; idx < jt * H2; idx += blockDim.x) {
-    const int jj = idx % jt, r2 = idx / jt;
+    const int jj = idx & (jt - 1), r2 = idx >> log_jt;
     const size_t row = (size_t)r1 + ((size_t)r2 << log_h1);
-    out[(row << log_w) + j0 + jj] = a[jj * H2 + r2];
+    out[(row << log_w) + j0 + jj] = a[swz(jj * H2 + r2)];
   }
 }
 
@@ -272,7 +283,7 @@ __global__ void k_dft_rows(const typename Elem<LANES>::T* __restrict__ y, typena
 // one CTA per twist b and column group, H = L*B.
 template <int LANES>
 __global__ void k_dft_coset(const typename Elem<LANES>::T* __restrict__ x, typename Elem<LANES>::T* __restrict__ out,
-                            int log_l, int log_b, int log_w, int jt, const uint32_t* __restrict__ tw_stage,
+                            int log_l, int log_b, int log_w, int log_jt, const uint32_t* __restrict__ tw_stage,
                             const uint32_t* __restrict__ tw_lo, const uint32_t* __restrict__ tw_hi) {
   using E = Elem<LANES>;
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -280,6 +291,7 @@ __global__ void k_dft_coset(const typename Elem<LANES>::T* __restrict__ x, typen
   typename E::T* a = reinterpret_cast<typename E::T*>(smem_raw + 2048 * sizeof(uint32_t));
   const int L = 1 << log_l;
   const uint32_t b = blockIdx.x;
+  const int jt = 1 << log_jt;
   const int j0 = blockIdx.y * jt;
   for (int i = threadIdx.x; i < 2048; i += blockDim.x) tw[i] = __ldg(tw_stage + i);
   for (int idx = threadIdx.x; idx < jt * L; idx += blockDim.x) {
@@ -287,20 +299,25 @@ __global__ void k_dft_coset(const typename Elem<LANES>::T* __restrict__ x, typen
     typename E::T v = x[(size_t)(j0 + jj) * L + i];
     const uint64_t e = (uint64_t)i * b;
     if (e) v = E::mulb(v, tw_pow(tw_lo, tw_hi, e));
-    a[jj * L + bitrev((uint32_t)i, log_l)] = v;
+    a[swz(jj * L + bitrev((uint32_t)i, log_l))] = v;
   }
   __syncthreads();
   smem_dft<LANES>(a, jt, log_l, tw);
   for (int idx = threadIdx.x; idx < jt * L; idx += blockDim.x) {
-    const int jj = idx % jt, r = idx / jt;
+    const int jj = idx & (jt - 1), r = idx >> log_jt;
     const size_t row = ((size_t)r << log_b) + b;
-    out[(row << log_w) + j0 + jj] = a[jj * L + r];
+    out[(row << log_w) + j0 + jj] = a[swz(jj * L + r)];
   }
 }
 
 static int pow2_clamp(long v, int lo, int hi) {
   int r = lo;
   while ((long)r * 2 <= v && r * 2 <= hi) r *= 2;
+  return r;
+}
+static int log2i(int v) {
+  int r = 0;
+  while ((1 << r) < v) r++;
   return r;
 }
 
@@ -325,11 +342,12 @@ cudaError_t dft_batch(const uint32_t* in, uint32_t* out, uint32_t* scratch, int 
     dim3 grid(1u << log_blowup, W / jt);
     if (lanes == 1) {
       set_smem(k_dft_coset<1>, smem);
-      k_dft_coset<1><<<grid, 256, smem, st>>>(in, out, log_chunk, log_blowup, log_w, jt, t.tw_stage, t.tw_lo, t.tw_hi);
+      k_dft_coset<1><<<grid, 256, smem, st>>>(in, out, log_chunk, log_blowup, log_w, log2i(jt), t.tw_stage, t.tw_lo,
+                                              t.tw_hi);
     } else {
       set_smem(k_dft_coset<4>, smem);
       k_dft_coset<4><<<grid, 256, smem, st>>>(reinterpret_cast<const uint4*>(in), reinterpret_cast<uint4*>(out),
-                                              log_chunk, log_blowup, log_w, jt, t.tw_stage, t.tw_lo, t.tw_hi);
+                                              log_chunk, log_blowup, log_w, log2i(jt), t.tw_stage, t.tw_lo, t.tw_hi);
     }
     LAUNCH_DONE();
   }
@@ -345,12 +363,12 @@ cudaError_t dft_batch(const uint32_t* in, uint32_t* out, uint32_t* scratch, int 
     dim3 grid(H2 / tile, W);
     if (lanes == 1) {
       set_smem(k_dft_cols<1>, smem);
-      k_dft_cols<1><<<grid, 512, smem, st>>>(in, scratch, log_chunk, log_h1, log_h2, log_h, tile, t.tw_stage,
+      k_dft_cols<1><<<grid, 512, smem, st>>>(in, scratch, log_chunk, log_h1, log_h2, log_h, log2i(tile), t.tw_stage,
                                              t.tw_lo, t.tw_hi);
     } else {
       set_smem(k_dft_cols<4>, smem);
       k_dft_cols<4><<<grid, 512, smem, st>>>(reinterpret_cast<const uint4*>(in), reinterpret_cast<uint4*>(scratch),
-                                             log_chunk, log_h1, log_h2, log_h, tile, t.tw_stage, t.tw_lo, t.tw_hi);
+                                             log_chunk, log_h1, log_h2, log_h, log2i(tile), t.tw_stage, t.tw_lo, t.tw_hi);
     }
     count_launch();
     cudaError_t e = cudaGetLastError();
@@ -361,11 +379,11 @@ cudaError_t dft_batch(const uint32_t* in, uint32_t* out, uint32_t* scratch, int 
   dim3 grid(H1, W / jt);
   if (lanes == 1) {
     set_smem(k_dft_rows<1>, smem);
-    k_dft_rows<1><<<grid, 512, smem, st>>>(scratch, out, log_h1, log_h2, log_h, log_w, jt, t.tw_stage);
+    k_dft_rows<1><<<grid, 512, smem, st>>>(scratch, out, log_h1, log_h2, log_h, log_w, log2i(jt), t.tw_stage);
   } else {
     set_smem(k_dft_rows<4>, smem);
     k_dft_rows<4><<<grid, 512, smem, st>>>(reinterpret_cast<const uint4*>(scratch), reinterpret_cast<uint4*>(out),
-                                           log_h1, log_h2, log_h, log_w, jt, t.tw_stage);
+                                           log_h1, log_h2, log_h, log_w, log2i(jt), t.tw_stage);
   }
   LAUNCH_DONE();
 }
@@ -569,20 +587,19 @@ cudaError_t merkle_open(const uint32_t* rows, const uint32_t* digests, int log_h
 // ---------------------------------------------------------------------------
 
 constexpr int GRIND_CTA = 256;
-constexpr int GRIND_PER_THREAD = 16;
 
+// Each claim is GRIND_CTA consecutive candidates, one per thread.
 __global__ void __launch_bounds__(GRIND_CTA) k_grind(const __grid_constant__ P2Consts p16, uint4 st0, uint4 st1,
                                                       uint4 st2, uint4 st3, int slot, int bits, uint64_t limit,
                                                       uint32_t* result, uint32_t* counter) {
   __shared__ uint64_t s_start;
   __shared__ int s_go;
   const uint32_t mask = (1u << bits) - 1u;
-  const uint64_t chunk_size = (uint64_t)GRIND_CTA * GRIND_PER_THREAD;
   const uint32_t base_state[16] = {st0.x, st0.y, st0.z, st0.w, st1.x, st1.y, st1.z, st1.w,
                                    st2.x, st2.y, st2.z, st2.w, st3.x, st3.y, st3.z, st3.w};
   for (;;) {
     if (threadIdx.x == 0) {
-      const uint64_t start = (uint64_t)atomicAdd(counter, 1u) * chunk_size;
+      const uint64_t start = (uint64_t)atomicAdd(counter, 1u) * GRIND_CTA;
       s_start = start;
       s_go = start < limit && start < (uint64_t)*(volatile uint32_t*)result;
     }
@@ -591,9 +608,8 @@ __global__ void __launch_bounds__(GRIND_CTA) k_grind(const __grid_constant__ P2C
     const int go = s_go;
     __syncthreads();
     if (!go) return;
-    for (int k = 0; k < GRIND_PER_THREAD; k++) {
-      const uint64_t w = start + (uint64_t)k * GRIND_CTA + threadIdx.x;
-      if (w >= limit) break;
+    const uint64_t w = start + threadIdx.x;
+    if (w < limit) {
       uint32_t s[16];
       const uint32_t wm = kb::to_mont((uint32_t)w);
 #pragma unroll
@@ -620,7 +636,11 @@ cudaError_t grind(const uint32_t* state, const uint32_t* in, int in_len, int bit
   count_launch();
   uint4 a = make_uint4(s[0], s[1], s[2], s[3]), b = make_uint4(s[4], s[5], s[6], s[7]);
   uint4 c = make_uint4(s[8], s[9], s[10], s[11]), d = make_uint4(s[12], s[13], s[14], s[15]);
-  k_grind<<<sm_count() * 4, GRIND_CTA, 0, st>>>(p16, a, b, c, d, in_len, bits, limit, result, counter);
+  // about 2^(bits+1) candidates in flight: enough to hide latency, little
+  // overshoot past the first witness for small `bits`
+  const uint64_t want = ((2ull << bits) + GRIND_CTA - 1) / GRIND_CTA;
+  const unsigned blocks = (unsigned)(want < (uint64_t)sm_count() * 8 ? want : (uint64_t)sm_count() * 8);
+  k_grind<<<blocks, GRIND_CTA, 0, st>>>(p16, a, b, c, d, in_len, bits, limit, result, counter);
   LAUNCH_DONE();
 }
 

@@ -11,9 +11,9 @@
 // TruncatedPermutation (2-to-1 compression) and DuplexChallenger.
 //
 // The round constants and diagonal are run-time data (`P2Consts`, Montgomery
-// form) so a caller can supply the exact permutation of its deployment; the
-// shapes (8 full rounds; 20 partial rounds at width 16, 23 at width 24) are
-// compile-time so that every constant becomes an immediate operand.
+// form, passed to kernels in the constant bank) so a caller can supply the
+// exact permutation of its deployment; the shapes (8 full rounds; 20 partial
+// rounds at width 16, 23 at width 24) are compile-time.
 #pragma once
 #include "kb.cuh"
 
@@ -71,31 +71,37 @@ KB_HD void ext_layer(uint32_t (&x)[T]) {
 
 KB_HD uint32_t cube(uint32_t v) { return kb::mul(kb::sqr(v), v); }
 
+template <int T>
+KB_HD void full_round(uint32_t (&x)[T], const uint32_t* rc) {
+  using namespace kb;
+#pragma unroll
+  for (int i = 0; i < T; i++) x[i] = cube(add(x[i], rc[i]));
+  ext_layer<T>(x);
+}
+
+template <int T>
+KB_HD void partial_round(uint32_t (&x)[T], uint32_t rc, const uint32_t* diag) {
+  using namespace kb;
+  x[0] = cube(add(x[0], rc));
+  uint32_t s = x[0];
+#pragma unroll
+  for (int i = 1; i < T; i++) s = add(s, x[i]);
+#pragma unroll
+  for (int i = 0; i < T; i++) x[i] = add(s, mul(diag[i], x[i]));
+}
+
+// The round loops stay rolled: a fully unrolled width-24 permutation is about
+// ten thousand instructions, more than the instruction cache holds, while one
+// round body is a few hundred. Round constants are read by index.
 template <int T, int RP>
 KB_HD void permute(uint32_t (&x)[T], const P2Consts& k) {
-  using namespace kb;
   ext_layer<T>(x);
-#pragma unroll
-  for (int r = 0; r < RF / 2; r++) {
-#pragma unroll
-    for (int i = 0; i < T; i++) x[i] = cube(add(x[i], k.ext_rc[r * T + i]));
-    ext_layer<T>(x);
-  }
-#pragma unroll
-  for (int r = 0; r < RP; r++) {
-    x[0] = cube(add(x[0], k.int_rc[r]));
-    uint32_t s = x[0];
-#pragma unroll
-    for (int i = 1; i < T; i++) s = add(s, x[i]);
-#pragma unroll
-    for (int i = 0; i < T; i++) x[i] = add(s, mul(k.diag[i], x[i]));
-  }
-#pragma unroll
-  for (int r = RF / 2; r < RF; r++) {
-#pragma unroll
-    for (int i = 0; i < T; i++) x[i] = cube(add(x[i], k.ext_rc[r * T + i]));
-    ext_layer<T>(x);
-  }
+#pragma unroll 1
+  for (int r = 0; r < RF / 2; r++) full_round<T>(x, k.ext_rc + r * T);
+#pragma unroll 1
+  for (int r = 0; r < RP; r++) partial_round<T>(x, k.int_rc[r], k.diag);
+#pragma unroll 1
+  for (int r = RF / 2; r < RF; r++) full_round<T>(x, k.ext_rc + r * T);
 }
 
 }  // namespace p2
