@@ -14,6 +14,14 @@ over ranks of the timed region divided by the proofs all ranks produced).
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
 
+Batching (64 independent proofs, num_variables log-uniform in [16, 22],
+folding factor in {3, 4}, rate 1/2 or 1/4) and serving (Poisson arrivals,
+num_variables uniform in [16, 24], 120 GB HBM budget) against the plain
+one-proof-at-a-time path:
+
+  python bench.py --batch [--workers W]
+  python bench.py --serve [--rates 10,50,100,200,500] [--workers W]
+
 Kernel-level microbenchmarks (the kernel configuration of the benchmark
 suite: eq expansion / evaluation / fold over 2^24 extension elements, the
 2^24 -> 2^25 LDE, a Poseidon2 Merkle tree over 2^21 leaves of 16 elements, and
@@ -227,6 +235,95 @@ def run_micro(args) -> None:
     ctx.close()
 
 
+def batch_jobs(pkg, count: int, seed: int):
+    """The batching workload: num_variables log-uniform in [16, 22], folding
+    factor 3 or 4, starting rate 1/2 or 1/4, 100-bit CapacityBound, pow 16,
+    rs reduction 3, one constraint each."""
+    rng = np.random.default_rng(seed)
+    jobs = []
+    for _ in range(count):
+        n = int(round(float(np.exp(rng.uniform(np.log(16), np.log(22))))))
+        k = int(rng.choice([3, 4]))
+        r = int(rng.choice([1, 2]))
+        params = pkg.ProtocolParameters(100, 16, pkg.FoldingFactor.constant(k), pkg.SecurityAssumption.CapacityBound,
+                                        r, 3, "poseidon2_24", 32)
+        poly = rng.integers(0, P, 1 << n, dtype=np.uint64).astype(np.uint32)
+        point = rng.integers(0, P, 4 * n, dtype=np.uint64).astype(np.uint32)
+        jobs.append((params, n, poly, point))
+    return jobs
+
+
+def run_batch(pkg, ctx, jobs, workers: int) -> dict:
+    import time as _t
+
+    for params, n, poly, point in jobs[:2]:  # warm the context and the pool allocator
+        pkg.commit_and_prove(ctx, params, n, poly, point)
+    t0 = _t.perf_counter()
+    plain = [pkg.commit_and_prove(ctx, params, n, poly, point)[0] for params, n, poly, point in jobs]
+    t_plain = _t.perf_counter() - t0
+    with pkg.Batch(ctx.device, workers=workers) as b:
+        warm = [pkg.ProofRequest(p, n, poly, pt) for p, n, poly, pt in jobs[:workers]]
+        b.run(warm)
+        reqs = [pkg.ProofRequest(p, n, poly, pt) for p, n, poly, pt in jobs]
+        t0 = _t.perf_counter()
+        b.run(reqs)
+        t_batch = _t.perf_counter() - t0
+    same = all(np.array_equal(r.proof, q) for r, q in zip(reqs, plain))
+    return {"instances": len(jobs), "workers": workers, "plain_proofs_per_s": round(len(jobs) / t_plain, 2),
+            "batched_proofs_per_s": round(len(jobs) / t_batch, 2), "speedup": round(t_plain / t_batch, 3),
+            "identical_to_plain": bool(same), "timing": "host wall clock around all proofs"}
+
+
+_SERVE_POLYS: dict = {}
+
+
+def serve_requests(pkg, count: int, seed: int):
+    """Requests with num_variables uniform in [16, 24] (k = 4, rate 1/2), each
+    with its own evaluation point; one seeded polynomial per size is shared."""
+    rng = np.random.default_rng(seed)
+    params = pkg.ProtocolParameters(100, 16, pkg.FoldingFactor.constant(4), pkg.SecurityAssumption.CapacityBound,
+                                    1, 3, "poseidon2_24", 32)
+    reqs = []
+    for _ in range(count):
+        n = int(rng.integers(16, 25))
+        if n not in _SERVE_POLYS:
+            _SERVE_POLYS[n] = np.random.default_rng(100 + n).integers(0, P, 1 << n, dtype=np.uint64).astype(np.uint32)
+        point = rng.integers(0, P, 4 * n, dtype=np.uint64).astype(np.uint32)
+        reqs.append((params, n, _SERVE_POLYS[n], point))
+    return reqs
+
+
+def run_serve(pkg, device: int, rate: float, workers: int, count: int, seed: int) -> dict:
+    """Poisson arrivals at `rate` req/s into the pool (served) and into a single
+    worker (the plain sequential path), same requests and arrival times."""
+    import time as _t
+
+    items = serve_requests(pkg, count, seed)
+    gaps = np.random.default_rng(seed + 1).exponential(1.0 / rate, count)
+    out = {}
+    for label, w in (("served", workers), ("plain", 1)):
+        with pkg.Batch(device, workers=w, hbm_budget_bytes=120 << 30) as b:
+            b.run([pkg.ProofRequest(p, n, poly, pt) for p, n, poly, pt in items[: max(w, 2)]])  # warm up
+            reqs = [pkg.ProofRequest(p, n, poly, pt) for p, n, poly, pt in items]
+            t0 = _t.perf_counter()
+            due = 0.0
+            for r, g in zip(reqs, gaps):
+                due += g
+                wait = due - (_t.perf_counter() - t0)
+                if wait > 0:
+                    _t.sleep(wait)
+                b.submit(r)
+            b.wait_all()
+            elapsed = max(r.job.t_done_ms for r in reqs) - min(r.job.t_submit_ms for r in reqs)
+        lat = np.array([r.latency_ms for r in reqs])
+        out[label] = {"throughput_per_s": round(count / (elapsed / 1e3), 2), "p50_ms": round(float(np.percentile(lat, 50)), 3),
+                      "p99_ms": round(float(np.percentile(lat, 99)), 3), "workers": w}
+        out[label + "_proofs"] = [r.proof for r in reqs]
+    same = all(np.array_equal(a, b) for a, b in zip(out.pop("served_proofs"), out.pop("plain_proofs")))
+    return {"rate_per_s": rate, "requests": count, **out, "identical_in_mix_and_alone": bool(same),
+            "throughput_ratio": round(out["served"]["throughput_per_s"] / out["plain"]["throughput_per_s"], 3)}
+
+
 def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -235,9 +332,30 @@ def main() -> None:
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--micro", default=None, choices=["all", "eq", "eval", "fold", "dft", "merkle", "grind"])
+    ap.add_argument("--batch", action="store_true")
+    ap.add_argument("--serve", action="store_true")
+    ap.add_argument("--workers", type=int, default=8)
+    ap.add_argument("--rates", default="10,50,100,200,500")
+    ap.add_argument("--no-batch", action="store_true", help="skip the batch/serve summary in the default run")
     args = ap.parse_args()
     if args.micro:
         run_micro(args)
+        return
+    if args.batch or args.serve:
+        import torch
+
+        import __graft_entry__
+
+        pkg = __graft_entry__.load_package()
+        torch.cuda.set_device(0)
+        ctx = pkg.Context(0)
+        if args.batch:
+            print(json.dumps({"mode": "batch", **run_batch(pkg, ctx, batch_jobs(pkg, 64, 4), args.workers)}), flush=True)
+        if args.serve:
+            for rate in [float(x) for x in args.rates.split(",")]:
+                count = int(min(400, max(40, rate * 1.0)))
+                print(json.dumps({"mode": "serve", **run_serve(pkg, 0, rate, args.workers, count, 5)}), flush=True)
+        ctx.close()
         return
     if args.impl == "reference":
         run_reference(args)
@@ -353,6 +471,10 @@ def main() -> None:
                 "peak_source": "MEASURED_PEAKS.json hbm_gbs (burst copy)" if peaks else "fallback 6650 GB/s",
                 "ms_per_launch": round(dft_ms, 4), "algorithmic_bytes": alg_bytes}
 
+    batch = serve = None
+    if rank == 0 and world == 1 and not args.no_batch:
+        batch = run_batch(pkg, ctx, batch_jobs(pkg, 64, 4), args.workers)
+        serve = run_serve(pkg, local, 200.0, args.workers, 120, 5)
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline_sample()
@@ -365,7 +487,8 @@ def main() -> None:
                 "proofs_per_s": round(1e3 / value, 3), "proof_words": int(ref_proof.size),
                 "e2e": {"value": round(e2e_value, 4), "unit": UNIT, "h2d_bytes_per_step": h2d * world,
                         "d2h_bytes_per_step": d2h * world},
-                "gpu_launches": int(launches), "roofline": roofline, "cpu_baseline": cpu, "clocks": clk}
+                "gpu_launches": int(launches), "roofline": roofline, "cpu_baseline": cpu, "clocks": clk,
+                "batched": batch, "served": serve}
         print(json.dumps(line), flush=True)
     ctx.close()
     if dist is not None:

@@ -235,6 +235,46 @@ int whir_commit_and_prove(whir_ctx* ctx, const whir_protocol_params* params, int
                           uint32_t* user_evals_out, uint32_t* proof_out, size_t cap_words, size_t* proof_words,
                           uint32_t* checkpoint);
 
+/* ---- batching and serving -------------------------------------------------
+ * A pool of worker threads on one device, each with its own context and CUDA
+ * stream, proves submitted jobs concurrently (the north star's batching and
+ * serving patterns; no counterpart in the reference, which proves one
+ * polynomial per call). Jobs are admitted in FIFO order when their device
+ * footprint fits the HBM budget (a job larger than the whole budget runs
+ * alone). Each job runs whir_commit_and_prove on its worker's context, so its
+ * proof is identical to the one-at-a-time result. */
+typedef struct whir_batch whir_batch;
+typedef struct {
+  whir_protocol_params params;
+  int32_t n;
+  const uint32_t* poly;      /* 2^n values: host canonical, or device Montgomery if poly_on_device */
+  int32_t poly_on_device;
+  const uint32_t* points;    /* num_points * n extension elements (may be NULL if num_points == 0) */
+  int32_t num_points;
+  uint32_t* evals_out;       /* num_points * 4 words, may be NULL */
+  uint32_t* proof_out;       /* proof_cap words */
+  size_t proof_cap;
+  size_t proof_words;        /* out */
+  uint32_t checkpoint[4];    /* out: challenger sample after the proof */
+  int32_t status;            /* out: WHIR_OK or an error code */
+  int32_t done;              /* out: set under the batch lock; read it through whir_batch_wait */
+  uint64_t footprint_bytes;  /* out: admitted device footprint */
+  double t_submit_ms, t_start_ms, t_done_ms; /* out: steady-clock timestamps */
+} whir_job;
+
+/* Device bytes one job holds at its peak (polynomial, trees, codewords, sumcheck arrays). */
+int whir_job_footprint(const whir_protocol_params* params, int32_t n, int32_t poly_on_device, uint64_t* bytes);
+int whir_batch_create(int32_t device, int32_t workers, const whir_poseidon2_params* p16,
+                      const whir_poseidon2_params* p24, uint64_t hbm_budget_bytes, whir_batch** out);
+int whir_batch_destroy(whir_batch* b);
+/* Enqueue (non-blocking). The job and its buffers must stay valid until it is done. */
+int whir_batch_submit(whir_batch* b, whir_job* job);
+/* Wait for one job (timeout_ms < 0: no limit); returns the job's status. */
+int whir_batch_wait(whir_batch* b, whir_job* job, int32_t timeout_ms);
+int whir_batch_wait_all(whir_batch* b);
+/* Submit `count` jobs and wait for all of them. */
+int whir_batch_run(whir_batch* b, whir_job* jobs, int32_t count);
+
 #ifdef __cplusplus
 }
 #endif

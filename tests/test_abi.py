@@ -116,3 +116,13 @@ def test_challenger_matches_oracle(pkg, host_ctx, oracle):
             b = bool(oracle.lib.or_chal_check_witness(C.byref(oc), C.byref(oracle.p16), bits, w))
             assert a == b
     assert list(ch.c.state) == list(oc.state)
+
+
+def test_job_footprint_grows_with_size(pkg):
+    params = pkg.ProtocolParameters(100, 16, pkg.FoldingFactor.constant(4), pkg.SecurityAssumption.CapacityBound, 1, 3)
+    sizes = [pkg.job_footprint(params, n) for n in range(12, 27)]
+    assert all(a < b for a, b in zip(sizes, sizes[1:]))
+    # n = 24: polynomial 64 + commit codeword 128 + commit digests 128 + f, w 32 MiB, plus the round-1
+    # peak: round-0 tree (64 + 16) + round-1 codeword 32 + digests 8 + DFT scratch 32 = 152 MiB
+    assert sizes[24 - 12] == (64 + 128 + 128 + 32 + 152) * 2**20
+    assert pkg.job_footprint(params, 24, True) == sizes[24 - 12] - 64 * 2**20

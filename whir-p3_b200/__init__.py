@@ -70,6 +70,15 @@ class _Chal(C.Structure):
                 ("output", C.c_uint32 * 8), ("output_len", C.c_int32)]
 
 
+class Job(C.Structure):
+    _fields_ = [("params", _Params), ("n", C.c_int32), ("poly", C.c_void_p), ("poly_on_device", C.c_int32),
+                ("points", C.c_void_p), ("num_points", C.c_int32), ("evals_out", C.c_void_p),
+                ("proof_out", C.c_void_p), ("proof_cap", C.c_size_t), ("proof_words", C.c_size_t),
+                ("checkpoint", C.c_uint32 * 4), ("status", C.c_int32), ("done", C.c_int32),
+                ("footprint_bytes", C.c_uint64), ("t_submit_ms", C.c_double), ("t_start_ms", C.c_double),
+                ("t_done_ms", C.c_double)]
+
+
 _u32 = np.ctypeslib.ndpointer(dtype=np.uint32, flags="C_CONTIGUOUS")
 _vp = C.c_void_p
 _i32 = C.c_int32
@@ -117,6 +126,14 @@ _SIGS = {
     "whir_witness_free": (C.c_int, [_vp]),
     "whir_commit_and_prove": (C.c_int, [_vp, C.POINTER(_Params), _i32, _vp, _i32, _vp, _i32, _vp, _vp, C.c_size_t,
                                         C.POINTER(C.c_size_t), _vp]),
+    "whir_job_footprint": (C.c_int, [C.POINTER(_Params), _i32, _i32, C.POINTER(C.c_uint64)]),
+    "whir_batch_create": (C.c_int, [_i32, _i32, C.POINTER(Poseidon2Params), C.POINTER(Poseidon2Params), C.c_uint64,
+                                    C.POINTER(_vp)]),
+    "whir_batch_destroy": (C.c_int, [_vp]),
+    "whir_batch_submit": (C.c_int, [_vp, C.POINTER(Job)]),
+    "whir_batch_wait": (C.c_int, [_vp, C.POINTER(Job), _i32]),
+    "whir_batch_wait_all": (C.c_int, [_vp]),
+    "whir_batch_run": (C.c_int, [_vp, C.POINTER(Job), _i32]),
 }
 
 _lib = None
@@ -597,3 +614,94 @@ def commit_and_prove(ctx: Context, params: ProtocolParameters, n: int, poly, poi
                                        int(on_dev), _ptr(pts), npts, evals.ctypes.data, buf.ctypes.data, cap,
                                        C.byref(words), cp.ctypes.data))
     return buf[: words.value].copy(), cp, evals[: 4 * npts]
+
+
+# ---------------------------------------------------------------------------
+# Batching and serving (worker pool with HBM-budget admission)
+# ---------------------------------------------------------------------------
+
+class ProofRequest:
+    """One commit+prove job; keeps its input and output buffers alive."""
+
+    def __init__(self, params: ProtocolParameters, n: int, poly, points=None):
+        self.params, self.n = params, n
+        self.cfg = WhirConfig(n, params)
+        self.on_device = isinstance(poly, DeviceArray)
+        self._poly = poly if self.on_device else _arr(poly, 1 << n)
+        self.points = None if points is None or len(points) == 0 else _arr(points)
+        npts = 0 if self.points is None else self.points.size // (4 * n)
+        self.evals = np.zeros(4 * max(npts, 1), dtype=np.uint32)
+        self.proof_buf = np.zeros(self.cfg.proof_words_bound(), dtype=np.uint32)
+        j = Job()
+        j.params = params._c()
+        j.n = n
+        j.poly = self._poly.ptr if self.on_device else self._poly.ctypes.data
+        j.poly_on_device = int(self.on_device)
+        j.points = _ptr(self.points)
+        j.num_points = npts
+        j.evals_out = self.evals.ctypes.data
+        j.proof_out = self.proof_buf.ctypes.data
+        j.proof_cap = self.proof_buf.size
+        self.job = j
+
+    @property
+    def proof(self) -> np.ndarray:
+        return self.proof_buf[: self.job.proof_words].copy()
+
+    @property
+    def checkpoint(self) -> np.ndarray:
+        return np.array(list(self.job.checkpoint), dtype=np.uint32)
+
+    @property
+    def latency_ms(self) -> float:
+        return self.job.t_done_ms - self.job.t_submit_ms
+
+
+def job_footprint(params: ProtocolParameters, n: int, poly_on_device: bool = False) -> int:
+    v = C.c_uint64()
+    _check(lib().whir_job_footprint(C.byref(params._c()), n, int(poly_on_device), C.byref(v)))
+    return int(v.value)
+
+
+class Batch:
+    """whir_batch: `workers` contexts on one device proving jobs concurrently."""
+
+    def __init__(self, device: int = 0, workers: int = 4, hbm_budget_bytes: int = 120 << 30,
+                 p16: Poseidon2Params | None = None, p24: Poseidon2Params | None = None):
+        h = _vp()
+        _check(lib().whir_batch_create(device, workers, None if p16 is None else C.byref(p16),
+                                       None if p24 is None else C.byref(p24), hbm_budget_bytes, C.byref(h)))
+        self.handle = h
+
+    def submit(self, req: ProofRequest) -> None:
+        _check(lib().whir_batch_submit(self.handle, C.byref(req.job)))
+
+    def wait(self, req: ProofRequest, timeout_ms: int = -1) -> None:
+        _check(lib().whir_batch_wait(self.handle, C.byref(req.job), timeout_ms))
+
+    def wait_all(self) -> None:
+        _check(lib().whir_batch_wait_all(self.handle))
+
+    def run(self, reqs: list[ProofRequest]) -> None:
+        for r in reqs:
+            self.submit(r)
+        self.wait_all()
+        for r in reqs:
+            _check(r.job.status)
+
+    def close(self) -> None:
+        if self.handle:
+            lib().whir_batch_destroy(self.handle)
+            self.handle = _vp()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
