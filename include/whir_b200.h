@@ -260,6 +260,7 @@ typedef struct {
   int32_t done;              /* out: set under the batch lock; read it through whir_batch_wait */
   uint64_t footprint_bytes;  /* out: admitted device footprint */
   double t_submit_ms, t_start_ms, t_done_ms; /* out: steady-clock timestamps */
+  char error[160];           /* out: message of a failed job (the worker thread's whir_last_error) */
 } whir_job;
 
 /* Device bytes one job holds at its peak (polynomial, trees, codewords, sumcheck arrays). */

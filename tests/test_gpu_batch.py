@@ -36,9 +36,9 @@ def check_against_single(pkg, ctx, jobs, reqs):
 
 
 def test_batch_matches_one_at_a_time(pkg, gpu_ctx, oracle):
-    jobs = make_jobs(pkg, 16, 1)
+    jobs = make_jobs(pkg, 32, 1, 10, 19)  # mixed sizes: concurrent DFTs of different shapes
     reqs = [pkg.ProofRequest(p, n, poly, pts if pts.size else None) for p, n, poly, pts in jobs]
-    with pkg.Batch(0, workers=6) as b:
+    with pkg.Batch(0, workers=8) as b:
         b.run(reqs)
     check_against_single(pkg, gpu_ctx, jobs, reqs)
     # and one of them against the oracle directly

@@ -76,7 +76,7 @@ class Job(C.Structure):
                 ("proof_out", C.c_void_p), ("proof_cap", C.c_size_t), ("proof_words", C.c_size_t),
                 ("checkpoint", C.c_uint32 * 4), ("status", C.c_int32), ("done", C.c_int32),
                 ("footprint_bytes", C.c_uint64), ("t_submit_ms", C.c_double), ("t_start_ms", C.c_double),
-                ("t_done_ms", C.c_double)]
+                ("t_done_ms", C.c_double), ("error", C.c_char * 160)]
 
 
 _u32 = np.ctypeslib.ndpointer(dtype=np.uint32, flags="C_CONTIGUOUS")
@@ -687,7 +687,8 @@ class Batch:
             self.submit(r)
         self.wait_all()
         for r in reqs:
-            _check(r.job.status)
+            if r.job.status != 0:
+                raise WhirError(r.job.status, f"job n={r.n}: {r.job.error.decode()}")
 
     def close(self) -> None:
         if self.handle:

@@ -6,6 +6,8 @@
 // the device with the proofs already in flight. Every job runs the same code
 // path as whir_commit_and_prove, so each proof is identical to the one the
 // job would produce alone.
+#include <stdio.h>
+
 #include <chrono>
 #include <condition_variable>
 #include <deque>
@@ -86,6 +88,9 @@ void run_job(whir_ctx* ctx, whir_job* j) {
   j->status = whir_commit_and_prove(ctx, &j->params, j->n, j->poly, j->poly_on_device, j->points, j->num_points,
                                     j->evals_out, j->proof_out, j->proof_cap, &words, j->checkpoint);
   j->proof_words = words;
+  if (j->status != WHIR_OK) {
+    snprintf(j->error, sizeof(j->error), "%s", whir_last_error());
+  }
   j->t_done_ms = now_ms();
 }
 
@@ -169,6 +174,7 @@ int whir_batch_submit(whir_batch* b, whir_job* j) {
   whir_config c;
   WH_TRY(wh::config_new(j->params, j->n, &c));
   j->footprint_bytes = wh::footprint(c, j->poly_on_device);
+  j->error[0] = 0;
   j->done = 0;
   j->status = WHIR_OK;
   j->t_submit_ms = now_ms();

@@ -10,6 +10,7 @@
 // in registers with every round constant an immediate (kernel parameters live
 // in the constant bank).
 #include <atomic>
+#include <mutex>
 
 #include "kernels.h"
 
@@ -321,9 +322,29 @@ static int log2i(int v) {
   return r;
 }
 
+// Dynamic shared memory limits are per-kernel process-wide attributes: they
+// are raised once to the largest size any launch uses and never lowered, so
+// launches from concurrent contexts cannot race a smaller setting.
+constexpr size_t kDftSmemMax = 2048 * 4 + 64 * 1024;
+constexpr size_t kSelectSmemMax = 160 * 1024;
+__global__ void k_add_select(ef* __restrict__ w, size_t N, int lo_bits, const uint32_t* __restrict__ pow_lo,
+                             const uint32_t* __restrict__ pow_hi, const ef* __restrict__ g, int m, int hi_bits);
+static std::once_flag g_attr_once;
+static void init_smem_attributes() {
+  std::call_once(g_attr_once, [] {
+    cudaFuncSetAttribute(k_dft_cols<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kDftSmemMax);
+    cudaFuncSetAttribute(k_dft_cols<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kDftSmemMax);
+    cudaFuncSetAttribute(k_dft_rows<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kDftSmemMax);
+    cudaFuncSetAttribute(k_dft_rows<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kDftSmemMax);
+    cudaFuncSetAttribute(k_dft_coset<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kDftSmemMax);
+    cudaFuncSetAttribute(k_dft_coset<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kDftSmemMax);
+    cudaFuncSetAttribute(k_add_select, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSelectSmemMax);
+    cudaGetLastError();
+  });
+}
 template <typename K>
-static void set_smem(K kernel, size_t bytes) {
-  cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+static void set_smem(K, size_t) {
+  init_smem_attributes();
 }
 
 cudaError_t dft_batch(const uint32_t* in, uint32_t* out, uint32_t* scratch, int log_chunk, int log_w,
@@ -921,8 +942,8 @@ cudaError_t add_select(ef* w, int n, const uint32_t* pow_lo, const uint32_t* pow
   const int threads = (int)(N < 256 ? N : 256);
   if (((size_t)1 << lo_bits) < (size_t)threads) return cudaErrorInvalidValue;
   const size_t smem = (size_t)m * sizeof(ef);
-  if (smem > 160 * 1024) return cudaErrorInvalidValue;
-  cudaFuncSetAttribute(k_add_select, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (smem > kSelectSmemMax) return cudaErrorInvalidValue;
+  init_smem_attributes();
   k_add_select<<<grid_for(N, threads), threads, smem, st>>>(w, N, lo_bits, pow_lo, pow_hi, g, m, n - lo_bits);
   LAUNCH_DONE();
 }
