@@ -84,6 +84,15 @@ class Clocks:
                                          stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
         except Exception:
             self.proc = None
+        # wait (up to 2 s) until the sampler has produced its first line
+        t0 = time.time()
+        while self.proc is not None and time.time() - t0 < 2.0:
+            try:
+                if self.path.stat().st_size > 0:
+                    break
+            except OSError:
+                pass
+            time.sleep(0.02)
 
     def stop(self) -> dict:
         if self.proc is None:
@@ -327,7 +336,7 @@ def run_serve(pkg, device: int, rate: float, workers: int, count: int, seed: int
 def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -443,33 +452,47 @@ def main() -> None:
     h2d = poly.nbytes + point.nbytes
     d2h = int(proof.size) * 4
 
-    # ---- dominant HBM kernel: the commit DFT (16 columns x 2^21 rows), timed alone ----
-    k = 4
-    log_chunk, log_h = N_VARS - k, N_VARS + 1 - k
-    d_out = pkg.DeviceArray(ctx, (1 << log_h) << k)
-    for _ in range(3):
-        pkg.dft_batch(ctx, d_poly, log_chunk, k, 1, False, d_out)
-    reps = 20
-    torch.cuda.synchronize()
-    s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    dft_ms = 0.0
-    for _ in range(reps):
+    # ---- per-stage device times and the dominant kernel, timed live with CUDA
+    # events on the context's stream over a second pass of the same steps ----
+    ctx.set_profiling(True)
+    ctx.stage_times(reset=True)
+    for _ in range(args.steps):
         flush.zero_()
-        s.record(stream)
-        pkg.dft_batch(ctx, d_poly, log_chunk, k, 1, False, d_out)
-        e.record(stream)
-        e.synchronize()
-        dft_ms += s.elapsed_time(e)
-    dft_ms /= reps
-    alg_bytes = (1 << N_VARS) * 4 + (1 << (log_h + k)) * 4
+        step(d_poly)
+    stages = ctx.stage_times(reset=True)
+    ctx.set_profiling(False)
+    stages_ms = {k: round(v[0] / args.steps, 4) for k, v in stages.items()}
+    leaf_ms, leaf_launches = stages["merkle_leaves"]
+    cfg = pkg.WhirConfig(N_VARS, params)
+    trees = [(N_VARS + 1 - 4, 16)]  # (log height, row words): commitment, then one per round
+    for i, rc in enumerate(cfg.round_parameters):
+        new_dom = rc.domain_size >> (cfg.rs_reduction if i == 0 else 1)
+        trees.append((new_dom.bit_length() - 1 - 4, 64))
+
+    def leaf_bytes(log_h, words):
+        h = 1 << log_h
+        lv = min(log_h, 7)
+        return h * words * 4 + sum(h >> l for l in range(lv + 1)) * 32
+
+    per_proof_bytes = sum(leaf_bytes(*t) for t in trees)
+    launch_ms = leaf_ms / max(leaf_launches, 1)
+    per_launch_bytes = per_proof_bytes / len(trees)
+    achieved = per_launch_bytes / (launch_ms * 1e-3) / 1e9
+    perms = sum((1 << lh) * ((w + 15) // 16) for lh, w in trees)
     peaks = json.loads((ROOT / "MEASURED_PEAKS.json").read_text()) if (ROOT / "MEASURED_PEAKS.json").exists() else {}
     peak = float(peaks.get("hbm_gbs", 6650.0))
-    achieved = alg_bytes / (dft_ms * 1e-3) / 1e9
-    roofline = {"kernel": "dft_batch (k_dft_cols + k_dft_rows), commit LDE 16 x 2^20 -> 16 x 2^21",
+    # DRAM traffic of the commitment-tree launch (ncu, 2^21 leaves x 16 words: 134.4 MB read + 90.5 MB
+    # written, profiles/poseidon2_grind_and_leaves_n24.md), scaled to the average launch by algorithmic bytes
+    traffic = 224.84e6 * per_launch_bytes / leaf_bytes(21, 16)
+    roofline = {"kernel": "k_merkle_leaves (Poseidon2-24 leaf sponge + in-CTA subtree compression)",
                 "bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
-                "frac": round(achieved / peak, 4), "traffic": None,
-                "peak_source": "MEASURED_PEAKS.json hbm_gbs (burst copy)" if peaks else "fallback 6650 GB/s",
-                "ms_per_launch": round(dft_ms, 4), "algorithmic_bytes": alg_bytes}
+                "frac": round(achieved / peak, 4), "traffic": round(traffic),
+                "peak_source": "MEASURED_PEAKS.json hbm_gbs" if peaks else "fallback 6650 GB/s",
+                "ms_per_launch": round(launch_ms, 4), "launches_per_proof": round(leaf_launches / args.steps, 2),
+                "algorithmic_bytes_per_launch": round(per_launch_bytes),
+                "compute_bound": {"leaf_permutations_per_s": round(perms / (leaf_ms / args.steps * 1e-3)),
+                                  "note": "integer-issue bound: FMA-heavy (IMAD) pipe ~92% busy, DRAM ~2% "
+                                          "(ncu, profiles/poseidon2_grind_and_leaves_n24.md)"}}
 
     batch = serve = None
     if rank == 0 and world == 1 and not args.no_batch:
@@ -487,7 +510,8 @@ def main() -> None:
                 "proofs_per_s": round(1e3 / value, 3), "proof_words": int(ref_proof.size),
                 "e2e": {"value": round(e2e_value, 4), "unit": UNIT, "h2d_bytes_per_step": h2d * world,
                         "d2h_bytes_per_step": d2h * world},
-                "gpu_launches": int(launches), "roofline": roofline, "cpu_baseline": cpu, "clocks": clk,
+                "gpu_launches": int(launches), "roofline": roofline, "stages_ms_per_proof": stages_ms,
+                "cpu_baseline": cpu, "clocks": clk,
                 "batched": batch, "served": serve}
         print(json.dumps(line), flush=True)
     ctx.close()

@@ -108,6 +108,14 @@ int whir_ctx_destroy(whir_ctx* ctx);
 /* Enqueue on a caller-owned cudaStream_t instead of the context's own stream. */
 int whir_ctx_set_stream(whir_ctx* ctx, void* cuda_stream);
 int whir_ctx_synchronize(whir_ctx* ctx);
+/* Per-stage device timing with CUDA events recorded on the context's stream
+ * (tracing; off by default). Stages: 0 DFT, 1 Merkle leaf hashing, 2 Merkle
+ * upper levels, 3 grinding, 4 sumcheck (coefficients, folds), 5 evaluations
+ * (OOD / constraint points), 6 constraint weights, 7 openings.
+ * whir_ctx_stage_times synchronizes, accumulates the recorded pairs and writes
+ * min(8, cap) entries (milliseconds and scope counts); returns the stage count. */
+int whir_ctx_set_profiling(whir_ctx* ctx, int32_t enable);
+int whir_ctx_stage_times(whir_ctx* ctx, double* ms, uint64_t* counts, int32_t cap, int32_t reset);
 /* Host permutation with the context's data (width taken from the state length 16 or 24). */
 int whir_poseidon2_permute(const whir_ctx* ctx, uint32_t* state, int32_t width);
 

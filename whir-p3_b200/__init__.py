@@ -93,6 +93,8 @@ _SIGS = {
     "whir_ctx_set_stream": (C.c_int, [_vp, _vp]),
     "whir_ctx_synchronize": (C.c_int, [_vp]),
     "whir_poseidon2_permute": (C.c_int, [_vp, _u32, _i32]),
+    "whir_ctx_set_profiling": (C.c_int, [_vp, _i32]),
+    "whir_ctx_stage_times": (C.c_int, [_vp, _vp, _vp, _i32, _i32]),
     "whir_config_new": (C.c_int, [C.POINTER(_Params), _i32, C.POINTER(_Config)]),
     "whir_domain_separator": (C.c_int, [C.POINTER(_Config), _i32, _vp, _i32]),
     "whir_challenger_init": (None, [C.POINTER(_Chal)]),
@@ -339,6 +341,17 @@ class Context:
 
     def set_stream(self, stream_ptr: int) -> None:
         _check(lib().whir_ctx_set_stream(self.handle, stream_ptr))
+
+    STAGES = ["dft", "merkle_leaves", "merkle_upper", "grind", "sumcheck", "eval", "weights", "open"]
+
+    def set_profiling(self, enable: bool) -> None:
+        _check(lib().whir_ctx_set_profiling(self.handle, int(enable)))
+
+    def stage_times(self, reset: bool = True) -> dict:
+        ms = np.zeros(8, dtype=np.float64)
+        cnt = np.zeros(8, dtype=np.uint64)
+        _check(lib().whir_ctx_stage_times(self.handle, ms.ctypes.data, cnt.ctypes.data, 8, int(reset)))
+        return {name: (float(m), int(c)) for name, m, c in zip(self.STAGES, ms, cnt)}
 
     def permute(self, state) -> np.ndarray:
         s = _arr(state).copy()

@@ -58,6 +58,25 @@ int sync(whir_ctx* ctx) {
 // shared with prover.cu
 namespace wh {
 
+StageTimer::StageTimer(whir_ctx* c, int s) : ctx(c), stage(s) {
+  if (!ctx || !ctx->profiling) return;
+  for (cudaEvent_t* e : {&a, &b}) {
+    if (!ctx->event_pool.empty()) {
+      *e = ctx->event_pool.back();
+      ctx->event_pool.pop_back();
+    } else if (cudaEventCreate(e) != cudaSuccess) {
+      *e = nullptr;
+    }
+  }
+  if (a) cudaEventRecord(a, ctx->stream);
+}
+
+StageTimer::~StageTimer() {
+  if (!ctx || !ctx->profiling || !a || !b) return;
+  cudaEventRecord(b, ctx->stream);
+  ctx->stage_events.push_back({stage, {a, b}});
+}
+
 int ensure_dft_tables(whir_ctx* ctx, int log_h, wk::DftTables* t) {
   auto it = ctx->dft.find(log_h);
   if (it == ctx->dft.end()) {
@@ -96,6 +115,7 @@ int split_eq_tables(whir_ctx* ctx, const ef* z, int n, const ef& scale, int lo_b
 // Results (Montgomery) land in ctx->d_small[0 .. 2^seg_bits).
 int dot_eq(whir_ctx* ctx, const uint32_t* d_f, int ext, int seg_bits, const ef* z, int m_bits) {
   if (m_bits > 40) return set_error("dot_eq: size"), WHIR_ERR_INVALID;
+  StageTimer timer(ctx, kStEval);
   const int lo_bits = std::min(m_bits, 8);
   ef* hi = reinterpret_cast<ef*>(ctx->d_arena);
   ef* lo = hi + ((size_t)1 << (m_bits - lo_bits));
@@ -138,7 +158,10 @@ int grind(whir_ctx* ctx, Chal& ch, int bits, uint32_t* witness) {
   }
   WH_CHECK(bits <= 30, "grinding bits above 30");
   // inputs pending beyond 7 never occur (8 inputs trigger a duplexing)
-  WH_TRY_CUDA(wk::grind(ch.st, ch.in, ch.in_len, bits, kb::P, ctx->d_words, ctx->d_words + 1, ctx->p16, ctx->stream));
+  {
+    StageTimer t(ctx, kStGrind);
+    WH_TRY_CUDA(wk::grind(ch.st, ch.in, ch.in_len, bits, kb::P, ctx->d_words, ctx->d_words + 1, ctx->p16, ctx->stream));
+  }
   uint32_t w = 0;
   WH_TRY(fetch(ctx, &w, ctx->d_words, 4));
   if (w >= kb::P) {
@@ -182,6 +205,7 @@ namespace wh {
 int add_eq_points(whir_ctx* ctx, ef* d_w, int n, const std::vector<std::vector<ef>>& pts, const std::vector<ef>& scales,
                   int accumulate) {
   const int m = (int)pts.size();
+  StageTimer timer(ctx, kStWeights);
   if (m == 0) {
     if (!accumulate) WH_TRY_CUDA(cudaMemsetAsync(d_w, 0, ((size_t)1 << n) * sizeof(ef), ctx->stream));
     return WHIR_OK;
@@ -216,6 +240,7 @@ int add_select_vars(whir_ctx* ctx, ef* d_w, int n, const std::vector<uint32_t>& 
   memcpy(host.data(), g.data(), (size_t)m * sizeof(ef));
   memcpy(host.data() + (size_t)m * sizeof(ef), vars.data(), (size_t)m * 4);
   WH_TRY(upload(ctx, d_g, host.data(), host.size()));
+  StageTimer timer(ctx, kStWeights);
   WH_TRY_CUDA(wk::select_tables(d_vars, m, n, lo_bits, pow_lo, pow_hi, ctx->stream));
   WH_TRY_CUDA(wk::add_select(d_w, n, pow_lo, pow_hi, lo_bits, d_g, m, ctx->stream));
   return WHIR_OK;
@@ -315,6 +340,11 @@ int whir_ctx_destroy(whir_ctx* c) {
     cudaFree(kv.second.tw_lo);
     cudaFree(kv.second.tw_hi);
   }
+  for (auto& rec : c->stage_events) {
+    cudaEventDestroy(rec.second.first);
+    cudaEventDestroy(rec.second.second);
+  }
+  for (cudaEvent_t e : c->event_pool) cudaEventDestroy(e);
   cudaFree(c->tw_stage);
   cudaFree(c->d_partials);
   cudaFree(c->d_small);
@@ -338,6 +368,37 @@ int whir_ctx_set_stream(whir_ctx* ctx, void* stream) {
 int whir_ctx_synchronize(whir_ctx* ctx) {
   WH_TRY(check_gpu(ctx));
   return sync(ctx);
+}
+
+int whir_ctx_set_profiling(whir_ctx* ctx, int32_t enable) {
+  WH_TRY(check_gpu(ctx));
+  ctx->profiling = enable != 0;
+  return WHIR_OK;
+}
+
+int whir_ctx_stage_times(whir_ctx* ctx, double* ms, uint64_t* counts, int32_t cap, int32_t reset) {
+  WH_TRY(check_gpu(ctx));
+  WH_TRY(sync(ctx));
+  for (auto& rec : ctx->stage_events) {
+    float t = 0.f;
+    if (cudaEventElapsedTime(&t, rec.second.first, rec.second.second) == cudaSuccess) {
+      ctx->stage_ms[rec.first] += t;
+      ctx->stage_launches[rec.first] += 1;
+    }
+    ctx->event_pool.push_back(rec.second.first);
+    ctx->event_pool.push_back(rec.second.second);
+  }
+  ctx->stage_events.clear();
+  for (int i = 0; i < wh::kStCount && i < cap; i++) {
+    if (ms) ms[i] = ctx->stage_ms[i];
+    if (counts) counts[i] = ctx->stage_launches[i];
+  }
+  if (reset)
+    for (int i = 0; i < wh::kStCount; i++) {
+      ctx->stage_ms[i] = 0.;
+      ctx->stage_launches[i] = 0;
+    }
+  return wh::kStCount;
 }
 
 int whir_poseidon2_permute(const whir_ctx* ctx, uint32_t* state, int32_t width) {

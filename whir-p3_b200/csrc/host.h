@@ -67,6 +67,10 @@ struct Chal {
   void store(whir_challenger& c) const;  // internal -> canonical
 };
 
+// Per-stage device timing (CUDA events on the context's stream), on when
+// profiling is enabled for the context.
+enum Stage { kStDft = 0, kStLeaves, kStNodes, kStGrind, kStSumcheck, kStEval, kStWeights, kStOpen, kStCount };
+
 struct DftCache {
   uint32_t* tw_lo = nullptr;
   uint32_t* tw_hi = nullptr;
@@ -90,4 +94,21 @@ struct whir_ctx {
   size_t arena_bytes = 0;
   void* h_pinned = nullptr;      // staging for small transfers
   size_t pinned_bytes = 0;
+  // stage timing
+  bool profiling = false;
+  std::vector<cudaEvent_t> event_pool;
+  std::vector<std::pair<int, std::pair<cudaEvent_t, cudaEvent_t>>> stage_events;
+  double stage_ms[wh::kStCount] = {};
+  uint64_t stage_launches[wh::kStCount] = {};
 };
+
+namespace wh {
+// Records a CUDA event pair around a scope when the context is profiling.
+struct StageTimer {
+  whir_ctx* ctx;
+  int stage;
+  cudaEvent_t a = nullptr, b = nullptr;
+  StageTimer(whir_ctx* c, int s);
+  ~StageTimer();
+};
+}  // namespace wh

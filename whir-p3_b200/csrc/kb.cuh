@@ -5,8 +5,11 @@
 // in [0, p). Reduction follows Montgomery (1985) in its "subtract" form:
 // for T < 2^64, m = T_lo * p^-1 mod 2^32 makes T - m*p divisible by 2^32, and
 // (T - m*p) / 2^32 = T_hi - mulhi(m, p) exactly (the low words cancel).
-// Additions use the unsigned-min trick: a + b < 2p, and min(s, s - p) picks the
-// reduced value because s - p wraps around when s < p.
+// Additions use the unsigned-min trick: with t = a + b - p (wrapping), the
+// reduced sum is min(t + p, t), since t wraps to a large value exactly when
+// a + b < p. Writing the sum as a three-input addition keeps it on the integer
+// ALU pipe (a multiply-add cannot express it), leaving the multiply pipe to
+// the Montgomery products.
 //
 // Reference types this replaces: p3-koala-bear `KoalaBear` and
 // p3-field `BinomialExtensionField<KoalaBear, 4>` (src/bin/main.rs:28-29).
@@ -31,12 +34,12 @@ constexpr int TWO_ADICITY = 24;
 KB_HD uint32_t umin32(uint32_t a, uint32_t b) { return a < b ? a : b; }
 
 KB_HD uint32_t add(uint32_t a, uint32_t b) {
-  uint32_t s = a + b;
-  return umin32(s, s - P);
+  uint32_t t = a + b - P;
+  return umin32(t + P, t);
 }
 KB_HD uint32_t sub(uint32_t a, uint32_t b) {
-  uint32_t d = a - b;
-  return umin32(d, d + P);
+  uint32_t t = a - b + P;
+  return umin32(t, t - P);
 }
 KB_HD uint32_t neg(uint32_t a) { return sub(0u, a); }
 KB_HD uint32_t dbl(uint32_t a) { return add(a, a); }
@@ -53,8 +56,8 @@ KB_HD uint32_t mulhi(uint32_t a, uint32_t b) {
 KB_HD uint32_t reduce(uint64_t t) {
   uint32_t lo = (uint32_t)t, hi = (uint32_t)(t >> 32);
   uint32_t m = lo * P_INV;
-  uint32_t r = hi - mulhi(m, P);
-  return umin32(r, r + P);
+  uint32_t r = hi - mulhi(m, P) + P;  // in (0, 2p)
+  return umin32(r, r - P);
 }
 // Montgomery reduction of T < 2p * 2^32 (any sum of up to four products < p^2).
 // Here hi - mulhi(m, p) lies in (-p, 2p); the two ranges overlap as unsigned

@@ -537,8 +537,8 @@ static int ilog2i(size_t v) {
   return r;
 }
 
-cudaError_t merkle_build(const uint32_t* rows, int log_h, int row_words, int leaf_hash, uint32_t* digests,
-                         const P2Consts& p16, const P2Consts& p24, cudaStream_t st) {
+cudaError_t merkle_leaves(const uint32_t* rows, int log_h, int row_words, int leaf_hash, uint32_t* digests,
+                          const P2Consts& p16, const P2Consts& p24, cudaStream_t st) {
   const size_t h = (size_t)1 << log_h;
   const int cta = (int)(h < (size_t)MERKLE_CTA ? h : (size_t)MERKLE_CTA);
   const int lv = ilog2i((size_t)cta);
@@ -547,9 +547,13 @@ cudaError_t merkle_build(const uint32_t* rows, int log_h, int row_words, int lea
     k_merkle_leaves<24, p2::RP24, 16><<<blocks, cta, 0, st>>>(rows, row_words, h, lv, digests, p24, p16);
   else
     k_merkle_leaves<16, p2::RP16, 8><<<blocks, cta, 0, st>>>(rows, row_words, h, lv, digests, p16, p16);
-  count_launch();
-  cudaError_t e = cudaGetLastError();
-  if (e != cudaSuccess) return e;
+  LAUNCH_DONE();
+}
+
+cudaError_t merkle_upper(int log_h, uint32_t* digests, const P2Consts& p16, cudaStream_t st) {
+  const size_t h = (size_t)1 << log_h;
+  const int cta = (int)(h < (size_t)MERKLE_CTA ? h : (size_t)MERKLE_CTA);
+  const int lv = ilog2i((size_t)cta);
   size_t off = 0, cnt = h;
   for (int l = 0; l < lv; l++) {
     off += cnt;
@@ -561,7 +565,7 @@ cudaError_t merkle_build(const uint32_t* rows, int log_h, int row_words, int lea
     const unsigned blocks2 = (unsigned)(cnt / c2);
     k_merkle_nodes<<<blocks2, c2 / 2, 0, st>>>(digests, off, cnt, levels, p16);
     count_launch();
-    e = cudaGetLastError();
+    cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
     for (int l = 0; l < levels; l++) {
       off += cnt;
@@ -569,6 +573,13 @@ cudaError_t merkle_build(const uint32_t* rows, int log_h, int row_words, int lea
     }
   }
   return cudaSuccess;
+}
+
+cudaError_t merkle_build(const uint32_t* rows, int log_h, int row_words, int leaf_hash, uint32_t* digests,
+                         const P2Consts& p16, const P2Consts& p24, cudaStream_t st) {
+  cudaError_t e = merkle_leaves(rows, log_h, row_words, leaf_hash, digests, p16, p24, st);
+  if (e != cudaSuccess) return e;
+  return merkle_upper(log_h, digests, p16, st);
 }
 
 // Mmcs::open_batch gather (src/whir/prover/mod.rs:248-300, 378-401)

@@ -38,6 +38,10 @@ cudaError_t dft_batch(const uint32_t* in, uint32_t* out, uint32_t* scratch, int 
 // over Poseidon2-24 rate 16; 1: Poseidon2-16 rate 8. Compression: Poseidon2-16.
 cudaError_t merkle_build(const uint32_t* rows, int log_h, int row_words, int leaf_hash, uint32_t* digests,
                          const p2::P2Consts& p16, const p2::P2Consts& p24, cudaStream_t st);
+// the two halves of merkle_build: leaf hashing with the CTA subtrees, then the upper levels
+cudaError_t merkle_leaves(const uint32_t* rows, int log_h, int row_words, int leaf_hash, uint32_t* digests,
+                          const p2::P2Consts& p16, const p2::P2Consts& p24, cudaStream_t st);
+cudaError_t merkle_upper(int log_h, uint32_t* digests, const p2::P2Consts& p16, cudaStream_t st);
 // gather opened rows and sibling paths for `count` indices
 cudaError_t merkle_open(const uint32_t* rows, const uint32_t* digests, int log_h, int row_words,
                         const uint64_t* d_idx, int count, uint32_t* d_rows_out, uint32_t* d_paths_out,

@@ -199,11 +199,23 @@ int commit_matrix(whir_ctx* ctx, const uint32_t* d_src, int log_chunk, int log_w
   WH_TRY(wh::ensure_dft_tables(ctx, t->log_h, &tab));
   uint32_t* scratch = nullptr;
   WH_TRY_CUDA(cudaMallocAsync(&scratch, words * 4, ctx->stream));
-  cudaError_t e = wk::dft_batch(d_src, t->rows, scratch, log_chunk, log_w, log_blowup, lanes, tab, ctx->stream);
+  cudaError_t e;
+  {
+    wh::StageTimer timer(ctx, wh::kStDft);
+    e = wk::dft_batch(d_src, t->rows, scratch, log_chunk, log_w, log_blowup, lanes, tab, ctx->stream);
+  }
   cudaFreeAsync(scratch, ctx->stream);
   if (e == cudaErrorInvalidValue) return wh::set_error("unsupported DFT shape"), WHIR_ERR_INVALID;
   WH_TRY_CUDA(e);
-  WH_TRY_CUDA(wk::merkle_build(t->rows, t->log_h, t->row_words, leaf_hash, t->digests, ctx->p16, ctx->p24, ctx->stream));
+  {
+    wh::StageTimer timer(ctx, wh::kStLeaves);
+    WH_TRY_CUDA(wk::merkle_leaves(t->rows, t->log_h, t->row_words, leaf_hash, t->digests, ctx->p16, ctx->p24,
+                                  ctx->stream));
+  }
+  {
+    wh::StageTimer timer(ctx, wh::kStNodes);
+    WH_TRY_CUDA(wk::merkle_upper(t->log_h, t->digests, ctx->p16, ctx->stream));
+  }
   uint32_t r[8];
   WH_TRY(wh::fetch(ctx, r, t->digests + (2 * h - 2) * 8, 32));
   for (int i = 0; i < 8; i++) root_canon[i] = kb::from_mont(r[i]);
@@ -222,7 +234,10 @@ int open_queries(whir_ctx* ctx, const Tree& t, const std::vector<uint64_t>& idx,
   uint32_t* d_paths = d_rows + (size_t)q * t.row_words;
   if (q == 0) return WHIR_OK;
   WH_TRY(wh::upload(ctx, d_idx, idx.data(), (size_t)q * 8));
-  WH_TRY_CUDA(wk::merkle_open(t.rows, t.digests, t.log_h, t.row_words, d_idx, q, d_rows, d_paths, ctx->stream));
+  {
+    wh::StageTimer timer(ctx, wh::kStOpen);
+    WH_TRY_CUDA(wk::merkle_open(t.rows, t.digests, t.log_h, t.row_words, d_idx, q, d_rows, d_paths, ctx->stream));
+  }
   std::vector<uint32_t> tmp((size_t)q * per);
   WH_TRY(wh::fetch(ctx, tmp.data(), d_rows, tmp.size() * 4));
   rows.assign(tmp.begin(), tmp.begin() + (size_t)q * t.row_words);
@@ -242,12 +257,18 @@ int open_queries(whir_ctx* ctx, const Tree& t, const std::vector<uint64_t>& idx,
 int sumcheck_round(whir_ctx* ctx, wh::Chal& ch, Sumcheck& sd, ef* d_f, ef* d_w, int m, ef* sum, int pow_bits,
                    ef* r_out) {
   const size_t half = (size_t)1 << (m - 1);
-  WH_TRY_CUDA(wk::sumcheck_coeffs(d_f, d_w, half, ctx->d_partials, ctx->d_small, ctx->stream));
+  {
+    wh::StageTimer timer(ctx, wh::kStSumcheck);
+    WH_TRY_CUDA(wk::sumcheck_coeffs(d_f, d_w, half, ctx->d_partials, ctx->d_small, ctx->stream));
+  }
   ef c[2];
   WH_TRY(wh::fetch(ctx, c, ctx->d_small, sizeof(c)));
   ef r;
   WH_TRY(observe_and_sample(ctx, ch, sd, c[0], c[1], pow_bits, &r));
-  WH_TRY_CUDA(wk::fold_ext(d_f, d_w, half, r, ctx->stream));
+  {
+    wh::StageTimer timer(ctx, wh::kStSumcheck);
+    WH_TRY_CUDA(wk::fold_ext(d_f, d_w, half, r, ctx->stream));
+  }
   *sum = extrapolate_012(c[0], kb::ef_sub(*sum, c[0]), c[1], r);
   *r_out = r;
   return WHIR_OK;
@@ -373,7 +394,10 @@ int do_prove(whir_ctx* ctx, whir_witness* wit, wh::Chal& ch) {
   } guard{ctx, &d_f, &d_w};
   {
     wk::EqSmall e = wh::eq_small_host(rs.data(), k0);
-    WH_TRY_CUDA(wk::fold_multi_base(wit->d_poly, k0, N, e, d_f, ctx->stream));
+    {
+      wh::StageTimer timer(ctx, wh::kStSumcheck);
+      WH_TRY_CUDA(wk::fold_multi_base(wit->d_poly, k0, N, e, d_f, ctx->stream));
+    }
     std::vector<std::vector<ef>> tails(m);
     std::vector<ef> scales(m);
     for (int i = 0; i < m; i++) {
