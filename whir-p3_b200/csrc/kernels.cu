@@ -192,28 +192,59 @@ __device__ __forceinline__ uint32_t tw_pow(const uint32_t* tw_lo, const uint32_t
   return kb::mul(__ldg(tw_lo + (e & 4095)), __ldg(tw_hi + (e >> 12)));
 }
 
+// K consecutive radix-2 DIT stages (first stage `s`, 1-based) in registers:
+// each thread owns 2^K elements of one vector spaced by h = 2^(s-1), which are
+// closed under the butterflies of these K stages.
+template <int LANES, int K>
+__device__ __forceinline__ void dft_stages(typename Elem<LANES>::T* a, int nv, int log_s, int s,
+                                           const uint32_t* tw) {
+  using E = Elem<LANES>;
+  constexpr int R = 1 << K;
+  const int h = 1 << (s - 1);
+  const int log_units = log_s - K;
+  const int total = nv << log_units;
+  for (int q = threadIdx.x; q < total; q += blockDim.x) {
+    const int v = q >> log_units;
+    const int u = q & ((1 << log_units) - 1);
+    const int lowpos = u & (h - 1);
+    const int base = (v << log_s) + ((u >> (s - 1)) << (s - 1 + K)) + lowpos;
+    typename E::T x[R];
+#pragma unroll
+    for (int j = 0; j < R; j++) x[j] = a[swz(base + j * h)];
+#pragma unroll
+    for (int t = 0; t < K; t++) {
+      const int tshift = 12 - (s + t);
+#pragma unroll
+      for (int j = 0; j < R; j++) {
+        if ((j >> t) & 1) continue;
+        const int pos = lowpos + (j & ((1 << t) - 1)) * h;
+        const typename E::T w = E::mulb(x[j + (1 << t)], tw[pos << tshift]);
+        const typename E::T u0 = x[j];
+        x[j] = E::add(u0, w);
+        x[j + (1 << t)] = E::sub(u0, w);
+      }
+    }
+#pragma unroll
+    for (int j = 0; j < R; j++) a[swz(base + j * h)] = x[j];
+  }
+}
+
 // In-place radix-2 DIT over `nv` vectors of S = 2^log_s points stored
-// contiguously (vector v at a[v*S]); inputs already in bit-reversed order.
+// contiguously (vector v at a[v*S], swizzled); inputs already in bit-reversed
+// order. Stages run three at a time in registers.
 template <int LANES>
 __device__ __forceinline__ void smem_dft(typename Elem<LANES>::T* a, int nv, int log_s, const uint32_t* tw) {
-  using E = Elem<LANES>;
-  const int S = 1 << log_s;
-  const int total = nv * (S >> 1);
-  for (int s = 1; s <= log_s; s++) {
-    const int half = 1 << (s - 1);
-    const int tshift = 12 - s;
-    for (int b = threadIdx.x; b < total; b += blockDim.x) {
-      const int v = b >> (log_s - 1);
-      const int k = b & ((S >> 1) - 1);
-      const int grp = k >> (s - 1), pos = k & (half - 1);
-      const int i0 = v * S + grp * (half << 1) + pos;
-      const int p0 = swz(i0), p1 = swz(i0 + half);
-      typename E::T u = a[p0];
-      typename E::T w = E::mulb(a[p1], tw[pos << tshift]);
-      a[p0] = E::add(u, w);
-      a[p1] = E::sub(u, w);
-    }
+  int s = 1;
+  while (s <= log_s) {
+    const int k = log_s - s + 1 >= 3 ? 3 : log_s - s + 1;
+    if (k == 3)
+      dft_stages<LANES, 3>(a, nv, log_s, s, tw);
+    else if (k == 2)
+      dft_stages<LANES, 2>(a, nv, log_s, s, tw);
+    else
+      dft_stages<LANES, 1>(a, nv, log_s, s, tw);
     __syncthreads();
+    s += k;
   }
 }
 
@@ -384,11 +415,11 @@ cudaError_t dft_batch(const uint32_t* in, uint32_t* out, uint32_t* scratch, int 
     dim3 grid(H2 / tile, W);
     if (lanes == 1) {
       set_smem(k_dft_cols<1>, smem);
-      k_dft_cols<1><<<grid, 512, smem, st>>>(in, scratch, log_chunk, log_h1, log_h2, log_h, log2i(tile), t.tw_stage,
+      k_dft_cols<1><<<grid, 256, smem, st>>>(in, scratch, log_chunk, log_h1, log_h2, log_h, log2i(tile), t.tw_stage,
                                              t.tw_lo, t.tw_hi);
     } else {
       set_smem(k_dft_cols<4>, smem);
-      k_dft_cols<4><<<grid, 512, smem, st>>>(reinterpret_cast<const uint4*>(in), reinterpret_cast<uint4*>(scratch),
+      k_dft_cols<4><<<grid, 256, smem, st>>>(reinterpret_cast<const uint4*>(in), reinterpret_cast<uint4*>(scratch),
                                              log_chunk, log_h1, log_h2, log_h, log2i(tile), t.tw_stage, t.tw_lo, t.tw_hi);
     }
     count_launch();
@@ -400,10 +431,10 @@ cudaError_t dft_batch(const uint32_t* in, uint32_t* out, uint32_t* scratch, int 
   dim3 grid(H1, W / jt);
   if (lanes == 1) {
     set_smem(k_dft_rows<1>, smem);
-    k_dft_rows<1><<<grid, 512, smem, st>>>(scratch, out, log_h1, log_h2, log_h, log_w, log2i(jt), t.tw_stage);
+    k_dft_rows<1><<<grid, 256, smem, st>>>(scratch, out, log_h1, log_h2, log_h, log_w, log2i(jt), t.tw_stage);
   } else {
     set_smem(k_dft_rows<4>, smem);
-    k_dft_rows<4><<<grid, 512, smem, st>>>(reinterpret_cast<const uint4*>(scratch), reinterpret_cast<uint4*>(out),
+    k_dft_rows<4><<<grid, 256, smem, st>>>(reinterpret_cast<const uint4*>(scratch), reinterpret_cast<uint4*>(out),
                                            log_h1, log_h2, log_h, log_w, log2i(jt), t.tw_stage);
   }
   LAUNCH_DONE();
