@@ -568,9 +568,93 @@ static int ilog2i(size_t v) {
   return r;
 }
 
+// Leaf digests only (level 0): one thread per row, full occupancy, no barriers.
+template <int T, int RP, int RATE>
+__global__ void __launch_bounds__(256) k_leaf_digests(const uint32_t* __restrict__ rows, int row_words, size_t h,
+                                                       uint32_t* __restrict__ digests,
+                                                       const __grid_constant__ P2Consts leaf) {
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < h; i += (size_t)gridDim.x * blockDim.x) {
+    uint32_t s[T];
+#pragma unroll
+    for (int k = 0; k < T; k++) s[k] = 0u;
+    const uint32_t* row = rows + i * (size_t)row_words;
+    for (int pos = 0; pos < row_words; pos += RATE) {
+      const int take = row_words - pos < RATE ? row_words - pos : RATE;
+      if (take == RATE && (row_words & 3) == 0) {
+#pragma unroll
+        for (int k = 0; k < RATE; k += 4) {
+          uint4 v = __ldg(reinterpret_cast<const uint4*>(row + pos + k));
+          s[k] = v.x;
+          s[k + 1] = v.y;
+          s[k + 2] = v.z;
+          s[k + 3] = v.w;
+        }
+      } else {
+#pragma unroll
+        for (int k = 0; k < RATE; k++)
+          if (k < take) s[k] = row[pos + k];
+      }
+      p2::permute<T, RP>(s, leaf);
+    }
+    uint4* d = reinterpret_cast<uint4*>(digests + i * 8);
+    d[0] = make_uint4(s[0], s[1], s[2], s[3]);
+    d[1] = make_uint4(s[4], s[5], s[6], s[7]);
+  }
+}
+
+// Two tree levels per launch: each thread compresses four nodes of level l
+// into two nodes of level l+1 (written out) and their parent at level l+2.
+__global__ void __launch_bounds__(256) k_merkle_two_levels(uint32_t* __restrict__ digests, size_t in_off,
+                                                            size_t in_count, const __grid_constant__ P2Consts comp) {
+  const size_t out_count = in_count >> 2;
+  const size_t mid_off = in_off + in_count, top_off = mid_off + (in_count >> 1);
+  for (size_t j = (size_t)blockIdx.x * blockDim.x + threadIdx.x; j < out_count; j += (size_t)gridDim.x * blockDim.x) {
+    const uint4* src = reinterpret_cast<const uint4*>(digests + (in_off + 4 * j) * 8);
+    uint32_t a[16], b[16];
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+      const uint4 va = src[q], vb = src[4 + q];
+      a[4 * q] = va.x; a[4 * q + 1] = va.y; a[4 * q + 2] = va.z; a[4 * q + 3] = va.w;
+      b[4 * q] = vb.x; b[4 * q + 1] = vb.y; b[4 * q + 2] = vb.z; b[4 * q + 3] = vb.w;
+    }
+    p2::permute<16, p2::RP16>(a, comp);
+    p2::permute<16, p2::RP16>(b, comp);
+    uint4* mid = reinterpret_cast<uint4*>(digests + (mid_off + 2 * j) * 8);
+    mid[0] = make_uint4(a[0], a[1], a[2], a[3]);
+    mid[1] = make_uint4(a[4], a[5], a[6], a[7]);
+    mid[2] = make_uint4(b[0], b[1], b[2], b[3]);
+    mid[3] = make_uint4(b[4], b[5], b[6], b[7]);
+    uint32_t c[16];
+#pragma unroll
+    for (int k = 0; k < 8; k++) {
+      c[k] = a[k];
+      c[8 + k] = b[k];
+    }
+    p2::permute<16, p2::RP16>(c, comp);
+    uint4* top = reinterpret_cast<uint4*>(digests + (top_off + j) * 8);
+    top[0] = make_uint4(c[0], c[1], c[2], c[3]);
+    top[1] = make_uint4(c[4], c[5], c[6], c[7]);
+  }
+}
+
+// Trees with at least kLevelPairMin leaves are built as: leaf digests, then
+// two levels per launch while a level has more than kSubtreeTop nodes, then
+// one in-CTA subtree for the top. Smaller trees use the in-CTA subtree kernels
+// throughout.
+constexpr size_t kLevelPairMin = (size_t)1 << 12;
+constexpr size_t kSubtreeTop = 512;
+
 cudaError_t merkle_leaves(const uint32_t* rows, int log_h, int row_words, int leaf_hash, uint32_t* digests,
                           const P2Consts& p16, const P2Consts& p24, cudaStream_t st) {
   const size_t h = (size_t)1 << log_h;
+  if (h >= kLevelPairMin) {
+    const unsigned blocks = grid_for(h, 256, 16);
+    if (leaf_hash == 0)
+      k_leaf_digests<24, p2::RP24, 16><<<blocks, 256, 0, st>>>(rows, row_words, h, digests, p24);
+    else
+      k_leaf_digests<16, p2::RP16, 8><<<blocks, 256, 0, st>>>(rows, row_words, h, digests, p16);
+    LAUNCH_DONE();
+  }
   const int cta = (int)(h < (size_t)MERKLE_CTA ? h : (size_t)MERKLE_CTA);
   const int lv = ilog2i((size_t)cta);
   const unsigned blocks = (unsigned)(h / cta);
@@ -583,12 +667,24 @@ cudaError_t merkle_leaves(const uint32_t* rows, int log_h, int row_words, int le
 
 cudaError_t merkle_upper(int log_h, uint32_t* digests, const P2Consts& p16, cudaStream_t st) {
   const size_t h = (size_t)1 << log_h;
-  const int cta = (int)(h < (size_t)MERKLE_CTA ? h : (size_t)MERKLE_CTA);
-  const int lv = ilog2i((size_t)cta);
   size_t off = 0, cnt = h;
-  for (int l = 0; l < lv; l++) {
-    off += cnt;
-    cnt >>= 1;
+  if (h >= kLevelPairMin) {
+    while (cnt > kSubtreeTop) {
+      const size_t out = cnt >> 2;
+      k_merkle_two_levels<<<grid_for(out, 256, 16), 256, 0, st>>>(digests, off, cnt, p16);
+      count_launch();
+      cudaError_t e = cudaGetLastError();
+      if (e != cudaSuccess) return e;
+      off += cnt + (cnt >> 1);
+      cnt >>= 2;
+    }
+  } else {
+    const int cta = (int)(h < (size_t)MERKLE_CTA ? h : (size_t)MERKLE_CTA);
+    const int lv = ilog2i((size_t)cta);
+    for (int l = 0; l < lv; l++) {
+      off += cnt;
+      cnt >>= 1;
+    }
   }
   while (cnt > 1) {
     const int c2 = (int)(cnt < (size_t)(2 * MERKLE_CTA) ? cnt : (size_t)(2 * MERKLE_CTA));
