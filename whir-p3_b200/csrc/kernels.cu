@@ -528,37 +528,6 @@ __global__ void __launch_bounds__(MERKLE_CTA) k_merkle_leaves(const uint32_t* __
   subtree_up(sh, blockDim.x, levels, (size_t)blockIdx.x * blockDim.x, digests, h, comp);
 }
 
-// One CTA consumes `blockDim.x*2` nodes of the input level (offset in_off, in words/8).
-__global__ void __launch_bounds__(MERKLE_CTA) k_merkle_nodes(uint32_t* __restrict__ digests, size_t in_off,
-                                                              size_t in_count, int levels,
-                                                              const __grid_constant__ P2Consts comp) {
-  __shared__ uint32_t sh[2 * MERKLE_CTA * 8];
-  const int t = threadIdx.x;
-  const size_t base = (size_t)blockIdx.x * blockDim.x * 2;
-  const int cnt = (int)min((size_t)blockDim.x * 2, in_count - base);
-  for (int k = t; k < cnt * 8; k += blockDim.x) sh[k] = digests[(in_off + base) * 8 + k];
-  __syncthreads();
-  // subtree_up expects `count` digests in sh and writes levels above in_off
-  size_t off = in_off, lsz = in_count;
-  for (int l = 1; l <= levels; l++) {
-    const int act = cnt >> l;
-    uint32_t d[8];
-    if (t < act) compress16(sh + 2 * t * 8, sh + (2 * t + 1) * 8, d, comp);
-    __syncthreads();
-    off += lsz;
-    lsz >>= 1;
-    if (t < act) {
-      const size_t node = (base >> l) + t;
-#pragma unroll
-      for (int i = 0; i < 8; i++) {
-        sh[t * 8 + i] = d[i];
-        digests[(off + node) * 8 + i] = d[i];
-      }
-    }
-    __syncthreads();
-  }
-}
-
 static int ilog2i(size_t v) {
   int r = -1;
   while (v) {
@@ -637,12 +606,96 @@ __global__ void __launch_bounds__(256) k_merkle_two_levels(uint32_t* __restrict_
   }
 }
 
+// Width-16 Poseidon2 spread over four consecutive lanes (q = lane & 3 holds
+// state words 4q .. 4q+3). The M4 blocks are lane-local; the cross-chunk sums
+// of the external layer and the full sum of the internal layer take two
+// xor-shuffle steps. About four times the per-permutation latency saving of a
+// one-thread permutation, for the narrow top levels of a tree. All 32 lanes
+// of the warp must call it together.
+__device__ __forceinline__ void coop_ext_layer(uint32_t (&x)[4]) {
+  using namespace kb;
+  p2::m4(x[0], x[1], x[2], x[3]);
+  uint32_t s[4] = {x[0], x[1], x[2], x[3]};
+#pragma unroll
+  for (int m = 1; m <= 2; m <<= 1)
+#pragma unroll
+    for (int j = 0; j < 4; j++) s[j] = add(s[j], __shfl_xor_sync(0xffffffffu, s[j], m));
+#pragma unroll
+  for (int j = 0; j < 4; j++) x[j] = add(x[j], s[j]);
+}
+
+__device__ __forceinline__ void coop_permute16(uint32_t (&x)[4], int q, const P2Consts& k) {
+  using namespace kb;
+  coop_ext_layer(x);
+#pragma unroll 1
+  for (int r = 0; r < p2::RF / 2; r++) {
+#pragma unroll
+    for (int j = 0; j < 4; j++) x[j] = p2::cube(add(x[j], k.ext_rc[r * 16 + 4 * q + j]));
+    coop_ext_layer(x);
+  }
+#pragma unroll 1
+  for (int r = 0; r < p2::RP16; r++) {
+    if (q == 0) x[0] = p2::cube(add(x[0], k.int_rc[r]));
+    uint32_t s = add(add(x[0], x[1]), add(x[2], x[3]));
+    s = add(s, __shfl_xor_sync(0xffffffffu, s, 1));
+    s = add(s, __shfl_xor_sync(0xffffffffu, s, 2));
+#pragma unroll
+    for (int j = 0; j < 4; j++) x[j] = add(s, mul(k.diag[4 * q + j], x[j]));
+  }
+#pragma unroll 1
+  for (int r = p2::RF / 2; r < p2::RF; r++) {
+#pragma unroll
+    for (int j = 0; j < 4; j++) x[j] = p2::cube(add(x[j], k.ext_rc[r * 16 + 4 * q + j]));
+    coop_ext_layer(x);
+  }
+}
+
+// Top of a tree: each CTA compresses up to 256 nodes of one level into a
+// subtree, one four-lane group per node pair, level by level in shared memory.
+constexpr int TOP_CTA = 512;
+constexpr int TOP_NODES = 256;
+__global__ void __launch_bounds__(TOP_CTA) k_merkle_top_coop(uint32_t* __restrict__ digests, size_t in_off,
+                                                              size_t in_count, int levels,
+                                                              const __grid_constant__ P2Consts comp) {
+  __shared__ uint32_t sh[TOP_NODES * 8];
+  const int t = threadIdx.x, g = t >> 2, q = t & 3;
+  const size_t base = (size_t)blockIdx.x * TOP_NODES;
+  const int cnt = (int)min((size_t)TOP_NODES, in_count - base);
+  for (int k = t; k < cnt * 8; k += blockDim.x) sh[k] = digests[(in_off + base) * 8 + k];
+  __syncthreads();
+  size_t off = in_off, lsz = in_count;
+  int cur = cnt;
+  for (int l = 1; l <= levels; l++) {
+    const int act = cur >> 1;
+    const bool on = g < act;
+    const int src = on ? 16 * g + 4 * q : 0;
+    uint32_t x[4];
+#pragma unroll
+    for (int j = 0; j < 4; j++) x[j] = sh[src + j];
+    coop_permute16(x, q, comp);
+    __syncthreads();
+    off += lsz;
+    lsz >>= 1;
+    if (on && q < 2) {
+      const size_t node = (base >> l) + g;
+#pragma unroll
+      for (int j = 0; j < 4; j++) {
+        sh[8 * g + 4 * q + j] = x[j];
+        digests[(off + node) * 8 + 4 * q + j] = x[j];
+      }
+    }
+    __syncthreads();
+    cur = act;
+  }
+}
+
 // Trees with at least kLevelPairMin leaves are built as: leaf digests, then
-// two levels per launch while a level has more than kSubtreeTop nodes, then
-// one in-CTA subtree for the top. Smaller trees use the in-CTA subtree kernels
-// throughout.
+// two levels per launch while a level has more than kCoopTop nodes, then
+// cooperative-permutation subtrees (k_merkle_top_coop) for the top. Smaller
+// trees hash their leaves with in-CTA subtrees and use the cooperative kernel
+// above those.
 constexpr size_t kLevelPairMin = (size_t)1 << 12;
-constexpr size_t kSubtreeTop = 512;
+constexpr size_t kCoopTop = (size_t)1 << 15;
 
 cudaError_t merkle_leaves(const uint32_t* rows, int log_h, int row_words, int leaf_hash, uint32_t* digests,
                           const P2Consts& p16, const P2Consts& p24, cudaStream_t st) {
@@ -669,7 +722,7 @@ cudaError_t merkle_upper(int log_h, uint32_t* digests, const P2Consts& p16, cuda
   const size_t h = (size_t)1 << log_h;
   size_t off = 0, cnt = h;
   if (h >= kLevelPairMin) {
-    while (cnt > kSubtreeTop) {
+    while (cnt > kCoopTop) {
       const size_t out = cnt >> 2;
       k_merkle_two_levels<<<grid_for(out, 256, 16), 256, 0, st>>>(digests, off, cnt, p16);
       count_launch();
@@ -687,10 +740,10 @@ cudaError_t merkle_upper(int log_h, uint32_t* digests, const P2Consts& p16, cuda
     }
   }
   while (cnt > 1) {
-    const int c2 = (int)(cnt < (size_t)(2 * MERKLE_CTA) ? cnt : (size_t)(2 * MERKLE_CTA));
+    const int c2 = (int)(cnt < (size_t)TOP_NODES ? cnt : (size_t)TOP_NODES);
     const int levels = ilog2i((size_t)c2);
     const unsigned blocks2 = (unsigned)(cnt / c2);
-    k_merkle_nodes<<<blocks2, c2 / 2, 0, st>>>(digests, off, cnt, levels, p16);
+    k_merkle_top_coop<<<blocks2, TOP_CTA, 0, st>>>(digests, off, cnt, levels, p16);
     count_launch();
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
