@@ -96,3 +96,22 @@ def test_e2e_headline_n24(pkg, gpu_ctx, oracle):
     k = 4, rate 1/2, 100-bit CapacityBound, pow_bits 16, rs reduction 3, one
     constraint, Poseidon2-24 leaves, DIGEST_ELEMS 32."""
     run_both(pkg, gpu_ctx, oracle, 24, 100, 16, 4, 4, 2, 1, 3, 0, 32, 1, 24)
+
+
+def test_e2e_n26_verified(pkg, gpu_ctx, oracle):
+    """n = 26 (the larger size of the full-prove configuration), rs reduction 1,
+    four constraints: the GPU proof is accepted by the oracle's verifier with an
+    agreeing transcript checkpoint (proving n = 26 on the CPU oracle as well
+    would take about a minute; n <= 24 is compared word for word above)."""
+    rng = np.random.default_rng(26)
+    n = 26
+    poly = rnd(rng, 1 << n)
+    pts = rnd(rng, 4 * n * 4)
+    params = pkg.ProtocolParameters(100, 16, pkg.FoldingFactor.constant(4), pkg.SecurityAssumption.CapacityBound, 1, 1,
+                                    "poseidon2_24", 32)
+    proof, cp, evals = pkg.commit_and_prove(gpu_ctx, params, n, poly, pts)
+    oprm = make_params(100, 16, 4, None, 2, 1, 1, 0, 32)
+    rc, vcp = oracle.verify(oprm, n, pts, evals, proof)
+    assert rc == 0 and np.array_equal(vcp, cp)
+    for i in range(4):
+        assert np.array_equal(evals[4 * i:4 * i + 4], oracle.eval_base(poly, pts[4 * n * i:4 * n * (i + 1)]))

@@ -168,8 +168,8 @@ int grind(whir_ctx* ctx, Chal& ch, int bits, uint32_t* witness) {
     set_error("proof-of-work search found no witness");
     return WHIR_ERR_NOT_FOUND;
   }
-  ch.observe(ctx->p16, kb::to_mont(w));
-  if (ch.sample_bits(ctx->p16, bits) != 0) {
+  ch.observe(ctx->hp16, kb::to_mont(w));
+  if (ch.sample_bits(ctx->hp16, bits) != 0) {
     set_error("device grinding returned an invalid witness");
     return WHIR_ERR_CUDA;
   }
@@ -275,6 +275,7 @@ int whir_ctx_create(int32_t device, const whir_poseidon2_params* p16, const whir
     c->p24_params = *p24;
     c->p16 = wh::to_consts(*p16);
     c->p24 = wh::to_consts(*p24);
+    c->hp16 = wh::host_consts16(*p16);
     *out = c;
     return WHIR_OK;
   }
@@ -297,6 +298,7 @@ int whir_ctx_create(int32_t device, const whir_poseidon2_params* p16, const whir
   c->p24_params = *p24;
   c->p16 = wh::to_consts(*p16);
   c->p24 = wh::to_consts(*p24);
+  c->hp16 = wh::host_consts16(*p16);
   auto fail = [&](int code) {
     whir_ctx_destroy(c);
     return code;
@@ -406,10 +408,7 @@ int whir_poseidon2_permute(const whir_ctx* ctx, uint32_t* state, int32_t width) 
   WH_CHECK(state && (width == 16 || width == 24), "width must be 16 or 24");
   WH_CHECK(canon_ok(state, (size_t)width), "state value out of range");
   if (width == 16) {
-    uint32_t s[16];
-    for (int i = 0; i < 16; i++) s[i] = kb::to_mont(state[i]);
-    p2::permute<16, p2::RP16>(s, ctx->p16);
-    for (int i = 0; i < 16; i++) state[i] = kb::from_mont(s[i]);
+    wh::host_permute16(state, ctx->hp16);
   } else {
     uint32_t s[24];
     for (int i = 0; i < 24; i++) s[i] = kb::to_mont(state[i]);
@@ -442,7 +441,7 @@ int whir_challenger_observe(const whir_ctx* ctx, whir_challenger* ch, const uint
   WH_CHECK(canon_ok(values, n), "value out of range");
   wh::Chal c;
   c.load(*ch);
-  for (size_t i = 0; i < n; i++) c.observe(ctx->p16, kb::to_mont(values[i]));
+  for (size_t i = 0; i < n; i++) c.observe(ctx->hp16, kb::to_mont(values[i]));
   c.store(*ch);
   return WHIR_OK;
 }
@@ -452,7 +451,7 @@ int whir_challenger_sample(const whir_ctx* ctx, whir_challenger* ch, uint32_t* o
   WH_CHECK(ch && (out || n == 0), "null argument");
   wh::Chal c;
   c.load(*ch);
-  for (size_t i = 0; i < n; i++) out[i] = kb::from_mont(c.sample(ctx->p16));
+  for (size_t i = 0; i < n; i++) out[i] = kb::from_mont(c.sample(ctx->hp16));
   c.store(*ch);
   return WHIR_OK;
 }
@@ -462,7 +461,7 @@ int whir_challenger_sample_bits(const whir_ctx* ctx, whir_challenger* ch, int32_
   WH_CHECK(ch && out && bits >= 0 && bits < 31, "bad argument");
   wh::Chal c;
   c.load(*ch);
-  *out = c.sample_bits(ctx->p16, bits);
+  *out = c.sample_bits(ctx->hp16, bits);
   c.store(*ch);
   return WHIR_OK;
 }
@@ -488,8 +487,8 @@ int whir_challenger_check_witness(const whir_ctx* ctx, whir_challenger* ch, int3
   if (bits == 0) return 1;
   wh::Chal c;
   c.load(*ch);
-  c.observe(ctx->p16, kb::to_mont(witness));
-  const int ok = c.sample_bits(ctx->p16, bits) == 0;
+  c.observe(ctx->hp16, kb::to_mont(witness));
+  const int ok = c.sample_bits(ctx->hp16, bits) == 0;
   c.store(*ch);
   return ok;
 }

@@ -49,6 +49,19 @@ int ff_at(const whir_config& c, int round);
 int rsr_at(const whir_config& c, int round);
 std::vector<uint32_t> domain_separator(const whir_config& c, int digest_elems);  // canonical
 
+// Host-side width-16 Poseidon2 for the transcript, in canonical form with
+// 64-bit lazy reduction: the linear layers accumulate unreduced (all sums stay
+// below 2^40) and every output is reduced once, about three times fewer
+// operations than reducing after each addition. Same permutation as
+// p2::permute<16, 20>.
+struct HostP16 {
+  uint32_t ext_rc[8 * 16];
+  uint32_t int_rc[20];
+  uint32_t diag[16];
+};
+HostP16 host_consts16(const whir_poseidon2_params& p);
+void host_permute16(uint32_t* state_canonical, const HostP16& k);
+
 // DuplexChallenger with Montgomery-form state
 struct Chal {
   uint32_t st[16];
@@ -57,12 +70,12 @@ struct Chal {
   uint32_t out[8];
   int out_len;
   void init();
-  void duplex(const p2::P2Consts& k);
-  void observe(const p2::P2Consts& k, uint32_t v);  // Montgomery value
-  uint32_t sample(const p2::P2Consts& k);           // Montgomery value
-  uint64_t sample_bits(const p2::P2Consts& k, int bits);
-  kb::ef sample_ef(const p2::P2Consts& k);
-  void observe_ef(const p2::P2Consts& k, const kb::ef& v);
+  void duplex(const HostP16& k);
+  void observe(const HostP16& k, uint32_t v);  // Montgomery value
+  uint32_t sample(const HostP16& k);           // Montgomery value
+  uint64_t sample_bits(const HostP16& k, int bits);
+  kb::ef sample_ef(const HostP16& k);
+  void observe_ef(const HostP16& k, const kb::ef& v);
   void load(const whir_challenger& c);   // canonical -> internal
   void store(whir_challenger& c) const;  // internal -> canonical
 };
@@ -84,6 +97,7 @@ struct whir_ctx {
   bool own_stream = false;
   whir_poseidon2_params p16_params, p24_params;
   p2::P2Consts p16, p24;  // Montgomery form
+  wh::HostP16 hp16;       // canonical, for the host transcript
   uint32_t* tw_stage = nullptr;
   std::map<int, wh::DftCache> dft;  // per log2(height)
   // scratch

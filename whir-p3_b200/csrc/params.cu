@@ -381,33 +381,90 @@ std::vector<uint32_t> domain_separator(const whir_config& c, int digest_elems) {
 // pending or no output is left, then pops the last output.
 // ---------------------------------------------------------------------------
 
+HostP16 host_consts16(const whir_poseidon2_params& p) {
+  HostP16 k;
+  memcpy(k.ext_rc, p.ext_rc, sizeof(k.ext_rc));
+  memcpy(k.int_rc, p.int_rc, sizeof(k.int_rc));
+  memcpy(k.diag, p.diag, sizeof(k.diag));
+  return k;
+}
+
+namespace {
+constexpr uint64_t P64 = kb::P;
+inline uint64_t cube64(uint64_t v) {  // v < 2p: v^2 < 2^64, (v^2 mod p) * v < 2^63
+  const uint64_t sq = (v * v) % P64;
+  return (sq * v) % P64;
+}
+// external layer on canonical inputs: M4 outputs < 16p, chunk sums < 64p,
+// results < 80p < 2^38, reduced once
+inline void ext_layer64(uint64_t* x) {
+  for (int c = 0; c < 16; c += 4) {
+    const uint64_t a = x[c], b = x[c + 1], cc = x[c + 2], d = x[c + 3];
+    const uint64_t t0 = a + b, t1 = cc + d, t2 = 2 * b + t1, t3 = 2 * d + t0;
+    const uint64_t t4 = 4 * t1 + t3, t5 = 4 * t0 + t2;
+    x[c] = t3 + t5;
+    x[c + 1] = t5;
+    x[c + 2] = t2 + t4;
+    x[c + 3] = t4;
+  }
+  for (int j = 0; j < 4; j++) {
+    const uint64_t s = x[j] + x[4 + j] + x[8 + j] + x[12 + j];
+    for (int c = 0; c < 16; c += 4) x[c + j] = (x[c + j] + s) % P64;
+  }
+}
+}  // namespace
+
+void host_permute16(uint32_t* st, const HostP16& k) {
+  uint64_t x[16];
+  for (int i = 0; i < 16; i++) x[i] = st[i];
+  ext_layer64(x);
+  for (int r = 0; r < 4; r++) {
+    for (int i = 0; i < 16; i++) x[i] = cube64(x[i] + k.ext_rc[r * 16 + i]);
+    ext_layer64(x);
+  }
+  for (int r = 0; r < p2::RP16; r++) {
+    x[0] = cube64(x[0] + k.int_rc[r]);
+    uint64_t s = 0;
+    for (int i = 0; i < 16; i++) s += x[i];  // < 16p
+    for (int i = 0; i < 16; i++) x[i] = (s + k.diag[i] * x[i]) % P64;  // < 16p + p^2 < 2^63
+  }
+  for (int r = 4; r < 8; r++) {
+    for (int i = 0; i < 16; i++) x[i] = cube64(x[i] + k.ext_rc[r * 16 + i]);
+    ext_layer64(x);
+  }
+  for (int i = 0; i < 16; i++) st[i] = (uint32_t)x[i];
+}
+
 void Chal::init() { memset(this, 0, sizeof(*this)); }
-void Chal::duplex(const p2::P2Consts& k) {
+void Chal::duplex(const HostP16& k) {
   for (int i = 0; i < in_len; i++) st[i] = in[i];
   in_len = 0;
-  p2::permute<16, p2::RP16>(st, k);
+  uint32_t c[16];
+  for (int i = 0; i < 16; i++) c[i] = kb::from_mont(st[i]);
+  host_permute16(c, k);
+  for (int i = 0; i < 16; i++) st[i] = kb::to_mont(c[i]);
   for (int i = 0; i < 8; i++) out[i] = st[i];
   out_len = 8;
 }
-void Chal::observe(const p2::P2Consts& k, uint32_t v) {
+void Chal::observe(const HostP16& k, uint32_t v) {
   out_len = 0;
   in[in_len++] = v;
   if (in_len == 8) duplex(k);
 }
-uint32_t Chal::sample(const p2::P2Consts& k) {
+uint32_t Chal::sample(const HostP16& k) {
   if (in_len > 0 || out_len == 0) duplex(k);
   return out[--out_len];
 }
-uint64_t Chal::sample_bits(const p2::P2Consts& k, int bits) {
+uint64_t Chal::sample_bits(const HostP16& k, int bits) {
   const uint32_t v = kb::from_mont(sample(k));
   return (uint64_t)v & ((1ull << bits) - 1);
 }
-kb::ef Chal::sample_ef(const p2::P2Consts& k) {
+kb::ef Chal::sample_ef(const HostP16& k) {
   kb::ef r;
   for (int i = 0; i < 4; i++) r.c[i] = sample(k);
   return r;
 }
-void Chal::observe_ef(const p2::P2Consts& k, const kb::ef& v) {
+void Chal::observe_ef(const HostP16& k, const kb::ef& v) {
   for (int i = 0; i < 4; i++) observe(k, v.c[i]);
 }
 void Chal::load(const whir_challenger& c) {

@@ -102,14 +102,14 @@ int observe_and_sample(whir_ctx* ctx, wh::Chal& ch, Sumcheck& sd, const ef& c0, 
   sd.polys.push_back(c0);
   sd.polys.push_back(c2);
   sd.npolys++;
-  ch.observe_ef(ctx->p16, c0);
-  ch.observe_ef(ctx->p16, c2);
+  ch.observe_ef(ctx->hp16, c0);
+  ch.observe_ef(ctx->hp16, c2);
   if (pow_bits > 0) {
     uint32_t w;
     WH_TRY(wh::grind(ctx, ch, pow_bits, &w));
     sd.pows.push_back(w);
   }
-  *r = ch.sample_ef(ctx->p16);
+  *r = ch.sample_ef(ctx->hp16);
   return WHIR_OK;
 }
 
@@ -131,7 +131,7 @@ std::vector<uint64_t> stir_queries(whir_ctx* ctx, wh::Chal& ch, uint64_t domain_
   std::vector<uint64_t> q;
   q.reserve(nq);
   if (total <= max_bits) {
-    uint64_t all = ch.sample_bits(ctx->p16, total);
+    uint64_t all = ch.sample_bits(ctx->hp16, total);
     const uint64_t mask = (1ull << bits) - 1;
     for (int i = 0; i < nq; i++) {
       q.push_back((all & mask) % folded);
@@ -144,7 +144,7 @@ std::vector<uint64_t> stir_queries(whir_ctx* ctx, wh::Chal& ch, uint64_t domain_
       int rem = nq;
       while (rem > 0) {
         const int b = std::min(rem, per);
-        uint64_t all = ch.sample_bits(ctx->p16, b * bits);
+        uint64_t all = ch.sample_bits(ctx->hp16, b * bits);
         for (int i = 0; i < b; i++) {
           q.push_back((all & mask) % folded);
           all >>= bits;
@@ -152,7 +152,7 @@ std::vector<uint64_t> stir_queries(whir_ctx* ctx, wh::Chal& ch, uint64_t domain_
         rem -= b;
       }
     } else {
-      for (int i = 0; i < nq; i++) q.push_back(ch.sample_bits(ctx->p16, bits));
+      for (int i = 0; i < nq; i++) q.push_back(ch.sample_bits(ctx->hp16, bits));
     }
   }
   std::sort(q.begin(), q.end());
@@ -314,14 +314,14 @@ int do_commit(whir_ctx* ctx, whir_witness* w, wh::Chal& ch, const uint32_t* user
   WH_TRY(commit_matrix(ctx, w->d_poly, n - k0, k0, c.starting_log_inv_rate, 0, w->params.leaf_hash, &w->commit_tree,
                        root));
   for (int i = 0; i < 8; i++) pf.push_back(root[i]);
-  for (int i = 0; i < 8; i++) ch.observe(ctx->p16, kb::to_mont(root[i]));
+  for (int i = 0; i < 8; i++) ch.observe(ctx->hp16, kb::to_mont(root[i]));
   pf.push_back((uint32_t)c.commitment_ood_samples);
   for (int i = 0; i < c.commitment_ood_samples; i++) {
-    const ef z = ch.sample_ef(ctx->p16);
+    const ef z = ch.sample_ef(ctx->hp16);
     Constraint con;
     WH_TRY(evaluate_constraint(ctx, w, expand_from_univariate(z, n), &con));
     put_ef(pf, con.eval);
-    ch.observe_ef(ctx->p16, con.eval);
+    ch.observe_ef(ctx->hp16, con.eval);
     w->cons.push_back(std::move(con));
   }
   return WHIR_OK;
@@ -334,7 +334,7 @@ int do_prove(whir_ctx* ctx, whir_witness* wit, wh::Chal& ch) {
   const int m = (int)wit->cons.size();
 
   // ---- initial sumcheck (Sumcheck::from_base_evals, sumcheck_prover.rs:237-292)
-  const ef alpha = ch.sample_ef(ctx->p16);
+  const ef alpha = ch.sample_ef(ctx->hp16);
   std::vector<ef> apow(m > 0 ? m : 1);
   ef sum = kb::ef_zero();
   {
@@ -421,19 +421,19 @@ int do_prove(whir_ctx* ctx, whir_witness* wit, wh::Chal& ch) {
     uint32_t root[8];
     WH_TRY(commit_matrix(ctx, reinterpret_cast<const uint32_t*>(d_f), nv - ffn, ffn, log_blowup, 1,
                          wit->params.leaf_hash, &nt, root));
-    for (int i = 0; i < 8; i++) ch.observe(ctx->p16, kb::to_mont(root[i]));
+    for (int i = 0; i < 8; i++) ch.observe(ctx->hp16, kb::to_mont(root[i]));
     for (int i = 0; i < 8; i++) pf.push_back(root[i]);
     // OOD samples
     std::vector<std::vector<ef>> opts;
     std::vector<ef> oevs;
     pf.push_back((uint32_t)rc.ood_samples);
     for (int i = 0; i < rc.ood_samples; i++) {
-      const ef z = ch.sample_ef(ctx->p16);
+      const ef z = ch.sample_ef(ctx->hp16);
       std::vector<ef> pt = expand_from_univariate(z, nv);
       WH_TRY(wh::dot_eq(ctx, reinterpret_cast<const uint32_t*>(d_f), 1, 0, pt.data(), nv));
       ef ev;
       WH_TRY(wh::fetch(ctx, &ev, ctx->d_small, sizeof(ef)));
-      ch.observe_ef(ctx->p16, ev);
+      ch.observe_ef(ctx->hp16, ev);
       put_ef(pf, ev);
       opts.push_back(std::move(pt));
       oevs.push_back(ev);
@@ -441,7 +441,7 @@ int do_prove(whir_ctx* ctx, whir_witness* wit, wh::Chal& ch) {
     uint32_t pw = 0;
     if (rc.pow_bits > 0) WH_TRY(wh::grind(ctx, ch, rc.pow_bits, &pw));
     pf.push_back(pw);
-    (void)ch.sample(ctx->p16);
+    (void)ch.sample(ctx->hp16);
     const std::vector<uint64_t> idx = stir_queries(ctx, ch, rc.domain_size, wh::ff_at(c, round), rc.num_queries);
     pf.push_back((uint32_t)idx.size());
     WH_TRY(open_queries(ctx, prev, idx, pf, rows));
@@ -462,7 +462,7 @@ int do_prove(whir_ctx* ctx, whir_witness* wit, wh::Chal& ch) {
       svars[q] = kb::pow(gen, idx[q]);
     }
     // Constraint::combine (constraints/mod.rs:234-248) then the sumcheck rounds
-    const ef gamma = ch.sample_ef(ctx->p16);
+    const ef gamma = ch.sample_ef(ctx->hp16);
     std::vector<ef> gpow(opts.size());
     ef g = kb::ef_one();
     for (size_t i = 0; i < opts.size(); i++) {
@@ -499,7 +499,7 @@ int do_prove(whir_ctx* ctx, whir_witness* wit, wh::Chal& ch) {
     WH_TRY(wh::fetch(ctx, fin.data(), d_f, fn * sizeof(ef)));
     pf.push_back((uint32_t)fn);
     for (size_t i = 0; i < fn; i++) {
-      ch.observe_ef(ctx->p16, fin[i]);
+      ch.observe_ef(ctx->hp16, fin[i]);
       put_ef(pf, fin[i]);
     }
     uint32_t pw = 0;
