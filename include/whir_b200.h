@@ -119,6 +119,50 @@ int whir_ctx_stage_times(whir_ctx* ctx, double* ms, uint64_t* counts, int32_t ca
 /* Host permutation with the context's data (width taken from the state length 16 or 24). */
 int whir_poseidon2_permute(const whir_ctx* ctx, uint32_t* state, int32_t width);
 
+/* ---- launch-shape tuning ---------------------------------------------------
+ * The DFT plan (four-step split, tile and CTA size of each pass), the Merkle
+ * leaf and node batch widths (threads per CTA, CTAs per SM) and the fold tile
+ * are chosen per shape: the first time a shape runs, every candidate is timed
+ * with CUDA events on the calling context's stream and the fastest is cached
+ * for the process (keyed by device ordinal). All candidates compute identical
+ * values. Mode 1 (default): tune on first use; mode 0: fixed default shapes
+ * (entries already cached stay in use until whir_tune_clear). No counterpart
+ * in the reference, whose CPU code has no launch shapes. */
+enum {
+  WHIR_TUNE_DFT = 1,
+  WHIR_TUNE_MERKLE_LEAVES = 2,
+  WHIR_TUNE_MERKLE_NODES = 3,
+  WHIR_TUNE_FOLD = 4
+};
+typedef struct {
+  int32_t kind;      /* WHIR_TUNE_* */
+  int32_t device;
+  int32_t key[4];    /* DFT: log_chunk, log_width, log_blowup, lanes (1 or 4); Merkle leaves: log_height,
+                        row_words, leaf_hash; nodes: log_height; fold: log2(pairs), arrays (1 or 2) */
+  int32_t choice[5]; /* DFT: log_h2 (0 = one pass), log_t1, threads1, log_t2, threads2; others: threads, per_sm */
+  int32_t candidates;
+  float ms_default;  /* device time of the default shape */
+  float ms_best;     /* device time of the chosen shape */
+} whir_tune_entry;
+int whir_tune_set_mode(int32_t mode);
+int whir_tune_get_mode(void);
+/* Returns the number of cached entries and writes min(count, cap). */
+int whir_tune_entries(whir_tune_entry* out, int32_t cap);
+int whir_tune_clear(void);
+/* Candidate DFT plans of a shape, 5 words each (the whir_tune_entry choice
+ * layout); returns the count and writes min(count, cap) plans. */
+int whir_dft_plans(int32_t log_chunk, int32_t log_width, int32_t log_blowup, int32_t ext, int32_t* plans,
+                   int32_t cap);
+/* whir_dft_batch / whir_merkle_commit / whir_fold_ext with an explicit launch
+ * shape instead of the tuned one: plan = 5 words as above; Merkle shape =
+ * {leaf threads, leaf CTAs per SM, node threads, node CTAs per SM}; fold
+ * shape = {threads, CTAs per SM} (CTAs per SM 0: no cap). */
+int whir_dft_batch_plan(whir_ctx* ctx, const uint32_t* d_chunks, int32_t log_chunk, int32_t log_width,
+                        int32_t log_blowup, int32_t ext, const int32_t* plan, uint32_t* d_out);
+int whir_merkle_commit_shaped(whir_ctx* ctx, const uint32_t* d_rows, int32_t log_height, int32_t row_words,
+                              int32_t leaf_hash, const int32_t* shape, uint32_t* d_digests, uint32_t* root);
+int whir_fold_ext_shaped(whir_ctx* ctx, uint32_t* d_evals, int32_t n, const uint32_t* r, const int32_t* shape);
+
 /* ---- parameters (WhirConfig::new, src/whir/parameters.rs:81-234) ----------- */
 int whir_config_new(const whir_protocol_params* params, int32_t num_variables, whir_config* out);
 /* DomainSeparator::commit_statement + add_whir_proof pattern

@@ -126,3 +126,35 @@ def test_job_footprint_grows_with_size(pkg):
     # peak: round-0 tree (64 + 16) + round-1 codeword 32 + digests 8 + DFT scratch 32 = 152 MiB
     assert sizes[24 - 12] == (64 + 128 + 128 + 32 + 152) * 2**20
     assert pkg.job_footprint(params, 24, True) == sizes[24 - 12] - 64 * 2**20
+
+
+@pytest.mark.parametrize("log_chunk,log_w,log_blowup,ext", [(20, 4, 1, 0), (16, 4, 3, 1), (8, 4, 3, 1), (0, 0, 0, 0),
+                                                           (12, 0, 12, 0), (4, 12, 1, 1), (24, 0, 0, 0)])
+def test_dft_candidate_plans_are_in_bounds(pkg, log_chunk, log_w, log_blowup, ext):
+    """Every plan the tuner may time keeps each pass <= 2^12 points, its tiles
+    within 128 KiB of shared memory and its tile counts within the shape."""
+    plans = pkg.dft_plans(log_chunk, log_w, log_blowup, bool(ext))
+    assert plans, "the default plan is always a candidate"
+    lanes = 4 if ext else 1
+    log_h = log_chunk + log_blowup
+    for h2, t1, th1, t2, th2 in plans:
+        assert th1 in (128, 256, 512) and th2 in (128, 256, 512)
+        if h2 == 0:
+            assert log_chunk <= 12 and 0 <= t1 <= log_w
+            assert (4 * lanes << t1 << log_chunk) <= 128 * 1024
+        else:
+            h1 = log_h - h2
+            assert 1 <= h2 <= min(12, log_chunk) and 0 <= h1 <= 12
+            assert 0 <= t1 <= h2 and (4 * lanes << t1 << h1) <= 128 * 1024
+            assert 0 <= t2 <= log_w and (4 * lanes << t2 << h2) <= 128 * 1024
+
+
+def test_tune_mode_switch(pkg):
+    assert pkg.tune_mode() == 1
+    with pytest.raises(pkg.WhirError):
+        pkg.set_tune_mode(2)
+    pkg.set_tune_mode(0)
+    assert pkg.tune_mode() == 0
+    pkg.set_tune_mode(1)
+    pkg.tune_clear()
+    assert pkg.tune_entries() == []

@@ -136,6 +136,14 @@ _SIGS = {
     "whir_batch_wait": (C.c_int, [_vp, C.POINTER(Job), _i32]),
     "whir_batch_wait_all": (C.c_int, [_vp]),
     "whir_batch_run": (C.c_int, [_vp, C.POINTER(Job), _i32]),
+    "whir_tune_set_mode": (C.c_int, [_i32]),
+    "whir_tune_get_mode": (C.c_int, []),
+    "whir_tune_entries": (C.c_int, [_vp, _i32]),
+    "whir_tune_clear": (C.c_int, []),
+    "whir_dft_plans": (C.c_int, [_i32, _i32, _i32, _i32, _vp, _i32]),
+    "whir_dft_batch_plan": (C.c_int, [_vp, _vp, _i32, _i32, _i32, _i32, _vp, _vp]),
+    "whir_merkle_commit_shaped": (C.c_int, [_vp, _vp, _i32, _i32, _i32, _vp, _vp, _u32]),
+    "whir_fold_ext_shaped": (C.c_int, [_vp, _vp, _i32, _u32, _vp]),
 }
 
 _lib = None
@@ -470,6 +478,72 @@ def merkle_commit(ctx: Context, rows: DeviceArray, log_height: int, row_words: i
     root = np.zeros(8, dtype=np.uint32)
     _check(lib().whir_merkle_commit(ctx.handle, rows.ptr, log_height, row_words, leaf_hash, digests.ptr, root))
     return root
+
+
+# ---------------------------------------------------------------------------
+# launch-shape tuning
+# ---------------------------------------------------------------------------
+
+TUNE_KINDS = {1: "dft", 2: "merkle_leaves", 3: "merkle_nodes", 4: "fold"}
+
+
+class TuneEntry(C.Structure):
+    _fields_ = [("kind", C.c_int32), ("device", C.c_int32), ("key", C.c_int32 * 4), ("choice", C.c_int32 * 5),
+                ("candidates", C.c_int32), ("ms_default", C.c_float), ("ms_best", C.c_float)]
+
+
+def set_tune_mode(mode: int) -> None:
+    """1: time every candidate launch shape on first use of a shape (default); 0: fixed default shapes."""
+    _check(lib().whir_tune_set_mode(int(mode)))
+
+
+def tune_mode() -> int:
+    return int(lib().whir_tune_get_mode())
+
+
+def tune_clear() -> None:
+    _check(lib().whir_tune_clear())
+
+
+def tune_entries() -> list[dict]:
+    """The cached launch-shape choices as dicts (kind, device, key, choice, candidates, ms_default, ms_best)."""
+    n = _check(lib().whir_tune_entries(None, 0))
+    arr = (TuneEntry * max(n, 1))()
+    n = min(n, _check(lib().whir_tune_entries(C.cast(arr, _vp), n)))
+    return [{"kind": TUNE_KINDS.get(e.kind, str(e.kind)), "device": e.device, "key": list(e.key),
+             "choice": list(e.choice), "candidates": e.candidates, "ms_default": e.ms_default,
+             "ms_best": e.ms_best} for e in arr[:n]]
+
+
+def dft_plans(log_chunk: int, log_width: int, log_blowup: int, ext: bool) -> list[tuple[int, ...]]:
+    """Candidate DFT plans (log_h2, log_t1, threads1, log_t2, threads2) the tuner times for a shape."""
+    n = _check(lib().whir_dft_plans(log_chunk, log_width, log_blowup, int(ext), None, 0))
+    buf = np.zeros(max(n, 1) * 5, dtype=np.int32)
+    _check(lib().whir_dft_plans(log_chunk, log_width, log_blowup, int(ext), buf.ctypes.data, n))
+    return [tuple(int(v) for v in buf[5 * i: 5 * i + 5]) for i in range(n)]
+
+
+def dft_batch_plan(ctx: Context, chunks: DeviceArray, log_chunk: int, log_width: int, log_blowup: int, ext: bool,
+                   plan, out: DeviceArray) -> DeviceArray:
+    p = np.ascontiguousarray(plan, dtype=np.int32)
+    _check(lib().whir_dft_batch_plan(ctx.handle, chunks.ptr, log_chunk, log_width, log_blowup, int(ext),
+                                     p.ctypes.data, out.ptr))
+    return out
+
+
+def merkle_commit_shaped(ctx: Context, rows: DeviceArray, log_height: int, row_words: int, leaf_hash: int,
+                         shape, digests: DeviceArray) -> np.ndarray:
+    """merkle_commit with shape = (leaf threads, leaf CTAs/SM, node threads, node CTAs/SM)."""
+    sh = np.ascontiguousarray(shape, dtype=np.int32)
+    root = np.zeros(8, dtype=np.uint32)
+    _check(lib().whir_merkle_commit_shaped(ctx.handle, rows.ptr, log_height, row_words, leaf_hash, sh.ctypes.data,
+                                           digests.ptr, root))
+    return root
+
+
+def fold_ext_shaped(ctx: Context, evals: DeviceArray, n: int, r, shape) -> None:
+    sh = np.ascontiguousarray(shape, dtype=np.int32)
+    _check(lib().whir_fold_ext_shaped(ctx.handle, evals.ptr, n, _arr(r, 4), sh.ctypes.data))
 
 
 def merkle_open(ctx: Context, rows: DeviceArray, digests: DeviceArray, log_height: int, row_words: int,

@@ -540,11 +540,9 @@ int whir_dft_batch(whir_ctx* ctx, const uint32_t* d_chunks, int32_t log_chunk, i
   uint32_t* scratch = nullptr;
   const size_t bytes = ((size_t)1 << (log_h + log_width)) * 4 * lanes;
   WH_TRY_CUDA(cudaMallocAsync(&scratch, bytes, ctx->stream));
-  cudaError_t e = wk::dft_batch(d_chunks, d_out, scratch, log_chunk, log_width, log_blowup, lanes, t, ctx->stream);
+  const int s = wh::run_dft(ctx, d_chunks, d_out, scratch, log_chunk, log_width, log_blowup, lanes, t);
   cudaFreeAsync(scratch, ctx->stream);
-  if (e == cudaErrorInvalidValue) return wh::set_error("unsupported DFT shape"), WHIR_ERR_INVALID;
-  WH_TRY_CUDA(e);
-  return WHIR_OK;
+  return s;
 }
 
 int whir_merkle_commit(whir_ctx* ctx, const uint32_t* d_rows, int32_t log_height, int32_t row_words,
@@ -553,7 +551,8 @@ int whir_merkle_commit(whir_ctx* ctx, const uint32_t* d_rows, int32_t log_height
   WH_CHECK(d_rows && d_digests && log_height >= 0 && log_height <= 30 && row_words > 0 &&
                (leaf_hash == 0 || leaf_hash == 1),
            "bad Merkle arguments");
-  WH_TRY_CUDA(wk::merkle_build(d_rows, log_height, row_words, leaf_hash, d_digests, ctx->p16, ctx->p24, ctx->stream));
+  WH_TRY(wh::run_merkle_leaves(ctx, d_rows, log_height, row_words, leaf_hash, d_digests));
+  WH_TRY(wh::run_merkle_upper(ctx, log_height, d_digests));
   if (root) {
     const size_t h = (size_t)1 << log_height;
     uint32_t r[8];
@@ -618,7 +617,7 @@ int whir_eval_ext(whir_ctx* ctx, const uint32_t* d_evals, int32_t n, const uint3
 int whir_fold_ext(whir_ctx* ctx, uint32_t* d_evals, int32_t n, const uint32_t* r) {
   WH_TRY(check_gpu(ctx));
   WH_CHECK(d_evals && r && n >= 1 && n <= 30 && canon_ok(r, 4), "bad fold arguments");
-  WH_TRY_CUDA(wk::fold_ext(reinterpret_cast<ef*>(d_evals), nullptr, (size_t)1 << (n - 1), load_ef_canon(r), ctx->stream));
+  WH_TRY(wh::run_fold(ctx, reinterpret_cast<ef*>(d_evals), nullptr, (size_t)1 << (n - 1), load_ef_canon(r)));
   return WHIR_OK;
 }
 

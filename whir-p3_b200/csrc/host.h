@@ -125,4 +125,15 @@ struct StageTimer {
   StageTimer(whir_ctx* c, int s);
   ~StageTimer();
 };
+
+int ensure_dft_tables(whir_ctx* ctx, int log_h, wk::DftTables* t);
+int fetch(whir_ctx* ctx, void* host, const void* dev, size_t bytes);
+
+// Tuned launches (launch shapes chosen per shape on first use, process-wide)
+int run_dft(whir_ctx* ctx, const uint32_t* in, uint32_t* out, uint32_t* scratch, int log_chunk, int log_w,
+            int log_blowup, int lanes, const wk::DftTables& t);
+int run_merkle_leaves(whir_ctx* ctx, const uint32_t* rows, int log_h, int row_words, int leaf_hash,
+                      uint32_t* digests);
+int run_merkle_upper(whir_ctx* ctx, int log_h, uint32_t* digests);
+int run_fold(whir_ctx* ctx, kb::ef* a, kb::ef* b, size_t half, const kb::ef& r);
 }  // namespace wh

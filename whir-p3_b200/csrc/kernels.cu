@@ -356,7 +356,9 @@ static int log2i(int v) {
 // Dynamic shared memory limits are per-kernel process-wide attributes: they
 // are raised once to the largest size any launch uses and never lowered, so
 // launches from concurrent contexts cannot race a smaller setting.
-constexpr size_t kDftSmemMax = 2048 * 4 + 64 * 1024;
+constexpr size_t kDftTwBytes = 2048 * 4;
+constexpr size_t kDftTileMax = 128 * 1024;
+constexpr size_t kDftSmemMax = kDftTwBytes + kDftTileMax;
 constexpr size_t kSelectSmemMax = 160 * 1024;
 __global__ void k_add_select(ef* __restrict__ w, size_t N, int lo_bits, const uint32_t* __restrict__ pow_lo,
                              const uint32_t* __restrict__ pow_hi, const ef* __restrict__ g, int m, int hi_bits);
@@ -370,74 +372,142 @@ static void init_smem_attributes() {
     cudaFuncSetAttribute(k_dft_coset<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kDftSmemMax);
     cudaFuncSetAttribute(k_dft_coset<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kDftSmemMax);
     cudaFuncSetAttribute(k_add_select, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSelectSmemMax);
-    cudaGetLastError();
   });
 }
-template <typename K>
-static void set_smem(K, size_t) {
-  init_smem_attributes();
+
+static bool dft_threads_ok(int t) { return t == 128 || t == 256 || t == 512; }
+
+// Tile bytes of one pass: 2^log_t vectors of 2^log_len elements.
+static size_t dft_tile_bytes(int log_t, int log_len, int lanes) { return ((size_t)4 * lanes << log_t) << log_len; }
+
+bool dft_plan_ok(const DftPlan& p, int log_chunk, int log_w, int log_blowup, int lanes) {
+  if (lanes != 1 && lanes != 4) return false;
+  if (log_chunk < 0 || log_blowup < 0 || log_w < 0 || log_w > 15) return false;
+  const int log_h = log_chunk + log_blowup;
+  if (log_h > 24 || !dft_threads_ok(p.threads1)) return false;
+  if (p.log_h2 == 0) {  // one pass
+    return log_chunk <= 12 && p.log_t1 >= 0 && p.log_t1 <= log_w &&
+           dft_tile_bytes(p.log_t1, log_chunk, lanes) <= kDftTileMax;
+  }
+  const int log_h1 = log_h - p.log_h2;
+  if (p.log_h2 < 1 || p.log_h2 > 12 || p.log_h2 > log_chunk || log_h1 < 0 || log_h1 > 12) return false;
+  if (!dft_threads_ok(p.threads2)) return false;
+  if (p.log_t1 < 0 || p.log_t1 > p.log_h2 || dft_tile_bytes(p.log_t1, log_h1, lanes) > kDftTileMax) return false;
+  if (p.log_t2 < 0 || p.log_t2 > log_w || dft_tile_bytes(p.log_t2, p.log_h2, lanes) > kDftTileMax) return false;
+  return true;
 }
 
-cudaError_t dft_batch(const uint32_t* in, uint32_t* out, uint32_t* scratch, int log_chunk, int log_w,
-                      int log_blowup, int lanes, const DftTables& t, cudaStream_t st) {
-  const int log_h = log_chunk + log_blowup;
-  if (log_h > 24 || log_chunk < 0 || log_blowup < 0 || (lanes != 1 && lanes != 4)) return cudaErrorInvalidValue;
-  const int W = 1 << log_w;
-  const long ebytes = 4 * lanes;
+DftPlan dft_default_plan(int log_chunk, int log_w, int log_blowup, int lanes) {
   const long budget = 64 * 1024;
-  const size_t tw_bytes = 2048 * 4;
+  const long ebytes = 4 * lanes;
+  const int W = 1 << log_w;
+  const int log_h = log_chunk + log_blowup;
+  DftPlan p{};
+  p.threads1 = p.threads2 = 256;
   const int max_single = lanes == 1 ? 12 : 11;
   if (log_chunk <= max_single) {
-    const int L = 1 << log_chunk;
-    const int jt = pow2_clamp(budget / (L * ebytes), 1, W);
-    const size_t smem = tw_bytes + (size_t)jt * L * ebytes;
-    dim3 grid(1u << log_blowup, W / jt);
-    if (lanes == 1) {
-      set_smem(k_dft_coset<1>, smem);
-      k_dft_coset<1><<<grid, 256, smem, st>>>(in, out, log_chunk, log_blowup, log_w, log2i(jt), t.tw_stage, t.tw_lo,
-                                              t.tw_hi);
-    } else {
-      set_smem(k_dft_coset<4>, smem);
-      k_dft_coset<4><<<grid, 256, smem, st>>>(reinterpret_cast<const uint4*>(in), reinterpret_cast<uint4*>(out),
-                                              log_chunk, log_blowup, log_w, log2i(jt), t.tw_stage, t.tw_lo, t.tw_hi);
-    }
-    LAUNCH_DONE();
+    p.log_h2 = 0;
+    p.log_t1 = log2i(pow2_clamp(budget / ((long)ebytes << log_chunk), 1, W));
+    return p;
   }
   int log_h2 = lanes == 1 ? 11 : 10;
   if (log_h - log_h2 > 12) log_h2 = log_h - 12;
-  int log_h1 = log_h - log_h2;
-  if (log_h2 > max_single || log_h1 > 12 || log_h1 < log_blowup || log_h2 > log_chunk) return cudaErrorInvalidValue;
+  const int log_h1 = log_h - log_h2;
+  p.log_h2 = log_h2;
+  int tile = pow2_clamp(budget / ((long)ebytes << log_h1), 1, lanes == 1 ? 16 : 8);
+  if (tile > (1 << log_h2)) tile = 1 << log_h2;
+  p.log_t1 = log2i(tile);
+  p.log_t2 = log2i(pow2_clamp(budget / ((long)ebytes << log_h2), 1, W));
+  return p;
+}
+
+// Candidates: the one-pass kernel when the chunk fits, and every four-step
+// split with both passes at least 2^4 long; per pass, tiles of 8 KiB to 128 KiB
+// (at most 32 vectors in pass 1, whose global accesses are tile-wide) at 256
+// and 512 threads. The default plan is always included.
+void dft_candidates(int log_chunk, int log_w, int log_blowup, int lanes, DftPlan* out, int* count, int cap) {
+  int n = 0;
+  auto push = [&](const DftPlan& p) {
+    if (n < cap && dft_plan_ok(p, log_chunk, log_w, log_blowup, lanes)) out[n++] = p;
+  };
+  push(dft_default_plan(log_chunk, log_w, log_blowup, lanes));
+  const int log_h = log_chunk + log_blowup;
+  const int threads[2] = {256, 512};
+  auto tile_ok = [&](int log_t, int log_len) {
+    const size_t b = dft_tile_bytes(log_t, log_len, lanes);
+    return b >= 8 * 1024 || log_t == 0;
+  };
+  if (log_chunk <= 12) {
+    for (int lt = 0; lt <= log_w; lt++)
+      for (int th : threads)
+        if (tile_ok(lt, log_chunk)) push(DftPlan{0, lt, th, 0, 256});
+  }
+  for (int h2 = 4; h2 <= 12; h2++) {
+    const int h1 = log_h - h2;
+    if (h1 < 4 || h1 > 12 || h2 > log_chunk) continue;
+    for (int t1 = 0; t1 <= 5 && t1 <= h2; t1++)
+      for (int th1 : threads)
+        if (tile_ok(t1, h1)) push(DftPlan{h2, t1, th1, 0, 256});
+    for (int t2 = 0; t2 <= log_w; t2++)
+      for (int th2 : threads)
+        if (tile_ok(t2, h2)) push(DftPlan{h2, 0, 256, t2, th2});
+  }
+  *count = n;
+}
+
+cudaError_t dft_batch(const uint32_t* in, uint32_t* out, uint32_t* scratch, int log_chunk, int log_w,
+                      int log_blowup, int lanes, const DftTables& t, const DftPlan& plan, int passes,
+                      cudaStream_t st) {
+  if (!dft_plan_ok(plan, log_chunk, log_w, log_blowup, lanes)) return cudaErrorInvalidValue;
+  init_smem_attributes();
+  const int log_h = log_chunk + log_blowup;
+  const int W = 1 << log_w;
+  if (plan.log_h2 == 0) {
+    const int jt = 1 << plan.log_t1;
+    const size_t smem = kDftTwBytes + dft_tile_bytes(plan.log_t1, log_chunk, lanes);
+    dim3 grid(1u << log_blowup, W / jt);
+    if (lanes == 1)
+      k_dft_coset<1><<<grid, plan.threads1, smem, st>>>(in, out, log_chunk, log_blowup, log_w, plan.log_t1,
+                                                        t.tw_stage, t.tw_lo, t.tw_hi);
+    else
+      k_dft_coset<4><<<grid, plan.threads1, smem, st>>>(reinterpret_cast<const uint4*>(in),
+                                                        reinterpret_cast<uint4*>(out), log_chunk, log_blowup, log_w,
+                                                        plan.log_t1, t.tw_stage, t.tw_lo, t.tw_hi);
+    LAUNCH_DONE();
+  }
+  const int log_h2 = plan.log_h2, log_h1 = log_h - log_h2;
   const int H1 = 1 << log_h1, H2 = 1 << log_h2;
-  {
-    int tile = pow2_clamp(budget / ((long)H1 * ebytes), 1, lanes == 1 ? 16 : 8);
-    if (tile > H2) tile = H2;
-    const size_t smem = tw_bytes + (size_t)tile * H1 * ebytes;
+  if (passes & 1) {
+    const int tile = 1 << plan.log_t1;
+    const size_t smem = kDftTwBytes + dft_tile_bytes(plan.log_t1, log_h1, lanes);
     dim3 grid(H2 / tile, W);
-    if (lanes == 1) {
-      set_smem(k_dft_cols<1>, smem);
-      k_dft_cols<1><<<grid, 256, smem, st>>>(in, scratch, log_chunk, log_h1, log_h2, log_h, log2i(tile), t.tw_stage,
-                                             t.tw_lo, t.tw_hi);
-    } else {
-      set_smem(k_dft_cols<4>, smem);
-      k_dft_cols<4><<<grid, 256, smem, st>>>(reinterpret_cast<const uint4*>(in), reinterpret_cast<uint4*>(scratch),
-                                             log_chunk, log_h1, log_h2, log_h, log2i(tile), t.tw_stage, t.tw_lo, t.tw_hi);
-    }
+    if (lanes == 1)
+      k_dft_cols<1><<<grid, plan.threads1, smem, st>>>(in, scratch, log_chunk, log_h1, log_h2, log_h, plan.log_t1,
+                                                       t.tw_stage, t.tw_lo, t.tw_hi);
+    else
+      k_dft_cols<4><<<grid, plan.threads1, smem, st>>>(reinterpret_cast<const uint4*>(in),
+                                                       reinterpret_cast<uint4*>(scratch), log_chunk, log_h1, log_h2,
+                                                       log_h, plan.log_t1, t.tw_stage, t.tw_lo, t.tw_hi);
     count_launch();
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
   }
-  const int jt = pow2_clamp(budget / ((long)H2 * ebytes), 1, W);
-  const size_t smem = tw_bytes + (size_t)jt * H2 * ebytes;
-  dim3 grid(H1, W / jt);
-  if (lanes == 1) {
-    set_smem(k_dft_rows<1>, smem);
-    k_dft_rows<1><<<grid, 256, smem, st>>>(scratch, out, log_h1, log_h2, log_h, log_w, log2i(jt), t.tw_stage);
-  } else {
-    set_smem(k_dft_rows<4>, smem);
-    k_dft_rows<4><<<grid, 256, smem, st>>>(reinterpret_cast<const uint4*>(scratch), reinterpret_cast<uint4*>(out),
-                                           log_h1, log_h2, log_h, log_w, log2i(jt), t.tw_stage);
+  if (passes & 2) {
+    const int jt = 1 << plan.log_t2;
+    const size_t smem = kDftTwBytes + dft_tile_bytes(plan.log_t2, log_h2, lanes);
+    dim3 grid(H1, W / jt);
+    if (lanes == 1)
+      k_dft_rows<1><<<grid, plan.threads2, smem, st>>>(scratch, out, log_h1, log_h2, log_h, log_w, plan.log_t2,
+                                                       t.tw_stage);
+    else
+      k_dft_rows<4><<<grid, plan.threads2, smem, st>>>(reinterpret_cast<const uint4*>(scratch),
+                                                       reinterpret_cast<uint4*>(out), log_h1, log_h2, log_h, log_w,
+                                                       plan.log_t2, t.tw_stage);
+    count_launch();
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
   }
-  LAUNCH_DONE();
+  return cudaSuccess;
 }
 
 // ---------------------------------------------------------------------------
@@ -538,8 +608,8 @@ static int ilog2i(size_t v) {
 }
 
 // Leaf digests only (level 0): one thread per row, full occupancy, no barriers.
-template <int T, int RP, int RATE>
-__global__ void __launch_bounds__(256) k_leaf_digests(const uint32_t* __restrict__ rows, int row_words, size_t h,
+template <int T, int RP, int RATE, int CTA>
+__global__ void __launch_bounds__(CTA) k_leaf_digests(const uint32_t* __restrict__ rows, int row_words, size_t h,
                                                        uint32_t* __restrict__ digests,
                                                        const __grid_constant__ P2Consts leaf) {
   for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < h; i += (size_t)gridDim.x * blockDim.x) {
@@ -573,7 +643,8 @@ __global__ void __launch_bounds__(256) k_leaf_digests(const uint32_t* __restrict
 
 // Two tree levels per launch: each thread compresses four nodes of level l
 // into two nodes of level l+1 (written out) and their parent at level l+2.
-__global__ void __launch_bounds__(256) k_merkle_two_levels(uint32_t* __restrict__ digests, size_t in_off,
+template <int CTA>
+__global__ void __launch_bounds__(CTA) k_merkle_two_levels(uint32_t* __restrict__ digests, size_t in_off,
                                                             size_t in_count, const __grid_constant__ P2Consts comp) {
   const size_t out_count = in_count >> 2;
   const size_t mid_off = in_off + in_count, top_off = mid_off + (in_count >> 1);
@@ -694,18 +765,46 @@ __global__ void __launch_bounds__(TOP_CTA) k_merkle_top_coop(uint32_t* __restric
 // cooperative-permutation subtrees (k_merkle_top_coop) for the top. Smaller
 // trees hash their leaves with in-CTA subtrees and use the cooperative kernel
 // above those.
-constexpr size_t kLevelPairMin = (size_t)1 << 12;
+constexpr size_t kLevelPairMin = (size_t)kMerkleLevelPairMin;
 constexpr size_t kCoopTop = (size_t)1 << 15;
 
+// CTAs for `work` items at `threads` per CTA, capped at per_sm CTAs per SM
+// (per_sm 0: no cap)
+static unsigned grid_shape(size_t work, Shape sh) {
+  size_t b = (work + sh.threads - 1) / sh.threads;
+  if (sh.per_sm > 0) {
+    const size_t cap = (size_t)sm_count() * sh.per_sm;
+    if (b > cap) b = cap;
+  }
+  if (b < 1) b = 1;
+  return (unsigned)b;
+}
+
+Shape merkle_leaf_default() { return Shape{256, 16}; }
+Shape merkle_node_default() { return Shape{256, 16}; }
+
+template <int T, int RP, int RATE>
+static void launch_leaf_digests(const uint32_t* rows, int row_words, size_t h, uint32_t* digests,
+                                const P2Consts& k, Shape sh, cudaStream_t st) {
+  const unsigned blocks = grid_shape(h, sh);
+  if (sh.threads == 128)
+    k_leaf_digests<T, RP, RATE, 128><<<blocks, 128, 0, st>>>(rows, row_words, h, digests, k);
+  else if (sh.threads == 512)
+    k_leaf_digests<T, RP, RATE, 512><<<blocks, 512, 0, st>>>(rows, row_words, h, digests, k);
+  else
+    k_leaf_digests<T, RP, RATE, 256><<<blocks, 256, 0, st>>>(rows, row_words, h, digests, k);
+}
+
 cudaError_t merkle_leaves(const uint32_t* rows, int log_h, int row_words, int leaf_hash, uint32_t* digests,
-                          const P2Consts& p16, const P2Consts& p24, cudaStream_t st) {
+                          const P2Consts& p16, const P2Consts& p24, Shape leaf, cudaStream_t st) {
   const size_t h = (size_t)1 << log_h;
   if (h >= kLevelPairMin) {
-    const unsigned blocks = grid_for(h, 256, 16);
+    if ((leaf.threads != 128 && leaf.threads != 256 && leaf.threads != 512) || leaf.per_sm < 0)
+      return cudaErrorInvalidValue;
     if (leaf_hash == 0)
-      k_leaf_digests<24, p2::RP24, 16><<<blocks, 256, 0, st>>>(rows, row_words, h, digests, p24);
+      launch_leaf_digests<24, p2::RP24, 16>(rows, row_words, h, digests, p24, leaf, st);
     else
-      k_leaf_digests<16, p2::RP16, 8><<<blocks, 256, 0, st>>>(rows, row_words, h, digests, p16);
+      launch_leaf_digests<16, p2::RP16, 8>(rows, row_words, h, digests, p16, leaf, st);
     LAUNCH_DONE();
   }
   const int cta = (int)(h < (size_t)MERKLE_CTA ? h : (size_t)MERKLE_CTA);
@@ -718,13 +817,18 @@ cudaError_t merkle_leaves(const uint32_t* rows, int log_h, int row_words, int le
   LAUNCH_DONE();
 }
 
-cudaError_t merkle_upper(int log_h, uint32_t* digests, const P2Consts& p16, cudaStream_t st) {
+cudaError_t merkle_upper(int log_h, uint32_t* digests, const P2Consts& p16, Shape node, cudaStream_t st) {
   const size_t h = (size_t)1 << log_h;
   size_t off = 0, cnt = h;
   if (h >= kLevelPairMin) {
+    if ((node.threads != 128 && node.threads != 256) || node.per_sm < 0) return cudaErrorInvalidValue;
     while (cnt > kCoopTop) {
       const size_t out = cnt >> 2;
-      k_merkle_two_levels<<<grid_for(out, 256, 16), 256, 0, st>>>(digests, off, cnt, p16);
+      const unsigned blocks = grid_shape(out, node);
+      if (node.threads == 128)
+        k_merkle_two_levels<128><<<blocks, 128, 0, st>>>(digests, off, cnt, p16);
+      else
+        k_merkle_two_levels<256><<<blocks, 256, 0, st>>>(digests, off, cnt, p16);
       count_launch();
       cudaError_t e = cudaGetLastError();
       if (e != cudaSuccess) return e;
@@ -757,9 +861,9 @@ cudaError_t merkle_upper(int log_h, uint32_t* digests, const P2Consts& p16, cuda
 
 cudaError_t merkle_build(const uint32_t* rows, int log_h, int row_words, int leaf_hash, uint32_t* digests,
                          const P2Consts& p16, const P2Consts& p24, cudaStream_t st) {
-  cudaError_t e = merkle_leaves(rows, log_h, row_words, leaf_hash, digests, p16, p24, st);
+  cudaError_t e = merkle_leaves(rows, log_h, row_words, leaf_hash, digests, p16, p24, merkle_leaf_default(), st);
   if (e != cudaSuccess) return e;
-  return merkle_upper(log_h, digests, p16, st);
+  return merkle_upper(log_h, digests, p16, merkle_node_default(), st);
 }
 
 // Mmcs::open_batch gather (src/whir/prover/mod.rs:248-300, 378-401)
@@ -960,7 +1064,8 @@ cudaError_t dot_split(const uint32_t* f, int ext, int seg_bits, int m_bits, cons
 // src/poly/evals.rs:127-148, 382-400, 422-447)
 // ---------------------------------------------------------------------------
 
-__global__ void k_fold_ext(ef* __restrict__ a, ef* __restrict__ b, size_t half, ef r) {
+template <int CTA>
+__global__ void __launch_bounds__(CTA) k_fold_ext(ef* __restrict__ a, ef* __restrict__ b, size_t half, ef r) {
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < half; i += (size_t)gridDim.x * blockDim.x) {
     ef lo = ld_ef(a + i), hi = ld_ef(a + i + half);
     st_ef(a + i, kb::ef_add(lo, kb::ef_mul(kb::ef_sub(hi, lo), r)));
@@ -971,8 +1076,18 @@ __global__ void k_fold_ext(ef* __restrict__ a, ef* __restrict__ b, size_t half, 
   }
 }
 
-cudaError_t fold_ext(ef* a, ef* b, size_t half, ef r, cudaStream_t st) {
-  k_fold_ext<<<grid_for(half, 256), 256, 0, st>>>(a, b, half, r);
+Shape fold_default() { return Shape{256, 8}; }
+
+cudaError_t fold_ext(ef* a, ef* b, size_t half, ef r, Shape shape, cudaStream_t st) {
+  if (shape.per_sm < 0 || (shape.threads != 128 && shape.threads != 256 && shape.threads != 512))
+    return cudaErrorInvalidValue;
+  const unsigned blocks = grid_shape(half, shape);
+  if (shape.threads == 128)
+    k_fold_ext<128><<<blocks, 128, 0, st>>>(a, b, half, r);
+  else if (shape.threads == 256)
+    k_fold_ext<256><<<blocks, 256, 0, st>>>(a, b, half, r);
+  else
+    k_fold_ext<512><<<blocks, 512, 0, st>>>(a, b, half, r);
   LAUNCH_DONE();
 }
 

@@ -29,19 +29,50 @@ cudaError_t decode(uint32_t* p, size_t n, cudaStream_t st);
 // tables: tw_stage needs 2^11 words, tw_lo/tw_hi 2^12 words each
 cudaError_t build_dft_tables(uint32_t* tw_stage, uint32_t* tw_lo, uint32_t* tw_hi, int log_h, cudaStream_t st);
 
+// Launch plan of dft_batch. log_h2 = 0 selects the one-pass twisted kernel
+// (chunks of at most 2^12 points, 2^log_t1 columns per CTA); otherwise the
+// four-step split H = H1 * H2 with H2 = 2^log_h2, pass 1 transforming
+// 2^log_t1 length-H1 columns per CTA and pass 2 2^log_t2 length-H2 rows.
+struct DftPlan {
+  int log_h2;
+  int log_t1, threads1;
+  int log_t2, threads2;
+};
+// the fixed plan used when tuning is off (64 KiB tiles, 256 threads)
+DftPlan dft_default_plan(int log_chunk, int log_w, int log_blowup, int lanes);
+// every candidate plan the tuner may time for this shape (all pass dft_plan_ok)
+void dft_candidates(int log_chunk, int log_w, int log_blowup, int lanes, DftPlan* out, int* count, int cap);
+bool dft_plan_ok(const DftPlan& p, int log_chunk, int log_w, int log_blowup, int lanes);
+
 // transpose & pad & DFT: 2^log_w chunks of 2^log_chunk elements -> row-major
 // (2^(log_chunk+log_blowup)) x 2^log_w; `scratch` needs out-size elements.
+// `passes` selects the four-step passes to run (bit 0: pass 1, bit 1: pass 2;
+// 3 for the whole transform); only the tuner runs a single pass.
 cudaError_t dft_batch(const uint32_t* in, uint32_t* out, uint32_t* scratch, int log_chunk, int log_w,
-                      int log_blowup, int lanes, const DftTables& t, cudaStream_t st);
+                      int log_blowup, int lanes, const DftTables& t, const DftPlan& plan, int passes,
+                      cudaStream_t st);
+
+// Grid shape of a streaming kernel: threads per CTA and a cap on CTAs per SM
+// (0: one CTA per `threads` work items, no cap).
+struct Shape {
+  int threads;
+  int per_sm;
+};
 
 // Merkle tree: digests has (2h-1)*8 words, leaves first. leaf_hash 0: sponge
 // over Poseidon2-24 rate 16; 1: Poseidon2-16 rate 8. Compression: Poseidon2-16.
 cudaError_t merkle_build(const uint32_t* rows, int log_h, int row_words, int leaf_hash, uint32_t* digests,
                          const p2::P2Consts& p16, const p2::P2Consts& p24, cudaStream_t st);
-// the two halves of merkle_build: leaf hashing with the CTA subtrees, then the upper levels
+// the two halves of merkle_build: leaf hashing with the CTA subtrees, then the
+// upper levels. `leaf` shapes the leaf-digest kernel of trees with at least
+// kMerkleLevelPairMin leaves (threads 128, 256 or 512), `node` the two-level
+// compression kernel (threads 128 or 256).
+constexpr int kMerkleLevelPairMin = 1 << 12;
+Shape merkle_leaf_default();
+Shape merkle_node_default();
 cudaError_t merkle_leaves(const uint32_t* rows, int log_h, int row_words, int leaf_hash, uint32_t* digests,
-                          const p2::P2Consts& p16, const p2::P2Consts& p24, cudaStream_t st);
-cudaError_t merkle_upper(int log_h, uint32_t* digests, const p2::P2Consts& p16, cudaStream_t st);
+                          const p2::P2Consts& p16, const p2::P2Consts& p24, Shape leaf, cudaStream_t st);
+cudaError_t merkle_upper(int log_h, uint32_t* digests, const p2::P2Consts& p16, Shape node, cudaStream_t st);
 // gather opened rows and sibling paths for `count` indices
 cudaError_t merkle_open(const uint32_t* rows, const uint32_t* digests, int log_h, int row_words,
                         const uint64_t* d_idx, int count, uint32_t* d_rows_out, uint32_t* d_paths_out,
@@ -70,8 +101,10 @@ cudaError_t eq_outer(const kb::ef* hi, const kb::ef* lo, int lo_bits, size_t n, 
 cudaError_t dot_split(const uint32_t* f, int ext, int seg_bits, int m_bits, const kb::ef* hi, const kb::ef* lo,
                       int lo_bits, kb::ef* partials, kb::ef* out, cudaStream_t st);
 
-// compress (fold the first variable) on one or two extension arrays in place
-cudaError_t fold_ext(kb::ef* a, kb::ef* b, size_t half, kb::ef r, cudaStream_t st);
+// compress (fold the first variable) on one or two extension arrays in place;
+// `shape` threads 128, 256 or 512
+Shape fold_default();
+cudaError_t fold_ext(kb::ef* a, kb::ef* b, size_t half, kb::ef r, Shape shape, cudaStream_t st);
 // compress_ext: base evals of 2*half entries -> extension evals of half entries
 cudaError_t fold_base(const uint32_t* f, size_t half, kb::ef r, kb::ef* out, cudaStream_t st);
 // compress_multi: out[x] = sum_{y < 2^k} eqrs[y] * f[y*M + x]

@@ -199,22 +199,20 @@ int commit_matrix(whir_ctx* ctx, const uint32_t* d_src, int log_chunk, int log_w
   WH_TRY(wh::ensure_dft_tables(ctx, t->log_h, &tab));
   uint32_t* scratch = nullptr;
   WH_TRY_CUDA(cudaMallocAsync(&scratch, words * 4, ctx->stream));
-  cudaError_t e;
+  int s;
   {
     wh::StageTimer timer(ctx, wh::kStDft);
-    e = wk::dft_batch(d_src, t->rows, scratch, log_chunk, log_w, log_blowup, lanes, tab, ctx->stream);
+    s = wh::run_dft(ctx, d_src, t->rows, scratch, log_chunk, log_w, log_blowup, lanes, tab);
   }
   cudaFreeAsync(scratch, ctx->stream);
-  if (e == cudaErrorInvalidValue) return wh::set_error("unsupported DFT shape"), WHIR_ERR_INVALID;
-  WH_TRY_CUDA(e);
+  WH_TRY(s);
   {
     wh::StageTimer timer(ctx, wh::kStLeaves);
-    WH_TRY_CUDA(wk::merkle_leaves(t->rows, t->log_h, t->row_words, leaf_hash, t->digests, ctx->p16, ctx->p24,
-                                  ctx->stream));
+    WH_TRY(wh::run_merkle_leaves(ctx, t->rows, t->log_h, t->row_words, leaf_hash, t->digests));
   }
   {
     wh::StageTimer timer(ctx, wh::kStNodes);
-    WH_TRY_CUDA(wk::merkle_upper(t->log_h, t->digests, ctx->p16, ctx->stream));
+    WH_TRY(wh::run_merkle_upper(ctx, t->log_h, t->digests));
   }
   uint32_t r[8];
   WH_TRY(wh::fetch(ctx, r, t->digests + (2 * h - 2) * 8, 32));
@@ -267,7 +265,7 @@ int sumcheck_round(whir_ctx* ctx, wh::Chal& ch, Sumcheck& sd, ef* d_f, ef* d_w, 
   WH_TRY(observe_and_sample(ctx, ch, sd, c[0], c[1], pow_bits, &r));
   {
     wh::StageTimer timer(ctx, wh::kStSumcheck);
-    WH_TRY_CUDA(wk::fold_ext(d_f, d_w, half, r, ctx->stream));
+    WH_TRY(wh::run_fold(ctx, d_f, d_w, half, r));
   }
   *sum = extrapolate_012(c[0], kb::ef_sub(*sum, c[0]), c[1], r);
   *r_out = r;
