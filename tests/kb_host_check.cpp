@@ -1,8 +1,8 @@
 // Test harness (not product code): compiles the product's field header for the
 // host and prints results of its arithmetic for inputs read from stdin, so the
 // CPU test suite can check the Montgomery and extension arithmetic exactly.
-// Input lines: "mul a b", "ef a0 a1 a2 a3 b0 b1 b2 b3", "red hi lo" (canonical values
-// for mul/ef; raw 64-bit halves for red).
+// Input lines: "mul a b", "ef a0 a1 a2 a3 b0 b1 b2 b3", "red t", "shoup a w" (canonical
+// values for mul/ef; a raw 64-bit value for red; any 32-bit a and canonical w for shoup).
 #include <cstdio>
 #include <cstring>
 
@@ -22,6 +22,10 @@ int main() {
       kb::ef z = kb::ef_mul(x, y);
       std::printf("%u %u %u %u\n", kb::from_mont(z.c[0]), kb::from_mont(z.c[1]), kb::from_mont(z.c[2]),
                   kb::from_mont(z.c[3]));
+    } else if (!std::strcmp(op, "shoup")) {
+      unsigned a, w;
+      std::scanf("%u %u", &a, &w);
+      std::printf("%u\n", kb::mul_shoup(a, w, kb::shoup_const(w)));
     } else if (!std::strcmp(op, "red")) {
       unsigned long long t;
       std::scanf("%llu", &t);

@@ -61,3 +61,15 @@ def test_extension_mul(harness):
     got = run(harness, ["ef " + " ".join(map(str, a + b)) for a, b in cases])
     for (a, b), g in zip(cases, got):
         assert list(map(int, g.split())) == efmul(a, b)
+
+
+def test_shoup_constant_product_any_32bit_input(harness):
+    """mul_shoup(a, w, shoup_const(w)) = a * w mod p, fully reduced, for every
+    32-bit a (Montgomery states never exceed p, but the bound holds to 2^32)."""
+    rnd = random.Random(4)
+    ws = [0, 1, 2, P - 1, P - 2, (P - 1) // 2, 1 << 24] + [rnd.randrange(P) for _ in range(40)]
+    aa = [0, 1, P - 1, P, P + 1, 2 * P - 1, 2 * P, (1 << 32) - 1, (1 << 31)] + [rnd.randrange(1 << 32) for _ in range(60)]
+    pairs = [(a, w) for a in aa for w in ws]
+    got = run(harness, [f"shoup {a} {w}" for a, w in pairs])
+    for (a, w), g in zip(pairs, got):
+        assert int(g) == a * w % P, (a, w)

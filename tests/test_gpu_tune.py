@@ -38,18 +38,19 @@ def test_every_dft_plan_matches_oracle(pkg, gpu_ctx, oracle, log_chunk, log_w, l
 
 LEAF_SHAPES = [(128, 0), (128, 8), (128, 16), (256, 0), (256, 4), (256, 8), (256, 16), (512, 0), (512, 2), (512, 4),
                (512, 8)]
-NODE_SHAPES = [(128, 0), (128, 8), (128, 16), (256, 0), (256, 8), (256, 16)]
+NODE_SHAPES = [(t, s, v) for v in (0, 1) for t, s in [(128, 0), (128, 8), (128, 16), (256, 0), (256, 8), (256, 16)]]
 
 
-@pytest.mark.parametrize("leaf_hash,row_words", [(0, 16), (1, 8)])
-def test_every_merkle_shape_matches_oracle(pkg, gpu_ctx, oracle, leaf_hash, row_words):
-    log_h = 17  # leaf-digest kernel (>= 2^12 leaves) and one two-level launch (> 2^15 nodes)
-    rng = np.random.default_rng(77 + leaf_hash)
+# 2^17 and 2^13 leaves: leaf-digest kernel, two-level launches and either top
+# kernel; 2^12: the smallest leaf-digest tree; 2^9: in-CTA leaf subtrees
+@pytest.mark.parametrize("leaf_hash,row_words,log_h", [(0, 16, 17), (1, 8, 13), (0, 64, 12), (1, 16, 9)])
+def test_every_merkle_shape_matches_oracle(pkg, gpu_ctx, oracle, leaf_hash, row_words, log_h):
+    rng = np.random.default_rng(77 + leaf_hash + 10 * log_h)
     rows = rnd(rng, (1 << log_h) * row_words)
     root_ref, dig_ref = oracle.merkle(rows, log_h, row_words, leaf_hash)
     d_rows = pkg.DeviceArray.from_host(gpu_ctx, rows)
     d_dig = pkg.DeviceArray(gpu_ctx, dig_ref.size)
-    shapes = [(t, s, 256, 16) for t, s in LEAF_SHAPES] + [(256, 16, t, s) for t, s in NODE_SHAPES]
+    shapes = [(t, s, 256, 16, 1) for t, s in LEAF_SHAPES] + [(256, 16, t, s, v) for t, s, v in NODE_SHAPES]
     for sh in shapes:
         root = pkg.merkle_commit_shaped(gpu_ctx, d_rows, log_h, row_words, leaf_hash, sh, d_dig)
         assert np.array_equal(root, root_ref), sh

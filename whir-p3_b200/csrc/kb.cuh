@@ -71,6 +71,29 @@ KB_HD uint32_t reduce_wide(uint64_t t) {
 }
 
 KB_HD uint32_t mul(uint32_t a, uint32_t b) { return reduce((uint64_t)a * b); }
+// Montgomery product left in (0, 2p), without the final conditional
+// subtraction: valid for a * b < p * 2^32 (e.g. a < 2p, b < p), and its result
+// may feed one more such product as the operand below 2p.
+KB_HD uint32_t mul_lazy(uint32_t a, uint32_t b) {
+  const uint64_t t = (uint64_t)a * b;
+  const uint32_t lo = (uint32_t)t, hi = (uint32_t)(t >> 32);
+  return hi - mulhi(lo * P_INV, P) + P;
+}
+
+// Product by a constant w < p with Shoup's precomputed quotient (Shoup, NTL;
+// Harvey, "Faster arithmetic for number-theoretic transforms", 2014):
+// ws = floor(w * 2^32 / p), q = floor(a * ws / 2^32) <= floor(a * w / p) and
+// a * w - q * p < 2p for every 32-bit a, so one conditional subtraction
+// finishes. Three 32-bit multiplies (a*w, mulhi(a, ws), q*p as a multiply-add)
+// instead of Montgomery's four. With a in Montgomery form and w canonical the
+// result is the Montgomery form of the product.
+KB_HD uint32_t shoup_const(uint32_t w) { return (uint32_t)(((uint64_t)w << 32) / P); }
+KB_HD uint32_t mul_shoup(uint32_t a, uint32_t w, uint32_t ws) {
+  const uint32_t q = mulhi(a, ws);
+  const uint32_t r = a * w - q * P;
+  return umin32(r, r - P);
+}
+
 KB_HD uint32_t sqr(uint32_t a) { return mul(a, a); }
 KB_HD uint32_t to_mont(uint32_t x) { return mul(x, R2); }
 KB_HD uint32_t from_mont(uint32_t x) { return reduce((uint64_t)x); }

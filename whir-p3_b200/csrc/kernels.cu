@@ -711,7 +711,7 @@ __device__ __forceinline__ void coop_permute16(uint32_t (&x)[4], int q, const P2
     s = add(s, __shfl_xor_sync(0xffffffffu, s, 1));
     s = add(s, __shfl_xor_sync(0xffffffffu, s, 2));
 #pragma unroll
-    for (int j = 0; j < 4; j++) x[j] = add(s, mul(k.diag[4 * q + j], x[j]));
+    for (int j = 0; j < 4; j++) x[j] = add(s, mul_shoup(x[j], k.diag_c[4 * q + j], k.diag_s[4 * q + j]));
   }
 #pragma unroll 1
   for (int r = p2::RF / 2; r < p2::RF; r++) {
@@ -760,13 +760,55 @@ __global__ void __launch_bounds__(TOP_CTA) k_merkle_top_coop(uint32_t* __restric
   }
 }
 
+// Top of a tree in one CTA: a level of at most 2 * TOP1_CTA nodes is
+// compressed to the root, one thread (one whole permutation) per node pair,
+// each new level kept in shared memory for the next and written out.
+constexpr int TOP1_CTA = 1024;
+__global__ void __launch_bounds__(TOP1_CTA) k_merkle_top_cta(uint32_t* __restrict__ digests, size_t in_off,
+                                                              int in_count, const __grid_constant__ P2Consts comp) {
+  __shared__ uint4 sh[2 * TOP1_CTA];  // node i at sh[2i], sh[2i + 1]
+  const int t = threadIdx.x;
+  size_t off = in_off;
+  int cnt = in_count;
+  for (int level = 0; cnt > 1; level++) {
+    const int act = cnt >> 1;
+    uint32_t x[16];
+    if (t < act) {
+      const uint4* src = level == 0 ? reinterpret_cast<const uint4*>(digests + (off + 2 * (size_t)t) * 8) : sh + 4 * t;
+#pragma unroll
+      for (int q = 0; q < 4; q++) {
+        const uint4 v = src[q];
+        x[4 * q] = v.x;
+        x[4 * q + 1] = v.y;
+        x[4 * q + 2] = v.z;
+        x[4 * q + 3] = v.w;
+      }
+      p2::permute<16, p2::RP16>(x, comp);
+    }
+    __syncthreads();
+    off += cnt;
+    if (t < act) {
+      const uint4 a = make_uint4(x[0], x[1], x[2], x[3]), b = make_uint4(x[4], x[5], x[6], x[7]);
+      sh[2 * t] = a;
+      sh[2 * t + 1] = b;
+      uint4* dst = reinterpret_cast<uint4*>(digests + (off + t) * 8);
+      dst[0] = a;
+      dst[1] = b;
+    }
+    __syncthreads();
+    cnt = act;
+  }
+}
+
 // Trees with at least kLevelPairMin leaves are built as: leaf digests, then
-// two levels per launch while a level has more than kCoopTop nodes, then
-// cooperative-permutation subtrees (k_merkle_top_coop) for the top. Smaller
-// trees hash their leaves with in-CTA subtrees and use the cooperative kernel
-// above those.
+// two levels per launch while a level is wider than the top kernel takes, then
+// the top: either cooperative-permutation subtrees (k_merkle_top_coop, node
+// shape variant 0, from 2^15 nodes) or one CTA (k_merkle_top_cta, variant 1,
+// from 2^11 nodes). Smaller trees hash their leaves with in-CTA subtrees and
+// use the same top kernels above those.
 constexpr size_t kLevelPairMin = (size_t)kMerkleLevelPairMin;
 constexpr size_t kCoopTop = (size_t)1 << 15;
+constexpr size_t kCtaTop = (size_t)2 * TOP1_CTA;
 
 // CTAs for `work` items at `threads` per CTA, capped at per_sm CTAs per SM
 // (per_sm 0: no cap)
@@ -780,8 +822,8 @@ static unsigned grid_shape(size_t work, Shape sh) {
   return (unsigned)b;
 }
 
-Shape merkle_leaf_default() { return Shape{256, 16}; }
-Shape merkle_node_default() { return Shape{256, 16}; }
+Shape merkle_leaf_default() { return Shape{256, 16, 0}; }
+Shape merkle_node_default() { return Shape{256, 16, 0}; }
 
 template <int T, int RP, int RATE>
 static void launch_leaf_digests(const uint32_t* rows, int row_words, size_t h, uint32_t* digests,
@@ -820,9 +862,11 @@ cudaError_t merkle_leaves(const uint32_t* rows, int log_h, int row_words, int le
 cudaError_t merkle_upper(int log_h, uint32_t* digests, const P2Consts& p16, Shape node, cudaStream_t st) {
   const size_t h = (size_t)1 << log_h;
   size_t off = 0, cnt = h;
+  if (node.variant != 0 && node.variant != 1) return cudaErrorInvalidValue;
+  const size_t top = node.variant == 1 ? kCtaTop : kCoopTop;
   if (h >= kLevelPairMin) {
     if ((node.threads != 128 && node.threads != 256) || node.per_sm < 0) return cudaErrorInvalidValue;
-    while (cnt > kCoopTop) {
+    while (cnt > top) {
       const size_t out = cnt >> 2;
       const unsigned blocks = grid_shape(out, node);
       if (node.threads == 128)
@@ -842,6 +886,14 @@ cudaError_t merkle_upper(int log_h, uint32_t* digests, const P2Consts& p16, Shap
       off += cnt;
       cnt >>= 1;
     }
+  }
+  if (node.variant == 1) {
+    if (cnt > 1) {
+      k_merkle_top_cta<<<1, TOP1_CTA, 0, st>>>(digests, off, (int)cnt, p16);
+      count_launch();
+      return cudaGetLastError();
+    }
+    return cudaSuccess;
   }
   while (cnt > 1) {
     const int c2 = (int)(cnt < (size_t)TOP_NODES ? cnt : (size_t)TOP_NODES);
@@ -1076,7 +1128,7 @@ __global__ void __launch_bounds__(CTA) k_fold_ext(ef* __restrict__ a, ef* __rest
   }
 }
 
-Shape fold_default() { return Shape{256, 8}; }
+Shape fold_default() { return Shape{256, 8, 0}; }
 
 cudaError_t fold_ext(ef* a, ef* b, size_t half, ef r, Shape shape, cudaStream_t st) {
   if (shape.per_sm < 0 || (shape.threads != 128 && shape.threads != 256 && shape.threads != 512))

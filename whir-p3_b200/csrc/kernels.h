@@ -52,11 +52,13 @@ cudaError_t dft_batch(const uint32_t* in, uint32_t* out, uint32_t* scratch, int 
                       int log_blowup, int lanes, const DftTables& t, const DftPlan& plan, int passes,
                       cudaStream_t st);
 
-// Grid shape of a streaming kernel: threads per CTA and a cap on CTAs per SM
-// (0: one CTA per `threads` work items, no cap).
+// Grid shape of a streaming kernel: threads per CTA, a cap on CTAs per SM
+// (0: one CTA per `threads` work items, no cap) and a kernel variant where a
+// launcher has several.
 struct Shape {
   int threads;
   int per_sm;
+  int variant;
 };
 
 // Merkle tree: digests has (2h-1)*8 words, leaves first. leaf_hash 0: sponge
@@ -66,7 +68,9 @@ cudaError_t merkle_build(const uint32_t* rows, int log_h, int row_words, int lea
 // the two halves of merkle_build: leaf hashing with the CTA subtrees, then the
 // upper levels. `leaf` shapes the leaf-digest kernel of trees with at least
 // kMerkleLevelPairMin leaves (threads 128, 256 or 512), `node` the two-level
-// compression kernel (threads 128 or 256).
+// compression kernel (threads 128 or 256) and picks the top kernel (variant 0:
+// cooperative four-lane permutations in many CTAs; 1: one CTA, one
+// permutation per thread).
 constexpr int kMerkleLevelPairMin = 1 << 12;
 Shape merkle_leaf_default();
 Shape merkle_node_default();

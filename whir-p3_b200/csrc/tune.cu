@@ -4,7 +4,8 @@
 //   DFT:     four-step split (or the one-pass kernel), tile and CTA size of
 //            each pass, timed pass by pass;
 //   Merkle:  the leaf-digest kernel's batch width (threads per CTA and CTAs
-//            per SM) and the same for the two-level compression kernel;
+//            per SM), the same for the two-level compression kernel, and
+//            the kernel that finishes the top of the tree;
 //   fold:    threads per CTA and CTAs per SM of the in-place fold.
 // All candidates compute the same values (they only tile the same exact
 // arithmetic differently), so tuning changes timing, never results.
@@ -176,13 +177,16 @@ int tune_dft(whir_ctx* ctx, const Key& k, const uint32_t* in, uint32_t* out, uin
   return WHIR_OK;
 }
 
-const wk::Shape kLeafShapes[] = {{128, 0}, {128, 8},  {128, 16}, {256, 0}, {256, 4}, {256, 8},
-                                 {256, 16}, {512, 0}, {512, 2},  {512, 4}, {512, 8}};
-const wk::Shape kNodeShapes[] = {{128, 0}, {128, 8}, {128, 16}, {256, 0}, {256, 8}, {256, 16}};
-const wk::Shape kFoldShapes[] = {{128, 0}, {128, 16}, {256, 0}, {256, 4}, {256, 8},
-                                 {256, 16}, {512, 0}, {512, 2}, {512, 4}, {512, 8}};
+const wk::Shape kLeafShapes[] = {{128, 0, 0},  {128, 8, 0}, {128, 16, 0}, {256, 0, 0}, {256, 4, 0}, {256, 8, 0},
+                                 {256, 16, 0}, {512, 0, 0}, {512, 2, 0},  {512, 4, 0}, {512, 8, 0}};
+const wk::Shape kNodeShapes[] = {{128, 0, 0}, {128, 8, 0}, {128, 16, 0}, {256, 0, 0}, {256, 8, 0}, {256, 16, 0},
+                                 {128, 0, 1}, {128, 8, 1}, {128, 16, 1}, {256, 0, 1}, {256, 8, 1}, {256, 16, 1}};
+const wk::Shape kFoldShapes[] = {{128, 0, 0},  {128, 16, 0}, {256, 0, 0}, {256, 4, 0}, {256, 8, 0},
+                                 {256, 16, 0}, {512, 0, 0},  {512, 2, 0}, {512, 4, 0}, {512, 8, 0}};
 
-bool same(const wk::Shape& a, const wk::Shape& b) { return a.threads == b.threads && a.per_sm == b.per_sm; }
+bool same(const wk::Shape& a, const wk::Shape& b) {
+  return a.threads == b.threads && a.per_sm == b.per_sm && a.variant == b.variant;
+}
 
 // Looks up or tunes the shape for `k` among `shapes`; launch(s) runs shape s.
 template <size_t N>
@@ -191,13 +195,13 @@ int pick_shape(whir_ctx* ctx, const Key& k, const wk::Shape (&shapes)[N], const 
   whir_tune_entry e;
   *out = def;
   if (lookup(k, &e)) {
-    *out = wk::Shape{e.choice[0], e.choice[1]};
+    *out = wk::Shape{e.choice[0], e.choice[1], e.choice[2]};
     return WHIR_OK;
   }
   if (g_mode.load() != 1) return WHIR_OK;
   std::lock_guard<std::mutex> session(g_session);
   if (lookup(k, &e)) {
-    *out = wk::Shape{e.choice[0], e.choice[1]};
+    *out = wk::Shape{e.choice[0], e.choice[1], e.choice[2]};
     return WHIR_OK;
   }
   std::vector<float> ms;
@@ -213,6 +217,7 @@ int pick_shape(whir_ctx* ctx, const Key& k, const wk::Shape (&shapes)[N], const 
   e = entry_for(k);
   e.choice[0] = out->threads;
   e.choice[1] = out->per_sm;
+  e.choice[2] = out->variant;
   e.candidates = (int)N;
   e.ms_default = t_def;
   e.ms_best = found ? ms[bi] : t_def;
@@ -284,7 +289,7 @@ int run_fold(whir_ctx* ctx, ef* a, ef* b, size_t half, const ef& r) {
     const Key k{WHIR_TUNE_FOLD, ctx->device, lg, b ? 2 : 1, 0, 0};
     whir_tune_entry e;
     if (lookup(k, &e)) {
-      sh = wk::Shape{e.choice[0], e.choice[1]};
+      sh = wk::Shape{e.choice[0], e.choice[1], e.choice[2]};
     } else if (g_mode.load() == 1) {
       const size_t n = 2 * half * (b ? 2 : 1);
       ef* tmp = nullptr;
@@ -385,7 +390,7 @@ int whir_merkle_commit_shaped(whir_ctx* ctx, const uint32_t* d_rows, int32_t log
   WH_CHECK(d_rows && d_digests && shape && log_height >= 0 && log_height <= 30 && row_words > 0 &&
                (leaf_hash == 0 || leaf_hash == 1),
            "bad Merkle arguments");
-  const wk::Shape leaf{shape[0], shape[1]}, node{shape[2], shape[3]};
+  const wk::Shape leaf{shape[0], shape[1], 0}, node{shape[2], shape[3], shape[4]};
   cudaError_t e = wk::merkle_leaves(d_rows, log_height, row_words, leaf_hash, d_digests, ctx->p16, ctx->p24, leaf,
                                     ctx->stream);
   if (e == cudaErrorInvalidValue) return wh::set_error("invalid Merkle shape"), WHIR_ERR_INVALID;
@@ -408,7 +413,7 @@ int whir_fold_ext_shaped(whir_ctx* ctx, uint32_t* d_evals, int32_t n, const uint
   for (int i = 0; i < 4; i++) WH_CHECK(r[i] < kb::P, "non-canonical field element");
   const ef rm{{kb::to_mont(r[0]), kb::to_mont(r[1]), kb::to_mont(r[2]), kb::to_mont(r[3])}};
   const cudaError_t e = wk::fold_ext(reinterpret_cast<ef*>(d_evals), nullptr, (size_t)1 << (n - 1), rm,
-                                     wk::Shape{shape[0], shape[1]}, ctx->stream);
+                                     wk::Shape{shape[0], shape[1], 0}, ctx->stream);
   if (e == cudaErrorInvalidValue) return wh::set_error("invalid fold shape"), WHIR_ERR_INVALID;
   WH_TRY_CUDA(e);
   return WHIR_OK;
