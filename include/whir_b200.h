@@ -139,8 +139,9 @@ typedef struct {
   int32_t device;
   int32_t key[4];    /* DFT: log_chunk, log_width, log_blowup, lanes (1 or 4); Merkle leaves: log_height,
                         row_words, leaf_hash; nodes: log_height; fold: log2(pairs), arrays (1 or 2) */
-  int32_t choice[5]; /* DFT: log_h2 (0 = one pass), log_t1, threads1, log_t2, threads2; others: threads, per_sm,
-                        variant (Merkle nodes: 0 = cooperative top subtrees, 1 = one-CTA top) */
+  int32_t choice[7]; /* DFT: log_h2 (0 = one pass), log_t1, threads1, log_t2, threads2, reg1, reg2 (pass runs
+                        the register-resident kernel); others: threads, per_sm, variant (Merkle nodes:
+                        0 = cooperative top subtrees, 1 = one-CTA top) */
   int32_t candidates;
   float ms_default;  /* device time of the default shape */
   float ms_best;     /* device time of the chosen shape */
@@ -150,12 +151,12 @@ int whir_tune_get_mode(void);
 /* Returns the number of cached entries and writes min(count, cap). */
 int whir_tune_entries(whir_tune_entry* out, int32_t cap);
 int whir_tune_clear(void);
-/* Candidate DFT plans of a shape, 5 words each (the whir_tune_entry choice
+/* Candidate DFT plans of a shape, 7 words each (the whir_tune_entry choice
  * layout); returns the count and writes min(count, cap) plans. */
 int whir_dft_plans(int32_t log_chunk, int32_t log_width, int32_t log_blowup, int32_t ext, int32_t* plans,
                    int32_t cap);
 /* whir_dft_batch / whir_merkle_commit / whir_fold_ext with an explicit launch
- * shape instead of the tuned one: plan = 5 words as above; Merkle shape =
+ * shape instead of the tuned one: plan = 7 words as above; Merkle shape =
  * {leaf threads, leaf CTAs per SM, node threads, node CTAs per SM, top variant}; fold
  * shape = {threads, CTAs per SM} (CTAs per SM 0: no cap). */
 int whir_dft_batch_plan(whir_ctx* ctx, const uint32_t* d_chunks, int32_t log_chunk, int32_t log_width,

@@ -137,16 +137,30 @@ def test_dft_candidate_plans_are_in_bounds(pkg, log_chunk, log_w, log_blowup, ex
     assert plans, "the default plan is always a candidate"
     lanes = 4 if ext else 1
     log_h = log_chunk + log_blowup
-    for h2, t1, th1, t2, th2 in plans:
-        assert th1 in (128, 256, 512) and th2 in (128, 256, 512)
+    def reg_ok(m, lt, threads):
+        # register pass: 2^m points as E x G (E >= G) with G threads per vector and 2^lt
+        # vectors per CTA, holding 2^lt * E * (G + 1) words of shared memory (plus padding)
+        lg = m // 2
+        le = m - lg
+        return 8 <= m <= 12 and threads == 1 << (lg + lt) and (4 << lt) * (1 << le) * ((1 << lg) + 1) <= 128 * 1024
+
+    for h2, t1, th1, t2, th2, reg1, reg2 in plans:
         if h2 == 0:
+            assert not reg1 and not reg2 and th1 in (128, 256, 512)
             assert log_chunk <= 12 and 0 <= t1 <= log_w
             assert (4 * lanes << t1 << log_chunk) <= 128 * 1024
         else:
             h1 = log_h - h2
             assert 1 <= h2 <= min(12, log_chunk) and 0 <= h1 <= 12
-            assert 0 <= t1 <= h2 and (4 * lanes << t1 << h1) <= 128 * 1024
-            assert 0 <= t2 <= log_w and (4 * lanes << t2 << h2) <= 128 * 1024
+            assert 0 <= t1 <= h2 and 0 <= t2 <= log_w
+            if reg1:
+                assert lanes == 1 and 2 <= t1 <= 4 and reg_ok(h1, t1, th1)
+            else:
+                assert th1 in (128, 256, 512) and (4 * lanes << t1 << h1) <= 128 * 1024
+            if reg2:
+                assert lanes == 1 and t2 <= 4 and reg_ok(h2, t2, th2)
+            else:
+                assert th2 in (128, 256, 512) and (4 * lanes << t2 << h2) <= 128 * 1024
 
 
 def test_tune_mode_switch(pkg):

@@ -13,9 +13,10 @@ def rnd(rng, n):
     return rng.integers(0, P, n, dtype=np.uint64).astype(np.uint32)
 
 
-# one-pass shapes (chunk <= 2^12) and four-step shapes, base and extension
+# one-pass shapes (chunk <= 2^12) and four-step shapes, base and extension;
+# the base shapes with a pass of 2^8..2^12 points include register-pass plans
 PLAN_SHAPES = [(6, 3, 2, 0), (10, 2, 1, 0), (12, 1, 1, 1), (9, 4, 3, 1), (14, 3, 1, 0), (13, 2, 2, 1),
-               (16, 1, 1, 0)]
+               (16, 1, 1, 0), (18, 4, 1, 0), (20, 1, 4, 0)]
 
 
 @pytest.mark.parametrize("log_chunk,log_w,log_blowup,ext", PLAN_SHAPES)
@@ -109,13 +110,13 @@ def test_tuning_on_first_use(pkg, gpu_ctx, oracle):
         assert dft["key"] == [log_chunk, log_w, log_blowup, 1]
         # the chosen plan joins the fastest pass 1 and pass 2 of one split: each
         # pass is a candidate's, and the joined plan reproduces the oracle
-        h2, t1, th1, t2, th2 = dft["choice"]
+        h2, t1, th1, t2, th2, reg1, reg2 = dft["choice"]
         cands = pkg.dft_plans(log_chunk, log_w, log_blowup, False)
         if h2 == 0:
             assert any(c[:3] == (0, t1, th1) for c in cands)
         else:
-            assert any(c[:3] == (h2, t1, th1) for c in cands)
-            assert any(c[0] == h2 and c[3:] == (t2, th2) for c in cands)
+            assert any(c[:3] == (h2, t1, th1) and c[5] == reg1 for c in cands)
+            assert any(c[0] == h2 and c[3:5] == (t2, th2) and c[6] == reg2 for c in cands)
         pkg.dft_batch_plan(gpu_ctx, d_in, log_chunk, log_w, log_blowup, False, dft["choice"], d_out)
         assert np.array_equal(d_out.to_host(), want)
         # cached: a second call adds nothing and still matches

@@ -488,7 +488,7 @@ TUNE_KINDS = {1: "dft", 2: "merkle_leaves", 3: "merkle_nodes", 4: "fold"}
 
 
 class TuneEntry(C.Structure):
-    _fields_ = [("kind", C.c_int32), ("device", C.c_int32), ("key", C.c_int32 * 4), ("choice", C.c_int32 * 5),
+    _fields_ = [("kind", C.c_int32), ("device", C.c_int32), ("key", C.c_int32 * 4), ("choice", C.c_int32 * 7),
                 ("candidates", C.c_int32), ("ms_default", C.c_float), ("ms_best", C.c_float)]
 
 
@@ -516,11 +516,11 @@ def tune_entries() -> list[dict]:
 
 
 def dft_plans(log_chunk: int, log_width: int, log_blowup: int, ext: bool) -> list[tuple[int, ...]]:
-    """Candidate DFT plans (log_h2, log_t1, threads1, log_t2, threads2) the tuner times for a shape."""
+    """Candidate DFT plans (log_h2, log_t1, threads1, log_t2, threads2, reg1, reg2) the tuner times for a shape."""
     n = _check(lib().whir_dft_plans(log_chunk, log_width, log_blowup, int(ext), None, 0))
-    buf = np.zeros(max(n, 1) * 5, dtype=np.int32)
+    buf = np.zeros(max(n, 1) * 7, dtype=np.int32)
     _check(lib().whir_dft_plans(log_chunk, log_width, log_blowup, int(ext), buf.ctypes.data, n))
-    return [tuple(int(v) for v in buf[5 * i: 5 * i + 5]) for i in range(n)]
+    return [tuple(int(v) for v in buf[7 * i: 7 * i + 7]) for i in range(n)]
 
 
 def dft_batch_plan(ctx: Context, chunks: DeviceArray, log_chunk: int, log_width: int, log_blowup: int, ext: bool,

@@ -87,6 +87,7 @@ int ensure_dft_tables(whir_ctx* ctx, int log_h, wk::DftTables* t) {
     it = ctx->dft.emplace(log_h, c).first;
   }
   t->tw_stage = ctx->tw_stage;
+  t->tw_sh = reinterpret_cast<const uint2*>(ctx->tw_stage + 2048);
   t->tw_lo = it->second.tw_lo;
   t->tw_hi = it->second.tw_hi;
   return WHIR_OK;
@@ -307,7 +308,7 @@ int whir_ctx_create(int32_t device, const whir_poseidon2_params* p16, const whir
   if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess)
     return wh::set_error("stream creation failed"), fail(WHIR_ERR_CUDA);
   c->own_stream = true;
-  if (cudaMalloc(&c->tw_stage, 2048 * 4) != cudaSuccess || cudaMalloc(&c->d_partials, 8192 * sizeof(ef)) != cudaSuccess ||
+  if (cudaMalloc(&c->tw_stage, wk::kDftStageTableWords * 4) != cudaSuccess || cudaMalloc(&c->d_partials, 8192 * sizeof(ef)) != cudaSuccess ||
       cudaMalloc(&c->d_small, 256 * sizeof(ef)) != cudaSuccess || cudaMalloc(&c->d_words, 64) != cudaSuccess ||
       cudaMalloc(&c->d_arena, kArenaBytes) != cudaSuccess)
     return wh::set_error("device allocation failed"), fail(WHIR_ERR_NOMEM);

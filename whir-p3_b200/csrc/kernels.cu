@@ -142,6 +142,8 @@ __global__ void k_dft_tables(uint32_t* tw_stage, uint32_t* tw_lo, uint32_t* tw_h
   if (i < 4096) {
     tw_lo[i] = kb::pow(wh, (uint64_t)i);
     tw_hi[i] = kb::pow(wh_hi, (uint64_t)i);
+    const uint32_t c = kb::from_mont(kb::pow(w12, (uint64_t)i));
+    reinterpret_cast<uint2*>(tw_stage + 2048)[i] = make_uint2(c, kb::shoup_const(c));
   }
 }
 
@@ -342,6 +344,270 @@ __global__ void k_dft_coset(const typename Elem<LANES>::T* __restrict__ x, typen
   }
 }
 
+// ---------------------------------------------------------------------------
+// Register-resident DFT passes (base field). A length-N = E * G transform of
+// one vector is split as in the four-step method but inside the CTA: with
+// input index i = g + G*e and output index n = k + E*l,
+//   X[k + E*l] = sum_g omega_G^(g*l) * omega_N^(g*k) * sum_e x[g + G*e] * omega_E^(e*k).
+// G threads per vector each run the E-point inner DFT on registers (radix-2
+// decimation in frequency, twiddles from the constant bank, products in Shoup
+// form), multiply by omega_N^(g*k), and exchange through shared memory once;
+// then each thread runs E/G of the G-point outer DFTs on registers. Every
+// element is read and written once in shared memory per pass, against once
+// per three stages in the radix-2 kernel, and no index arithmetic runs per
+// butterfly.
+// ---------------------------------------------------------------------------
+
+namespace dftreg {
+
+constexpr uint32_t cpow(uint64_t b, uint64_t e) {
+  uint64_t r = 1;
+  while (e) {
+    if (e & 1) r = r * b % kb::P;
+    b = b * b % kb::P;
+    e >>= 1;
+  }
+  return (uint32_t)r;
+}
+// omega_64^j (canonical) and its Shoup constant, j < 32
+struct Tw64 {
+  uint32_t w[32];
+  uint32_t s[32];
+};
+constexpr Tw64 make_tw64() {
+  Tw64 t{};
+  const uint64_t g = cpow(3, (uint64_t)(kb::P - 1) / 64);
+  uint64_t cur = 1;
+  for (int j = 0; j < 32; j++) {
+    t.w[j] = (uint32_t)cur;
+    t.s[j] = (uint32_t)((cur << 32) / kb::P);
+    cur = cur * g % kb::P;
+  }
+  return t;
+}
+__constant__ Tw64 c_tw64 = make_tw64();
+
+__host__ __device__ constexpr int bitrev(int x, int bits) {
+  int r = 0;
+  for (int i = 0; i < bits; i++) r |= ((x >> i) & 1) << (bits - 1 - i);
+  return r;
+}
+
+// In-place DIF DFT of length 2^L <= 64 over registers: natural order in,
+// a[r] = X[bitrev_L(r)] out.
+template <int L>
+__device__ __forceinline__ void dif(uint32_t (&a)[1 << L]) {
+  constexpr int M = 1 << L;
+#pragma unroll
+  for (int half = M / 2; half >= 1; half >>= 1) {
+#pragma unroll
+    for (int start = 0; start < M; start += 2 * half) {
+#pragma unroll
+      for (int j = 0; j < half; j++) {
+        const uint32_t u = a[start + j], v = a[start + j + half];
+        a[start + j] = kb::add(u, v);
+        const uint32_t d = kb::sub(u, v);
+        const int tj = j * (32 / half);  // omega_{2*half}^j = omega_64^(j * 32 / half)
+        a[start + j + half] = tj == 0 ? d : kb::mul_shoup(d, c_tw64.w[tj], c_tw64.s[tj]);
+      }
+    }
+  }
+}
+
+// shared-memory layout of one vector: E rows (k) of G + 1 words (g); vectors
+// `vs` words apart with vs = rest (mod 32), so lanes of a warp that differ in
+// the vector or in k fall in different banks
+template <int E, int G>
+__host__ __device__ constexpr int vstride(int rest) {
+  return E * (G + 1) + ((rest - (E * (G + 1)) % 32) % 32 + 32) % 32;
+}
+
+}  // namespace dftreg
+
+// pass 1: T = 2^LT columns i2 per CTA, threads (t, g) with t fastest in both phases
+template <int LE, int LG, int LT>
+__global__ void __launch_bounds__(1 << (LG + LT))
+    k_dft_cols_reg(const uint32_t* __restrict__ x, uint32_t* __restrict__ y, int log_l, int log_h2, int log_h,
+                   const uint2* __restrict__ tw_sh, const uint32_t* __restrict__ tw_lo,
+                   const uint32_t* __restrict__ tw_hi) {
+  constexpr int E = 1 << LE, G = 1 << LG, T = 1 << LT, N = E * G;
+  constexpr int RS = G + 1;
+  constexpr int VS = dftreg::vstride<E, G>(T >= 32 ? 1 : 32 / T);
+  extern __shared__ uint32_t sm[];
+  const int H2 = 1 << log_h2;
+  const size_t L = (size_t)1 << log_l;
+  const int L1 = (int)(L >> log_h2);  // nonzero entries of each column vector
+  const int j = blockIdx.y;
+  const int i2_0 = blockIdx.x * T;
+  const int t = threadIdx.x & (T - 1), g = threadIdx.x >> LT;
+  {
+    uint32_t a[E];
+    const uint32_t* xj = x + (size_t)j * L + i2_0 + t;
+#pragma unroll
+    for (int e = 0; e < E; e++) {
+      const int i1 = g + G * e;
+      a[e] = i1 < L1 ? __ldg(xj + (size_t)i1 * H2) : 0u;
+    }
+    dftreg::dif<LE>(a);
+#pragma unroll
+    for (int r = 0; r < E; r++) {
+      constexpr int kshift = 12 - LE - LG;
+      const int k = dftreg::bitrev(r, LE);
+      uint32_t v = a[r];
+      if (k != 0) {
+        const uint2 w = __ldg(tw_sh + (((g * k) & (N - 1)) << kshift));
+        v = kb::mul_shoup(v, w.x, w.y);
+      }
+      sm[t * VS + k * RS + g] = v;
+    }
+  }
+  __syncthreads();
+  const size_t i2 = (size_t)(i2_0 + t);
+#pragma unroll
+  for (int q = 0; q < E / G; q++) {
+    const int k = g + G * q;
+    uint32_t b[G];
+#pragma unroll
+    for (int gg = 0; gg < G; gg++) b[gg] = sm[t * VS + k * RS + gg];
+    dftreg::dif<LG>(b);
+#pragma unroll
+    for (int r = 0; r < G; r++) {
+      const int r1 = k + E * dftreg::bitrev(r, LG);
+      const uint64_t ex = i2 * (uint64_t)r1;
+      uint32_t v = b[r];
+      if (ex) v = kb::mul(v, kb::mul(__ldg(tw_lo + (ex & 4095)), __ldg(tw_hi + (ex >> 12))));
+      y[((size_t)j << log_h) + ((size_t)r1 << log_h2) + i2] = v;
+    }
+  }
+}
+
+// pass 2: T = 2^LT columns j per CTA (one r1); loads with g fastest (rows are
+// contiguous in i2), outer DFTs and stores with t fastest (output rows are
+// contiguous in j)
+template <int LE, int LG, int LT>
+__global__ void __launch_bounds__(1 << (LG + LT))
+    k_dft_rows_reg(const uint32_t* __restrict__ y, uint32_t* __restrict__ out, int log_h1, int log_h, int log_w,
+                   const uint2* __restrict__ tw_sh) {
+  constexpr int E = 1 << LE, G = 1 << LG, T = 1 << LT, N = E * G;
+  constexpr int RS = G + 1;
+  constexpr int VS = dftreg::vstride<E, G>(T >= 32 ? 1 : 32 / T);
+  extern __shared__ uint32_t sm[];
+  const int r1 = blockIdx.x;
+  const int j0 = blockIdx.y * T;
+  {
+    const int g = threadIdx.x & (G - 1), t = threadIdx.x >> LG;
+    uint32_t a[E];
+    const uint32_t* src = y + ((size_t)(j0 + t) << log_h) + ((size_t)r1 * N) + g;
+#pragma unroll
+    for (int e = 0; e < E; e++) a[e] = __ldg(src + G * e);
+    dftreg::dif<LE>(a);
+#pragma unroll
+    for (int r = 0; r < E; r++) {
+      constexpr int kshift = 12 - LE - LG;
+      const int k = dftreg::bitrev(r, LE);
+      uint32_t v = a[r];
+      if (k != 0) {
+        const uint2 w = __ldg(tw_sh + (((g * k) & (N - 1)) << kshift));
+        v = kb::mul_shoup(v, w.x, w.y);
+      }
+      sm[t * VS + k * RS + g] = v;
+    }
+  }
+  __syncthreads();
+  const int t = threadIdx.x & (T - 1), gq = threadIdx.x >> LT;
+#pragma unroll
+  for (int q = 0; q < E / G; q++) {
+    const int k = gq + G * q;
+    uint32_t b[G];
+#pragma unroll
+    for (int gg = 0; gg < G; gg++) b[gg] = sm[t * VS + k * RS + gg];
+    dftreg::dif<LG>(b);
+#pragma unroll
+    for (int r = 0; r < G; r++) {
+      const size_t n = (size_t)(k + E * dftreg::bitrev(r, LG));
+      out[(((size_t)r1 + (n << log_h1)) << log_w) + j0 + t] = b[r];
+    }
+  }
+}
+
+// (LE, LG) of the register passes by length: E >= G, E * G = 2^m
+static bool reg_split(int m, int* le, int* lg) {
+  if (m < 8 || m > 12) return false;
+  *lg = m / 2;
+  *le = m - *lg;
+  return true;
+}
+static size_t reg_smem(int m, int lt) {
+  int le, lg;
+  if (!reg_split(m, &le, &lg)) return 0;
+  const int E = 1 << le, G = 1 << lg, T = 1 << lt;
+  const int rest = T >= 32 ? 1 : 32 / T;
+  const int vs = E * (G + 1) + ((rest - (E * (G + 1)) % 32) % 32 + 32) % 32;
+  return (size_t)T * vs * 4;
+}
+
+// The dynamic shared-memory limit is raised once per kernel instantiation (the
+// once-flag lives in each launcher instantiation; all instantiations share one
+// function-pointer type) to the same value, so concurrent contexts never race.
+constexpr int kDftRegSmemMax = 128 * 1024;  // plans keep register-pass tiles within this
+template <typename K>
+static void raise_smem(K kernel) {
+  cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kDftRegSmemMax);
+}
+
+template <int LE, int LG, int LT>
+static void launch_cols_reg(dim3 grid, size_t smem, cudaStream_t st, const uint32_t* x, uint32_t* y, int log_l,
+                            int log_h2, int log_h, const DftTables& t) {
+  static std::once_flag once;
+  std::call_once(once, [] { raise_smem(k_dft_cols_reg<LE, LG, LT>); });
+  k_dft_cols_reg<LE, LG, LT><<<grid, 1 << (LG + LT), smem, st>>>(x, y, log_l, log_h2, log_h, t.tw_sh, t.tw_lo,
+                                                                  t.tw_hi);
+}
+template <int LE, int LG, int LT>
+static void launch_rows_reg(dim3 grid, size_t smem, cudaStream_t st, const uint32_t* y, uint32_t* out, int log_h1,
+                            int log_h, int log_w, const DftTables& t) {
+  static std::once_flag once;
+  std::call_once(once, [] { raise_smem(k_dft_rows_reg<LE, LG, LT>); });
+  k_dft_rows_reg<LE, LG, LT><<<grid, 1 << (LG + LT), smem, st>>>(y, out, log_h1, log_h, log_w, t.tw_sh);
+}
+
+// supported (m, lt): pass 1 lt in {2, 3, 4}, pass 2 lt in {0, .., 4}
+#define WK_REG_CASES(F, m, lt, ...)                                      \
+  switch (m * 16 + lt) {                                                 \
+    case 8 * 16 + 0: F<4, 4, 0>(__VA_ARGS__); break;                     \
+    case 8 * 16 + 1: F<4, 4, 1>(__VA_ARGS__); break;                     \
+    case 8 * 16 + 2: F<4, 4, 2>(__VA_ARGS__); break;                     \
+    case 8 * 16 + 3: F<4, 4, 3>(__VA_ARGS__); break;                     \
+    case 8 * 16 + 4: F<4, 4, 4>(__VA_ARGS__); break;                     \
+    case 9 * 16 + 0: F<5, 4, 0>(__VA_ARGS__); break;                     \
+    case 9 * 16 + 1: F<5, 4, 1>(__VA_ARGS__); break;                     \
+    case 9 * 16 + 2: F<5, 4, 2>(__VA_ARGS__); break;                     \
+    case 9 * 16 + 3: F<5, 4, 3>(__VA_ARGS__); break;                     \
+    case 9 * 16 + 4: F<5, 4, 4>(__VA_ARGS__); break;                     \
+    case 10 * 16 + 0: F<5, 5, 0>(__VA_ARGS__); break;                    \
+    case 10 * 16 + 1: F<5, 5, 1>(__VA_ARGS__); break;                    \
+    case 10 * 16 + 2: F<5, 5, 2>(__VA_ARGS__); break;                    \
+    case 10 * 16 + 3: F<5, 5, 3>(__VA_ARGS__); break;                    \
+    case 10 * 16 + 4: F<5, 5, 4>(__VA_ARGS__); break;                    \
+    case 11 * 16 + 0: F<6, 5, 0>(__VA_ARGS__); break;                    \
+    case 11 * 16 + 1: F<6, 5, 1>(__VA_ARGS__); break;                    \
+    case 11 * 16 + 2: F<6, 5, 2>(__VA_ARGS__); break;                    \
+    case 11 * 16 + 3: F<6, 5, 3>(__VA_ARGS__); break;                    \
+    case 11 * 16 + 4: F<6, 5, 4>(__VA_ARGS__); break;                    \
+    case 12 * 16 + 0: F<6, 6, 0>(__VA_ARGS__); break;                    \
+    case 12 * 16 + 1: F<6, 6, 1>(__VA_ARGS__); break;                    \
+    case 12 * 16 + 2: F<6, 6, 2>(__VA_ARGS__); break;                    \
+    case 12 * 16 + 3: F<6, 6, 3>(__VA_ARGS__); break;                    \
+    default: break;                                                      \
+  }
+
+// threads of a register pass of length 2^m with 2^lt vectors per CTA
+static int reg_threads(int m, int lt) {
+  int le, lg;
+  if (!reg_split(m, &le, &lg)) return 0;
+  return 1 << (lg + lt);
+}
+
 static int pow2_clamp(long v, int lo, int hi) {
   int r = lo;
   while ((long)r * 2 <= v && r * 2 <= hi) r *= 2;
@@ -384,16 +650,29 @@ bool dft_plan_ok(const DftPlan& p, int log_chunk, int log_w, int log_blowup, int
   if (lanes != 1 && lanes != 4) return false;
   if (log_chunk < 0 || log_blowup < 0 || log_w < 0 || log_w > 15) return false;
   const int log_h = log_chunk + log_blowup;
-  if (log_h > 24 || !dft_threads_ok(p.threads1)) return false;
+  if (log_h > 24 || (!p.reg1 && !dft_threads_ok(p.threads1))) return false;
   if (p.log_h2 == 0) {  // one pass
+    if (p.reg1 || p.reg2) return false;
     return log_chunk <= 12 && p.log_t1 >= 0 && p.log_t1 <= log_w &&
            dft_tile_bytes(p.log_t1, log_chunk, lanes) <= kDftTileMax;
   }
   const int log_h1 = log_h - p.log_h2;
   if (p.log_h2 < 1 || p.log_h2 > 12 || p.log_h2 > log_chunk || log_h1 < 0 || log_h1 > 12) return false;
-  if (!dft_threads_ok(p.threads2)) return false;
-  if (p.log_t1 < 0 || p.log_t1 > p.log_h2 || dft_tile_bytes(p.log_t1, log_h1, lanes) > kDftTileMax) return false;
-  if (p.log_t2 < 0 || p.log_t2 > log_w || dft_tile_bytes(p.log_t2, p.log_h2, lanes) > kDftTileMax) return false;
+  if (p.log_t1 < 0 || p.log_t1 > p.log_h2 || p.log_t2 < 0 || p.log_t2 > log_w) return false;
+  if (p.reg1) {  // register pass 1: base field, 2^8..2^12 points, 4..16 columns per CTA
+    if (lanes != 1 || p.log_t1 < 2 || p.log_t1 > 4 || p.threads1 != reg_threads(log_h1, p.log_t1) ||
+        p.threads1 == 0 || reg_smem(log_h1, p.log_t1) > (size_t)kDftRegSmemMax)
+      return false;
+  } else if (dft_tile_bytes(p.log_t1, log_h1, lanes) > kDftTileMax) {
+    return false;
+  }
+  if (p.reg2) {  // register pass 2: base field, 2^8..2^12 points, 1..16 columns per CTA
+    if (lanes != 1 || p.log_t2 > 4 || p.threads2 != reg_threads(p.log_h2, p.log_t2) || p.threads2 == 0 ||
+        reg_smem(p.log_h2, p.log_t2) > (size_t)kDftRegSmemMax)
+      return false;
+  } else if (!dft_threads_ok(p.threads2) || dft_tile_bytes(p.log_t2, p.log_h2, lanes) > kDftTileMax) {
+    return false;
+  }
   return true;
 }
 
@@ -404,6 +683,7 @@ DftPlan dft_default_plan(int log_chunk, int log_w, int log_blowup, int lanes) {
   const int log_h = log_chunk + log_blowup;
   DftPlan p{};
   p.threads1 = p.threads2 = 256;
+  p.reg1 = p.reg2 = 0;
   const int max_single = lanes == 1 ? 12 : 11;
   if (log_chunk <= max_single) {
     p.log_h2 = 0;
@@ -440,17 +720,21 @@ void dft_candidates(int log_chunk, int log_w, int log_blowup, int lanes, DftPlan
   if (log_chunk <= 12) {
     for (int lt = 0; lt <= log_w; lt++)
       for (int th : threads)
-        if (tile_ok(lt, log_chunk)) push(DftPlan{0, lt, th, 0, 256});
+        if (tile_ok(lt, log_chunk)) push(DftPlan{0, lt, th, 0, 256, 0, 0});
   }
   for (int h2 = 4; h2 <= 12; h2++) {
     const int h1 = log_h - h2;
     if (h1 < 4 || h1 > 12 || h2 > log_chunk) continue;
     for (int t1 = 0; t1 <= 5 && t1 <= h2; t1++)
       for (int th1 : threads)
-        if (tile_ok(t1, h1)) push(DftPlan{h2, t1, th1, 0, 256});
+        if (tile_ok(t1, h1)) push(DftPlan{h2, t1, th1, 0, 256, 0, 0});
     for (int t2 = 0; t2 <= log_w; t2++)
       for (int th2 : threads)
-        if (tile_ok(t2, h2)) push(DftPlan{h2, 0, 256, t2, th2});
+        if (tile_ok(t2, h2)) push(DftPlan{h2, 0, 256, t2, th2, 0, 0});
+    if (lanes == 1) {
+      for (int t1 = 2; t1 <= 4; t1++) push(DftPlan{h2, t1, reg_threads(h1, t1), 0, 256, 1, 0});
+      for (int t2 = 0; t2 <= 4; t2++) push(DftPlan{h2, 0, 256, t2, reg_threads(h2, t2), 0, 1});
+    }
   }
   *count = n;
 }
@@ -477,7 +761,15 @@ cudaError_t dft_batch(const uint32_t* in, uint32_t* out, uint32_t* scratch, int 
   }
   const int log_h2 = plan.log_h2, log_h1 = log_h - log_h2;
   const int H1 = 1 << log_h1, H2 = 1 << log_h2;
-  if (passes & 1) {
+  if ((passes & 1) && plan.reg1) {
+    const int tile = 1 << plan.log_t1;
+    dim3 grid(H2 / tile, W);
+    WK_REG_CASES(launch_cols_reg, log_h1, plan.log_t1, grid, reg_smem(log_h1, plan.log_t1), st, in, scratch,
+                 log_chunk, log_h2, log_h, t)
+    count_launch();
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+  } else if (passes & 1) {
     const int tile = 1 << plan.log_t1;
     const size_t smem = kDftTwBytes + dft_tile_bytes(plan.log_t1, log_h1, lanes);
     dim3 grid(H2 / tile, W);
@@ -492,7 +784,15 @@ cudaError_t dft_batch(const uint32_t* in, uint32_t* out, uint32_t* scratch, int 
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
   }
-  if (passes & 2) {
+  if ((passes & 2) && plan.reg2) {
+    const int jt = 1 << plan.log_t2;
+    dim3 grid(H1, W / jt);
+    WK_REG_CASES(launch_rows_reg, log_h2, plan.log_t2, grid, reg_smem(log_h2, plan.log_t2), st, scratch, out,
+                 log_h1, log_h, log_w, t)
+    count_launch();
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+  } else if (passes & 2) {
     const int jt = 1 << plan.log_t2;
     const size_t smem = kDftTwBytes + dft_tile_bytes(plan.log_t2, log_h2, lanes);
     dim3 grid(H1, W / jt);

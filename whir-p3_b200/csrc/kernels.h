@@ -18,25 +18,32 @@ void count_launch();
 
 // small device-side tables owned by the caller
 struct DftTables {
-  const uint32_t* tw_stage;  // omega_{2^12}^k, k < 2^11
+  const uint32_t* tw_stage;  // omega_{2^12}^k, k < 2^11 (Montgomery)
+  const uint2* tw_sh;        // omega_{2^12}^k, k < 2^12: (canonical, Shoup constant)
   const uint32_t* tw_lo;     // omega_H^e, e < 2^12
   const uint32_t* tw_hi;     // omega_H^(e * 2^12), e < 2^12
 };
+// words of the per-context stage table: 2^11 Montgomery twiddles, then 2^12 Shoup pairs
+constexpr int kDftStageTableWords = 2048 + 2 * 4096;
 
 cudaError_t encode(uint32_t* p, size_t n, cudaStream_t st);
 cudaError_t decode(uint32_t* p, size_t n, cudaStream_t st);
 
-// tables: tw_stage needs 2^11 words, tw_lo/tw_hi 2^12 words each
+// tables: tw_stage needs kDftStageTableWords words, tw_lo/tw_hi 2^12 words each
 cudaError_t build_dft_tables(uint32_t* tw_stage, uint32_t* tw_lo, uint32_t* tw_hi, int log_h, cudaStream_t st);
 
 // Launch plan of dft_batch. log_h2 = 0 selects the one-pass twisted kernel
 // (chunks of at most 2^12 points, 2^log_t1 columns per CTA); otherwise the
 // four-step split H = H1 * H2 with H2 = 2^log_h2, pass 1 transforming
 // 2^log_t1 length-H1 columns per CTA and pass 2 2^log_t2 length-H2 rows.
+// A pass runs either the shared-memory radix-2 kernel (threads1/threads2 per
+// CTA) or, with reg1/reg2 set, the register-resident kernel, whose CTA size
+// is fixed by the pass length and tile.
 struct DftPlan {
   int log_h2;
   int log_t1, threads1;
   int log_t2, threads2;
+  int reg1, reg2;  // pass uses the register-resident kernel (base field, 2^8..2^12 points)
 };
 // the fixed plan used when tuning is off (64 KiB tiles, 256 threads)
 DftPlan dft_default_plan(int log_chunk, int log_w, int log_blowup, int lanes);

@@ -100,7 +100,7 @@ int time_all(whir_ctx* ctx, int count, int reps, const std::function<cudaError_t
 }
 
 wk::DftPlan plan_of(const whir_tune_entry& e) {
-  return wk::DftPlan{e.choice[0], e.choice[1], e.choice[2], e.choice[3], e.choice[4]};
+  return wk::DftPlan{e.choice[0], e.choice[1], e.choice[2], e.choice[3], e.choice[4], e.choice[5], e.choice[6]};
 }
 
 // Times every candidate plan of a DFT shape: one-pass plans whole, four-step
@@ -116,15 +116,15 @@ int tune_dft(whir_ctx* ctx, const Key& k, const uint32_t* in, uint32_t* out, uin
     int passes;
   };
   std::vector<Run> runs;
-  std::set<std::tuple<int, int, int, int>> seen;
+  std::set<std::tuple<int, int, int, int, int>> seen;
   for (int i = 0; i < nc; i++) {
     const wk::DftPlan& p = cand[i];
     if (p.log_h2 == 0) {
-      if (seen.insert(std::make_tuple(0, p.log_t1, p.threads1, 0)).second) runs.push_back({p, 3});
+      if (seen.insert(std::make_tuple(0, p.log_t1, p.threads1, 0, 0)).second) runs.push_back({p, 3});
       continue;
     }
-    if (seen.insert(std::make_tuple(p.log_h2, p.log_t1, p.threads1, 1)).second) runs.push_back({p, 1});
-    if (seen.insert(std::make_tuple(p.log_h2, p.log_t2, p.threads2, 2)).second) runs.push_back({p, 2});
+    if (seen.insert(std::make_tuple(p.log_h2, p.log_t1, p.threads1, p.reg1, 1)).second) runs.push_back({p, 1});
+    if (seen.insert(std::make_tuple(p.log_h2, p.log_t2, p.threads2, p.reg2, 2)).second) runs.push_back({p, 2});
   }
   std::vector<float> ms;
   WH_TRY(time_all(ctx, (int)runs.size(), kReps,
@@ -150,8 +150,10 @@ int tune_dft(whir_ctx* ctx, const Key& k, const uint32_t* in, uint32_t* out, uin
     int& slot = r.passes == 1 ? s.first : s.second;
     if (slot < 0 || ms[i] < ms[slot]) slot = i;
     if (def.log_h2 == r.p.log_h2) {
-      if (r.passes == 1 && r.p.log_t1 == def.log_t1 && r.p.threads1 == def.threads1) t_def += ms[i];
-      if (r.passes == 2 && r.p.log_t2 == def.log_t2 && r.p.threads2 == def.threads2) t_def += ms[i];
+      if (r.passes == 1 && r.p.log_t1 == def.log_t1 && r.p.threads1 == def.threads1 && r.p.reg1 == def.reg1)
+        t_def += ms[i];
+      if (r.passes == 2 && r.p.log_t2 == def.log_t2 && r.p.threads2 == def.threads2 && r.p.reg2 == def.reg2)
+        t_def += ms[i];
     }
   }
   for (const auto& kv : split) {
@@ -160,7 +162,8 @@ int tune_dft(whir_ctx* ctx, const Key& k, const uint32_t* in, uint32_t* out, uin
     const float tot = ms[a] + ms[b];
     if (tot < best) {
       best = tot;
-      *plan = wk::DftPlan{kv.first, runs[a].p.log_t1, runs[a].p.threads1, runs[b].p.log_t2, runs[b].p.threads2};
+      *plan = wk::DftPlan{kv.first,         runs[a].p.log_t1, runs[a].p.threads1, runs[b].p.log_t2,
+                          runs[b].p.threads2, runs[a].p.reg1,   runs[b].p.reg2};
     }
   }
   if (best >= kNever) *plan = def;
@@ -170,6 +173,8 @@ int tune_dft(whir_ctx* ctx, const Key& k, const uint32_t* in, uint32_t* out, uin
   e.choice[2] = plan->threads1;
   e.choice[3] = plan->log_t2;
   e.choice[4] = plan->threads2;
+  e.choice[5] = plan->reg1;
+  e.choice[6] = plan->reg2;
   e.candidates = (int)runs.size();
   e.ms_default = t_def;
   e.ms_best = best < kNever ? best : t_def;
@@ -355,11 +360,13 @@ int whir_dft_plans(int32_t log_chunk, int32_t log_width, int32_t log_blowup, int
   int nc = 0;
   wk::dft_candidates(log_chunk, log_width, log_blowup, ext ? 4 : 1, cand, &nc, 256);
   for (int i = 0; i < nc && i < cap; i++) {
-    plans[5 * i] = cand[i].log_h2;
-    plans[5 * i + 1] = cand[i].log_t1;
-    plans[5 * i + 2] = cand[i].threads1;
-    plans[5 * i + 3] = cand[i].log_t2;
-    plans[5 * i + 4] = cand[i].threads2;
+    plans[7 * i] = cand[i].log_h2;
+    plans[7 * i + 1] = cand[i].log_t1;
+    plans[7 * i + 2] = cand[i].threads1;
+    plans[7 * i + 3] = cand[i].log_t2;
+    plans[7 * i + 4] = cand[i].threads2;
+    plans[7 * i + 5] = cand[i].reg1;
+    plans[7 * i + 6] = cand[i].reg2;
   }
   return nc;
 }
@@ -369,7 +376,7 @@ int whir_dft_batch_plan(whir_ctx* ctx, const uint32_t* d_chunks, int32_t log_chu
   WH_TRY(tune_check_gpu(ctx));
   WH_CHECK(d_chunks && d_out && plan, "null argument");
   const int lanes = ext ? 4 : 1;
-  const wk::DftPlan p{plan[0], plan[1], plan[2], plan[3], plan[4]};
+  const wk::DftPlan p{plan[0], plan[1], plan[2], plan[3], plan[4], plan[5], plan[6]};
   WH_CHECK(wk::dft_plan_ok(p, log_chunk, log_width, log_blowup, lanes), "invalid DFT plan for this shape");
   const int log_h = log_chunk + log_blowup;
   wk::DftTables t;
