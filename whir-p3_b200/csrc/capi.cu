@@ -313,6 +313,7 @@ int whir_ctx_create(int32_t device, const whir_poseidon2_params* p16, const whir
       cudaMalloc(&c->d_arena, kArenaBytes) != cudaSuccess)
     return wh::set_error("device allocation failed"), fail(WHIR_ERR_NOMEM);
   c->arena_bytes = kArenaBytes;
+  if (cudaMemset(c->d_words, 0, 64) != cudaSuccess) return wh::set_error("device memset failed"), fail(WHIR_ERR_CUDA);
   if (cudaHostAlloc(&c->h_pinned, kPinnedBytes, cudaHostAllocDefault) != cudaSuccess)
     return wh::set_error("pinned allocation failed"), fail(WHIR_ERR_NOMEM);
   c->pinned_bytes = kPinnedBytes;

@@ -103,7 +103,7 @@ struct whir_ctx {
   // scratch
   kb::ef* d_partials = nullptr;  // 8192 ef
   kb::ef* d_small = nullptr;     // 256 ef
-  uint32_t* d_words = nullptr;   // 4 words (grind result, counter)
+  uint32_t* d_words = nullptr;   // 16 words: grind result and claim counter (0, 1), sumcheck round counter (8)
   void* d_arena = nullptr;       // general scratch (tables, gathers)
   size_t arena_bytes = 0;
   void* h_pinned = nullptr;      // staging for small transfers

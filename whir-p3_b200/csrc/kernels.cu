@@ -1304,10 +1304,29 @@ cudaError_t grind(const uint32_t* state, const uint32_t* in, int in_len, int bit
   count_launch();
   uint4 a = make_uint4(s[0], s[1], s[2], s[3]), b = make_uint4(s[4], s[5], s[6], s[7]);
   uint4 c = make_uint4(s[8], s[9], s[10], s[11]), d = make_uint4(s[12], s[13], s[14], s[15]);
-  // about 2^(bits+1) candidates in flight: enough to hide latency, little
-  // overshoot past the first witness for small `bits`
-  const uint64_t want = ((2ull << bits) + GRIND_CTA - 1) / GRIND_CTA;
-  const unsigned blocks = (unsigned)(want < (uint64_t)sm_count() * 8 ? want : (uint64_t)sm_count() * 8);
+  // Candidates in flight: once the smallest witness w is found, every claim
+  // already running still completes, so a search costs about w + W
+  // permutations for W in flight, while the rate grows with W. Expected cost
+  // (2^bits + W) / rate(W), minimised over CTAs per SM with the rates measured
+  // for Poseidon2-16 on B200 (relative to 8 CTAs of 256 per SM). Searches too
+  // small to fill the GPU keep about 2^(bits+1) candidates in flight.
+  static const int kPerSm[6] = {1, 2, 3, 4, 6, 8};
+  static const double kRate[6] = {0.892, 0.923, 0.946, 0.965, 0.986, 1.0};
+  const double expect = (double)(1ull << bits);
+  unsigned blocks = (unsigned)(((2ull << bits) + GRIND_CTA - 1) / GRIND_CTA);
+  if (blocks > (unsigned)sm_count()) {
+    double best = 0.0;
+    unsigned pick = (unsigned)sm_count();
+    for (int i = 0; i < 6; i++) {
+      const unsigned b = (unsigned)sm_count() * kPerSm[i];
+      const double cost = (expect + (double)b * GRIND_CTA) / kRate[i];
+      if (i == 0 || cost < best) {
+        best = cost;
+        pick = b;
+      }
+    }
+    if (pick < blocks) blocks = pick;
+  }
   k_grind<<<blocks, GRIND_CTA, 0, st>>>(p16, a, b, c, d, in_len, bits, limit, result, counter);
   LAUNCH_DONE();
 }
@@ -1505,6 +1524,78 @@ cudaError_t sumcheck_coeffs(const ef* f, const ef* w, size_t half, ef* partials,
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return e;
   k_sum_partials<<<2, 256, 0, st>>>(partials, (int)b, out);
+  LAUNCH_DONE();
+}
+
+// One launch per sumcheck round in the prover: optionally the previous
+// round's fold (FOLD: f, w hold 4q entries; f'(i) = f(i) + r (f(i + 2q) - f(i))
+// for i < 2q, in place, each thread owning i, i + q, i + 2q, i + 3q), then the
+// round's coefficients over the pairs (i, i + q) of the (folded) arrays. Each
+// CTA writes its two partial sums; the last CTA to finish (atomic counter, no
+// waiting) adds them up, writes out[0] = c0 and out[1] = c2, and re-arms the
+// counter, so no second launch is needed.
+template <bool FOLD>
+__global__ void __launch_bounds__(256) k_sumcheck_round(ef* __restrict__ f, ef* __restrict__ w, size_t q, ef r,
+                                                         ef* __restrict__ partials, unsigned* __restrict__ counter,
+                                                         ef* __restrict__ out) {
+  __shared__ ef sh[2][32];
+  __shared__ bool s_last;
+  ef v[2] = {kb::ef_zero(), kb::ef_zero()};
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < q; i += (size_t)gridDim.x * blockDim.x) {
+    ef el, eh, wl, wh;
+    if (FOLD) {
+      const ef fa = ld_ef(f + i), fb = ld_ef(f + i + 2 * q), fc = ld_ef(f + i + q), fd = ld_ef(f + i + 3 * q);
+      const ef wa = ld_ef(w + i), wb = ld_ef(w + i + 2 * q), wc = ld_ef(w + i + q), wd = ld_ef(w + i + 3 * q);
+      el = kb::ef_add(fa, kb::ef_mul(kb::ef_sub(fb, fa), r));
+      eh = kb::ef_add(fc, kb::ef_mul(kb::ef_sub(fd, fc), r));
+      wl = kb::ef_add(wa, kb::ef_mul(kb::ef_sub(wb, wa), r));
+      wh = kb::ef_add(wc, kb::ef_mul(kb::ef_sub(wd, wc), r));
+      st_ef(f + i, el);
+      st_ef(f + i + q, eh);
+      st_ef(w + i, wl);
+      st_ef(w + i + q, wh);
+    } else {
+      el = ld_ef(f + i);
+      eh = ld_ef(f + i + q);
+      wl = ld_ef(w + i);
+      wh = ld_ef(w + i + q);
+    }
+    v[0] = kb::ef_add(v[0], kb::ef_mul(el, wl));
+    v[1] = kb::ef_add(v[1], kb::ef_mul(kb::ef_sub(kb::ef_dbl(eh), el), kb::ef_sub(kb::ef_dbl(wh), wl)));
+  }
+  block_sum<2>(v, sh);
+  if (threadIdx.x == 0) {
+    partials[blockIdx.x] = v[0];
+    partials[gridDim.x + blockIdx.x] = v[1];
+    __threadfence();
+    s_last = atomicAdd(counter, 1u) == gridDim.x - 1;
+  }
+  __syncthreads();
+  if (!s_last) return;
+  __threadfence();
+  ef a[2] = {kb::ef_zero(), kb::ef_zero()};
+  for (unsigned b = threadIdx.x; b < gridDim.x; b += blockDim.x) {
+    const uint4 x0 = __ldcg(reinterpret_cast<const uint4*>(partials + b));
+    const uint4 x1 = __ldcg(reinterpret_cast<const uint4*>(partials + gridDim.x + b));
+    a[0] = kb::ef_add(a[0], ef{{x0.x, x0.y, x0.z, x0.w}});
+    a[1] = kb::ef_add(a[1], ef{{x1.x, x1.y, x1.z, x1.w}});
+  }
+  block_sum<2>(a, sh);
+  if (threadIdx.x == 0) {
+    out[0] = a[0];
+    out[1] = a[1];
+    *counter = 0u;
+  }
+}
+
+cudaError_t sumcheck_round(ef* f, ef* w, size_t q, int fold, ef r, ef* partials, unsigned* counter, ef* out,
+                           cudaStream_t st) {
+  if (q == 0) return cudaErrorInvalidValue;
+  const unsigned b = grid_for(q, 256, 8);
+  if (fold)
+    k_sumcheck_round<true><<<b, 256, 0, st>>>(f, w, q, r, partials, counter, out);
+  else
+    k_sumcheck_round<false><<<b, 256, 0, st>>>(f, w, q, r, partials, counter, out);
   LAUNCH_DONE();
 }
 

@@ -128,6 +128,14 @@ cudaError_t fold_multi_base(const uint32_t* f, int k, size_t m, const EqSmall& e
 cudaError_t sumcheck_coeffs(const kb::ef* f, const kb::ef* w, size_t half, kb::ef* partials, kb::ef* out,
                             cudaStream_t st);
 
+// One prover sumcheck round in one launch: with `fold`, first fold f and w
+// (4q entries each) in place by r into 2q entries; then out[0] = c0, out[1] =
+// c2 over the pairs (i, i + q). `partials` needs 2 * grid_for(q) entries and
+// `counter` (device, one word) must hold 0 before the first launch; the
+// kernel leaves it at 0.
+cudaError_t sumcheck_round(kb::ef* f, kb::ef* w, size_t q, int fold, kb::ef r, kb::ef* partials, unsigned* counter,
+                           kb::ef* out, cudaStream_t st);
+
 // The same reduction with the block count capped at max_blocks, so that the
 // partials fit a fixed-size buffer (2 * max_blocks entries).
 cudaError_t sumcheck_coeffs_capped(const kb::ef* f, const kb::ef* w, size_t half, kb::ef* partials,

@@ -251,22 +251,47 @@ int open_queries(whir_ctx* ctx, const Tree& t, const std::vector<uint64_t>& idx,
   return WHIR_OK;
 }
 
-// One ProductPolynomial::round on the device arrays f, w of 2^m entries
-int sumcheck_round(whir_ctx* ctx, wh::Chal& ch, Sumcheck& sd, ef* d_f, ef* d_w, int m, ef* sum, int pow_bits,
-                   ef* r_out) {
-  const size_t half = (size_t)1 << (m - 1);
+// A fold by the last sampled challenge that has not been applied yet. The
+// next sumcheck round applies it in the same launch as its coefficients;
+// flush_fold applies it before anything else reads f or w.
+struct PendingFold {
+  bool on = false;
+  ef r;
+  size_t half = 0;  // pairs folded: the arrays hold 2 * half entries before the fold
+};
+
+int flush_fold(whir_ctx* ctx, ef* d_f, ef* d_w, PendingFold& pend) {
+  if (!pend.on) return WHIR_OK;
   {
     wh::StageTimer timer(ctx, wh::kStSumcheck);
-    WH_TRY_CUDA(wk::sumcheck_coeffs(d_f, d_w, half, ctx->d_partials, ctx->d_small, ctx->stream));
+    WH_TRY(wh::run_fold(ctx, d_f, d_w, pend.half, pend.r));
   }
+  pend.on = false;
+  return WHIR_OK;
+}
+
+unsigned* round_counter(whir_ctx* ctx) { return reinterpret_cast<unsigned*>(ctx->d_words) + 8; }
+
+// One ProductPolynomial::round on the device arrays f, w of 2^m entries (of
+// 2^(m+1) entries still to be folded by pend.r when a fold is pending); leaves
+// this round's fold pending.
+int sumcheck_round(whir_ctx* ctx, wh::Chal& ch, Sumcheck& sd, ef* d_f, ef* d_w, int m, ef* sum, int pow_bits,
+                   ef* r_out, PendingFold& pend) {
+  const size_t half = (size_t)1 << (m - 1);
+  WH_CHECK(!pend.on || pend.half == 2 * half, "pending fold does not match the round size");
+  {
+    wh::StageTimer timer(ctx, wh::kStSumcheck);
+    WH_TRY_CUDA(wk::sumcheck_round(d_f, d_w, half, pend.on ? 1 : 0, pend.on ? pend.r : kb::ef_zero(),
+                                   ctx->d_partials, round_counter(ctx), ctx->d_small, ctx->stream));
+  }
+  pend.on = false;
   ef c[2];
   WH_TRY(wh::fetch(ctx, c, ctx->d_small, sizeof(c)));
   ef r;
   WH_TRY(observe_and_sample(ctx, ch, sd, c[0], c[1], pow_bits, &r));
-  {
-    wh::StageTimer timer(ctx, wh::kStSumcheck);
-    WH_TRY(wh::run_fold(ctx, d_f, d_w, half, r));
-  }
+  pend.on = true;
+  pend.r = r;
+  pend.half = half;
   *sum = extrapolate_012(c[0], kb::ef_sub(*sum, c[0]), c[1], r);
   *r_out = r;
   return WHIR_OK;
@@ -406,6 +431,8 @@ int do_prove(whir_ctx* ctx, whir_witness* wit, wh::Chal& ch) {
   }
 
   pf.push_back((uint32_t)c.n_rounds);
+  PendingFold pend;
+  WH_TRY_CUDA(cudaMemsetAsync(round_counter(ctx), 0, sizeof(unsigned), ctx->stream));
   Tree prev = wit->commit_tree;
   bool prev_owned = false;  // the commit tree belongs to the witness
   std::vector<ef> fold_rs = rs;
@@ -417,6 +444,7 @@ int do_prove(whir_ctx* ctx, whir_witness* wit, wh::Chal& ch) {
     const int log_blowup = ilog2u(new_dom) - nv;
     Tree nt;
     uint32_t root[8];
+    WH_TRY(flush_fold(ctx, d_f, d_w, pend));
     WH_TRY(commit_matrix(ctx, reinterpret_cast<const uint32_t*>(d_f), nv - ffn, ffn, log_blowup, 1,
                          wit->params.leaf_hash, &nt, root));
     for (int i = 0; i < 8; i++) ch.observe(ctx->hp16, kb::to_mont(root[i]));
@@ -480,7 +508,7 @@ int do_prove(whir_ctx* ctx, whir_witness* wit, wh::Chal& ch) {
     fold_rs.clear();
     for (int j = 0; j < ffn; j++) {
       ef r;
-      WH_TRY(sumcheck_round(ctx, ch, sd, d_f, d_w, nv - j, &sum, rc.folding_pow_bits, &r));
+      WH_TRY(sumcheck_round(ctx, ch, sd, d_f, d_w, nv - j, &sum, rc.folding_pow_bits, &r, pend));
       fold_rs.push_back(r);
     }
     sd.emit(pf);
@@ -494,6 +522,7 @@ int do_prove(whir_ctx* ctx, whir_witness* wit, wh::Chal& ch) {
   {
     const size_t fn = (size_t)1 << nv;
     std::vector<ef> fin(fn);
+    WH_TRY(flush_fold(ctx, d_f, d_w, pend));
     WH_TRY(wh::fetch(ctx, fin.data(), d_f, fn * sizeof(ef)));
     pf.push_back((uint32_t)fn);
     for (size_t i = 0; i < fn; i++) {
@@ -511,7 +540,7 @@ int do_prove(whir_ctx* ctx, whir_witness* wit, wh::Chal& ch) {
       Sumcheck sd;
       for (int j = 0; j < c.final_sumcheck_rounds; j++) {
         ef r;
-        WH_TRY(sumcheck_round(ctx, ch, sd, d_f, d_w, nv - j, &sum, c.final_folding_pow_bits, &r));
+        WH_TRY(sumcheck_round(ctx, ch, sd, d_f, d_w, nv - j, &sum, c.final_folding_pow_bits, &r, pend));
       }
       pf.push_back(1u);
       sd.emit(pf);
