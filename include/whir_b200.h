@@ -14,7 +14,10 @@
  *     whir_monty_encode / whir_monty_decode convert device buffers in place.
  *   - A whir_ctx owns one CUDA stream on one device; calls on a context are
  *     ordered on its stream and must come from one host thread at a time.
- *     Functions that return values to the host synchronize that stream.
+ *     Functions that return values to the host return once every earlier
+ *     operation on that stream has completed (small values arrive through
+ *     mapped host memory; a one-CTA copy kernel of the context may still be
+ *     retiring, and it touches only context-owned memory).
  *
  * Each entry point cites the reference interface it replaces (paths are
  * inside the reference project; Plonky3 items are at git rev c38eb05).

@@ -108,6 +108,12 @@ struct whir_ctx {
   size_t arena_bytes = 0;
   void* h_pinned = nullptr;      // staging for small transfers
   size_t pinned_bytes = 0;
+  // mailbox for small results: mapped host memory the GPU writes directly
+  // (payload, then a sequence flag), polled by the host instead of a copy and
+  // a stream synchronisation
+  uint32_t* h_mail = nullptr;
+  uint32_t* d_mail = nullptr;  // device alias of h_mail
+  uint32_t mail_seq = 0;
   // stage timing
   bool profiling = false;
   std::vector<cudaEvent_t> event_pool;

@@ -111,6 +111,19 @@ __device__ __forceinline__ void block_sum(ef (&v)[K], ef (&sh)[K][32]) {
   }
 }
 
+__global__ void k_publish(const uint32_t* __restrict__ src, int words, volatile uint32_t* mail, uint32_t seq) {
+  for (int i = threadIdx.x; i < words; i += blockDim.x) mail[i] = src[i];
+  __threadfence_system();
+  __syncthreads();
+  if (threadIdx.x == 0) mail[kMailWords] = seq;
+}
+
+cudaError_t publish(const uint32_t* src, int words, uint32_t* mail, uint32_t seq, cudaStream_t st) {
+  if (words < 0 || words > kMailWords) return cudaErrorInvalidValue;
+  k_publish<<<1, 128, 0, st>>>(src, words, mail, seq);
+  LAUNCH_DONE();
+}
+
 // out[i] = sum_{b < nparts} partials[i * nparts + b]
 __global__ void k_sum_partials(const ef* partials, int nparts, ef* out) {
   __shared__ ef sh[1][32];

@@ -26,6 +26,13 @@ struct DftTables {
 // words of the per-context stage table: 2^11 Montgomery twiddles, then 2^12 Shoup pairs
 constexpr int kDftStageTableWords = 2048 + 2 * 4096;
 
+// Mailbox of small results in mapped host memory: kMailWords payload words,
+// then the sequence flag at word kMailWords.
+constexpr int kMailWords = 512;
+// copy `words` (<= kMailWords) device words into the mailbox, then (after a
+// system-wide fence) write `seq` to the flag
+cudaError_t publish(const uint32_t* src, int words, uint32_t* mail, uint32_t seq, cudaStream_t st);
+
 cudaError_t encode(uint32_t* p, size_t n, cudaStream_t st);
 cudaError_t decode(uint32_t* p, size_t n, cudaStream_t st);
 
