@@ -103,13 +103,12 @@ int split_eq_tables(whir_ctx* ctx, const ef* z, int n, const ef& scale, int lo_b
   a.h = n - lo_bits;
   for (int i = 0; i < a.h; i++) a.z[i] = z[i];
   a.scale = scale;
-  WH_TRY_CUDA(wk::eq_table_small(a, hi, ctx->stream));
   wk::EqPoint b;
   memset(&b, 0, sizeof(b));
   b.h = lo_bits;
   for (int i = 0; i < lo_bits; i++) b.z[i] = z[n - lo_bits + i];
   b.scale = kb::ef_one();
-  WH_TRY_CUDA(wk::eq_table_small(b, lo, ctx->stream));
+  WH_TRY_CUDA(wk::eq_table_pair(a, hi, b, lo, ctx->stream));
   return WHIR_OK;
 }
 
@@ -123,7 +122,8 @@ int dot_eq(whir_ctx* ctx, const uint32_t* d_f, int ext, int seg_bits, const ef* 
   ef* hi = reinterpret_cast<ef*>(ctx->d_arena);
   ef* lo = hi + ((size_t)1 << (m_bits - lo_bits));
   WH_TRY(split_eq_tables(ctx, z, m_bits, kb::ef_one(), lo_bits, hi, lo));
-  WH_TRY_CUDA(wk::dot_split(d_f, ext, seg_bits, m_bits, hi, lo, lo_bits, ctx->d_partials, ctx->d_small, ctx->stream));
+  WH_TRY_CUDA(wk::dot_split(d_f, ext, seg_bits, m_bits, hi, lo, lo_bits, ctx->d_partials,
+                            reinterpret_cast<unsigned*>(ctx->d_words) + 9, ctx->d_small, ctx->stream));
   return WHIR_OK;
 }
 

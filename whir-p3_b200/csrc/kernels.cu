@@ -1362,6 +1362,29 @@ __global__ void k_eq_small(const __grid_constant__ EqPoint pt, ef* out) {
   }
 }
 
+// two eq tables in one launch (the hi and lo tables of a split point)
+__global__ void k_eq_pair(const __grid_constant__ EqPoint p1, ef* out1, const __grid_constant__ EqPoint p2, ef* out2) {
+  const size_t n1 = (size_t)1 << p1.h, n2 = (size_t)1 << p2.h;
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n1 + n2; i += (size_t)gridDim.x * blockDim.x) {
+    const EqPoint& pt = i < n1 ? p1 : p2;
+    const size_t x = i < n1 ? i : i - n1;
+    ef acc = pt.scale;
+    for (int j = 0; j < pt.h; j++) {
+      const ef& z = pt.z[j];
+      const bool bit = (x >> (pt.h - 1 - j)) & 1;
+      acc = kb::ef_mul(acc, bit ? z : kb::ef_sub(kb::ef_one(), z));
+    }
+    st_ef((i < n1 ? out1 : out2) + x, acc);
+  }
+}
+
+cudaError_t eq_table_pair(const EqPoint& p1, ef* out1, const EqPoint& p2, ef* out2, cudaStream_t st) {
+  if (p1.h < 0 || p1.h > 20 || p2.h < 0 || p2.h > 20) return cudaErrorInvalidValue;
+  const size_t n = ((size_t)1 << p1.h) + ((size_t)1 << p2.h);
+  k_eq_pair<<<grid_for(n, 256), 256, 0, st>>>(p1, out1, p2, out2);
+  LAUNCH_DONE();
+}
+
 cudaError_t eq_table_small(const EqPoint& pt, ef* out, cudaStream_t st) {
   if (pt.h < 0 || pt.h > 20) return cudaErrorInvalidValue;
   const size_t n = (size_t)1 << pt.h;
@@ -1394,13 +1417,41 @@ constexpr int DOT_CTA = 256;
 template <int EXT>
 __global__ void __launch_bounds__(DOT_CTA) k_dot_split(const uint32_t* __restrict__ f, int m_bits,
                                                         const ef* __restrict__ hi, const ef* __restrict__ lo,
-                                                        int lo_bits, ef* __restrict__ partials) {
+                                                        int lo_bits, int wide, ef* __restrict__ partials,
+                                                        unsigned* __restrict__ counter, ef* __restrict__ out) {
   __shared__ ef sh[1][32];
+  __shared__ bool s_last;
   const size_t M = (size_t)1 << m_bits;
   const int seg = blockIdx.y;
   const uint32_t lomask = (1u << lo_bits) - 1;
   ef total = kb::ef_zero();
-  if ((size_t)threadIdx.x < M || M >= DOT_CTA) {
+  if (!EXT && wide) {
+    // four consecutive base entries per thread and step (one 16-byte load):
+    // they share their high index (lo_bits >= 2), and the stride is a multiple
+    // of 2^lo_bits, so each of the four keeps its low index across steps
+    const uint32_t x0 = 4u * threadIdx.x;
+    ef acc[4];
+    kb::ef_acc lazy[4];
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+      acc[j] = kb::ef_zero();
+      lazy[j].clear();
+    }
+    const uint4* f4 = reinterpret_cast<const uint4*>(f + (size_t)seg * M);
+    for (size_t x = (size_t)blockIdx.x * DOT_CTA * 4 + x0; x < M; x += (size_t)gridDim.x * DOT_CTA * 4) {
+      const uint4 v = __ldg(f4 + (x >> 2));
+      const ef h = ld_ef(hi + (x >> lo_bits));
+      lazy[0].mac(h, v.x, acc[0]);
+      lazy[1].mac(h, v.y, acc[1]);
+      lazy[2].mac(h, v.z, acc[2]);
+      lazy[3].mac(h, v.w, acc[3]);
+    }
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+      lazy[j].fold(acc[j]);
+      total = kb::ef_add(total, kb::ef_mul(acc[j], ld_ef(lo + ((x0 + j) & lomask))));
+    }
+  } else if ((size_t)threadIdx.x < M || M >= DOT_CTA) {
     const uint32_t xl = threadIdx.x & lomask;
     ef acc = kb::ef_zero();
     kb::ef_acc lazy;
@@ -1419,27 +1470,44 @@ __global__ void __launch_bounds__(DOT_CTA) k_dot_split(const uint32_t* __restric
   }
   ef v[1] = {total};
   block_sum<1>(v, sh);
-  if (threadIdx.x == 0) partials[(size_t)seg * gridDim.x + blockIdx.x] = v[0];
+  // the last CTA to finish adds up every segment's partial sums
+  const unsigned nblocks = gridDim.x * gridDim.y;
+  if (threadIdx.x == 0) {
+    partials[(size_t)seg * gridDim.x + blockIdx.x] = v[0];
+    __threadfence();
+    s_last = atomicAdd(counter, 1u) == nblocks - 1;
+  }
+  __syncthreads();
+  if (!s_last) return;
+  __threadfence();
+  for (unsigned s2 = 0; s2 < gridDim.y; s2++) {
+    ef a[1] = {kb::ef_zero()};
+    for (unsigned b = threadIdx.x; b < gridDim.x; b += blockDim.x) {
+      const uint4 x = __ldcg(reinterpret_cast<const uint4*>(partials + (size_t)s2 * gridDim.x + b));
+      a[0] = kb::ef_add(a[0], ef{{x.x, x.y, x.z, x.w}});
+    }
+    block_sum<1>(a, sh);
+    if (threadIdx.x == 0) out[s2] = a[0];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) *counter = 0u;
 }
 
 cudaError_t dot_split(const uint32_t* f, int ext, int seg_bits, int m_bits, const ef* hi, const ef* lo, int lo_bits,
-                      ef* partials, ef* out, cudaStream_t st) {
-  if (lo_bits > 8 || lo_bits > m_bits) return cudaErrorInvalidValue;
+                      ef* partials, unsigned* counter, ef* out, cudaStream_t st) {
+  if (lo_bits > 8 || lo_bits > m_bits || seg_bits < 0 || seg_bits > 8) return cudaErrorInvalidValue;
   const size_t M = (size_t)1 << m_bits;
   const int segs = 1 << seg_bits;
-  unsigned bx = grid_for(M, DOT_CTA, 8);
+  const int wide = !ext && lo_bits >= 2 && M >= 4 * (size_t)DOT_CTA && ((uintptr_t)f & 15) == 0;
+  unsigned bx = grid_for(wide ? M / 4 : M, DOT_CTA, 8);
   unsigned cap = (unsigned)((sm_count() * 8 + segs - 1) / segs);
   if (bx > cap) bx = cap;
   if (bx < 1) bx = 1;
   dim3 grid(bx, segs);
   if (ext)
-    k_dot_split<1><<<grid, DOT_CTA, 0, st>>>(f, m_bits, hi, lo, lo_bits, partials);
+    k_dot_split<1><<<grid, DOT_CTA, 0, st>>>(f, m_bits, hi, lo, lo_bits, 0, partials, counter, out);
   else
-    k_dot_split<0><<<grid, DOT_CTA, 0, st>>>(f, m_bits, hi, lo, lo_bits, partials);
-  count_launch();
-  cudaError_t e = cudaGetLastError();
-  if (e != cudaSuccess) return e;
-  k_sum_partials<<<segs, 256, 0, st>>>(partials, (int)bx, out);
+    k_dot_split<0><<<grid, DOT_CTA, 0, st>>>(f, m_bits, hi, lo, lo_bits, wide, partials, counter, out);
   LAUNCH_DONE();
 }
 

@@ -113,11 +113,16 @@ cudaError_t eq_table_small(const EqPoint& pt, kb::ef* out, cudaStream_t st);
 // out[x] = hi[x >> lo_bits] * lo[x & (2^lo_bits - 1)]
 cudaError_t eq_outer(const kb::ef* hi, const kb::ef* lo, int lo_bits, size_t n, kb::ef* out, cudaStream_t st);
 
+// both tables of a split point in one launch
+cudaError_t eq_table_pair(const EqPoint& p1, kb::ef* out1, const EqPoint& p2, kb::ef* out2, cudaStream_t st);
+
 // segmented split-eq dot products:
 //   out[s] = sum_{x < M} f[s*M + x] * hi[x >> lo_bits] * lo[x & mask],  M = 2^m_bits, s < 2^seg_bits
-// f is base (ext=0) or extension (ext=1). partials needs blocks*2^seg_bits ef.
+// f is base (ext=0) or extension (ext=1). partials needs blocks*2^seg_bits ef
+// (at most 8 * SMs); the last CTA to finish reduces them into out, using
+// `counter` (device, one word, 0 before the first launch, left at 0).
 cudaError_t dot_split(const uint32_t* f, int ext, int seg_bits, int m_bits, const kb::ef* hi, const kb::ef* lo,
-                      int lo_bits, kb::ef* partials, kb::ef* out, cudaStream_t st);
+                      int lo_bits, kb::ef* partials, unsigned* counter, kb::ef* out, cudaStream_t st);
 
 // compress (fold the first variable) on one or two extension arrays in place;
 // `shape` threads 128, 256 or 512
