@@ -115,49 +115,79 @@ int split_eq_tables(whir_ctx* ctx, const ef* z, int n, const ef& scale, int lo_b
 // sum_x f[x] eq(z, x) for extension (ext=1) or base f of 2^n entries, split
 // into 2^seg_bits segments of 2^(n - seg_bits) (the point covers one segment).
 // Results (Montgomery) land in ctx->d_small[0 .. 2^seg_bits).
-int dot_eq(whir_ctx* ctx, const uint32_t* d_f, int ext, int seg_bits, const ef* z, int m_bits) {
+// The results also go to the mailbox when they fit: *posted receives the
+// sequence to wait for (0 when not posted).
+int dot_eq(whir_ctx* ctx, const uint32_t* d_f, int ext, int seg_bits, const ef* z, int m_bits, uint32_t* posted) {
   if (m_bits > 40) return set_error("dot_eq: size"), WHIR_ERR_INVALID;
   StageTimer timer(ctx, kStEval);
   const int lo_bits = std::min(m_bits, 8);
   ef* hi = reinterpret_cast<ef*>(ctx->d_arena);
   ef* lo = hi + ((size_t)1 << (m_bits - lo_bits));
   WH_TRY(split_eq_tables(ctx, z, m_bits, kb::ef_one(), lo_bits, hi, lo));
+  const bool post = posted && ctx->h_mail && (4 << seg_bits) <= wk::kMailWords;
+  const uint32_t seq = post ? mail_next(ctx) : 0u;
+  if (posted) *posted = seq;
   WH_TRY_CUDA(wk::dot_split(d_f, ext, seg_bits, m_bits, hi, lo, lo_bits, ctx->d_partials,
-                            reinterpret_cast<unsigned*>(ctx->d_words) + 9, ctx->d_small, ctx->stream));
+                            reinterpret_cast<unsigned*>(ctx->d_words) + 9, ctx->d_small, post ? ctx->d_mail : nullptr,
+                            seq, ctx->stream));
   return WHIR_OK;
 }
 
-// Small results come back through the mailbox: a one-CTA kernel queued after
-// the producer writes them into mapped host memory and then bumps a sequence
-// flag, which this thread polls (about 9 us per round trip on B200 against
-// 16 us for a copy plus a stream synchronisation). While polling it checks
-// the stream for errors and gives up after a minute without progress.
-int fetch_mail(whir_ctx* ctx, void* host, const void* dev, size_t bytes) {
+int mail_wait(whir_ctx* ctx, uint32_t seq, void* host, size_t bytes);
+
+// spin-loop hint: lets a sibling hardware thread run and lowers the cost of
+// polling
+inline void cpu_relax() {
+#if defined(__x86_64__) || defined(__i386__)
+  __builtin_ia32_pause();
+#elif defined(__aarch64__)
+  asm volatile("yield");
+#endif
+}
+
+// Small results come back through the mailbox: the producing kernel (or a
+// one-CTA copy kernel queued after it) writes them into mapped host memory and
+// then bumps a sequence flag, which this thread polls (about 9 us per round
+// trip on B200 against 16 us for a copy plus a stream synchronisation).
+uint32_t mail_next(whir_ctx* ctx) {
   uint32_t seq = ++ctx->mail_seq;
   if (seq == 0) seq = ++ctx->mail_seq;
+  return seq;
+}
+
+int fetch_mail(whir_ctx* ctx, void* host, const void* dev, size_t bytes) {
+  const uint32_t seq = mail_next(ctx);
   WH_TRY_CUDA(wk::publish(static_cast<const uint32_t*>(dev), (int)((bytes + 3) / 4), ctx->d_mail, seq, ctx->stream));
+  return mail_wait(ctx, seq, host, bytes);
+}
+
+// Waits until the mailbox flag reaches `seq` and copies `bytes` of payload.
+int mail_wait(whir_ctx* ctx, uint32_t seq, void* host, size_t bytes) {
   volatile uint32_t* flag = ctx->h_mail + wk::kMailWords;
+  // Poll for a short while (typical results arrive within tens of
+  // microseconds); past that, block in a stream synchronisation instead of
+  // spinning, so that many waiting contexts (batch workers) do not take the
+  // host's cores from each other. The result is posted before the stream
+  // completes, so it is in place once the synchronisation returns.
   const auto t0 = std::chrono::steady_clock::now();
   for (uint64_t n = 1; *flag != seq; n++) {
-    if ((n & 1023) == 0) {
-      const cudaError_t e = cudaStreamQuery(ctx->stream);
-      if (e != cudaSuccess && e != cudaErrorNotReady) {
-        set_error(std::string("waiting for a device result: ") + cudaGetErrorString(e));
-        return WHIR_ERR_CUDA;
-      }
-      if (e == cudaSuccess && *flag != seq) {
+    cpu_relax();
+    if ((n & 255) == 0 && std::chrono::steady_clock::now() - t0 > std::chrono::microseconds(30)) {
+      WH_TRY_CUDA(cudaStreamSynchronize(ctx->stream));
+      if (*flag != seq) {
         set_error("device result missing after the stream completed");
         return WHIR_ERR_CUDA;
       }
-      if (std::chrono::steady_clock::now() - t0 > std::chrono::seconds(60)) {
-        set_error("timed out waiting for a device result");
-        return WHIR_ERR_CUDA;
-      }
+      break;
     }
   }
   std::atomic_thread_fence(std::memory_order_acquire);
   memcpy(host, const_cast<const uint32_t*>(ctx->h_mail), bytes);
   return WHIR_OK;
+}
+
+int fetch_posted(whir_ctx* ctx, uint32_t seq, void* host, const void* dev, size_t bytes) {
+  return seq ? mail_wait(ctx, seq, host, bytes) : fetch(ctx, host, dev, bytes);
 }
 
 int fetch(whir_ctx* ctx, void* host, const void* dev, size_t bytes) {
@@ -195,12 +225,14 @@ int grind(whir_ctx* ctx, Chal& ch, int bits, uint32_t* witness) {
   }
   WH_CHECK(bits <= 30, "grinding bits above 30");
   // inputs pending beyond 7 never occur (8 inputs trigger a duplexing)
+  const uint32_t seq = ctx->h_mail ? mail_next(ctx) : 0u;
   {
     StageTimer t(ctx, kStGrind);
-    WH_TRY_CUDA(wk::grind(ch.st, ch.in, ch.in_len, bits, kb::P, ctx->d_words, ctx->d_words + 1, ctx->p16, ctx->stream));
+    WH_TRY_CUDA(wk::grind(ch.st, ch.in, ch.in_len, bits, kb::P, ctx->d_words, ctx->d_words + 1, ctx->d_words + 2,
+                          ctx->h_mail ? ctx->d_mail : nullptr, seq, ctx->p16, ctx->stream));
   }
   uint32_t w = 0;
-  WH_TRY(fetch(ctx, &w, ctx->d_words, 4));
+  WH_TRY(fetch_posted(ctx, ctx->h_mail ? seq : 0u, &w, ctx->d_words, 4));
   if (w >= kb::P) {
     set_error("proof-of-work search found no witness");
     return WHIR_ERR_NOT_FOUND;
@@ -643,9 +675,10 @@ static int eval_common(whir_ctx* ctx, const uint32_t* d_evals, int32_t n, const 
   WH_CHECK(canon_ok(point, 4 * (size_t)n), "value out of range");
   std::vector<ef> z(n > 0 ? n : 1);
   for (int i = 0; i < n; i++) z[i] = load_ef_canon(point + 4 * i);
-  WH_TRY(wh::dot_eq(ctx, d_evals, ext, 0, z.data(), n));
+  uint32_t posted = 0;
+  WH_TRY(wh::dot_eq(ctx, d_evals, ext, 0, z.data(), n, &posted));
   ef r;
-  WH_TRY(wh::fetch(ctx, &r, ctx->d_small, sizeof(ef)));
+  WH_TRY(wh::fetch_posted(ctx, posted, &r, ctx->d_small, sizeof(ef)));
   store_ef_canon(out, r);
   return WHIR_OK;
 }
@@ -735,9 +768,10 @@ int whir_svo_partial_evals(whir_ctx* ctx, const uint32_t* d_poly, int32_t n, int
   WH_CHECK(canon_ok(point, 4 * (size_t)n), "value out of range");
   std::vector<ef> z(n > 0 ? n : 1);
   for (int i = 0; i < n; i++) z[i] = load_ef_canon(point + 4 * i);
-  WH_TRY(wh::dot_eq(ctx, d_poly, 0, l, z.data() + l, n - l));
+  uint32_t posted = 0;
+  WH_TRY(wh::dot_eq(ctx, d_poly, 0, l, z.data() + l, n - l, &posted));
   std::vector<ef> g((size_t)1 << l);
-  WH_TRY(wh::fetch(ctx, g.data(), ctx->d_small, g.size() * sizeof(ef)));
+  WH_TRY(wh::fetch_posted(ctx, posted, g.data(), ctx->d_small, g.size() * sizeof(ef)));
   ef eval = kb::ef_zero();
   wk::EqSmall e = wh::eq_small_host(z.data(), l);
   for (size_t y = 0; y < g.size(); y++) {

@@ -134,6 +134,12 @@ struct StageTimer {
 
 int ensure_dft_tables(whir_ctx* ctx, int log_h, wk::DftTables* t);
 int fetch(whir_ctx* ctx, void* host, const void* dev, size_t bytes);
+// mailbox: the next sequence number, a wait for a posted result, and a fetch
+// that waits for `seq` when it is nonzero (else copies `dev`)
+uint32_t mail_next(whir_ctx* ctx);
+int mail_wait(whir_ctx* ctx, uint32_t seq, void* host, size_t bytes);
+int fetch_posted(whir_ctx* ctx, uint32_t seq, void* host, const void* dev, size_t bytes);
+int dot_eq(whir_ctx* ctx, const uint32_t* d_f, int ext, int seg_bits, const kb::ef* z, int m_bits, uint32_t* posted);
 
 // Tuned launches (launch shapes chosen per shape on first use, process-wide)
 int run_dft(whir_ctx* ctx, const uint32_t* in, uint32_t* out, uint32_t* scratch, int log_chunk, int log_w,

@@ -111,6 +111,13 @@ __device__ __forceinline__ void block_sum(ef (&v)[K], ef (&sh)[K][32]) {
   }
 }
 
+// Mailbox write by one thread: payload, a system-wide fence, then the flag.
+__device__ __forceinline__ void mail_post(volatile uint32_t* mail, const uint32_t* src, int words, uint32_t seq) {
+  for (int i = 0; i < words; i++) mail[i] = src[i];
+  __threadfence_system();
+  mail[kMailWords] = seq;
+}
+
 __global__ void k_publish(const uint32_t* __restrict__ src, int words, volatile uint32_t* mail, uint32_t seq) {
   for (int i = threadIdx.x; i < words; i += blockDim.x) mail[i] = src[i];
   __threadfence_system();
@@ -1272,7 +1279,8 @@ constexpr int GRIND_CTA = 256;
 // Each claim is GRIND_CTA consecutive candidates, one per thread.
 __global__ void __launch_bounds__(GRIND_CTA) k_grind(const __grid_constant__ P2Consts p16, uint4 st0, uint4 st1,
                                                       uint4 st2, uint4 st3, int slot, int bits, uint64_t limit,
-                                                      uint32_t* result, uint32_t* counter) {
+                                                      uint32_t* result, uint32_t* counter, uint32_t* done,
+                                                      uint32_t* mail, uint32_t seq) {
   __shared__ uint64_t s_start;
   __shared__ int s_go;
   const uint32_t mask = (1u << bits) - 1u;
@@ -1288,7 +1296,18 @@ __global__ void __launch_bounds__(GRIND_CTA) k_grind(const __grid_constant__ P2C
     const uint64_t start = s_start;
     const int go = s_go;
     __syncthreads();
-    if (!go) return;
+    if (!go) {
+      // every atomicMin of this CTA precedes the barriers above; the last CTA
+      // to stop holds the final result and posts it to the mailbox
+      if (threadIdx.x == 0 && mail) {
+        __threadfence();
+        if (atomicAdd(done, 1u) == gridDim.x - 1) {
+          const uint32_t r = atomicAdd(result, 0u);
+          mail_post(mail, &r, 1, seq);
+        }
+      }
+      return;
+    }
     const uint64_t w = start + threadIdx.x;
     if (w < limit) {
       uint32_t s[16];
@@ -1301,19 +1320,21 @@ __global__ void __launch_bounds__(GRIND_CTA) k_grind(const __grid_constant__ P2C
   }
 }
 
-__global__ void k_grind_init(uint32_t* result, uint32_t* counter) {
+__global__ void k_grind_init(uint32_t* result, uint32_t* counter, uint32_t* done) {
   *result = kb::P;
   *counter = 0u;
+  *done = 0u;
 }
 
 cudaError_t grind(const uint32_t* state, const uint32_t* in, int in_len, int bits, uint64_t limit,
-                  uint32_t* result, uint32_t* counter, const P2Consts& p16, cudaStream_t st) {
+                  uint32_t* result, uint32_t* counter, uint32_t* done, uint32_t* mail, uint32_t seq,
+                  const P2Consts& p16, cudaStream_t st) {
   if (in_len < 0 || in_len > 7 || bits < 0 || bits > 30) return cudaErrorInvalidValue;
   if (limit > kb::P) limit = kb::P;
   uint32_t s[16];
   for (int i = 0; i < 16; i++) s[i] = state[i];
   for (int i = 0; i < in_len; i++) s[i] = in[i];
-  k_grind_init<<<1, 1, 0, st>>>(result, counter);
+  k_grind_init<<<1, 1, 0, st>>>(result, counter, done);
   count_launch();
   uint4 a = make_uint4(s[0], s[1], s[2], s[3]), b = make_uint4(s[4], s[5], s[6], s[7]);
   uint4 c = make_uint4(s[8], s[9], s[10], s[11]), d = make_uint4(s[12], s[13], s[14], s[15]);
@@ -1340,7 +1361,7 @@ cudaError_t grind(const uint32_t* state, const uint32_t* in, int in_len, int bit
     }
     if (pick < blocks) blocks = pick;
   }
-  k_grind<<<blocks, GRIND_CTA, 0, st>>>(p16, a, b, c, d, in_len, bits, limit, result, counter);
+  k_grind<<<blocks, GRIND_CTA, 0, st>>>(p16, a, b, c, d, in_len, bits, limit, result, counter, done, mail, seq);
   LAUNCH_DONE();
 }
 
@@ -1418,7 +1439,8 @@ template <int EXT>
 __global__ void __launch_bounds__(DOT_CTA) k_dot_split(const uint32_t* __restrict__ f, int m_bits,
                                                         const ef* __restrict__ hi, const ef* __restrict__ lo,
                                                         int lo_bits, int wide, ef* __restrict__ partials,
-                                                        unsigned* __restrict__ counter, ef* __restrict__ out) {
+                                                        unsigned* __restrict__ counter, ef* __restrict__ out,
+                                                        uint32_t* mail, uint32_t seq) {
   __shared__ ef sh[1][32];
   __shared__ bool s_last;
   const size_t M = (size_t)1 << m_bits;
@@ -1428,29 +1450,51 @@ __global__ void __launch_bounds__(DOT_CTA) k_dot_split(const uint32_t* __restric
   if (!EXT && wide) {
     // four consecutive base entries per thread and step (one 16-byte load):
     // they share their high index (lo_bits >= 2), and the stride is a multiple
-    // of 2^lo_bits, so each of the four keeps its low index across steps
+    // of 2^lo_bits, so each of the four keeps its low index across steps. Four
+    // steps' loads are issued together; each accumulator then takes four
+    // products (< 4p^2 < 2^64) and is reduced once.
     const uint32_t x0 = 4u * threadIdx.x;
     ef acc[4];
-    kb::ef_acc lazy[4];
+    uint64_t t[4][4];
 #pragma unroll
-    for (int j = 0; j < 4; j++) {
-      acc[j] = kb::ef_zero();
-      lazy[j].clear();
-    }
+    for (int j = 0; j < 4; j++) acc[j] = kb::ef_zero();
     const uint4* f4 = reinterpret_cast<const uint4*>(f + (size_t)seg * M);
-    for (size_t x = (size_t)blockIdx.x * DOT_CTA * 4 + x0; x < M; x += (size_t)gridDim.x * DOT_CTA * 4) {
+    const size_t S = (size_t)gridDim.x * DOT_CTA * 4;
+    size_t x = (size_t)blockIdx.x * DOT_CTA * 4 + x0;
+    for (; x + 3 * S < M; x += 4 * S) {
+      uint4 v[4];
+      ef h[4];
+#pragma unroll
+      for (int u = 0; u < 4; u++) v[u] = __ldg(f4 + ((x + u * S) >> 2));
+#pragma unroll
+      for (int u = 0; u < 4; u++) h[u] = ld_ef(hi + ((x + u * S) >> lo_bits));
+#pragma unroll
+      for (int j = 0; j < 4; j++)
+#pragma unroll
+        for (int c = 0; c < 4; c++) t[j][c] = 0;
+#pragma unroll
+      for (int u = 0; u < 4; u++) {
+        const uint32_t e[4] = {v[u].x, v[u].y, v[u].z, v[u].w};
+#pragma unroll
+        for (int j = 0; j < 4; j++)
+#pragma unroll
+          for (int c = 0; c < 4; c++) t[j][c] += (uint64_t)h[u].c[c] * e[j];
+      }
+#pragma unroll
+      for (int j = 0; j < 4; j++)
+        acc[j] = kb::ef_add(acc[j], ef{{kb::reduce_wide(t[j][0]), kb::reduce_wide(t[j][1]),
+                                        kb::reduce_wide(t[j][2]), kb::reduce_wide(t[j][3])}});
+    }
+    for (; x < M; x += S) {
       const uint4 v = __ldg(f4 + (x >> 2));
       const ef h = ld_ef(hi + (x >> lo_bits));
-      lazy[0].mac(h, v.x, acc[0]);
-      lazy[1].mac(h, v.y, acc[1]);
-      lazy[2].mac(h, v.z, acc[2]);
-      lazy[3].mac(h, v.w, acc[3]);
+      acc[0] = kb::ef_add(acc[0], kb::ef_mul_base(h, v.x));
+      acc[1] = kb::ef_add(acc[1], kb::ef_mul_base(h, v.y));
+      acc[2] = kb::ef_add(acc[2], kb::ef_mul_base(h, v.z));
+      acc[3] = kb::ef_add(acc[3], kb::ef_mul_base(h, v.w));
     }
 #pragma unroll
-    for (int j = 0; j < 4; j++) {
-      lazy[j].fold(acc[j]);
-      total = kb::ef_add(total, kb::ef_mul(acc[j], ld_ef(lo + ((x0 + j) & lomask))));
-    }
+    for (int j = 0; j < 4; j++) total = kb::ef_add(total, kb::ef_mul(acc[j], ld_ef(lo + ((x0 + j) & lomask))));
   } else if ((size_t)threadIdx.x < M || M >= DOT_CTA) {
     const uint32_t xl = threadIdx.x & lomask;
     ef acc = kb::ef_zero();
@@ -1487,14 +1531,25 @@ __global__ void __launch_bounds__(DOT_CTA) k_dot_split(const uint32_t* __restric
       a[0] = kb::ef_add(a[0], ef{{x.x, x.y, x.z, x.w}});
     }
     block_sum<1>(a, sh);
-    if (threadIdx.x == 0) out[s2] = a[0];
+    if (threadIdx.x == 0) {
+      out[s2] = a[0];
+      if (mail)
+        for (int c = 0; c < 4; c++) reinterpret_cast<volatile uint32_t*>(mail)[4 * s2 + c] = a[0].c[c];
+    }
     __syncthreads();
   }
-  if (threadIdx.x == 0) *counter = 0u;
+  if (threadIdx.x == 0) {
+    *counter = 0u;
+    if (mail) {
+      __threadfence_system();
+      reinterpret_cast<volatile uint32_t*>(mail)[kMailWords] = seq;
+    }
+  }
 }
 
 cudaError_t dot_split(const uint32_t* f, int ext, int seg_bits, int m_bits, const ef* hi, const ef* lo, int lo_bits,
-                      ef* partials, unsigned* counter, ef* out, cudaStream_t st) {
+                      ef* partials, unsigned* counter, ef* out, uint32_t* mail, uint32_t seq, cudaStream_t st) {
+  if (mail && (4 << seg_bits) > kMailWords) return cudaErrorInvalidValue;
   if (lo_bits > 8 || lo_bits > m_bits || seg_bits < 0 || seg_bits > 8) return cudaErrorInvalidValue;
   const size_t M = (size_t)1 << m_bits;
   const int segs = 1 << seg_bits;
@@ -1505,9 +1560,9 @@ cudaError_t dot_split(const uint32_t* f, int ext, int seg_bits, int m_bits, cons
   if (bx < 1) bx = 1;
   dim3 grid(bx, segs);
   if (ext)
-    k_dot_split<1><<<grid, DOT_CTA, 0, st>>>(f, m_bits, hi, lo, lo_bits, 0, partials, counter, out);
+    k_dot_split<1><<<grid, DOT_CTA, 0, st>>>(f, m_bits, hi, lo, lo_bits, 0, partials, counter, out, mail, seq);
   else
-    k_dot_split<0><<<grid, DOT_CTA, 0, st>>>(f, m_bits, hi, lo, lo_bits, wide, partials, counter, out);
+    k_dot_split<0><<<grid, DOT_CTA, 0, st>>>(f, m_bits, hi, lo, lo_bits, wide, partials, counter, out, mail, seq);
   LAUNCH_DONE();
 }
 
@@ -1618,7 +1673,7 @@ cudaError_t sumcheck_coeffs(const ef* f, const ef* w, size_t half, ef* partials,
 template <bool FOLD>
 __global__ void __launch_bounds__(256) k_sumcheck_round(ef* __restrict__ f, ef* __restrict__ w, size_t q, ef r,
                                                          ef* __restrict__ partials, unsigned* __restrict__ counter,
-                                                         ef* __restrict__ out) {
+                                                         ef* __restrict__ out, uint32_t* mail, uint32_t seq) {
   __shared__ ef sh[2][32];
   __shared__ bool s_last;
   ef v[2] = {kb::ef_zero(), kb::ef_zero()};
@@ -1666,17 +1721,18 @@ __global__ void __launch_bounds__(256) k_sumcheck_round(ef* __restrict__ f, ef* 
     out[0] = a[0];
     out[1] = a[1];
     *counter = 0u;
+    if (mail) mail_post(mail, a[0].c, 8, seq);
   }
 }
 
 cudaError_t sumcheck_round(ef* f, ef* w, size_t q, int fold, ef r, ef* partials, unsigned* counter, ef* out,
-                           cudaStream_t st) {
+                           uint32_t* mail, uint32_t seq, cudaStream_t st) {
   if (q == 0) return cudaErrorInvalidValue;
   const unsigned b = grid_for(q, 256, 8);
   if (fold)
-    k_sumcheck_round<true><<<b, 256, 0, st>>>(f, w, q, r, partials, counter, out);
+    k_sumcheck_round<true><<<b, 256, 0, st>>>(f, w, q, r, partials, counter, out, mail, seq);
   else
-    k_sumcheck_round<false><<<b, 256, 0, st>>>(f, w, q, r, partials, counter, out);
+    k_sumcheck_round<false><<<b, 256, 0, st>>>(f, w, q, r, partials, counter, out, mail, seq);
   LAUNCH_DONE();
 }
 

@@ -99,9 +99,12 @@ cudaError_t merkle_open(const uint32_t* rows, const uint32_t* digests, int log_h
 // PoW search: smallest w in [0, limit) such that the duplex challenger whose
 // sponge state is `state` (16 words) with pending inputs in[0..in_len) samples
 // `bits` zero low bits after observing w. `result` (device, 1 word) receives
-// the witness or p if none; `counter` (device, 1 word) is scratch.
+// the witness or p if none; `counter` and `done` (device, 1 word each) are
+// scratch. With `mail` set, the result is also posted to that mailbox with
+// flag `seq` by the last CTA to stop.
 cudaError_t grind(const uint32_t* state, const uint32_t* in, int in_len, int bits, uint64_t limit,
-                  uint32_t* result, uint32_t* counter, const p2::P2Consts& p16, cudaStream_t st);
+                  uint32_t* result, uint32_t* counter, uint32_t* done, uint32_t* mail, uint32_t seq,
+                  const p2::P2Consts& p16, cudaStream_t st);
 
 // eq table of `h` coordinates scaled by `scale`: out[x] = scale * prod eq(z_j, bit_j(x)), MSB <-> z[0].
 struct EqPoint {
@@ -120,9 +123,12 @@ cudaError_t eq_table_pair(const EqPoint& p1, kb::ef* out1, const EqPoint& p2, kb
 //   out[s] = sum_{x < M} f[s*M + x] * hi[x >> lo_bits] * lo[x & mask],  M = 2^m_bits, s < 2^seg_bits
 // f is base (ext=0) or extension (ext=1). partials needs blocks*2^seg_bits ef
 // (at most 8 * SMs); the last CTA to finish reduces them into out, using
-// `counter` (device, one word, 0 before the first launch, left at 0).
+// `counter` (device, one word, 0 before the first launch, left at 0), and with
+// `mail` set also posts them to that mailbox with flag `seq` (needs
+// 4 * 2^seg_bits <= kMailWords).
 cudaError_t dot_split(const uint32_t* f, int ext, int seg_bits, int m_bits, const kb::ef* hi, const kb::ef* lo,
-                      int lo_bits, kb::ef* partials, unsigned* counter, kb::ef* out, cudaStream_t st);
+                      int lo_bits, kb::ef* partials, unsigned* counter, kb::ef* out, uint32_t* mail, uint32_t seq,
+                      cudaStream_t st);
 
 // compress (fold the first variable) on one or two extension arrays in place;
 // `shape` threads 128, 256 or 512
@@ -144,9 +150,10 @@ cudaError_t sumcheck_coeffs(const kb::ef* f, const kb::ef* w, size_t half, kb::e
 // (4q entries each) in place by r into 2q entries; then out[0] = c0, out[1] =
 // c2 over the pairs (i, i + q). `partials` needs 2 * grid_for(q) entries and
 // `counter` (device, one word) must hold 0 before the first launch; the
-// kernel leaves it at 0.
+// kernel leaves it at 0. With `mail` set, (c0, c2) are also posted to that
+// mailbox with flag `seq`.
 cudaError_t sumcheck_round(kb::ef* f, kb::ef* w, size_t q, int fold, kb::ef r, kb::ef* partials, unsigned* counter,
-                           kb::ef* out, cudaStream_t st);
+                           kb::ef* out, uint32_t* mail, uint32_t seq, cudaStream_t st);
 
 // The same reduction with the block count capped at max_blocks, so that the
 // partials fit a fixed-size buffer (2 * max_blocks entries).

@@ -21,7 +21,6 @@ using kb::ef;
 
 namespace wh {
 int ensure_dft_tables(whir_ctx* ctx, int log_h, wk::DftTables* t);
-int dot_eq(whir_ctx* ctx, const uint32_t* d_f, int ext, int seg_bits, const ef* z, int m_bits);
 int fetch(whir_ctx* ctx, void* host, const void* dev, size_t bytes);
 int upload(whir_ctx* ctx, void* dev, const void* host, size_t bytes);
 int grind(whir_ctx* ctx, Chal& ch, int bits, uint32_t* witness);
@@ -279,14 +278,16 @@ int sumcheck_round(whir_ctx* ctx, wh::Chal& ch, Sumcheck& sd, ef* d_f, ef* d_w, 
                    ef* r_out, PendingFold& pend) {
   const size_t half = (size_t)1 << (m - 1);
   WH_CHECK(!pend.on || pend.half == 2 * half, "pending fold does not match the round size");
+  const uint32_t seq = ctx->h_mail ? wh::mail_next(ctx) : 0u;
   {
     wh::StageTimer timer(ctx, wh::kStSumcheck);
     WH_TRY_CUDA(wk::sumcheck_round(d_f, d_w, half, pend.on ? 1 : 0, pend.on ? pend.r : kb::ef_zero(),
-                                   ctx->d_partials, round_counter(ctx), ctx->d_small, ctx->stream));
+                                   ctx->d_partials, round_counter(ctx), ctx->d_small,
+                                   ctx->h_mail ? ctx->d_mail : nullptr, seq, ctx->stream));
   }
   pend.on = false;
   ef c[2];
-  WH_TRY(wh::fetch(ctx, c, ctx->d_small, sizeof(c)));
+  WH_TRY(wh::fetch_posted(ctx, seq, c, ctx->d_small, sizeof(c)));
   ef r;
   WH_TRY(observe_and_sample(ctx, ch, sd, c[0], c[1], pow_bits, &r));
   pend.on = true;
@@ -301,10 +302,11 @@ int sumcheck_round(whir_ctx* ctx, wh::Chal& ch, Sumcheck& sd, ef* d_f, ef* d_w, 
 // the first k0 variables, then the full evaluation.
 int evaluate_constraint(whir_ctx* ctx, whir_witness* w, const std::vector<ef>& point, Constraint* out) {
   const int n = w->n, k0 = w->cfg.folding_factor_0;
-  WH_TRY(wh::dot_eq(ctx, w->d_poly, 0, k0, point.data() + k0, n - k0));
+  uint32_t posted = 0;
+  WH_TRY(wh::dot_eq(ctx, w->d_poly, 0, k0, point.data() + k0, n - k0, &posted));
   out->point = point;
   out->partial.resize((size_t)1 << k0);
-  WH_TRY(wh::fetch(ctx, out->partial.data(), ctx->d_small, out->partial.size() * sizeof(ef)));
+  WH_TRY(wh::fetch_posted(ctx, posted, out->partial.data(), ctx->d_small, out->partial.size() * sizeof(ef)));
   wk::EqSmall e = wh::eq_small_host(point.data(), k0);
   ef eval = kb::ef_zero();
   for (size_t y = 0; y < out->partial.size(); y++) eval = kb::ef_add(eval, kb::ef_mul(e.v[y], out->partial[y]));
@@ -456,9 +458,10 @@ int do_prove(whir_ctx* ctx, whir_witness* wit, wh::Chal& ch) {
     for (int i = 0; i < rc.ood_samples; i++) {
       const ef z = ch.sample_ef(ctx->hp16);
       std::vector<ef> pt = expand_from_univariate(z, nv);
-      WH_TRY(wh::dot_eq(ctx, reinterpret_cast<const uint32_t*>(d_f), 1, 0, pt.data(), nv));
+      uint32_t posted = 0;
+      WH_TRY(wh::dot_eq(ctx, reinterpret_cast<const uint32_t*>(d_f), 1, 0, pt.data(), nv, &posted));
       ef ev;
-      WH_TRY(wh::fetch(ctx, &ev, ctx->d_small, sizeof(ef)));
+      WH_TRY(wh::fetch_posted(ctx, posted, &ev, ctx->d_small, sizeof(ef)));
       ch.observe_ef(ctx->hp16, ev);
       put_ef(pf, ev);
       opts.push_back(std::move(pt));
