@@ -151,16 +151,16 @@ def test_dft_candidate_plans_are_in_bounds(pkg, log_chunk, log_w, log_blowup, ex
             assert (4 * lanes << t1 << log_chunk) <= 128 * 1024
         else:
             h1 = log_h - h2
+            ls = 2 if ext else 0  # register passes count tiles in words
             assert 1 <= h2 <= min(12, log_chunk) and 0 <= h1 <= 12
-            assert 0 <= t1 <= h2 and 0 <= t2 <= log_w
             if reg1:
-                assert lanes == 1 and 2 <= t1 <= 4 and reg_ok(h1, t1, th1)
+                assert 2 <= t1 <= 4 and t1 <= h2 + ls and reg_ok(h1, t1, th1)
             else:
-                assert th1 in (128, 256, 512) and (4 * lanes << t1 << h1) <= 128 * 1024
+                assert 0 <= t1 <= h2 and th1 in (128, 256, 512) and (4 * lanes << t1 << h1) <= 128 * 1024
             if reg2:
-                assert lanes == 1 and t2 <= 4 and reg_ok(h2, t2, th2)
+                assert ls <= t2 <= 4 and t2 <= log_w + ls and reg_ok(h2, t2, th2)
             else:
-                assert th2 in (128, 256, 512) and (4 * lanes << t2 << h2) <= 128 * 1024
+                assert 0 <= t2 <= log_w and th2 in (128, 256, 512) and (4 * lanes << t2 << h2) <= 128 * 1024
 
 
 def test_tune_mode_switch(pkg):

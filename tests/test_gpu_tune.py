@@ -14,9 +14,9 @@ def rnd(rng, n):
 
 
 # one-pass shapes (chunk <= 2^12) and four-step shapes, base and extension;
-# the base shapes with a pass of 2^8..2^12 points include register-pass plans
+# shapes with a pass of 2^8..2^12 points include register-pass plans
 PLAN_SHAPES = [(6, 3, 2, 0), (10, 2, 1, 0), (12, 1, 1, 1), (9, 4, 3, 1), (14, 3, 1, 0), (13, 2, 2, 1),
-               (16, 1, 1, 0), (18, 4, 1, 0), (20, 1, 4, 0)]
+               (16, 1, 1, 0), (18, 4, 1, 0), (20, 1, 4, 0), (14, 4, 2, 1), (12, 2, 5, 1), (8, 4, 8, 1)]
 
 
 @pytest.mark.parametrize("log_chunk,log_w,log_blowup,ext", PLAN_SHAPES)

@@ -444,11 +444,14 @@ __host__ __device__ constexpr int vstride(int rest) {
 
 }  // namespace dftreg
 
-// pass 1: T = 2^LT columns i2 per CTA, threads (t, g) with t fastest in both phases
+// pass 1: T = 2^LT columns i2 per CTA, threads (t, g) with t fastest in both
+// phases. Extension data (4 words per element) runs as 4 base columns per
+// element: the caller passes word-level sizes (log_l, log_h2, log_h + 2) and
+// ls = 2, and the twist exponent uses the element column i2 >> ls.
 template <int LE, int LG, int LT>
 __global__ void __launch_bounds__(1 << (LG + LT))
     k_dft_cols_reg(const uint32_t* __restrict__ x, uint32_t* __restrict__ y, int log_l, int log_h2, int log_h,
-                   const uint2* __restrict__ tw_sh, const uint32_t* __restrict__ tw_lo,
+                   int ls, const uint2* __restrict__ tw_sh, const uint32_t* __restrict__ tw_lo,
                    const uint32_t* __restrict__ tw_hi) {
   constexpr int E = 1 << LE, G = 1 << LG, T = 1 << LT, N = E * G;
   constexpr int RS = G + 1;
@@ -493,7 +496,7 @@ __global__ void __launch_bounds__(1 << (LG + LT))
 #pragma unroll
     for (int r = 0; r < G; r++) {
       const int r1 = k + E * dftreg::bitrev(r, LG);
-      const uint64_t ex = i2 * (uint64_t)r1;
+      const uint64_t ex = (i2 >> ls) * (uint64_t)r1;
       uint32_t v = b[r];
       if (ex) v = kb::mul(v, kb::mul(__ldg(tw_lo + (ex & 4095)), __ldg(tw_hi + (ex >> 12))));
       y[((size_t)j << log_h) + ((size_t)r1 << log_h2) + i2] = v;
@@ -501,13 +504,15 @@ __global__ void __launch_bounds__(1 << (LG + LT))
   }
 }
 
-// pass 2: T = 2^LT columns j per CTA (one r1); loads with g fastest (rows are
-// contiguous in i2), outer DFTs and stores with t fastest (output rows are
-// contiguous in j)
+// pass 2: T = 2^LT word columns per CTA (one r1); loads with g fastest (rows
+// are contiguous in i2), outer DFTs and stores with t fastest (output rows are
+// contiguous in j). Extension data (ls = 2) runs each element's 4 words as 4
+// columns t = 4 * column + coefficient: loads take the coefficient fastest,
+// then g, and log_w counts words.
 template <int LE, int LG, int LT>
 __global__ void __launch_bounds__(1 << (LG + LT))
     k_dft_rows_reg(const uint32_t* __restrict__ y, uint32_t* __restrict__ out, int log_h1, int log_h, int log_w,
-                   const uint2* __restrict__ tw_sh) {
+                   int ls, const uint2* __restrict__ tw_sh) {
   constexpr int E = 1 << LE, G = 1 << LG, T = 1 << LT, N = E * G;
   constexpr int RS = G + 1;
   constexpr int VS = dftreg::vstride<E, G>(T >= 32 ? 1 : 32 / T);
@@ -515,11 +520,14 @@ __global__ void __launch_bounds__(1 << (LG + LT))
   const int r1 = blockIdx.x;
   const int j0 = blockIdx.y * T;
   {
-    const int g = threadIdx.x & (G - 1), t = threadIdx.x >> LG;
+    const int c = threadIdx.x & ((1 << ls) - 1);
+    const int g = (threadIdx.x >> ls) & (G - 1);
+    const int tq = threadIdx.x >> (ls + LG);
+    const int t = (tq << ls) | c;
     uint32_t a[E];
-    const uint32_t* src = y + ((size_t)(j0 + t) << log_h) + ((size_t)r1 * N) + g;
+    const uint32_t* src = y + (((((size_t)((j0 >> ls) + tq)) << log_h) + (size_t)r1 * N + g) << ls) + c;
 #pragma unroll
-    for (int e = 0; e < E; e++) a[e] = __ldg(src + G * e);
+    for (int e = 0; e < E; e++) a[e] = __ldg(src + ((size_t)(G * e) << ls));
     dftreg::dif<LE>(a);
 #pragma unroll
     for (int r = 0; r < E; r++) {
@@ -577,18 +585,18 @@ static void raise_smem(K kernel) {
 
 template <int LE, int LG, int LT>
 static void launch_cols_reg(dim3 grid, size_t smem, cudaStream_t st, const uint32_t* x, uint32_t* y, int log_l,
-                            int log_h2, int log_h, const DftTables& t) {
+                            int log_h2, int log_h, int ls, const DftTables& t) {
   static std::once_flag once;
   std::call_once(once, [] { raise_smem(k_dft_cols_reg<LE, LG, LT>); });
-  k_dft_cols_reg<LE, LG, LT><<<grid, 1 << (LG + LT), smem, st>>>(x, y, log_l, log_h2, log_h, t.tw_sh, t.tw_lo,
+  k_dft_cols_reg<LE, LG, LT><<<grid, 1 << (LG + LT), smem, st>>>(x, y, log_l, log_h2, log_h, ls, t.tw_sh, t.tw_lo,
                                                                   t.tw_hi);
 }
 template <int LE, int LG, int LT>
 static void launch_rows_reg(dim3 grid, size_t smem, cudaStream_t st, const uint32_t* y, uint32_t* out, int log_h1,
-                            int log_h, int log_w, const DftTables& t) {
+                            int log_h, int log_w, int ls, const DftTables& t) {
   static std::once_flag once;
   std::call_once(once, [] { raise_smem(k_dft_rows_reg<LE, LG, LT>); });
-  k_dft_rows_reg<LE, LG, LT><<<grid, 1 << (LG + LT), smem, st>>>(y, out, log_h1, log_h, log_w, t.tw_sh);
+  k_dft_rows_reg<LE, LG, LT><<<grid, 1 << (LG + LT), smem, st>>>(y, out, log_h1, log_h, log_w, ls, t.tw_sh);
 }
 
 // supported (m, lt): pass 1 lt in {2, 3, 4}, pass 2 lt in {0, .., 4}
@@ -678,19 +686,21 @@ bool dft_plan_ok(const DftPlan& p, int log_chunk, int log_w, int log_blowup, int
   }
   const int log_h1 = log_h - p.log_h2;
   if (p.log_h2 < 1 || p.log_h2 > 12 || p.log_h2 > log_chunk || log_h1 < 0 || log_h1 > 12) return false;
-  if (p.log_t1 < 0 || p.log_t1 > p.log_h2 || p.log_t2 < 0 || p.log_t2 > log_w) return false;
-  if (p.reg1) {  // register pass 1: base field, 2^8..2^12 points, 4..16 columns per CTA
-    if (lanes != 1 || p.log_t1 < 2 || p.log_t1 > 4 || p.threads1 != reg_threads(log_h1, p.log_t1) ||
+  // register passes count their tiles in words (4 per extension element)
+  const int ls = lanes == 4 ? 2 : 0;
+  if (p.reg1) {  // register pass 1: 2^8..2^12 points, 4..16 word columns per CTA
+    if (p.log_t1 < 2 || p.log_t1 > 4 || p.log_t1 > p.log_h2 + ls || p.threads1 != reg_threads(log_h1, p.log_t1) ||
         p.threads1 == 0 || reg_smem(log_h1, p.log_t1) > (size_t)kDftRegSmemMax)
       return false;
-  } else if (dft_tile_bytes(p.log_t1, log_h1, lanes) > kDftTileMax) {
+  } else if (p.log_t1 < 0 || p.log_t1 > p.log_h2 || dft_tile_bytes(p.log_t1, log_h1, lanes) > kDftTileMax) {
     return false;
   }
-  if (p.reg2) {  // register pass 2: base field, 2^8..2^12 points, 1..16 columns per CTA
-    if (lanes != 1 || p.log_t2 > 4 || p.threads2 != reg_threads(p.log_h2, p.log_t2) || p.threads2 == 0 ||
-        reg_smem(p.log_h2, p.log_t2) > (size_t)kDftRegSmemMax)
+  if (p.reg2) {  // register pass 2: 2^8..2^12 points, 1..16 word columns per CTA (4..16 for extensions)
+    if (p.log_t2 < ls || p.log_t2 > 4 || p.log_t2 > log_w + ls || p.threads2 != reg_threads(p.log_h2, p.log_t2) ||
+        p.threads2 == 0 || reg_smem(p.log_h2, p.log_t2) > (size_t)kDftRegSmemMax)
       return false;
-  } else if (!dft_threads_ok(p.threads2) || dft_tile_bytes(p.log_t2, p.log_h2, lanes) > kDftTileMax) {
+  } else if (p.log_t2 < 0 || p.log_t2 > log_w || !dft_threads_ok(p.threads2) ||
+             dft_tile_bytes(p.log_t2, p.log_h2, lanes) > kDftTileMax) {
     return false;
   }
   return true;
@@ -751,10 +761,8 @@ void dft_candidates(int log_chunk, int log_w, int log_blowup, int lanes, DftPlan
     for (int t2 = 0; t2 <= log_w; t2++)
       for (int th2 : threads)
         if (tile_ok(t2, h2)) push(DftPlan{h2, 0, 256, t2, th2, 0, 0});
-    if (lanes == 1) {
-      for (int t1 = 2; t1 <= 4; t1++) push(DftPlan{h2, t1, reg_threads(h1, t1), 0, 256, 1, 0});
-      for (int t2 = 0; t2 <= 4; t2++) push(DftPlan{h2, 0, 256, t2, reg_threads(h2, t2), 0, 1});
-    }
+    for (int t1 = 2; t1 <= 4; t1++) push(DftPlan{h2, t1, reg_threads(h1, t1), 0, 256, 1, 0});
+    for (int t2 = 0; t2 <= 4; t2++) push(DftPlan{h2, 0, 256, t2, reg_threads(h2, t2), 0, 1});
   }
   *count = n;
 }
@@ -781,11 +789,12 @@ cudaError_t dft_batch(const uint32_t* in, uint32_t* out, uint32_t* scratch, int 
   }
   const int log_h2 = plan.log_h2, log_h1 = log_h - log_h2;
   const int H1 = 1 << log_h1, H2 = 1 << log_h2;
+  const int ls = lanes == 4 ? 2 : 0;  // register passes run extension data as 4 base columns per element
   if ((passes & 1) && plan.reg1) {
     const int tile = 1 << plan.log_t1;
-    dim3 grid(H2 / tile, W);
+    dim3 grid((H2 << ls) / tile, W);
     WK_REG_CASES(launch_cols_reg, log_h1, plan.log_t1, grid, reg_smem(log_h1, plan.log_t1), st, in, scratch,
-                 log_chunk, log_h2, log_h, t)
+                 log_chunk + ls, log_h2 + ls, log_h + ls, ls, t)
     count_launch();
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
@@ -806,9 +815,9 @@ cudaError_t dft_batch(const uint32_t* in, uint32_t* out, uint32_t* scratch, int 
   }
   if ((passes & 2) && plan.reg2) {
     const int jt = 1 << plan.log_t2;
-    dim3 grid(H1, W / jt);
+    dim3 grid(H1, (W << ls) / jt);
     WK_REG_CASES(launch_rows_reg, log_h2, plan.log_t2, grid, reg_smem(log_h2, plan.log_t2), st, scratch, out,
-                 log_h1, log_h, log_w, t)
+                 log_h1, log_h, log_w + ls, ls, t)
     count_launch();
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
