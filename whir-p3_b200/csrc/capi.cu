@@ -80,18 +80,11 @@ StageTimer::~StageTimer() {
 }
 
 int ensure_dft_tables(whir_ctx* ctx, int log_h, wk::DftTables* t) {
-  auto it = ctx->dft.find(log_h);
-  if (it == ctx->dft.end()) {
-    DftCache c;
-    WH_TRY_CUDA(cudaMalloc(&c.tw_lo, 4096 * 4));
-    WH_TRY_CUDA(cudaMalloc(&c.tw_hi, 4096 * 4));
-    WH_TRY_CUDA(wk::build_dft_tables(ctx->tw_stage, c.tw_lo, c.tw_hi, log_h, ctx->stream));
-    it = ctx->dft.emplace(log_h, c).first;
-  }
+  WH_CHECK(log_h >= 0 && log_h < kDftLogHeights && ctx->tw_heights, "DFT height out of range");
   t->tw_stage = ctx->tw_stage;
   t->tw_sh = reinterpret_cast<const uint2*>(ctx->tw_stage + 2048);
-  t->tw_lo = it->second.tw_lo;
-  t->tw_hi = it->second.tw_hi;
+  t->tw_lo = ctx->tw_heights + (size_t)log_h * kDftTableWords;
+  t->tw_hi = t->tw_lo + 4096;
   return WHIR_OK;
 }
 
@@ -376,6 +369,18 @@ int whir_ctx_create(int32_t device, const whir_poseidon2_params* p16, const whir
   if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess)
     return wh::set_error("stream creation failed"), fail(WHIR_ERR_CUDA);
   c->own_stream = true;
+  {
+    // the context's own pool, keeping freed blocks cached between proofs
+    cudaMemPoolProps props;
+    memset(&props, 0, sizeof(props));
+    props.allocType = cudaMemAllocationTypePinned;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = device;
+    if (cudaMemPoolCreate(&c->pool, &props) != cudaSuccess)
+      return wh::set_error("memory pool creation failed"), fail(WHIR_ERR_CUDA);
+    uint64_t thr = UINT64_MAX;
+    cudaMemPoolSetAttribute(c->pool, cudaMemPoolAttrReleaseThreshold, &thr);
+  }
   if (cudaMalloc(&c->tw_stage, wk::kDftStageTableWords * 4) != cudaSuccess || cudaMalloc(&c->d_partials, 8192 * sizeof(ef)) != cudaSuccess ||
       cudaMalloc(&c->d_small, 256 * sizeof(ef)) != cudaSuccess || cudaMalloc(&c->d_words, 64) != cudaSuccess ||
       cudaMalloc(&c->d_arena, kArenaBytes) != cudaSuccess)
@@ -389,17 +394,15 @@ int whir_ctx_create(int32_t device, const whir_poseidon2_params* p16, const whir
       cudaHostGetDevicePointer(reinterpret_cast<void**>(&c->d_mail), c->h_mail, 0) != cudaSuccess)
     return wh::set_error("mapped allocation failed"), fail(WHIR_ERR_NOMEM);
   memset(c->h_mail, 0, (wk::kMailWords + 32) * 4);
-  // stage twiddles omega_{2^12}^k come with the first table build
-  wk::DftTables t;
-  int s = wh::ensure_dft_tables(c, 12, &t);
-  if (s != WHIR_OK) return fail(s);
-  if (cudaStreamSynchronize(c->stream) != cudaSuccess) return wh::set_error("initial sync failed"), fail(WHIR_ERR_CUDA);
-  // keep stream-ordered allocations cached between proofs
-  cudaMemPool_t pool;
-  if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) {
-    uint64_t thr = UINT64_MAX;
-    cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr);
+  // twiddle tables of every subgroup height (the stage tables come with them)
+  if (cudaMalloc(&c->tw_heights, wh::kDftLogHeights * wh::kDftTableWords * 4) != cudaSuccess)
+    return wh::set_error("device allocation failed"), fail(WHIR_ERR_NOMEM);
+  for (int lh = 0; lh < wh::kDftLogHeights; lh++) {
+    uint32_t* lo = c->tw_heights + (size_t)lh * wh::kDftTableWords;
+    if (wk::build_dft_tables(c->tw_stage, lo, lo + 4096, lh, c->stream) != cudaSuccess)
+      return wh::set_error("DFT table build failed"), fail(WHIR_ERR_CUDA);
   }
+  if (cudaStreamSynchronize(c->stream) != cudaSuccess) return wh::set_error("initial sync failed"), fail(WHIR_ERR_CUDA);
   *out = c;
   return WHIR_OK;
 }
@@ -412,10 +415,7 @@ int whir_ctx_destroy(whir_ctx* c) {
   }
   cudaSetDevice(c->device);
   if (c->stream) cudaStreamSynchronize(c->stream);
-  for (auto& kv : c->dft) {
-    cudaFree(kv.second.tw_lo);
-    cudaFree(kv.second.tw_hi);
-  }
+  cudaFree(c->tw_heights);
   for (auto& rec : c->stage_events) {
     cudaEventDestroy(rec.second.first);
     cudaEventDestroy(rec.second.second);
@@ -429,6 +429,7 @@ int whir_ctx_destroy(whir_ctx* c) {
   if (c->h_pinned) cudaFreeHost(c->h_pinned);
   if (c->h_mail) cudaFreeHost(c->h_mail);
   if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);
+  if (c->pool) cudaMemPoolDestroy(c->pool);
   delete c;
   return WHIR_OK;
 }
@@ -614,7 +615,7 @@ int whir_dft_batch(whir_ctx* ctx, const uint32_t* d_chunks, int32_t log_chunk, i
   WH_TRY(wh::ensure_dft_tables(ctx, log_h, &t));
   uint32_t* scratch = nullptr;
   const size_t bytes = ((size_t)1 << (log_h + log_width)) * 4 * lanes;
-  WH_TRY_CUDA(cudaMallocAsync(&scratch, bytes, ctx->stream));
+  WH_TRY_CUDA(wh::ctx_malloc(ctx, &scratch, bytes));
   const int s = wh::run_dft(ctx, d_chunks, d_out, scratch, log_chunk, log_width, log_blowup, lanes, t);
   cudaFreeAsync(scratch, ctx->stream);
   return s;
@@ -627,11 +628,12 @@ int whir_merkle_commit(whir_ctx* ctx, const uint32_t* d_rows, int32_t log_height
                (leaf_hash == 0 || leaf_hash == 1),
            "bad Merkle arguments");
   WH_TRY(wh::run_merkle_leaves(ctx, d_rows, log_height, row_words, leaf_hash, d_digests));
-  WH_TRY(wh::run_merkle_upper(ctx, log_height, d_digests));
+  uint32_t posted = 0;
+  WH_TRY(wh::run_merkle_upper(ctx, log_height, d_digests, root ? &posted : nullptr));
   if (root) {
     const size_t h = (size_t)1 << log_height;
     uint32_t r[8];
-    WH_TRY(wh::fetch(ctx, r, d_digests + (2 * h - 2) * 8, 32));
+    WH_TRY(wh::fetch_posted(ctx, posted, r, d_digests + (2 * h - 2) * 8, 32));
     for (int i = 0; i < 8; i++) root[i] = kb::from_mont(r[i]);
   }
   return WHIR_OK;

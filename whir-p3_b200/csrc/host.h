@@ -84,10 +84,9 @@ struct Chal {
 // profiling is enabled for the context.
 enum Stage { kStDft = 0, kStLeaves, kStNodes, kStGrind, kStSumcheck, kStEval, kStWeights, kStOpen, kStCount };
 
-struct DftCache {
-  uint32_t* tw_lo = nullptr;
-  uint32_t* tw_hi = nullptr;
-};
+// twiddle tables of one subgroup height: omega_H^e and omega_H^(e * 2^12), e < 2^12
+constexpr int kDftLogHeights = 25;  // heights 2^0 .. 2^24
+constexpr size_t kDftTableWords = 2 * 4096;
 
 }  // namespace wh
 
@@ -99,11 +98,14 @@ struct whir_ctx {
   p2::P2Consts p16, p24;  // Montgomery form
   wh::HostP16 hp16;       // canonical, for the host transcript
   uint32_t* tw_stage = nullptr;
-  std::map<int, wh::DftCache> dft;  // per log2(height)
+  // twiddle tables of every height, built at creation so that proving never
+  // allocates them (a device allocation mid-run would stall other contexts)
+  uint32_t* tw_heights = nullptr;  // kDftLogHeights * kDftTableWords words
   // scratch
   kb::ef* d_partials = nullptr;  // 8192 ef
   kb::ef* d_small = nullptr;     // 256 ef
-  uint32_t* d_words = nullptr;   // 16 words: grind result and claim counter (0, 1), sumcheck round counter (8)
+  uint32_t* d_words = nullptr;   // 16 words: grind result, claim and done counters (0-2), sumcheck round (8),
+                                 // dot product (9) and tree-top (10) counters
   void* d_arena = nullptr;       // general scratch (tables, gathers)
   size_t arena_bytes = 0;
   void* h_pinned = nullptr;      // staging for small transfers
@@ -114,6 +116,10 @@ struct whir_ctx {
   uint32_t* h_mail = nullptr;
   uint32_t* d_mail = nullptr;  // device alias of h_mail
   uint32_t mail_seq = 0;
+  // this context's stream-ordered memory pool: a pool per context keeps the
+  // allocator from reusing one stream's freed blocks on another stream (which
+  // would make concurrent contexts wait on each other's queued work)
+  cudaMemPool_t pool = nullptr;
   // stage timing
   bool profiling = false;
   std::vector<cudaEvent_t> event_pool;
@@ -123,6 +129,10 @@ struct whir_ctx {
 };
 
 namespace wh {
+// Stream-ordered allocation from the context's pool.
+inline cudaError_t ctx_malloc(whir_ctx* ctx, void* p, size_t bytes) {
+  return cudaMallocFromPoolAsync(reinterpret_cast<void**>(p), bytes, ctx->pool, ctx->stream);
+}
 // Records a CUDA event pair around a scope when the context is profiling.
 struct StageTimer {
   whir_ctx* ctx;
@@ -146,6 +156,8 @@ int run_dft(whir_ctx* ctx, const uint32_t* in, uint32_t* out, uint32_t* scratch,
             int log_blowup, int lanes, const wk::DftTables& t);
 int run_merkle_leaves(whir_ctx* ctx, const uint32_t* rows, int log_h, int row_words, int leaf_hash,
                       uint32_t* digests);
-int run_merkle_upper(whir_ctx* ctx, int log_h, uint32_t* digests);
+// with posted_seq set, the root goes to the mailbox: *posted_seq receives the
+// sequence to wait for (0 when nothing was posted)
+int run_merkle_upper(whir_ctx* ctx, int log_h, uint32_t* digests, uint32_t* posted_seq);
 int run_fold(whir_ctx* ctx, kb::ef* a, kb::ef* b, size_t half, const kb::ef& r);
 }  // namespace wh

@@ -1050,20 +1050,13 @@ __device__ __forceinline__ void coop_permute16(uint32_t (&x)[4], int q, const P2
   }
 }
 
-// Top of a tree: each CTA compresses up to 256 nodes of one level into a
-// subtree, one four-lane group per node pair, level by level in shared memory.
-constexpr int TOP_CTA = 512;
-constexpr int TOP_NODES = 256;
-__global__ void __launch_bounds__(TOP_CTA) k_merkle_top_coop(uint32_t* __restrict__ digests, size_t in_off,
-                                                              size_t in_count, int levels,
-                                                              const __grid_constant__ P2Consts comp) {
-  __shared__ uint32_t sh[TOP_NODES * 8];
+// Compresses `levels` levels above the `cnt` nodes in sh (8 words each), one
+// four-lane group per node pair, writing every new level to global; `base` is
+// the first node's index in its level, `off` and `lsz` the level's offset and
+// size in `digests` (advanced past the levels done).
+__device__ __forceinline__ void coop_levels(uint32_t* sh, int cnt, int levels, size_t base, size_t& off, size_t& lsz,
+                                            uint32_t* __restrict__ digests, const P2Consts& comp) {
   const int t = threadIdx.x, g = t >> 2, q = t & 3;
-  const size_t base = (size_t)blockIdx.x * TOP_NODES;
-  const int cnt = (int)min((size_t)TOP_NODES, in_count - base);
-  for (int k = t; k < cnt * 8; k += blockDim.x) sh[k] = digests[(in_off + base) * 8 + k];
-  __syncthreads();
-  size_t off = in_off, lsz = in_count;
   int cur = cnt;
   for (int l = 1; l <= levels; l++) {
     const int act = cur >> 1;
@@ -1089,12 +1082,53 @@ __global__ void __launch_bounds__(TOP_CTA) k_merkle_top_coop(uint32_t* __restric
   }
 }
 
+// Top of a tree: each CTA compresses up to 256 nodes of one level into a
+// subtree, one four-lane group per node pair, level by level in shared memory.
+// With several CTAs (at most 256), the last one to finish (atomic counter, no
+// waiting) loads their subtree roots and compresses them to the root in the
+// same launch. With `mail` set, the root is posted to that mailbox.
+constexpr int TOP_CTA = 512;
+constexpr int TOP_NODES = 256;
+__global__ void __launch_bounds__(TOP_CTA) k_merkle_top_coop(uint32_t* __restrict__ digests, size_t in_off,
+                                                              size_t in_count, int levels,
+                                                              const __grid_constant__ P2Consts comp,
+                                                              unsigned* __restrict__ counter, uint32_t* mail,
+                                                              uint32_t seq) {
+  __shared__ uint32_t sh[TOP_NODES * 8];
+  __shared__ bool s_last;
+  const int t = threadIdx.x;
+  const size_t base = (size_t)blockIdx.x * TOP_NODES;
+  const int cnt = (int)min((size_t)TOP_NODES, in_count - base);
+  for (int k = t; k < cnt * 8; k += blockDim.x) sh[k] = digests[(in_off + base) * 8 + k];
+  __syncthreads();
+  size_t off = in_off, lsz = in_count;
+  coop_levels(sh, cnt, levels, base, off, lsz, digests, comp);
+  if (gridDim.x > 1) {
+    if (t == 0) {
+      __threadfence();
+      s_last = atomicAdd(counter, 1u) == gridDim.x - 1;
+    }
+    __syncthreads();
+    if (!s_last) return;
+    __threadfence();
+    const int n = (int)gridDim.x;  // subtree roots, level `off`
+    for (int k = t; k < n * 8; k += blockDim.x) sh[k] = __ldcg(digests + off * 8 + k);
+    __syncthreads();
+    int top = 0;
+    while ((1 << top) < n) top++;
+    coop_levels(sh, n, top, 0, off, lsz, digests, comp);
+    if (t == 0) *counter = 0u;
+  }
+  if (t == 0 && mail) mail_post(mail, sh, 8, seq);
+}
+
 // Top of a tree in one CTA: a level of at most 2 * TOP1_CTA nodes is
 // compressed to the root, one thread (one whole permutation) per node pair,
 // each new level kept in shared memory for the next and written out.
 constexpr int TOP1_CTA = 1024;
 __global__ void __launch_bounds__(TOP1_CTA) k_merkle_top_cta(uint32_t* __restrict__ digests, size_t in_off,
-                                                              int in_count, const __grid_constant__ P2Consts comp) {
+                                                              int in_count, const __grid_constant__ P2Consts comp,
+                                                              uint32_t* mail, uint32_t seq) {
   __shared__ uint4 sh[2 * TOP1_CTA];  // node i at sh[2i], sh[2i + 1]
   const int t = threadIdx.x;
   size_t off = in_off;
@@ -1127,6 +1161,7 @@ __global__ void __launch_bounds__(TOP1_CTA) k_merkle_top_cta(uint32_t* __restric
     __syncthreads();
     cnt = act;
   }
+  if (threadIdx.x == 0 && mail) mail_post(mail, reinterpret_cast<const uint32_t*>(sh), 8, seq);
 }
 
 // Trees with at least kLevelPairMin leaves are built as: leaf digests, then
@@ -1188,7 +1223,9 @@ cudaError_t merkle_leaves(const uint32_t* rows, int log_h, int row_words, int le
   LAUNCH_DONE();
 }
 
-cudaError_t merkle_upper(int log_h, uint32_t* digests, const P2Consts& p16, Shape node, cudaStream_t st) {
+cudaError_t merkle_upper(int log_h, uint32_t* digests, const P2Consts& p16, Shape node, unsigned* counter,
+                         uint32_t* mail, uint32_t seq, int* posted, cudaStream_t st) {
+  if (posted) *posted = 0;
   const size_t h = (size_t)1 << log_h;
   size_t off = 0, cnt = h;
   if (node.variant != 0 && node.variant != 1) return cudaErrorInvalidValue;
@@ -1216,35 +1253,27 @@ cudaError_t merkle_upper(int log_h, uint32_t* digests, const P2Consts& p16, Shap
       cnt >>= 1;
     }
   }
+  if (cnt <= 1) return cudaSuccess;
   if (node.variant == 1) {
-    if (cnt > 1) {
-      k_merkle_top_cta<<<1, TOP1_CTA, 0, st>>>(digests, off, (int)cnt, p16);
-      count_launch();
-      return cudaGetLastError();
-    }
-    return cudaSuccess;
-  }
-  while (cnt > 1) {
+    k_merkle_top_cta<<<1, TOP1_CTA, 0, st>>>(digests, off, (int)cnt, p16, mail, seq);
+  } else {
+    // one launch: subtrees of 256 nodes, then the last CTA joins their roots
     const int c2 = (int)(cnt < (size_t)TOP_NODES ? cnt : (size_t)TOP_NODES);
-    const int levels = ilog2i((size_t)c2);
     const unsigned blocks2 = (unsigned)(cnt / c2);
-    k_merkle_top_coop<<<blocks2, TOP_CTA, 0, st>>>(digests, off, cnt, levels, p16);
-    count_launch();
-    cudaError_t e = cudaGetLastError();
-    if (e != cudaSuccess) return e;
-    for (int l = 0; l < levels; l++) {
-      off += cnt;
-      cnt >>= 1;
-    }
+    if (blocks2 > (unsigned)TOP_NODES || (blocks2 > 1 && !counter)) return cudaErrorInvalidValue;
+    k_merkle_top_coop<<<blocks2, TOP_CTA, 0, st>>>(digests, off, cnt, ilog2i((size_t)c2), p16, counter, mail, seq);
   }
-  return cudaSuccess;
+  count_launch();
+  const cudaError_t e = cudaGetLastError();
+  if (e == cudaSuccess && posted && mail) *posted = 1;
+  return e;
 }
 
 cudaError_t merkle_build(const uint32_t* rows, int log_h, int row_words, int leaf_hash, uint32_t* digests,
-                         const P2Consts& p16, const P2Consts& p24, cudaStream_t st) {
+                         const P2Consts& p16, const P2Consts& p24, unsigned* counter, cudaStream_t st) {
   cudaError_t e = merkle_leaves(rows, log_h, row_words, leaf_hash, digests, p16, p24, merkle_leaf_default(), st);
   if (e != cudaSuccess) return e;
-  return merkle_upper(log_h, digests, p16, merkle_node_default(), st);
+  return merkle_upper(log_h, digests, p16, merkle_node_default(), counter, nullptr, 0u, nullptr, st);
 }
 
 // Mmcs::open_batch gather (src/whir/prover/mod.rs:248-300, 378-401)

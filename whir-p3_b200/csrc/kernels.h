@@ -77,8 +77,10 @@ struct Shape {
 
 // Merkle tree: digests has (2h-1)*8 words, leaves first. leaf_hash 0: sponge
 // over Poseidon2-24 rate 16; 1: Poseidon2-16 rate 8. Compression: Poseidon2-16.
+// `counter` (device, one word, 0 before the first launch, left at 0) joins the
+// CTAs of the top kernel
 cudaError_t merkle_build(const uint32_t* rows, int log_h, int row_words, int leaf_hash, uint32_t* digests,
-                         const p2::P2Consts& p16, const p2::P2Consts& p24, cudaStream_t st);
+                         const p2::P2Consts& p16, const p2::P2Consts& p24, unsigned* counter, cudaStream_t st);
 // the two halves of merkle_build: leaf hashing with the CTA subtrees, then the
 // upper levels. `leaf` shapes the leaf-digest kernel of trees with at least
 // kMerkleLevelPairMin leaves (threads 128, 256 or 512), `node` the two-level
@@ -90,7 +92,10 @@ Shape merkle_leaf_default();
 Shape merkle_node_default();
 cudaError_t merkle_leaves(const uint32_t* rows, int log_h, int row_words, int leaf_hash, uint32_t* digests,
                           const p2::P2Consts& p16, const p2::P2Consts& p24, Shape leaf, cudaStream_t st);
-cudaError_t merkle_upper(int log_h, uint32_t* digests, const p2::P2Consts& p16, Shape node, cudaStream_t st);
+// With `mail` set the top kernel posts the root (8 words) to that mailbox with
+// flag `seq` and *posted becomes 1 (trees of one leaf post nothing).
+cudaError_t merkle_upper(int log_h, uint32_t* digests, const p2::P2Consts& p16, Shape node, unsigned* counter,
+                         uint32_t* mail, uint32_t seq, int* posted, cudaStream_t st);
 // gather opened rows and sibling paths for `count` indices
 cudaError_t merkle_open(const uint32_t* rows, const uint32_t* digests, int log_h, int row_words,
                         const uint64_t* d_idx, int count, uint32_t* d_rows_out, uint32_t* d_paths_out,

@@ -192,12 +192,12 @@ int commit_matrix(whir_ctx* ctx, const uint32_t* d_src, int log_chunk, int log_w
   t->ext = ext;
   const size_t h = (size_t)1 << t->log_h;
   const size_t words = h * (size_t)t->row_words;
-  WH_TRY_CUDA(cudaMallocAsync(&t->rows, words * 4, ctx->stream));
-  WH_TRY_CUDA(cudaMallocAsync(&t->digests, (2 * h - 1) * 8 * 4, ctx->stream));
+  WH_TRY_CUDA(wh::ctx_malloc(ctx, &t->rows, words * 4));
+  WH_TRY_CUDA(wh::ctx_malloc(ctx, &t->digests, (2 * h - 1) * 8 * 4));
   wk::DftTables tab;
   WH_TRY(wh::ensure_dft_tables(ctx, t->log_h, &tab));
   uint32_t* scratch = nullptr;
-  WH_TRY_CUDA(cudaMallocAsync(&scratch, words * 4, ctx->stream));
+  WH_TRY_CUDA(wh::ctx_malloc(ctx, &scratch, words * 4));
   int s;
   {
     wh::StageTimer timer(ctx, wh::kStDft);
@@ -209,12 +209,13 @@ int commit_matrix(whir_ctx* ctx, const uint32_t* d_src, int log_chunk, int log_w
     wh::StageTimer timer(ctx, wh::kStLeaves);
     WH_TRY(wh::run_merkle_leaves(ctx, t->rows, t->log_h, t->row_words, leaf_hash, t->digests));
   }
+  uint32_t posted = 0;
   {
     wh::StageTimer timer(ctx, wh::kStNodes);
-    WH_TRY(wh::run_merkle_upper(ctx, t->log_h, t->digests));
+    WH_TRY(wh::run_merkle_upper(ctx, t->log_h, t->digests, &posted));
   }
   uint32_t r[8];
-  WH_TRY(wh::fetch(ctx, r, t->digests + (2 * h - 2) * 8, 32));
+  WH_TRY(wh::fetch_posted(ctx, posted, r, t->digests + (2 * h - 2) * 8, 32));
   for (int i = 0; i < 8; i++) root_canon[i] = kb::from_mont(r[i]);
   return WHIR_OK;
 }
@@ -406,8 +407,8 @@ int do_prove(whir_ctx* ctx, whir_witness* wit, wh::Chal& ch) {
   int nv = n - k0;
   const size_t N = (size_t)1 << nv;
   ef *d_f = nullptr, *d_w = nullptr;
-  WH_TRY_CUDA(cudaMallocAsync(&d_f, N * sizeof(ef), ctx->stream));
-  WH_TRY_CUDA(cudaMallocAsync(&d_w, N * sizeof(ef), ctx->stream));
+  WH_TRY_CUDA(wh::ctx_malloc(ctx, &d_f, N * sizeof(ef)));
+  WH_TRY_CUDA(wh::ctx_malloc(ctx, &d_w, N * sizeof(ef)));
   struct Guard {
     whir_ctx* ctx;
     ef** a;
@@ -590,7 +591,7 @@ int whir_commit(whir_ctx* ctx, const whir_protocol_params* params, int32_t n, co
     w->d_poly = const_cast<uint32_t*>(poly);
   } else {
     // values are KoalaBear elements, canonical by type as in the reference
-    if (cudaMallocAsync(&w->d_poly, N * 4, ctx->stream) != cudaSuccess) {
+    if (wh::ctx_malloc(ctx, &w->d_poly, N * 4) != cudaSuccess) {
       delete w;
       wh::set_error("polynomial allocation failed");
       return WHIR_ERR_NOMEM;

@@ -271,16 +271,24 @@ int run_merkle_leaves(whir_ctx* ctx, const uint32_t* rows, int log_h, int row_wo
   return WHIR_OK;
 }
 
-int run_merkle_upper(whir_ctx* ctx, int log_h, uint32_t* digests) {
+int run_merkle_upper(whir_ctx* ctx, int log_h, uint32_t* digests, uint32_t* posted_seq) {
+  unsigned* counter = reinterpret_cast<unsigned*>(ctx->d_words) + 10;
   wk::Shape sh = wk::merkle_node_default();
   // the two-level kernel runs only on levels wider than 2^15 nodes
   if (log_h > 15) {
     const Key k{WHIR_TUNE_MERKLE_NODES, ctx->device, log_h, 0, 0, 0};
     WH_TRY(pick_shape(ctx, k, kNodeShapes, sh,
-                      [&](const wk::Shape& s) { return wk::merkle_upper(log_h, digests, ctx->p16, s, ctx->stream); },
+                      [&](const wk::Shape& s) {
+                        return wk::merkle_upper(log_h, digests, ctx->p16, s, counter, nullptr, 0u, nullptr,
+                                                ctx->stream);
+                      },
                       &sh));
   }
-  WH_TRY_CUDA(wk::merkle_upper(log_h, digests, ctx->p16, sh, ctx->stream));
+  const uint32_t seq = posted_seq && ctx->h_mail ? mail_next(ctx) : 0u;
+  int posted = 0;
+  WH_TRY_CUDA(wk::merkle_upper(log_h, digests, ctx->p16, sh, counter, seq ? ctx->d_mail : nullptr, seq, &posted,
+                               ctx->stream));
+  if (posted_seq) *posted_seq = posted ? seq : 0u;
   return WHIR_OK;
 }
 
@@ -298,7 +306,7 @@ int run_fold(whir_ctx* ctx, ef* a, ef* b, size_t half, const ef& r) {
     } else if (g_mode.load() == 1) {
       const size_t n = 2 * half * (b ? 2 : 1);
       ef* tmp = nullptr;
-      WH_TRY_CUDA(cudaMallocAsync(&tmp, n * sizeof(ef), ctx->stream));
+      WH_TRY_CUDA(wh::ctx_malloc(ctx, &tmp, n * sizeof(ef)));
       cudaMemsetAsync(tmp, 0, n * sizeof(ef), ctx->stream);
       ef* ta = tmp;
       ef* tb = b ? tmp + 2 * half : nullptr;
@@ -383,7 +391,7 @@ int whir_dft_batch_plan(whir_ctx* ctx, const uint32_t* d_chunks, int32_t log_chu
   WH_TRY(wh::ensure_dft_tables(ctx, log_h, &t));
   uint32_t* scratch = nullptr;
   if (p.log_h2 != 0)
-    WH_TRY_CUDA(cudaMallocAsync(&scratch, ((size_t)1 << (log_h + log_width)) * 4 * lanes, ctx->stream));
+    WH_TRY_CUDA(wh::ctx_malloc(ctx, &scratch, ((size_t)1 << (log_h + log_width)) * 4 * lanes));
   const cudaError_t e =
       wk::dft_batch(d_chunks, d_out, scratch, log_chunk, log_width, log_blowup, lanes, t, p, 3, ctx->stream);
   if (scratch) cudaFreeAsync(scratch, ctx->stream);
@@ -402,7 +410,8 @@ int whir_merkle_commit_shaped(whir_ctx* ctx, const uint32_t* d_rows, int32_t log
                                     ctx->stream);
   if (e == cudaErrorInvalidValue) return wh::set_error("invalid Merkle shape"), WHIR_ERR_INVALID;
   WH_TRY_CUDA(e);
-  e = wk::merkle_upper(log_height, d_digests, ctx->p16, node, ctx->stream);
+  e = wk::merkle_upper(log_height, d_digests, ctx->p16, node, reinterpret_cast<unsigned*>(ctx->d_words) + 10,
+                      nullptr, 0u, nullptr, ctx->stream);
   if (e == cudaErrorInvalidValue) return wh::set_error("invalid Merkle shape"), WHIR_ERR_INVALID;
   WH_TRY_CUDA(e);
   if (root) {
