@@ -1538,6 +1538,7 @@ __global__ void __launch_bounds__(DOT_CTA) k_dot_split(const uint32_t* __restric
     ef acc = kb::ef_zero();
     kb::ef_acc lazy;
     lazy.clear();
+#pragma unroll 4
     for (size_t x = (size_t)blockIdx.x * DOT_CTA + threadIdx.x; x < M; x += (size_t)gridDim.x * DOT_CTA) {
       const ef h = ld_ef(hi + (x >> lo_bits));
       if (EXT) {
@@ -1562,19 +1563,41 @@ __global__ void __launch_bounds__(DOT_CTA) k_dot_split(const uint32_t* __restric
   __syncthreads();
   if (!s_last) return;
   __threadfence();
-  for (unsigned s2 = 0; s2 < gridDim.y; s2++) {
-    ef a[1] = {kb::ef_zero()};
-    for (unsigned b = threadIdx.x; b < gridDim.x; b += blockDim.x) {
-      const uint4 x = __ldcg(reinterpret_cast<const uint4*>(partials + (size_t)s2 * gridDim.x + b));
-      a[0] = kb::ef_add(a[0], ef{{x.x, x.y, x.z, x.w}});
+  const unsigned segs = gridDim.y, nb = gridDim.x;
+  if (segs >= 8 && DOT_CTA % segs == 0 && DOT_CTA / segs <= 32) {
+    // one group of DOT_CTA / segs lanes per segment, all segments at once
+    const unsigned gsz = DOT_CTA / segs, lane = threadIdx.x % gsz, sg = threadIdx.x / gsz;
+    ef a = kb::ef_zero();
+    for (unsigned b = lane; b < nb; b += gsz) {
+      const uint4 x = __ldcg(reinterpret_cast<const uint4*>(partials + (size_t)sg * nb + b));
+      a = kb::ef_add(a, ef{{x.x, x.y, x.z, x.w}});
     }
-    block_sum<1>(a, sh);
-    if (threadIdx.x == 0) {
-      out[s2] = a[0];
-      if (mail)
-        for (int c = 0; c < 4; c++) reinterpret_cast<volatile uint32_t*>(mail)[4 * s2 + c] = a[0].c[c];
+    for (unsigned o = gsz / 2; o >= 1; o >>= 1)
+#pragma unroll
+      for (int c = 0; c < 4; c++) a.c[c] = kb::add(a.c[c], __shfl_xor_sync(0xffffffffu, a.c[c], o));
+    if (lane == 0) {
+      out[sg] = a;
+      if (mail) {
+        for (int c = 0; c < 4; c++) reinterpret_cast<volatile uint32_t*>(mail)[4 * sg + c] = a.c[c];
+        __threadfence_system();
+      }
     }
     __syncthreads();
+  } else {
+    for (unsigned s2 = 0; s2 < segs; s2++) {
+      ef a[1] = {kb::ef_zero()};
+      for (unsigned b = threadIdx.x; b < nb; b += blockDim.x) {
+        const uint4 x = __ldcg(reinterpret_cast<const uint4*>(partials + (size_t)s2 * nb + b));
+        a[0] = kb::ef_add(a[0], ef{{x.x, x.y, x.z, x.w}});
+      }
+      block_sum<1>(a, sh);
+      if (threadIdx.x == 0) {
+        out[s2] = a[0];
+        if (mail)
+          for (int c = 0; c < 4; c++) reinterpret_cast<volatile uint32_t*>(mail)[4 * s2 + c] = a[0].c[c];
+      }
+      __syncthreads();
+    }
   }
   if (threadIdx.x == 0) {
     *counter = 0u;
@@ -1592,8 +1615,20 @@ cudaError_t dot_split(const uint32_t* f, int ext, int seg_bits, int m_bits, cons
   const size_t M = (size_t)1 << m_bits;
   const int segs = 1 << seg_bits;
   const int wide = !ext && lo_bits >= 2 && M >= 4 * (size_t)DOT_CTA && ((uintptr_t)f & 15) == 0;
-  unsigned bx = grid_for(wide ? M / 4 : M, DOT_CTA, 8);
-  unsigned cap = (unsigned)((sm_count() * 8 + segs - 1) / segs);
+  // one wave of resident CTAs (the wide path holds many registers): more CTAs
+  // than fit would only queue behind the first wave
+  static int resident[2] = {0, 0};
+  int& per_sm = resident[ext ? 1 : 0];
+  if (per_sm == 0) {
+    int n = 0;
+    if (ext)
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_dot_split<1>, DOT_CTA, 0);
+    else
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_dot_split<0>, DOT_CTA, 0);
+    per_sm = n > 0 ? n : 1;
+  }
+  unsigned bx = grid_for(wide ? M / 4 : M, DOT_CTA, per_sm);
+  unsigned cap = (unsigned)((sm_count() * per_sm + segs - 1) / segs);
   if (bx > cap) bx = cap;
   if (bx < 1) bx = 1;
   dim3 grid(bx, segs);
@@ -1650,15 +1685,27 @@ cudaError_t fold_base(const uint32_t* f, size_t half, ef r, ef* out, cudaStream_
   LAUNCH_DONE();
 }
 
+// Loads of four strided inputs are issued together, then their four products
+// (< 4p^2 < 2^64 per coefficient) are summed and reduced once.
 __global__ void k_fold_multi_base(const uint32_t* __restrict__ f, int k, size_t m,
                                   const __grid_constant__ EqSmall eqrs, ef* __restrict__ out) {
   const int K = 1 << k;
   for (size_t x = blockIdx.x * (size_t)blockDim.x + threadIdx.x; x < m; x += (size_t)gridDim.x * blockDim.x) {
     ef acc = kb::ef_zero();
-    kb::ef_acc lazy;
-    lazy.clear();
-    for (int y = 0; y < K; y++) lazy.mac(eqrs.v[y], __ldg(f + (size_t)y * m + x), acc);
-    lazy.fold(acc);
+    int y = 0;
+    for (; y + 4 <= K; y += 4) {
+      uint32_t v[4];
+#pragma unroll
+      for (int u = 0; u < 4; u++) v[u] = __ldg(f + (size_t)(y + u) * m + x);
+      uint64_t t[4] = {0, 0, 0, 0};
+#pragma unroll
+      for (int u = 0; u < 4; u++)
+#pragma unroll
+        for (int c = 0; c < 4; c++) t[c] += (uint64_t)eqrs.v[y + u].c[c] * v[u];
+      acc = kb::ef_add(acc, ef{{kb::reduce_wide(t[0]), kb::reduce_wide(t[1]), kb::reduce_wide(t[2]),
+                                kb::reduce_wide(t[3])}});
+    }
+    for (; y < K; y++) acc = kb::ef_add(acc, kb::ef_mul_base(eqrs.v[y], __ldg(f + (size_t)y * m + x)));
     st_ef(out + x, acc);
   }
 }
@@ -1851,10 +1898,25 @@ __global__ void k_add_select(ef* __restrict__ w, size_t N, int lo_bits, const ui
     const size_t x = x0 + threadIdx.x;
     const size_t xl = x & (Lc - 1);
     ef acc = ld_ef(w + x);
-    kb::ef_acc lazy;
-    lazy.clear();
-    for (int s = 0; s < m; s++) lazy.mac(cs[s], __ldg(pow_lo + s * Lc + xl), acc);
-    lazy.fold(acc);
+    // four constraints per step: their loads are issued together, then the
+    // four products (< 4p^2 < 2^64 per coefficient) are summed and reduced once
+    int s = 0;
+    const uint32_t* pp = pow_lo + xl;  // row s of the power table at pp
+    for (; s + 4 <= m; s += 4, pp += 4 * Lc) {
+      uint32_t pv[4];
+#pragma unroll
+      for (int u = 0; u < 4; u++) pv[u] = __ldg(pp + u * Lc);
+      uint64_t t[4] = {0, 0, 0, 0};
+#pragma unroll
+      for (int u = 0; u < 4; u++) {
+        const ef c = cs[s + u];
+#pragma unroll
+        for (int q = 0; q < 4; q++) t[q] += (uint64_t)c.c[q] * pv[u];
+      }
+      acc = kb::ef_add(acc, ef{{kb::reduce_wide(t[0]), kb::reduce_wide(t[1]), kb::reduce_wide(t[2]),
+                                kb::reduce_wide(t[3])}});
+    }
+    for (; s < m; s++) acc = kb::ef_add(acc, kb::ef_mul_base(cs[s], __ldg(pow_lo + (size_t)s * Lc + xl)));
     st_ef(w + x, acc);
   }
 }
