@@ -13,6 +13,9 @@
  *                    first, then the width-24 set, mirroring the reference's
  *                    one-RNG-two-permutations set-up (src/bin/main.rs:100-102).
  *                    The values themselves are not Plonky3's (parity unpinned).
+ *                    The internal diagonal is fixed, not drawn: small integers
+ *                    and signed powers of two, the form of p3-koala-bear's
+ *                    internal layer (which takes only round constants).
  *   Sponges ........ PaddingFreeSponge (overwrite mode) and
  *                    TruncatedPermutation as used at src/bin/main.rs:35-36.
  *   Challenger ..... DuplexChallenger<F, P16, 16, 8> duplex sponge
@@ -58,18 +61,27 @@ static void p2_fill(or_p2_params* p, uint32_t width, uint32_t rp, uint64_t* s) {
   for (uint32_t r = 0; r < rp; r++) p->int_rc[r] = sm64_field(s);
   for (uint32_t r = 4; r < 8; r++)
     for (uint32_t i = 0; i < width; i++) p->ext_rc[r * width + i] = sm64_field(s);
-  /* internal diagonal: nonzero, and 1 + sum(1/mu_i) != 0 so that the
-   * internal matrix is invertible */
-  for (;;) {
-    uint32_t acc = 1;
-    for (uint32_t i = 0; i < width; i++) {
-      uint32_t d;
-      do d = sm64_field(s);
-      while (d == 0);
-      p->diag[i] = d;
-      acc = or_add(acc, or_inv(d));
-    }
-    if (acc != 0) break;
+  /* internal diagonal: fixed, drawn from no RNG. Entries are small integers
+   * and signed powers of two: width 16
+   *   -2, 1, 2, 1/2, 3, 4, -1/2, -3, -4, 2^-8, 2^-3, 2^-24, -2^-8, -2^-3, -2^-4, -2^-24
+   * width 24
+   *   -2, 1, 2, 1/2, 3, 4, -1/2, -3, -4, 2^-8, 2^-2, 2^-3, 2^-4, 2^-5, 2^-6, 2^-24,
+   *   -2^-8, -2^-3, -2^-4, -2^-5, -2^-6, -2^-7, -2^-9, -2^-24 */
+  static const int small[9] = {-2, 1, 2, 0, 3, 4, 0, -3, -4}; /* 0 marks +-1/2 */
+  static const int pow16[7] = {8, 3, 24, -8, -3, -4, -24};
+  static const int pow24[15] = {8, 2, 3, 4, 5, 6, 24, -8, -3, -4, -5, -6, -7, -9, -24};
+  const uint32_t half = (OR_P + 1) / 2;
+  for (uint32_t i = 0; i < 9; i++) {
+    if (small[i] > 0) p->diag[i] = (uint32_t)small[i];
+    else if (small[i] < 0) p->diag[i] = OR_P - (uint32_t)(-small[i]);
+    else p->diag[i] = i == 3 ? half : OR_P - half;
+  }
+  const int* pw = width == 16 ? pow16 : pow24;
+  for (uint32_t i = 9; i < width; i++) {
+    const int e = pw[i - 9] < 0 ? -pw[i - 9] : pw[i - 9];
+    uint32_t v = 1;
+    for (int j = 0; j < e; j++) v = or_mul(v, half);
+    p->diag[i] = pw[i - 9] < 0 ? OR_P - v : v;
   }
 }
 

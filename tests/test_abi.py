@@ -43,6 +43,34 @@ def test_default_poseidon2_matches_oracle(pkg, oracle):
 
 
 @pytest.mark.parametrize("width", [16, 24])
+def test_internal_matrix_conditions(oracle, width):
+    """The fixed internal matrix 1*1^T + diag(mu) meets the Poseidon2 paper's
+    conditions (eprint 2023/323, sec. 5.3): invertible, and the characteristic
+    polynomial of every power M^k, k = 1 .. 2t, irreducible (no invariant
+    subspace trails)."""
+    sympy = pytest.importorskip("sympy")
+    d = [int(v) for v in (oracle.p16 if width == 16 else oracle.p24).diag[:width]]
+    assert all(d) and (1 + sum(pow(v, P - 2, P) for v in d)) % P != 0
+    m = sympy.Matrix(width, width, lambda i, j: (1 + (d[i] if i == j else 0)) % P)
+    x = sympy.symbols("x")
+    mk = m
+    for k in range(1, 2 * width + 1):
+        if k > 1:
+            mk = (mk * m).applyfunc(lambda v: v % P)
+        assert sympy.Poly(mk.charpoly(x).as_expr(), x, modulus=P).is_irreducible, k
+
+
+def test_custom_internal_diagonal_rejected(pkg):
+    """The internal diagonal is fixed, as in p3-koala-bear; a parameter set
+    carrying another one is refused at context creation."""
+    p16, p24 = pkg.default_poseidon2()
+    p24.diag[5] = (p24.diag[5] + 1) % P
+    with pytest.raises(pkg.WhirError) as e:
+        pkg.Context(-1, p16, p24)
+    assert e.value.code == -1 and "diagonal" in str(e.value)
+
+
+@pytest.mark.parametrize("width", [16, 24])
 def test_permutation_matches_oracle(host_ctx, oracle, width):
     rng = np.random.default_rng(width)
     for _ in range(20):

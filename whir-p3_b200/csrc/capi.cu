@@ -487,9 +487,9 @@ int whir_poseidon2_permute(const whir_ctx* ctx, uint32_t* state, int32_t width) 
     wh::host_permute16(state, ctx->hp16);
   } else {
     uint32_t s[24];
-    for (int i = 0; i < 24; i++) s[i] = kb::to_mont(state[i]);
-    p2::permute<24, p2::RP24>(s, ctx->p24);
-    for (int i = 0; i < 24; i++) state[i] = kb::from_mont(s[i]);
+    for (int i = 0; i < 24; i++) s[i] = state[i];
+    p2::permute_canonical<24, p2::RP24>(s, ctx->p24);
+    for (int i = 0; i < 24; i++) state[i] = s[i];
   }
   return WHIR_OK;
 }

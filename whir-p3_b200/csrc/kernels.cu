@@ -848,6 +848,17 @@ cudaError_t dft_batch(const uint32_t* in, uint32_t* out, uint32_t* scratch, int 
 
 constexpr int MERKLE_CTA = 128;
 
+// TruncatedPermutation<P16, 2, 8, 16> on Montgomery-form digests: the
+// permutation runs on canonical values, and only the kept half of the output
+// is converted back.
+__device__ __forceinline__ void compress_mont(uint32_t (&s)[16], const P2Consts& k) {
+#pragma unroll
+  for (int i = 0; i < 16; i++) s[i] = kb::from_mont(s[i]);
+  p2::permute_canonical<16, p2::RP16>(s, k);
+#pragma unroll
+  for (int i = 0; i < 8; i++) s[i] = kb::to_mont(s[i]);
+}
+
 __device__ __forceinline__ void compress16(const uint32_t* l, const uint32_t* r, uint32_t* out,
                                            const P2Consts& k) {
   uint32_t s[16];
@@ -856,7 +867,7 @@ __device__ __forceinline__ void compress16(const uint32_t* l, const uint32_t* r,
     s[i] = l[i];
     s[i + 8] = r[i];
   }
-  p2::permute<16, p2::RP16>(s, k);
+  compress_mont(s, k);
 #pragma unroll
   for (int i = 0; i < 8; i++) out[i] = s[i];
 }
@@ -905,20 +916,21 @@ __global__ void __launch_bounds__(MERKLE_CTA) k_merkle_leaves(const uint32_t* __
 #pragma unroll
         for (int k = 0; k < RATE; k += 4) {
           uint4 v = __ldg(reinterpret_cast<const uint4*>(row + pos + k));
-          s[k] = v.x;
-          s[k + 1] = v.y;
-          s[k + 2] = v.z;
-          s[k + 3] = v.w;
+          s[k] = kb::from_mont(v.x);
+          s[k + 1] = kb::from_mont(v.y);
+          s[k + 2] = kb::from_mont(v.z);
+          s[k + 3] = kb::from_mont(v.w);
         }
       } else {
 #pragma unroll
         for (int k = 0; k < RATE; k++)
-          if (k < take) s[k] = row[pos + k];
+          if (k < take) s[k] = kb::from_mont(row[pos + k]);
       }
-      p2::permute<T, RP>(s, leaf);
+      p2::permute_canonical<T, RP>(s, leaf);
     }
 #pragma unroll
     for (int k = 0; k < 8; k++) {
+      s[k] = kb::to_mont(s[k]);
       sh[threadIdx.x * 8 + k] = s[k];
       digests[i * 8 + k] = s[k];
     }
@@ -952,18 +964,20 @@ __global__ void __launch_bounds__(CTA) k_leaf_digests(const uint32_t* __restrict
 #pragma unroll
         for (int k = 0; k < RATE; k += 4) {
           uint4 v = __ldg(reinterpret_cast<const uint4*>(row + pos + k));
-          s[k] = v.x;
-          s[k + 1] = v.y;
-          s[k + 2] = v.z;
-          s[k + 3] = v.w;
+          s[k] = kb::from_mont(v.x);
+          s[k + 1] = kb::from_mont(v.y);
+          s[k + 2] = kb::from_mont(v.z);
+          s[k + 3] = kb::from_mont(v.w);
         }
       } else {
 #pragma unroll
         for (int k = 0; k < RATE; k++)
-          if (k < take) s[k] = row[pos + k];
+          if (k < take) s[k] = kb::from_mont(row[pos + k]);
       }
-      p2::permute<T, RP>(s, leaf);
+      p2::permute_canonical<T, RP>(s, leaf);
     }
+#pragma unroll
+    for (int k = 0; k < 8; k++) s[k] = kb::to_mont(s[k]);
     uint4* d = reinterpret_cast<uint4*>(digests + i * 8);
     d[0] = make_uint4(s[0], s[1], s[2], s[3]);
     d[1] = make_uint4(s[4], s[5], s[6], s[7]);
@@ -986,20 +1000,30 @@ __global__ void __launch_bounds__(CTA) k_merkle_two_levels(uint32_t* __restrict_
       a[4 * q] = va.x; a[4 * q + 1] = va.y; a[4 * q + 2] = va.z; a[4 * q + 3] = va.w;
       b[4 * q] = vb.x; b[4 * q + 1] = vb.y; b[4 * q + 2] = vb.z; b[4 * q + 3] = vb.w;
     }
-    p2::permute<16, p2::RP16>(a, comp);
-    p2::permute<16, p2::RP16>(b, comp);
-    uint4* mid = reinterpret_cast<uint4*>(digests + (mid_off + 2 * j) * 8);
-    mid[0] = make_uint4(a[0], a[1], a[2], a[3]);
-    mid[1] = make_uint4(a[4], a[5], a[6], a[7]);
-    mid[2] = make_uint4(b[0], b[1], b[2], b[3]);
-    mid[3] = make_uint4(b[4], b[5], b[6], b[7]);
-    uint32_t c[16];
+#pragma unroll
+    for (int k = 0; k < 16; k++) {
+      a[k] = kb::from_mont(a[k]);
+      b[k] = kb::from_mont(b[k]);
+    }
+    p2::permute_canonical<16, p2::RP16>(a, comp);
+    p2::permute_canonical<16, p2::RP16>(b, comp);
+    // the parent's inputs stay canonical
+    uint32_t c[16], am[8], bm[8];
 #pragma unroll
     for (int k = 0; k < 8; k++) {
       c[k] = a[k];
       c[8 + k] = b[k];
+      am[k] = kb::to_mont(a[k]);
+      bm[k] = kb::to_mont(b[k]);
     }
-    p2::permute<16, p2::RP16>(c, comp);
+    uint4* mid = reinterpret_cast<uint4*>(digests + (mid_off + 2 * j) * 8);
+    mid[0] = make_uint4(am[0], am[1], am[2], am[3]);
+    mid[1] = make_uint4(am[4], am[5], am[6], am[7]);
+    mid[2] = make_uint4(bm[0], bm[1], bm[2], bm[3]);
+    mid[3] = make_uint4(bm[4], bm[5], bm[6], bm[7]);
+    p2::permute_canonical<16, p2::RP16>(c, comp);
+#pragma unroll
+    for (int k = 0; k < 8; k++) c[k] = kb::to_mont(c[k]);
     uint4* top = reinterpret_cast<uint4*>(digests + (top_off + j) * 8);
     top[0] = make_uint4(c[0], c[1], c[2], c[3]);
     top[1] = make_uint4(c[4], c[5], c[6], c[7]);
@@ -1026,6 +1050,8 @@ __device__ __forceinline__ void coop_ext_layer(uint32_t (&x)[4]) {
 
 __device__ __forceinline__ void coop_permute16(uint32_t (&x)[4], int q, const P2Consts& k) {
   using namespace kb;
+#pragma unroll
+  for (int j = 0; j < 4; j++) x[j] = from_mont(x[j]);
   coop_ext_layer(x);
 #pragma unroll 1
   for (int r = 0; r < p2::RF / 2; r++) {
@@ -1048,6 +1074,8 @@ __device__ __forceinline__ void coop_permute16(uint32_t (&x)[4], int q, const P2
     for (int j = 0; j < 4; j++) x[j] = p2::cube(add(x[j], k.ext_rc[r * 16 + 4 * q + j]));
     coop_ext_layer(x);
   }
+#pragma unroll
+  for (int j = 0; j < 4; j++) x[j] = to_mont(x[j]);
 }
 
 // Compresses `levels` levels above the `cnt` nodes in sh (8 words each), one
@@ -1146,7 +1174,7 @@ __global__ void __launch_bounds__(TOP1_CTA) k_merkle_top_cta(uint32_t* __restric
         x[4 * q + 2] = v.z;
         x[4 * q + 3] = v.w;
       }
-      p2::permute<16, p2::RP16>(x, comp);
+      compress_mont(x, comp);
     }
     __syncthreads();
     off += cnt;
@@ -1349,11 +1377,10 @@ __global__ void __launch_bounds__(GRIND_CTA) k_grind(const __grid_constant__ P2C
     const uint64_t w = start + threadIdx.x;
     if (w < limit) {
       uint32_t s[16];
-      const uint32_t wm = kb::to_mont((uint32_t)w);
 #pragma unroll
-      for (int i = 0; i < 16; i++) s[i] = i == slot ? wm : base_state[i];
-      p2::permute<16, p2::RP16>(s, p16);
-      if ((kb::from_mont(s[7]) & mask) == 0u) atomicMin(result, (uint32_t)w);
+      for (int i = 0; i < 16; i++) s[i] = i == slot ? (uint32_t)w : base_state[i];
+      p2::permute_canonical<16, p2::RP16>(s, p16);
+      if ((s[7] & mask) == 0u) atomicMin(result, (uint32_t)w);
     }
   }
 }
@@ -1369,9 +1396,11 @@ cudaError_t grind(const uint32_t* state, const uint32_t* in, int in_len, int bit
                   const P2Consts& p16, cudaStream_t st) {
   if (in_len < 0 || in_len > 7 || bits < 0 || bits > 30) return cudaErrorInvalidValue;
   if (limit > kb::P) limit = kb::P;
+  // the sponge state with the pending inputs, canonical (a witness w < p is
+  // its own canonical value)
   uint32_t s[16];
-  for (int i = 0; i < 16; i++) s[i] = state[i];
-  for (int i = 0; i < in_len; i++) s[i] = in[i];
+  for (int i = 0; i < 16; i++) s[i] = kb::from_mont(state[i]);
+  for (int i = 0; i < in_len; i++) s[i] = kb::from_mont(in[i]);
   k_grind_init<<<1, 1, 0, st>>>(result, counter, done);
   count_launch();
   uint4 a = make_uint4(s[0], s[1], s[2], s[3]), b = make_uint4(s[4], s[5], s[6], s[7]);

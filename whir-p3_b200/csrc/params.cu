@@ -21,10 +21,9 @@ p2::P2Consts to_consts(const whir_poseidon2_params& p) {
   k.width = p.width;
   k.rounds_f = p.rounds_f;
   k.rounds_p = p.rounds_p;
-  for (int i = 0; i < 8 * 24; i++) k.ext_rc[i] = kb::to_mont(p.ext_rc[i]);
-  for (int i = 0; i < 32; i++) k.int_rc[i] = kb::to_mont(p.int_rc[i]);
+  memcpy(k.ext_rc, p.ext_rc, sizeof(k.ext_rc));
+  memcpy(k.int_rc, p.int_rc, sizeof(k.int_rc));
   for (int i = 0; i < 24; i++) {
-    k.diag[i] = kb::to_mont(p.diag[i]);
     k.diag_c[i] = p.diag[i];
     k.diag_s[i] = kb::shoup_const(p.diag[i]);
   }
@@ -42,8 +41,15 @@ int validate_params(const whir_poseidon2_params& p, uint32_t width) {
     if (p.ext_rc[i] >= kb::P) return set_error("Poseidon2 constant out of range"), WHIR_ERR_INVALID;
   for (int i = 0; i < 32; i++)
     if (p.int_rc[i] >= kb::P) return set_error("Poseidon2 constant out of range"), WHIR_ERR_INVALID;
-  for (int i = 0; i < 24; i++)
-    if (p.diag[i] >= kb::P) return set_error("Poseidon2 constant out of range"), WHIR_ERR_INVALID;
+  // the internal diagonal is fixed (p3-koala-bear's internal layer takes only
+  // round constants); the field is kept so the struct carries the whole
+  // permutation, and must hold that diagonal
+  for (uint32_t i = 0; i < width; i++) {
+    if (p.diag[i] != p2::diag_value(p2::diag_code((int)width, (int)i)))
+      return set_error("Poseidon2 internal diagonal differs from the fixed KoalaBear diagonal at entry " +
+                       std::to_string(i)),
+             WHIR_ERR_INVALID;
+  }
   return WHIR_OK;
 }
 
@@ -66,18 +72,6 @@ struct SplitMix {
   }
 };
 
-// canonical helpers for the diagonal check
-uint32_t cmul(uint32_t a, uint32_t b) { return (uint32_t)(((uint64_t)a * b) % kb::P); }
-uint32_t cinv(uint32_t a) {
-  uint32_t r = 1, e = kb::P - 2;
-  while (e) {
-    if (e & 1) r = cmul(r, a);
-    a = cmul(a, a);
-    e >>= 1;
-  }
-  return r;
-}
-
 void fill(whir_poseidon2_params* p, uint32_t width, uint32_t rp, SplitMix& g) {
   memset(p, 0, sizeof(*p));
   p->width = width;
@@ -88,18 +82,7 @@ void fill(whir_poseidon2_params* p, uint32_t width, uint32_t rp, SplitMix& g) {
   for (uint32_t r = 0; r < rp; r++) p->int_rc[r] = g.field();
   for (uint32_t r = 4; r < 8; r++)
     for (uint32_t i = 0; i < width; i++) p->ext_rc[r * width + i] = g.field();
-  // diagonal: nonzero entries with 1 + sum(1/mu_i) != 0 (invertible internal matrix)
-  for (;;) {
-    uint32_t acc = 1;
-    for (uint32_t i = 0; i < width; i++) {
-      uint32_t d;
-      do d = g.field();
-      while (d == 0);
-      p->diag[i] = d;
-      acc = (acc + cinv(d)) % kb::P;
-    }
-    if (acc) break;
-  }
+  for (uint32_t i = 0; i < width; i++) p->diag[i] = p2::diag_value(p2::diag_code((int)width, (int)i));
 }
 }  // namespace
 

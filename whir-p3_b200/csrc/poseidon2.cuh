@@ -10,10 +10,22 @@
 // `<24>` (src/bin/main.rs:31-32), used by PaddingFreeSponge (leaf hashing),
 // TruncatedPermutation (2-to-1 compression) and DuplexChallenger.
 //
-// The round constants and diagonal are run-time data (`P2Consts`, Montgomery
-// form, passed to kernels in the constant bank) so a caller can supply the
-// exact permutation of its deployment; the shapes (8 full rounds; 20 partial
-// rounds at width 16, 23 at width 24) are compile-time.
+// The round constants are run-time data (`P2Consts`, canonical form, passed
+// to kernels in the constant bank) so a caller can supply the constants of
+// its deployment. The internal diagonal is fixed, as in p3-koala-bear, whose
+// internal layer takes only round constants: its entries are small integers
+// and signed powers of two, so every diagonal product is a few shifts and
+// additions instead of a modular multiplication. The shapes (8 full rounds;
+// 20 partial rounds at width 16, 23 at width 24) are compile-time.
+//
+// The permutation runs on canonical values. On the device the S-box products
+// take their quotient from a double-precision estimate (the floating-point
+// quotient method of Shoup's NTL MulMod): for a, b < 2^31,
+// q = round(a * fl(b / p)) is within one of a * b / p, so r = a * b - q * p,
+// computed modulo 2^32, lies in (-p, p) and one signed correction gives the
+// residue. This moves the high halves of the products from the integer
+// multiply pipe (which also carries every other product of the permutation)
+// to the double-precision pipe.
 #pragma once
 #include "kb.cuh"
 
@@ -25,12 +37,29 @@ constexpr int RP24 = 23;
 
 struct P2Consts {
   uint32_t width, rounds_f, rounds_p;
-  uint32_t ext_rc[8 * 24];
-  uint32_t int_rc[32];
-  uint32_t diag[24];    // Montgomery form
-  uint32_t diag_c[24];  // canonical, the Shoup multiplier
-  uint32_t diag_s[24];  // kb::shoup_const(diag_c)
+  uint32_t ext_rc[8 * 24];  // canonical
+  uint32_t int_rc[32];      // canonical
+  uint32_t diag_c[24];      // the fixed diagonal, canonical (run-time indexed uses)
+  uint32_t diag_s[24];      // kb::shoup_const(diag_c)
 };
+
+// Internal diagonal codes: an integer v in [-4, 4] \ {0} is v itself;
+// 100 + k is 2^-k and 200 + k is -2^-k (1 <= k <= 24).
+KB_HD constexpr int diag_code(int width, int i) {
+  const int d16[16] = {-2, 1, 2, 101, 3, 4, 201, -3, -4, 108, 103, 124, 208, 203, 204, 224};
+  const int d24[24] = {-2, 1,   2,   101, 3,   4,   201, -3,  -4,  108, 102, 103,
+                       104, 105, 106, 124, 208, 203, 204, 205, 206, 207, 209, 224};
+  return width == 16 ? d16[i] : d24[i];
+}
+
+// Canonical value of a diagonal code (2^-k = ((p + 1) / 2)^k).
+inline uint32_t diag_value(int code) {
+  if (code >= -4 && code <= 4) return code >= 0 ? (uint32_t)code : (uint32_t)((int64_t)kb::P + code);
+  const int k = code % 100;
+  uint64_t v = 1;
+  for (int j = 0; j < k; j++) v = v * ((kb::P + 1) / 2) % kb::P;
+  return code < 200 ? (uint32_t)v : (uint32_t)((kb::P - v) % kb::P);
+}
 
 // M4 = [[5,7,1,3],[4,6,1,1],[1,3,5,7],[1,1,4,6]] via the paper's addition chain.
 KB_HD void m4(uint32_t& x0, uint32_t& x1, uint32_t& x2, uint32_t& x3) {
@@ -69,8 +98,73 @@ KB_HD void ext_layer(uint32_t (&x)[T]) {
   }
 }
 
-// v^3 with the square left unreduced: v^2 < 2p, and (v^2) * v < 2p^2 < p * 2^32
-KB_HD uint32_t cube(uint32_t v) { return kb::mul(kb::mul_lazy(v, v), v); }
+#ifdef __CUDA_ARCH__
+// a as an exact double: the bit pattern of 2^52 + a, minus 2^52
+__device__ __forceinline__ double exact_double(uint32_t a) {
+  return __hiloint2double(0x43300000, (int)a) - 4503599627370496.0;
+}
+// a * b mod p for a, b < 2^31, given a as a double and bp = fl(b / p): adding
+// 1.5 * 2^52 rounds the quotient estimate to an integer held in the low
+// mantissa bits, read back as the low word.
+__device__ __forceinline__ uint32_t mulmod_q(uint32_t a, double ad, double bp, uint32_t b) {
+  const double q = fma(ad, bp, 6755399441055744.0);
+  const uint32_t r = a * b - (uint32_t)__double2loint(q) * kb::P;
+  return kb::umin32(r, r + kb::P);  // r in (-p, p) as a signed value
+}
+#endif
+
+// v^3 mod p, v canonical
+KB_HD uint32_t cube(uint32_t v) {
+#ifdef __CUDA_ARCH__
+  constexpr double kInvP = 1.0 / 2130706433.0;
+  const double vd = exact_double(v);
+  const double vp = vd * kInvP;
+  const uint32_t v2 = mulmod_q(v, vd, vp, v);
+  return mulmod_q(v2, exact_double(v2), vp, v);
+#else
+  const uint64_t sq = (uint64_t)v * v % kb::P;
+  return (uint32_t)(sq * v % kb::P);
+#endif
+}
+
+// x / 2, x canonical: (x + p) / 2 for odd x
+KB_HD uint32_t halve(uint32_t x) { return (x >> 1) + (x & 1u) * ((kb::P + 1) / 2); }
+
+// s +- x * 2^-k for canonical s, x and 1 <= k <= 24. With x = hi * 2^k + lo,
+// x * 2^-k = hi + lo * 2^-k and 2^-k = -127 * 2^(24-k) (mod p), because
+// 127 * 2^24 = p - 1; lo * 127 * 2^(24-k) < p.
+KB_HD uint32_t add_shr(uint32_t s, uint32_t x, int k) {
+  const uint32_t hi = x >> k, lo = x & ((1u << k) - 1u);
+  uint32_t u = s + kb::P - lo * (127u << (24 - k));  // (s, s + p]
+  u = kb::umin32(u, u - kb::P);
+  u += hi;  // < p + p / 2
+  return kb::umin32(u, u - kb::P);
+}
+KB_HD uint32_t sub_shr(uint32_t s, uint32_t x, int k) {
+  const uint32_t hi = x >> k, lo = x & ((1u << k) - 1u);
+  uint32_t u = s + lo * (127u << (24 - k));  // < 2p
+  u = kb::umin32(u, u - kb::P);
+  u = u + kb::P - hi;  // (p / 2, 2p)
+  return kb::umin32(u, u - kb::P);
+}
+
+// s + mu * x for the diagonal code of mu (a compile-time constant after
+// unrolling, so the switch folds away)
+KB_HD uint32_t diag_axpy(int code, uint32_t s, uint32_t x) {
+  using namespace kb;
+  switch (code) {
+    case 1: return add(s, x);
+    case 2: return add(s, dbl(x));
+    case 3: return add(s, add(dbl(x), x));
+    case 4: return add(s, dbl(dbl(x)));
+    case -2: return sub(s, dbl(x));
+    case -3: return sub(s, add(dbl(x), x));
+    case -4: return sub(s, dbl(dbl(x)));
+    case 101: return add(s, halve(x));
+    case 201: return sub(s, halve(x));
+    default: return code > 200 ? sub_shr(s, x, code - 200) : add_shr(s, x, code - 100);
+  }
+}
 
 template <int T>
 KB_HD void full_round(uint32_t (&x)[T], const uint32_t* rc) {
@@ -79,12 +173,10 @@ KB_HD void full_round(uint32_t (&x)[T], const uint32_t* rc) {
   ext_layer<T>(x);
 }
 
-// Internal round: S-box on x[0], then x_i <- sum(x) + mu_i * x_i, the sum as
-// a tree of four-element partial sums and the diagonal products in Shoup form
-// (canonical mu_i times a Montgomery-form x_i is the Montgomery form of the
-// product).
+// Internal round: S-box on x[0], then x_i <- sum(x) + mu_i * x_i with the sum
+// as a tree of four-element partial sums.
 template <int T>
-KB_HD void partial_round(uint32_t (&x)[T], uint32_t rc, const P2Consts& k) {
+KB_HD void partial_round(uint32_t (&x)[T], uint32_t rc) {
   using namespace kb;
   x[0] = cube(add(x[0], rc));
   uint32_t part[T / 4];
@@ -94,21 +186,33 @@ KB_HD void partial_round(uint32_t (&x)[T], uint32_t rc, const P2Consts& k) {
 #pragma unroll
   for (int c = 1; c < T / 4; c++) s = add(s, part[c]);
 #pragma unroll
-  for (int i = 0; i < T; i++) x[i] = add(s, mul_shoup(x[i], k.diag_c[i], k.diag_s[i]));
+  for (int i = 0; i < T; i++) x[i] = diag_axpy(diag_code(T, i), s, x[i]);
 }
 
-// The round loops stay rolled: a fully unrolled width-24 permutation is about
-// ten thousand instructions, more than the instruction cache holds, while one
-// round body is a few hundred. Round constants are read by index.
+// The permutation on canonical values. The round loops stay rolled: a fully
+// unrolled width-24 permutation is about ten thousand instructions, more than
+// the instruction cache holds, while one round body is a few hundred. Round
+// constants are read by index.
 template <int T, int RP>
-KB_HD void permute(uint32_t (&x)[T], const P2Consts& k) {
+KB_HD void permute_canonical(uint32_t (&x)[T], const P2Consts& k) {
   ext_layer<T>(x);
 #pragma unroll 1
   for (int r = 0; r < RF / 2; r++) full_round<T>(x, k.ext_rc + r * T);
 #pragma unroll 1
-  for (int r = 0; r < RP; r++) partial_round<T>(x, k.int_rc[r], k);
+  for (int r = 0; r < RP; r++) partial_round<T>(x, k.int_rc[r]);
 #pragma unroll 1
   for (int r = RF / 2; r < RF; r++) full_round<T>(x, k.ext_rc + r * T);
+}
+
+// The permutation on Montgomery-form values (the representation of every
+// field element stored on the device).
+template <int T, int RP>
+KB_HD void permute(uint32_t (&x)[T], const P2Consts& k) {
+#pragma unroll
+  for (int i = 0; i < T; i++) x[i] = kb::from_mont(x[i]);
+  permute_canonical<T, RP>(x, k);
+#pragma unroll
+  for (int i = 0; i < T; i++) x[i] = kb::to_mont(x[i]);
 }
 
 }  // namespace p2
