@@ -54,7 +54,9 @@ typedef struct {
   uint32_t rounds_p;
   uint32_t ext_rc[8 * 24]; /* rounds_f rows of `width`: first half before, second half after the partial rounds */
   uint32_t int_rc[32];     /* one per partial round, added to lane 0 */
-  uint32_t diag[24];       /* internal matrix = all-ones + diag(diag) */
+  uint32_t diag[24];       /* internal matrix = all-ones + diag(diag); fixed, as p3-koala-bear's internal
+                            * layer takes no diagonal: must equal whir_poseidon2_default_params' diag
+                            * (small integers and signed powers of two), else WHIR_ERR_INVALID */
 } whir_poseidon2_params;
 
 /* ProtocolParameters (src/parameters/mod.rs:147-166) plus the hash and
