@@ -99,10 +99,10 @@ KB_HD void ext_layer(uint32_t (&x)[T]) {
 }
 
 #ifdef __CUDA_ARCH__
-// a as an exact double: the bit pattern of 2^52 + a, minus 2^52
-__device__ __forceinline__ double exact_double(uint32_t a) {
-  return __hiloint2double(0x43300000, (int)a) - 4503599627370496.0;
-}
+// a as a double (exact: a < 2^53). A single conversion instruction; it was
+// measured faster in this permutation than building 2^52 + a from its bit
+// pattern and subtracting 2^52 (one instruction instead of two moves and an add).
+__device__ __forceinline__ double exact_double(uint32_t a) { return __uint2double_rn(a); }
 // a * b mod p for a, b < 2^31, given a as a double and bp = fl(b / p): adding
 // 1.5 * 2^52 rounds the quotient estimate to an integer held in the low
 // mantissa bits, read back as the low word.
@@ -173,18 +173,27 @@ KB_HD void full_round(uint32_t (&x)[T], const uint32_t* rc) {
   ext_layer<T>(x);
 }
 
-// Internal round: S-box on x[0], then x_i <- sum(x) + mu_i * x_i with the sum
-// as a tree of four-element partial sums.
+// Sum of T canonical values mod p without a reduction per addition: pairs of
+// values < p sum below 2^32, the pair sums accumulate in 64 bits (below
+// 2^36), and the total is reduced once with 2^32 = 2^25 - 2 (mod p).
+template <int T>
+KB_HD uint32_t sum_mod(const uint32_t (&x)[T]) {
+  uint64_t acc = 0;
+#pragma unroll
+  for (int i = 0; i < T; i += 2) acc += (uint64_t)(x[i] + x[i + 1]);
+  const uint32_t lo = (uint32_t)acc, hi = (uint32_t)(acc >> 32);
+  uint32_t u = kb::umin32(lo, lo - 2u * kb::P);  // lo < 2^32 < 3p
+  u = kb::umin32(u, u - kb::P);
+  u += hi * 33554430u;  // hi < 2^4: u < p + 2^29
+  return kb::umin32(u, u - kb::P);
+}
+
+// Internal round: S-box on x[0], then x_i <- sum(x) + mu_i * x_i.
 template <int T>
 KB_HD void partial_round(uint32_t (&x)[T], uint32_t rc) {
   using namespace kb;
   x[0] = cube(add(x[0], rc));
-  uint32_t part[T / 4];
-#pragma unroll
-  for (int c = 0; c < T / 4; c++) part[c] = add(add(x[4 * c], x[4 * c + 1]), add(x[4 * c + 2], x[4 * c + 3]));
-  uint32_t s = part[0];
-#pragma unroll
-  for (int c = 1; c < T / 4; c++) s = add(s, part[c]);
+  const uint32_t s = sum_mod<T>(x);
 #pragma unroll
   for (int i = 0; i < T; i++) x[i] = diag_axpy(diag_code(T, i), s, x[i]);
 }
