@@ -80,7 +80,7 @@ def test_eq_table(pkg, gpu_ctx, oracle, n):
     assert np.array_equal(d.to_host(), want)
 
 
-@pytest.mark.parametrize("n", [0, 1, 2, 8, 9, 13, 17, 20])
+@pytest.mark.parametrize("n", [0, 1, 2, 8, 9, 12, 13, 17, 20, 23])
 def test_eval_base_and_ext(pkg, gpu_ctx, oracle, n):
     rng = np.random.default_rng(n + 21)
     f = rnd(rng, 1 << n)
@@ -145,7 +145,9 @@ def test_combine_select(pkg, gpu_ctx, oracle, n, m):
     assert np.array_equal(d.to_host(), oracle.combine_select(w, vars_, g))
 
 
-@pytest.mark.parametrize("n,l", [(1, 1), (4, 4), (9, 3), (14, 4), (20, 6)])
+# from 2^12 elements per segment the base-field dot streams through shared
+# memory by bulk copies (one 4096-element chunk per stage)
+@pytest.mark.parametrize("n,l", [(1, 1), (4, 4), (9, 3), (14, 4), (16, 4), (20, 6), (21, 3), (22, 8)])
 def test_svo_partial_evals(pkg, gpu_ctx, oracle, n, l):
     rng = np.random.default_rng(n + 100 * l)
     f = rnd(rng, 1 << n)

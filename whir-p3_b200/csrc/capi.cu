@@ -122,7 +122,7 @@ int dot_eq(whir_ctx* ctx, const uint32_t* d_f, int ext, int seg_bits, const ef* 
   if (posted) *posted = seq;
   WH_TRY_CUDA(wk::dot_split(d_f, ext, seg_bits, m_bits, hi, lo, lo_bits, ctx->d_partials,
                             reinterpret_cast<unsigned*>(ctx->d_words) + 9, ctx->d_small, post ? ctx->d_mail : nullptr,
-                            seq, ctx->stream));
+                            seq, ctx->d_words + 11, ctx->stream));
   return WHIR_OK;
 }
 
@@ -681,6 +681,7 @@ static int eval_common(whir_ctx* ctx, const uint32_t* d_evals, int32_t n, const 
   WH_TRY(wh::dot_eq(ctx, d_evals, ext, 0, z.data(), n, &posted));
   ef r;
   WH_TRY(wh::fetch_posted(ctx, posted, &r, ctx->d_small, sizeof(ef)));
+  WH_TRY(wh::check_dot(&r, sizeof(ef)));
   store_ef_canon(out, r);
   return WHIR_OK;
 }
@@ -774,6 +775,7 @@ int whir_svo_partial_evals(whir_ctx* ctx, const uint32_t* d_poly, int32_t n, int
   WH_TRY(wh::dot_eq(ctx, d_poly, 0, l, z.data() + l, n - l, &posted));
   std::vector<ef> g((size_t)1 << l);
   WH_TRY(wh::fetch_posted(ctx, posted, g.data(), ctx->d_small, g.size() * sizeof(ef)));
+  WH_TRY(wh::check_dot(g.data(), g.size() * sizeof(ef)));
   ef eval = kb::ef_zero();
   wk::EqSmall e = wh::eq_small_host(z.data(), l);
   for (size_t y = 0; y < g.size(); y++) {

@@ -105,7 +105,7 @@ struct whir_ctx {
   kb::ef* d_partials = nullptr;  // 8192 ef
   kb::ef* d_small = nullptr;     // 256 ef
   uint32_t* d_words = nullptr;   // 16 words: grind result, claim and done counters (0-2), sumcheck round (8),
-                                 // dot product (9) and tree-top (10) counters
+                                 // dot product (9) and tree-top (10) counters, streamed-dot wait flag (11)
   void* d_arena = nullptr;       // general scratch (tables, gathers)
   size_t arena_bytes = 0;
   void* h_pinned = nullptr;      // staging for small transfers
@@ -129,6 +129,14 @@ struct whir_ctx {
 };
 
 namespace wh {
+// Dot-product results are field elements (< p); 0xffffffff in every word marks a
+// bounded device wait that gave up.
+inline int check_dot(const void* v, size_t bytes) {
+  const uint32_t* w = static_cast<const uint32_t*>(v);
+  for (size_t i = 0; i < bytes / 4; i++)
+    if (w[i] >= kb::P) return set_error("a device wait of the dot product timed out"), WHIR_ERR_CUDA;
+  return WHIR_OK;
+}
 // Stream-ordered allocation from the context's pool.
 inline cudaError_t ctx_malloc(whir_ctx* ctx, void* p, size_t bytes) {
   return cudaMallocFromPoolAsync(reinterpret_cast<void**>(p), bytes, ctx->pool, ctx->stream);

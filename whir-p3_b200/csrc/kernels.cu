@@ -1059,14 +1059,23 @@ __device__ __forceinline__ void coop_permute16(uint32_t (&x)[4], int q, const P2
     for (int j = 0; j < 4; j++) x[j] = p2::cube(add(x[j], k.ext_rc[r * 16 + 4 * q + j]));
     coop_ext_layer(x);
   }
+  // Internal rounds with word 0 replicated in all four lanes (w0): every lane
+  // computes its S-box, so the result needs no broadcast, and the sum of the
+  // other fifteen words (lane-local, then two shuffles) is independent of it,
+  // which leaves S-box, one addition and the diagonal product of word 0 as
+  // the round's dependent chain.
+  uint32_t w0 = __shfl_sync(0xffffffffu, x[0], (threadIdx.x & 31) & ~3);
 #pragma unroll 1
   for (int r = 0; r < p2::RP16; r++) {
-    if (q == 0) x[0] = p2::cube(add(x[0], k.int_rc[r]));
-    uint32_t s = add(add(x[0], x[1]), add(x[2], x[3]));
-    s = add(s, __shfl_xor_sync(0xffffffffu, s, 1));
-    s = add(s, __shfl_xor_sync(0xffffffffu, s, 2));
+    uint32_t o = add(add(q == 0 ? 0u : x[0], x[1]), add(x[2], x[3]));
+    o = add(o, __shfl_xor_sync(0xffffffffu, o, 1));
+    o = add(o, __shfl_xor_sync(0xffffffffu, o, 2));
+    const uint32_t y0 = p2::cube(add(w0, k.int_rc[r]));
+    const uint32_t s = add(o, y0);
 #pragma unroll
     for (int j = 0; j < 4; j++) x[j] = add(s, mul_shoup(x[j], k.diag_c[4 * q + j], k.diag_s[4 * q + j]));
+    w0 = p2::diag_axpy(p2::diag_code(16, 0), s, y0);
+    if (q == 0) x[0] = w0;
   }
 #pragma unroll 1
   for (int r = p2::RF / 2; r < p2::RF; r++) {
@@ -1502,14 +1511,81 @@ cudaError_t eq_outer(const ef* hi, const ef* lo, int lo_bits, size_t n, ef* out,
 
 constexpr int DOT_CTA = 256;
 
+// Block sum of each thread's `total`; the last CTA to finish (atomic counter,
+// no waiting) adds up every segment's partial sums into out[segment] and, with
+// `mail`, posts them to the mailbox. If *poison is set (a device wait in the
+// caller gave up), the results are 0xffffffff, which no field element is.
+__device__ __forceinline__ void dot_finish(ef total, ef* __restrict__ partials, unsigned* __restrict__ counter,
+                                           ef* __restrict__ out, uint32_t* mail, uint32_t seq,
+                                           const uint32_t* poison) {
+  __shared__ ef sh[1][32];
+  __shared__ bool s_last;
+  ef v[1] = {total};
+  block_sum<1>(v, sh);
+  // the last CTA to finish adds up every segment's partial sums
+  const unsigned nblocks = gridDim.x * gridDim.y;
+  if (threadIdx.x == 0) {
+    partials[(size_t)blockIdx.y * gridDim.x + blockIdx.x] = v[0];
+    __threadfence();
+    s_last = atomicAdd(counter, 1u) == nblocks - 1;
+  }
+  __syncthreads();
+  if (!s_last) return;
+  __threadfence();
+  const bool bad = poison && *reinterpret_cast<volatile const uint32_t*>(poison) != 0u;
+  const unsigned segs = gridDim.y, nb = gridDim.x;
+  if (segs >= 8 && DOT_CTA % segs == 0 && DOT_CTA / segs <= 32) {
+    // one group of DOT_CTA / segs lanes per segment, all segments at once
+    const unsigned gsz = DOT_CTA / segs, lane = threadIdx.x % gsz, sg = threadIdx.x / gsz;
+    ef a = kb::ef_zero();
+    for (unsigned b = lane; b < nb; b += gsz) {
+      const uint4 x = __ldcg(reinterpret_cast<const uint4*>(partials + (size_t)sg * nb + b));
+      a = kb::ef_add(a, ef{{x.x, x.y, x.z, x.w}});
+    }
+    for (unsigned o = gsz / 2; o >= 1; o >>= 1)
+#pragma unroll
+      for (int c = 0; c < 4; c++) a.c[c] = kb::add(a.c[c], __shfl_xor_sync(0xffffffffu, a.c[c], o));
+    if (bad) a = ef{{0xffffffffu, 0xffffffffu, 0xffffffffu, 0xffffffffu}};
+    if (lane == 0) {
+      out[sg] = a;
+      if (mail) {
+        for (int c = 0; c < 4; c++) reinterpret_cast<volatile uint32_t*>(mail)[4 * sg + c] = a.c[c];
+        __threadfence_system();
+      }
+    }
+    __syncthreads();
+  } else {
+    for (unsigned s2 = 0; s2 < segs; s2++) {
+      ef a[1] = {kb::ef_zero()};
+      for (unsigned b = threadIdx.x; b < nb; b += blockDim.x) {
+        const uint4 x = __ldcg(reinterpret_cast<const uint4*>(partials + (size_t)s2 * nb + b));
+        a[0] = kb::ef_add(a[0], ef{{x.x, x.y, x.z, x.w}});
+      }
+      block_sum<1>(a, sh);
+      if (bad) a[0] = ef{{0xffffffffu, 0xffffffffu, 0xffffffffu, 0xffffffffu}};
+      if (threadIdx.x == 0) {
+        out[s2] = a[0];
+        if (mail)
+          for (int c = 0; c < 4; c++) reinterpret_cast<volatile uint32_t*>(mail)[4 * s2 + c] = a[0].c[c];
+      }
+      __syncthreads();
+    }
+  }
+  if (threadIdx.x == 0) {
+    *counter = 0u;
+    if (mail) {
+      __threadfence_system();
+      reinterpret_cast<volatile uint32_t*>(mail)[kMailWords] = seq;
+    }
+  }
+}
+
 template <int EXT>
 __global__ void __launch_bounds__(DOT_CTA) k_dot_split(const uint32_t* __restrict__ f, int m_bits,
                                                         const ef* __restrict__ hi, const ef* __restrict__ lo,
                                                         int lo_bits, int wide, ef* __restrict__ partials,
                                                         unsigned* __restrict__ counter, ef* __restrict__ out,
                                                         uint32_t* mail, uint32_t seq) {
-  __shared__ ef sh[1][32];
-  __shared__ bool s_last;
   const size_t M = (size_t)1 << m_bits;
   const int seg = blockIdx.y;
   const uint32_t lomask = (1u << lo_bits) - 1;
@@ -1580,69 +1656,156 @@ __global__ void __launch_bounds__(DOT_CTA) k_dot_split(const uint32_t* __restric
     if (!EXT) lazy.fold(acc);
     total = kb::ef_mul(acc, ld_ef(lo + xl));
   }
-  ef v[1] = {total};
-  block_sum<1>(v, sh);
-  // the last CTA to finish adds up every segment's partial sums
-  const unsigned nblocks = gridDim.x * gridDim.y;
-  if (threadIdx.x == 0) {
-    partials[(size_t)seg * gridDim.x + blockIdx.x] = v[0];
-    __threadfence();
-    s_last = atomicAdd(counter, 1u) == nblocks - 1;
+  dot_finish(total, partials, counter, out, mail, seq, nullptr);
+}
+
+// Base-field dot product streamed through shared memory: each CTA takes a
+// contiguous run of its segment in 16 KiB chunks, which one thread loads with
+// bulk copies (cp.async.bulk, completion counted on an mbarrier per stage) four
+// stages ahead, so the copy engine keeps the bytes in flight while every thread
+// computes from shared memory. Thread t takes the 16-byte words t + 256u
+// (u < 4) of a chunk: elements 4t + 1024u + j, whose high index is shared by
+// the four j (lo_bits >= 2) and whose low index (4t + j) & lomask is the same
+// in every chunk (1024 is a multiple of 2^lo_bits, lo_bits <= 8).
+namespace dstream {
+constexpr int kCta = 256, kStages = 4, kChunk = kCta * 16;  // elements per stage
+constexpr uint32_t kBytes = kChunk * 4;
+constexpr uint32_t kPolls = 1u << 22;  // bound on the polls of one wait
+__device__ __forceinline__ uint32_t saddr(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+__device__ __forceinline__ void bar_init(uint64_t* b) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(saddr(b)) : "memory");
+}
+__device__ __forceinline__ void bar_expect(uint64_t* b, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(saddr(b)), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ bool bar_test(uint64_t* b, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\tmbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, p;\n}"
+      : "=r"(ok)
+      : "r"(saddr(b)), "r"(parity)
+      : "memory");
+  return ok != 0u;
+}
+// Waits for the phase of `parity` to complete; false after kPolls polls.
+__device__ __forceinline__ bool bar_wait(uint64_t* b, uint32_t parity) {
+  for (uint32_t i = 0; i < kPolls; i++) {
+    if (bar_test(b, parity)) return true;
+    if (i >= 64) __nanosleep(128);
+  }
+  return false;
+}
+__device__ __forceinline__ void bulk_load(void* dst, const void* src, uint64_t* b) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                   saddr(dst)),
+               "l"(src), "r"(kBytes), "r"(saddr(b))
+               : "memory");
+}
+}  // namespace dstream
+
+__global__ void __launch_bounds__(dstream::kCta) k_dot_stream(const uint32_t* __restrict__ f, int m_bits,
+                                                               const ef* __restrict__ hi, const ef* __restrict__ lo,
+                                                               int lo_bits, ef* __restrict__ partials,
+                                                               unsigned* __restrict__ counter, ef* __restrict__ out,
+                                                               uint32_t* mail, uint32_t seq, uint32_t* err) {
+  using namespace dstream;
+  extern __shared__ __align__(128) uint4 stage_buf[];  // kStages * kCta * 4 words of 16 bytes
+  __shared__ __align__(8) uint64_t full[kStages];
+  const size_t M = (size_t)1 << m_bits;
+  const int seg = blockIdx.y, t = threadIdx.x;
+  const unsigned nch = (unsigned)(M / kChunk);
+  const unsigned c0 = (unsigned)((uint64_t)nch * blockIdx.x / gridDim.x);
+  const unsigned n = (unsigned)((uint64_t)nch * (blockIdx.x + 1) / gridDim.x) - c0;
+  const uint32_t* src = f + (size_t)seg * M + (size_t)c0 * kChunk;
+  if (t == 0) {
+    for (int st = 0; st < kStages; st++) bar_init(&full[st]);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    for (unsigned i = 0; i < n && i < (unsigned)kStages; i++) {
+      bar_expect(&full[i], kBytes);
+      bulk_load(stage_buf + (size_t)i * kCta * 4, src + (size_t)i * kChunk, &full[i]);
+    }
   }
   __syncthreads();
-  if (!s_last) return;
-  __threadfence();
-  const unsigned segs = gridDim.y, nb = gridDim.x;
-  if (segs >= 8 && DOT_CTA % segs == 0 && DOT_CTA / segs <= 32) {
-    // one group of DOT_CTA / segs lanes per segment, all segments at once
-    const unsigned gsz = DOT_CTA / segs, lane = threadIdx.x % gsz, sg = threadIdx.x / gsz;
-    ef a = kb::ef_zero();
-    for (unsigned b = lane; b < nb; b += gsz) {
-      const uint4 x = __ldcg(reinterpret_cast<const uint4*>(partials + (size_t)sg * nb + b));
-      a = kb::ef_add(a, ef{{x.x, x.y, x.z, x.w}});
-    }
-    for (unsigned o = gsz / 2; o >= 1; o >>= 1)
+  ef acc[4];
 #pragma unroll
-      for (int c = 0; c < 4; c++) a.c[c] = kb::add(a.c[c], __shfl_xor_sync(0xffffffffu, a.c[c], o));
-    if (lane == 0) {
-      out[sg] = a;
-      if (mail) {
-        for (int c = 0; c < 4; c++) reinterpret_cast<volatile uint32_t*>(mail)[4 * sg + c] = a.c[c];
-        __threadfence_system();
+  for (int j = 0; j < 4; j++) acc[j] = kb::ef_zero();
+  unsigned i = 0;
+  bool bad = false;
+  for (; i < n; i++) {
+    const int st = (int)(i % kStages);
+    const bool ok = bar_wait(&full[st], (i / kStages) & 1u);
+    if (ok) {
+      const uint4* b = stage_buf + (size_t)st * kCta * 4;
+      const size_t cb = (size_t)(c0 + i) * kChunk;
+      uint64_t acc64[4][4];
+#pragma unroll
+      for (int j = 0; j < 4; j++)
+#pragma unroll
+        for (int c = 0; c < 4; c++) acc64[j][c] = 0;
+#pragma unroll
+      for (int u = 0; u < 4; u++) {
+        const uint4 v = b[t + kCta * u];
+        const ef h = ld_ef(hi + ((cb + 4u * t + 1024u * u) >> lo_bits));
+        const uint32_t e[4] = {v.x, v.y, v.z, v.w};
+#pragma unroll
+        for (int j = 0; j < 4; j++)
+#pragma unroll
+          for (int c = 0; c < 4; c++) acc64[j][c] += (uint64_t)h.c[c] * e[j];  // four products < 2^64
       }
+#pragma unroll
+      for (int j = 0; j < 4; j++)
+        acc[j] = kb::ef_add(acc[j], ef{{kb::reduce_wide(acc64[j][0]), kb::reduce_wide(acc64[j][1]),
+                                        kb::reduce_wide(acc64[j][2]), kb::reduce_wide(acc64[j][3])}});
     }
-    __syncthreads();
-  } else {
-    for (unsigned s2 = 0; s2 < segs; s2++) {
-      ef a[1] = {kb::ef_zero()};
-      for (unsigned b = threadIdx.x; b < nb; b += blockDim.x) {
-        const uint4 x = __ldcg(reinterpret_cast<const uint4*>(partials + (size_t)s2 * nb + b));
-        a[0] = kb::ef_add(a[0], ef{{x.x, x.y, x.z, x.w}});
-      }
-      block_sum<1>(a, sh);
-      if (threadIdx.x == 0) {
-        out[s2] = a[0];
-        if (mail)
-          for (int c = 0; c < 4; c++) reinterpret_cast<volatile uint32_t*>(mail)[4 * s2 + c] = a[0].c[c];
-      }
-      __syncthreads();
+    // every thread has read stage st (or the CTA gives up together)
+    if (__syncthreads_or(!ok)) {
+      bad = true;
+      break;
+    }
+    if (t == 0 && i + kStages < n) {
+      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+      bar_expect(&full[st], kBytes);
+      bulk_load(stage_buf + (size_t)st * kCta * 4, src + (size_t)(i + kStages) * kChunk, &full[st]);
     }
   }
-  if (threadIdx.x == 0) {
-    *counter = 0u;
-    if (mail) {
-      __threadfence_system();
-      reinterpret_cast<volatile uint32_t*>(mail)[kMailWords] = seq;
-    }
+  if (bad && t == 0) {
+    // a wait gave up: flag it, then wait (bounded again) for the copies this
+    // CTA still has in flight before its shared memory is released
+    atomicOr(err, 1u);
+    for (unsigned k = i; k < n && k < i + kStages; k++) bar_wait(&full[k % kStages], (k / kStages) & 1u);
   }
+  const uint32_t lomask = (1u << lo_bits) - 1;
+  ef total = kb::ef_zero();
+#pragma unroll
+  for (int j = 0; j < 4; j++) total = kb::ef_add(total, kb::ef_mul(acc[j], ld_ef(lo + ((4u * t + j) & lomask))));
+  dot_finish(total, partials, counter, out, mail, seq, err);
 }
 
 cudaError_t dot_split(const uint32_t* f, int ext, int seg_bits, int m_bits, const ef* hi, const ef* lo, int lo_bits,
-                      ef* partials, unsigned* counter, ef* out, uint32_t* mail, uint32_t seq, cudaStream_t st) {
+                      ef* partials, unsigned* counter, ef* out, uint32_t* mail, uint32_t seq, uint32_t* err,
+                      cudaStream_t st) {
   if (mail && (4 << seg_bits) > kMailWords) return cudaErrorInvalidValue;
   if (lo_bits > 8 || lo_bits > m_bits || seg_bits < 0 || seg_bits > 8) return cudaErrorInvalidValue;
   const size_t M = (size_t)1 << m_bits;
   const int segs = 1 << seg_bits;
+  if (!ext && err && lo_bits >= 2 && M >= (size_t)dstream::kChunk && ((uintptr_t)f & 15) == 0) {
+    constexpr int smem = dstream::kStages * dstream::kCta * 64;
+    static std::once_flag once;
+    static int per_sm = 1;
+    std::call_once(once, [] {
+      cudaFuncSetAttribute(k_dot_stream, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+      int n = 0;
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_dot_stream, dstream::kCta, smem);
+      per_sm = n > 0 ? n : 1;
+    });
+    const size_t nch = M / dstream::kChunk;
+    size_t bx = ((size_t)sm_count() * per_sm + segs - 1) / segs;
+    if (bx > nch) bx = nch;
+    if (bx < 1) bx = 1;
+    k_dot_stream<<<dim3((unsigned)bx, segs), dstream::kCta, smem, st>>>(f, m_bits, hi, lo, lo_bits, partials,
+                                                                         counter, out, mail, seq, err);
+    LAUNCH_DONE();
+  }
   const int wide = !ext && lo_bits >= 2 && M >= 4 * (size_t)DOT_CTA && ((uintptr_t)f & 15) == 0;
   // one wave of resident CTAs (the wide path holds many registers): more CTAs
   // than fit would only queue behind the first wave

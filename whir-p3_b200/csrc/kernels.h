@@ -130,10 +130,13 @@ cudaError_t eq_table_pair(const EqPoint& p1, kb::ef* out1, const EqPoint& p2, kb
 // (at most 8 * SMs); the last CTA to finish reduces them into out, using
 // `counter` (device, one word, 0 before the first launch, left at 0), and with
 // `mail` set also posts them to that mailbox with flag `seq` (needs
-// 4 * 2^seg_bits <= kMailWords).
+// 4 * 2^seg_bits <= kMailWords). Base-field inputs (16-byte aligned, at least
+// 4096 per segment) stream through shared memory by bulk copies; `err`
+// (device, one word) is set if one of that kernel's bounded waits gives up,
+// and then every result is 0xffffffff.
 cudaError_t dot_split(const uint32_t* f, int ext, int seg_bits, int m_bits, const kb::ef* hi, const kb::ef* lo,
                       int lo_bits, kb::ef* partials, unsigned* counter, kb::ef* out, uint32_t* mail, uint32_t seq,
-                      cudaStream_t st);
+                      uint32_t* err, cudaStream_t st);
 
 // compress (fold the first variable) on one or two extension arrays in place;
 // `shape` threads 128, 256 or 512

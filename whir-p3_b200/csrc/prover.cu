@@ -308,6 +308,7 @@ int evaluate_constraint(whir_ctx* ctx, whir_witness* w, const std::vector<ef>& p
   out->point = point;
   out->partial.resize((size_t)1 << k0);
   WH_TRY(wh::fetch_posted(ctx, posted, out->partial.data(), ctx->d_small, out->partial.size() * sizeof(ef)));
+  WH_TRY(wh::check_dot(out->partial.data(), out->partial.size() * sizeof(ef)));
   wk::EqSmall e = wh::eq_small_host(point.data(), k0);
   ef eval = kb::ef_zero();
   for (size_t y = 0; y < out->partial.size(); y++) eval = kb::ef_add(eval, kb::ef_mul(e.v[y], out->partial[y]));
