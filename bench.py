@@ -229,6 +229,8 @@ def run_micro(args) -> None:
     if "eq" in kinds:
         emit("eq_table 2^24 ext", timed(lambda: pkg.eq_table(ctx, point, scale, f)), alg_bytes=16 * N)
     if "eval" in kinds:
+        fb = pkg.DeviceArray.from_host(ctx, rng.integers(0, P, N, dtype=np.uint64).astype(np.uint32))
+        emit("eval_base 2^24 base", timed(lambda: pkg.eval_base(ctx, fb, point)), alg_bytes=4 * N)
         emit("eval_ext 2^24 ext", timed(lambda: pkg.eval_ext(ctx, f, point)), alg_bytes=16 * N)
     if "fold" in kinds:
         r = rng.integers(0, P, 4, dtype=np.uint64).astype(np.uint32)
