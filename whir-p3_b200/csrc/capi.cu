@@ -242,22 +242,29 @@ int grind(whir_ctx* ctx, Chal& ch, int bits, uint32_t* witness) {
 }  // namespace wh
 
 namespace wh {
-// eq table of k <= 6 challenge coordinates on the host (Montgomery)
-wk::EqSmall eq_small_host(const ef* rs, int k) {
-  wk::EqSmall e;
-  memset(&e, 0, sizeof(e));
-  e.v[0] = kb::ef_one();
+// eq table of k challenge coordinates on the host (Montgomery), 2^k entries
+std::vector<ef> eq_host(const ef* rs, int k) {
+  std::vector<ef> v((size_t)1 << k, kb::ef_zero());
+  v[0] = kb::ef_one();
   for (int i = 0; i < k; i++) {
     // bit i (from the bottom) of y <-> rs[k-1-i]
     const ef z = rs[k - 1 - i];
-    const int half = 1 << i;
-    for (int y = 0; y < half; y++) {
-      ef lo = e.v[y];
-      ef hi = kb::ef_mul(lo, z);
-      e.v[y + half] = hi;
-      e.v[y] = kb::ef_sub(lo, hi);
+    const size_t half = (size_t)1 << i;
+    for (size_t y = 0; y < half; y++) {
+      const ef lo = v[y];
+      const ef hi = kb::ef_mul(lo, z);
+      v[y + half] = hi;
+      v[y] = kb::ef_sub(lo, hi);
     }
   }
+  return v;
+}
+// the same for k <= 6 (the kernels' fixed-size table; callers check k)
+wk::EqSmall eq_small_host(const ef* rs, int k) {
+  wk::EqSmall e;
+  memset(&e, 0, sizeof(e));
+  const std::vector<ef> v = eq_host(rs, k < 6 ? k : 6);
+  for (size_t y = 0; y < v.size(); y++) e.v[y] = v[y];
   return e;
 }
 }  // namespace wh
@@ -777,10 +784,10 @@ int whir_svo_partial_evals(whir_ctx* ctx, const uint32_t* d_poly, int32_t n, int
   WH_TRY(wh::fetch_posted(ctx, posted, g.data(), ctx->d_small, g.size() * sizeof(ef)));
   WH_TRY(wh::check_dot(g.data(), g.size() * sizeof(ef)));
   ef eval = kb::ef_zero();
-  wk::EqSmall e = wh::eq_small_host(z.data(), l);
+  const std::vector<ef> e = wh::eq_host(z.data(), l);  // 2^l <= 256 entries
   for (size_t y = 0; y < g.size(); y++) {
     store_ef_canon(out + 4 * y, g[y]);
-    eval = kb::ef_add(eval, kb::ef_mul(e.v[y], g[y]));
+    eval = kb::ef_add(eval, kb::ef_mul(e[y], g[y]));
   }
   if (eval_out) store_ef_canon(eval_out, eval);
   return WHIR_OK;
