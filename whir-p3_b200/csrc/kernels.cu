@@ -1662,14 +1662,18 @@ __global__ void __launch_bounds__(DOT_CTA) k_dot_split(const uint32_t* __restric
 // Base-field dot product streamed through shared memory: each CTA takes a
 // contiguous run of its segment in 16 KiB chunks, which one thread loads with
 // bulk copies (cp.async.bulk, completion counted on an mbarrier per stage) four
-// stages ahead, so the copy engine keeps the bytes in flight while every thread
-// computes from shared memory. Thread t takes the 16-byte words t + 256u
-// (u < 4) of a chunk: elements 4t + 1024u + j, whose high index is shared by
-// the four j (lo_bits >= 2) and whose low index (4t + j) & lomask is the same
-// in every chunk (1024 is a multiple of 2^lo_bits, lo_bits <= 8).
+// stages ahead, together with the chunk's 16 high-index eq entries, so the
+// copy engine keeps the bytes in flight while every thread computes from
+// shared memory. With lo_bits = 8, thread t takes the 16-byte words t + 256u
+// (u < 4) of a chunk: elements 4t + 1024u + j, whose high index is entry
+// (t >> 6) + 4u of the chunk's slice and whose low index (4t + j) is the same
+// in every chunk.
 namespace dstream {
 constexpr int kCta = 256, kStages = 4, kChunk = kCta * 16;  // elements per stage
 constexpr uint32_t kBytes = kChunk * 4;
+constexpr int kHi = kChunk >> 8;                    // high-index entries per chunk
+constexpr uint32_t kHiBytes = kHi * 16;
+constexpr int kStageWords = kCta * 4 + kHi;         // 16-byte words per stage
 constexpr uint32_t kPolls = 1u << 22;  // bound on the polls of one wait
 __device__ __forceinline__ uint32_t saddr(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
 __device__ __forceinline__ void bar_init(uint64_t* b) {
@@ -1695,35 +1699,39 @@ __device__ __forceinline__ bool bar_wait(uint64_t* b, uint32_t parity) {
   }
   return false;
 }
-__device__ __forceinline__ void bulk_load(void* dst, const void* src, uint64_t* b) {
+__device__ __forceinline__ void bulk_load(void* dst, const void* src, uint32_t bytes, uint64_t* b) {
   asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
                    saddr(dst)),
-               "l"(src), "r"(kBytes), "r"(saddr(b))
+               "l"(src), "r"(bytes), "r"(saddr(b))
                : "memory");
+}
+// chunk c of the segment and its high-index slice into stage buffer `buf`
+__device__ __forceinline__ void load_chunk(uint4* buf, const uint32_t* src, const kb::ef* hi, unsigned c, uint64_t* b) {
+  bar_expect(b, kBytes + kHiBytes);
+  bulk_load(buf, src + (size_t)c * kChunk, kBytes, b);
+  bulk_load(buf + kCta * 4, hi + (size_t)c * kHi, kHiBytes, b);
 }
 }  // namespace dstream
 
 __global__ void __launch_bounds__(dstream::kCta) k_dot_stream(const uint32_t* __restrict__ f, int m_bits,
                                                                const ef* __restrict__ hi, const ef* __restrict__ lo,
-                                                               int lo_bits, ef* __restrict__ partials,
+                                                               ef* __restrict__ partials,
                                                                unsigned* __restrict__ counter, ef* __restrict__ out,
                                                                uint32_t* mail, uint32_t seq, uint32_t* err) {
   using namespace dstream;
-  extern __shared__ __align__(128) uint4 stage_buf[];  // kStages * kCta * 4 words of 16 bytes
+  extern __shared__ __align__(128) uint4 stage_buf[];  // kStages * kStageWords words of 16 bytes
   __shared__ __align__(8) uint64_t full[kStages];
   const size_t M = (size_t)1 << m_bits;
   const int seg = blockIdx.y, t = threadIdx.x;
   const unsigned nch = (unsigned)(M / kChunk);
   const unsigned c0 = (unsigned)((uint64_t)nch * blockIdx.x / gridDim.x);
   const unsigned n = (unsigned)((uint64_t)nch * (blockIdx.x + 1) / gridDim.x) - c0;
-  const uint32_t* src = f + (size_t)seg * M + (size_t)c0 * kChunk;
+  const uint32_t* src = f + (size_t)seg * M;
   if (t == 0) {
     for (int st = 0; st < kStages; st++) bar_init(&full[st]);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-    for (unsigned i = 0; i < n && i < (unsigned)kStages; i++) {
-      bar_expect(&full[i], kBytes);
-      bulk_load(stage_buf + (size_t)i * kCta * 4, src + (size_t)i * kChunk, &full[i]);
-    }
+    for (unsigned i = 0; i < n && i < (unsigned)kStages; i++)
+      load_chunk(stage_buf + (size_t)i * kStageWords, src, hi, c0 + i, &full[i]);
   }
   __syncthreads();
   ef acc[4];
@@ -1735,8 +1743,7 @@ __global__ void __launch_bounds__(dstream::kCta) k_dot_stream(const uint32_t* __
     const int st = (int)(i % kStages);
     const bool ok = bar_wait(&full[st], (i / kStages) & 1u);
     if (ok) {
-      const uint4* b = stage_buf + (size_t)st * kCta * 4;
-      const size_t cb = (size_t)(c0 + i) * kChunk;
+      const uint4* b = stage_buf + (size_t)st * kStageWords;
       uint64_t acc64[4][4];
 #pragma unroll
       for (int j = 0; j < 4; j++)
@@ -1745,7 +1752,8 @@ __global__ void __launch_bounds__(dstream::kCta) k_dot_stream(const uint32_t* __
 #pragma unroll
       for (int u = 0; u < 4; u++) {
         const uint4 v = b[t + kCta * u];
-        const ef h = ld_ef(hi + ((cb + 4u * t + 1024u * u) >> lo_bits));
+        const uint4 hw = b[kCta * 4 + (t >> 6) + 4 * u];
+        const ef h{{hw.x, hw.y, hw.z, hw.w}};
         const uint32_t e[4] = {v.x, v.y, v.z, v.w};
 #pragma unroll
         for (int j = 0; j < 4; j++)
@@ -1764,8 +1772,7 @@ __global__ void __launch_bounds__(dstream::kCta) k_dot_stream(const uint32_t* __
     }
     if (t == 0 && i + kStages < n) {
       asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-      bar_expect(&full[st], kBytes);
-      bulk_load(stage_buf + (size_t)st * kCta * 4, src + (size_t)(i + kStages) * kChunk, &full[st]);
+      load_chunk(stage_buf + (size_t)st * kStageWords, src, hi, c0 + i + kStages, &full[st]);
     }
   }
   if (bad && t == 0) {
@@ -1774,10 +1781,9 @@ __global__ void __launch_bounds__(dstream::kCta) k_dot_stream(const uint32_t* __
     atomicOr(err, 1u);
     for (unsigned k = i; k < n && k < i + kStages; k++) bar_wait(&full[k % kStages], (k / kStages) & 1u);
   }
-  const uint32_t lomask = (1u << lo_bits) - 1;
   ef total = kb::ef_zero();
 #pragma unroll
-  for (int j = 0; j < 4; j++) total = kb::ef_add(total, kb::ef_mul(acc[j], ld_ef(lo + ((4u * t + j) & lomask))));
+  for (int j = 0; j < 4; j++) total = kb::ef_add(total, kb::ef_mul(acc[j], ld_ef(lo + ((4u * t + j) & 255u))));
   dot_finish(total, partials, counter, out, mail, seq, err);
 }
 
@@ -1788,8 +1794,9 @@ cudaError_t dot_split(const uint32_t* f, int ext, int seg_bits, int m_bits, cons
   if (lo_bits > 8 || lo_bits > m_bits || seg_bits < 0 || seg_bits > 8) return cudaErrorInvalidValue;
   const size_t M = (size_t)1 << m_bits;
   const int segs = 1 << seg_bits;
-  if (!ext && err && lo_bits >= 2 && M >= (size_t)dstream::kChunk && ((uintptr_t)f & 15) == 0) {
-    constexpr int smem = dstream::kStages * dstream::kCta * 64;
+  if (!ext && err && lo_bits == 8 && M >= (size_t)dstream::kChunk && ((uintptr_t)f & 15) == 0 &&
+      ((uintptr_t)hi & 15) == 0) {
+    constexpr int smem = dstream::kStages * dstream::kStageWords * 16;
     static std::once_flag once;
     static int per_sm = 1;
     std::call_once(once, [] {
@@ -1802,8 +1809,8 @@ cudaError_t dot_split(const uint32_t* f, int ext, int seg_bits, int m_bits, cons
     size_t bx = ((size_t)sm_count() * per_sm + segs - 1) / segs;
     if (bx > nch) bx = nch;
     if (bx < 1) bx = 1;
-    k_dot_stream<<<dim3((unsigned)bx, segs), dstream::kCta, smem, st>>>(f, m_bits, hi, lo, lo_bits, partials,
-                                                                         counter, out, mail, seq, err);
+    k_dot_stream<<<dim3((unsigned)bx, segs), dstream::kCta, smem, st>>>(f, m_bits, hi, lo, partials, counter, out,
+                                                                         mail, seq, err);
     LAUNCH_DONE();
   }
   const int wide = !ext && lo_bits >= 2 && M >= 4 * (size_t)DOT_CTA && ((uintptr_t)f & 15) == 0;
