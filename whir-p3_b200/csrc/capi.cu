@@ -394,6 +394,8 @@ int whir_ctx_create(int32_t device, const whir_poseidon2_params* p16, const whir
     return wh::set_error("device allocation failed"), fail(WHIR_ERR_NOMEM);
   c->arena_bytes = kArenaBytes;
   if (cudaMemset(c->d_words, 0, 64) != cudaSuccess) return wh::set_error("device memset failed"), fail(WHIR_ERR_CUDA);
+  if (wk::grind_reset(c->d_words, c->d_words + 1, c->d_words + 2, c->stream) != cudaSuccess)
+    return wh::set_error("grind state initialisation failed"), fail(WHIR_ERR_CUDA);
   if (cudaHostAlloc(&c->h_pinned, kPinnedBytes, cudaHostAllocDefault) != cudaSuccess)
     return wh::set_error("pinned allocation failed"), fail(WHIR_ERR_NOMEM);
   c->pinned_bytes = kPinnedBytes;

@@ -1373,12 +1373,17 @@ __global__ void __launch_bounds__(GRIND_CTA) k_grind(const __grid_constant__ P2C
     __syncthreads();
     if (!go) {
       // every atomicMin of this CTA precedes the barriers above; the last CTA
-      // to stop holds the final result and posts it to the mailbox
+      // to stop holds the final result, posts it to the mailbox and resets
+      // the search state for the next search (every other CTA has finished
+      // with it), which then needs no initialising launch
       if (threadIdx.x == 0 && mail) {
         __threadfence();
         if (atomicAdd(done, 1u) == gridDim.x - 1) {
           const uint32_t r = atomicAdd(result, 0u);
           mail_post(mail, &r, 1, seq);
+          *result = kb::P;
+          *counter = 0u;
+          *done = 0u;
         }
       }
       return;
@@ -1400,6 +1405,11 @@ __global__ void k_grind_init(uint32_t* result, uint32_t* counter, uint32_t* done
   *done = 0u;
 }
 
+cudaError_t grind_reset(uint32_t* result, uint32_t* counter, uint32_t* done, cudaStream_t st) {
+  k_grind_init<<<1, 1, 0, st>>>(result, counter, done);
+  LAUNCH_DONE();
+}
+
 cudaError_t grind(const uint32_t* state, const uint32_t* in, int in_len, int bits, uint64_t limit,
                   uint32_t* result, uint32_t* counter, uint32_t* done, uint32_t* mail, uint32_t seq,
                   const P2Consts& p16, cudaStream_t st) {
@@ -1410,8 +1420,12 @@ cudaError_t grind(const uint32_t* state, const uint32_t* in, int in_len, int bit
   uint32_t s[16];
   for (int i = 0; i < 16; i++) s[i] = kb::from_mont(state[i]);
   for (int i = 0; i < in_len; i++) s[i] = kb::from_mont(in[i]);
-  k_grind_init<<<1, 1, 0, st>>>(result, counter, done);
-  count_launch();
+  // with a mailbox the previous search left the state reset (grind_reset
+  // initialises it once per context)
+  if (!mail) {
+    k_grind_init<<<1, 1, 0, st>>>(result, counter, done);
+    count_launch();
+  }
   uint4 a = make_uint4(s[0], s[1], s[2], s[3]), b = make_uint4(s[4], s[5], s[6], s[7]);
   uint4 c = make_uint4(s[8], s[9], s[10], s[11]), d = make_uint4(s[12], s[13], s[14], s[15]);
   // Candidates in flight: once the smallest witness w is found, every claim

@@ -107,6 +107,9 @@ cudaError_t merkle_open(const uint32_t* rows, const uint32_t* digests, int log_h
 // the witness or p if none; `counter` and `done` (device, 1 word each) are
 // scratch. With `mail` set, the result is also posted to that mailbox with
 // flag `seq` by the last CTA to stop.
+// Search state (result = p, counters 0) before the first search with a
+// mailbox on these words; each such search leaves it reset for the next.
+cudaError_t grind_reset(uint32_t* result, uint32_t* counter, uint32_t* done, cudaStream_t st);
 cudaError_t grind(const uint32_t* state, const uint32_t* in, int in_len, int bits, uint64_t limit,
                   uint32_t* result, uint32_t* counter, uint32_t* done, uint32_t* mail, uint32_t seq,
                   const p2::P2Consts& p16, cudaStream_t st);
