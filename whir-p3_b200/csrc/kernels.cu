@@ -486,6 +486,14 @@ __global__ void __launch_bounds__(1 << (LG + LT))
   }
   __syncthreads();
   const size_t i2 = (size_t)(i2_0 + t);
+  // Four-step twist omega_H^(I r1) for the element column I = i2 >> ls and
+  // r1 = k + E m: omega^(I k) times (omega^(I E))^m, as two running powers
+  // (even and odd m, stepping by omega^(2 I E)) instead of a table lookup pair
+  // per element. I k and I E stay below H.
+  const uint32_t I = (uint32_t)(i2 >> ls);
+  const auto twist = [&](uint32_t e) { return kb::mul(__ldg(tw_lo + (e & 4095u)), __ldg(tw_hi + (e >> 12))); };
+  const uint32_t step = twist(I * (uint32_t)E);
+  const uint32_t step2 = kb::mul(step, step);
 #pragma unroll
   for (int q = 0; q < E / G; q++) {
     const int k = g + G * q;
@@ -493,13 +501,17 @@ __global__ void __launch_bounds__(1 << (LG + LT))
 #pragma unroll
     for (int gg = 0; gg < G; gg++) b[gg] = sm[t * VS + k * RS + gg];
     dftreg::dif<LG>(b);
+    uint32_t we = twist(I * (uint32_t)k);  // m even
+    uint32_t wo = kb::mul(we, step);        // m odd
 #pragma unroll
-    for (int r = 0; r < G; r++) {
-      const int r1 = k + E * dftreg::bitrev(r, LG);
-      const uint64_t ex = (i2 >> ls) * (uint64_t)r1;
-      uint32_t v = b[r];
-      if (ex) v = kb::mul(v, kb::mul(__ldg(tw_lo + (ex & 4095)), __ldg(tw_hi + (ex >> 12))));
-      y[((size_t)j << log_h) + ((size_t)r1 << log_h2) + i2] = v;
+    for (int m = 0; m < G; m += 2) {
+      const int r1 = k + E * m;
+      y[((size_t)j << log_h) + ((size_t)r1 << log_h2) + i2] = kb::mul(b[dftreg::bitrev(m, LG)], we);
+      y[((size_t)j << log_h) + ((size_t)(r1 + E) << log_h2) + i2] = kb::mul(b[dftreg::bitrev(m + 1, LG)], wo);
+      if (m + 2 < G) {
+        we = kb::mul(we, step2);
+        wo = kb::mul(wo, step2);
+      }
     }
   }
 }
