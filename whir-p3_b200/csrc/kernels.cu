@@ -1114,7 +1114,10 @@ __device__ __forceinline__ void coop_levels(uint32_t* sh, int cnt, int levels, s
     uint32_t x[4];
 #pragma unroll
     for (int j = 0; j < 4; j++) x[j] = sh[src + j];
-    coop_permute16(x, q, comp);
+    // a warp holds groups 8w .. 8w+7: warps with none of this level's pairs
+    // skip the permutation (warp-uniform, so its shuffles stay full-warp),
+    // which leaves the upper levels latency-bound rather than issue-bound
+    if ((t >> 5) * 8 < act) coop_permute16(x, q, comp);
     __syncthreads();
     off += lsz;
     lsz >>= 1;
