@@ -165,7 +165,7 @@ def test_grind_smallest_witness(pkg, gpu_ctx, oracle, bits):
     ch = pkg.DuplexChallenger(gpu_ctx)
     oc = Chal()
     oracle.lib.or_chal_init(C.byref(oc))
-    for pending in (0, 3, 7):
+    for pending in range(8):  # the witness lands at position `pending` of the sponge
         vals = rnd(rng, 8 + pending)
         ch.observe_slice(vals)
         for v in vals:
