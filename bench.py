@@ -530,9 +530,9 @@ def main() -> None:
     perms = sum((1 << lh) * ((w + 15) // 16) for lh, w in trees)
     peaks = json.loads((ROOT / "MEASURED_PEAKS.json").read_text()) if (ROOT / "MEASURED_PEAKS.json").exists() else {}
     peak = float(peaks.get("hbm_gbs", 6650.0))
-    # DRAM traffic of the commitment-tree launch (ncu, 2^21 leaves x 16 words: 134.4 MB read + 38.4 MB
+    # DRAM traffic of the commitment-tree launch (ncu, 2^21 leaves x 16 words: 134.6 MB read + 38.0 MB
     # written, profiles/poseidon2_grind_and_leaves_n24.md), scaled to the average launch by algorithmic bytes
-    traffic = 172.80e6 * per_launch_bytes / leaf_bytes(21, 16)
+    traffic = 172.60e6 * per_launch_bytes / leaf_bytes(21, 16)
     roofline = {"kernel": "k_leaf_digests (Poseidon2-24 leaf sponge, one row per thread)",
                 "bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                 "frac": round(achieved / peak, 4), "traffic": round(traffic),
@@ -540,9 +540,9 @@ def main() -> None:
                 "ms_per_launch": round(launch_ms, 4), "launches_per_proof": round(leaf_launches / args.steps, 2),
                 "algorithmic_bytes_per_launch": round(per_launch_bytes),
                 "compute_bound": {"leaf_permutations_per_s": round(perms / (leaf_ms / args.steps * 1e-3)),
-                                  "alu_pipe_busy": 0.801, "issue_active": 0.825,
-                                  "note": "integer-issue bound: ALU pipe 80.1% and issue 82.5% active, FMA-heavy "
-                                          "63.3%, FP64 17.6% (S-box quotients), DRAM 2.6% "
+                                  "alu_pipe_busy": 0.779, "issue_active": 0.808,
+                                  "note": "integer-issue bound: ALU pipe 77.9% and issue 80.8% active, FMA-heavy "
+                                          "61.0%, FP64 11.2% (S-box quotients), DRAM 3.1% "
                                           "(ncu, profiles/poseidon2_grind_and_leaves_n24.md)"}}
 
     batch = serve = None

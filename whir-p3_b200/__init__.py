@@ -684,20 +684,35 @@ class Prover:
         return buf[: words.value].copy()
 
 
+_PROVE_SETUP: dict = {}
+
+
+def _prove_setup(params: ProtocolParameters, n: int):
+    """The C parameter struct and the proof-length bound of (params, n),
+    computed once per distinct pair (this is per-call host work otherwise)."""
+    key = (params.security_level, params.pow_bits, params.folding_factor.first, params.folding_factor.rest,
+           int(params.soundness_type), params.starting_log_inv_rate, params.rs_domain_initial_reduction_factor,
+           params.leaf_hash, params.ds_digest_elems, n)
+    v = _PROVE_SETUP.get(key)
+    if v is None:
+        v = (params._c(), WhirConfig(n, params).proof_words_bound())
+        _PROVE_SETUP[key] = v
+    return v
+
+
 def commit_and_prove(ctx: Context, params: ProtocolParameters, n: int, poly, points=None):
     """Domain separator, commit, prove and a post-proof checkpoint sample, as
     in src/whir/mod.rs:103-141. Returns (proof words, checkpoint, user evals)."""
-    cfg = WhirConfig(n, params)
+    cparams, cap = _prove_setup(params, n)
     on_dev = isinstance(poly, DeviceArray)
     host = None if on_dev else _arr(poly, 1 << n)
     pts = None if points is None or len(points) == 0 else _arr(points)
     npts = 0 if pts is None else pts.size // (4 * n)
     evals = np.zeros(4 * max(npts, 1), dtype=np.uint32)
-    cap = cfg.proof_words_bound()
-    buf = np.zeros(cap, dtype=np.uint32)
+    buf = np.empty(cap, dtype=np.uint32)
     words = C.c_size_t()
     cp = np.zeros(4, dtype=np.uint32)
-    _check(lib().whir_commit_and_prove(ctx.handle, C.byref(params._c()), n, poly.ptr if on_dev else host.ctypes.data,
+    _check(lib().whir_commit_and_prove(ctx.handle, C.byref(cparams), n, poly.ptr if on_dev else host.ctypes.data,
                                        int(on_dev), _ptr(pts), npts, evals.ctypes.data, buf.ctypes.data, cap,
                                        C.byref(words), cp.ctypes.data))
     return buf[: words.value].copy(), cp, evals[: 4 * npts]

@@ -5,6 +5,7 @@
 #include <algorithm>
 #include <atomic>
 #include <chrono>
+#include <thread>
 
 #include "host.h"
 
@@ -157,21 +158,40 @@ int fetch_mail(whir_ctx* ctx, void* host, const void* dev, size_t bytes) {
 // Waits until the mailbox flag reaches `seq` and copies `bytes` of payload.
 int mail_wait(whir_ctx* ctx, uint32_t seq, void* host, size_t bytes) {
   volatile uint32_t* flag = ctx->h_mail + wk::kMailWords;
-  // Poll for a short while (typical results arrive within tens of
-  // microseconds); past that, block in a stream synchronisation instead of
-  // spinning, so that many waiting contexts (batch workers) do not take the
-  // host's cores from each other. The result is posted before the stream
-  // completes, so it is in place once the synchronisation returns.
-  const auto t0 = std::chrono::steady_clock::now();
+  // Spin for a short while (typical results arrive within tens of
+  // microseconds); past that, poll with a yield between checks, so that many
+  // waiting contexts (batch workers) leave the host's cores to each other,
+  // and ask the stream every ~100 us whether it failed or finished without
+  // posting (the result is posted before the stream completes). Polling
+  // rather than a stream synchronisation also returns as soon as the result
+  // is posted, not when the work queued behind its producer is done.
+  using clk = std::chrono::steady_clock;
+  const auto t0 = clk::now();
+  bool spinning = true;
+  auto next_query = t0;
   for (uint64_t n = 1; *flag != seq; n++) {
-    cpu_relax();
-    if ((n & 255) == 0 && std::chrono::steady_clock::now() - t0 > std::chrono::microseconds(30)) {
-      WH_TRY_CUDA(cudaStreamSynchronize(ctx->stream));
-      if (*flag != seq) {
-        set_error("device result missing after the stream completed");
-        return WHIR_ERR_CUDA;
-      }
-      break;
+    if (spinning) {
+      cpu_relax();
+      if ((n & 255) == 0 && clk::now() - t0 > std::chrono::microseconds(30)) spinning = false;
+      continue;
+    }
+    std::this_thread::yield();
+    const auto now = clk::now();
+    if (now < next_query) continue;
+    next_query = now + std::chrono::microseconds(100);
+    const cudaError_t q = cudaStreamQuery(ctx->stream);
+    std::atomic_thread_fence(std::memory_order_acquire);
+    if (q == cudaSuccess && *flag != seq) {
+      set_error("device result missing after the stream completed");
+      return WHIR_ERR_CUDA;
+    }
+    if (q != cudaSuccess && q != cudaErrorNotReady) {
+      set_error(std::string("stream failed while waiting for a result: ") + cudaGetErrorString(q));
+      return WHIR_ERR_CUDA;
+    }
+    if (now - t0 > std::chrono::seconds(120)) {
+      set_error("timed out waiting for a device result");
+      return WHIR_ERR_CUDA;
     }
   }
   std::atomic_thread_fence(std::memory_order_acquire);
