@@ -71,15 +71,6 @@ KB_HD uint32_t reduce_wide(uint64_t t) {
 }
 
 KB_HD uint32_t mul(uint32_t a, uint32_t b) { return reduce((uint64_t)a * b); }
-// Montgomery product left in (0, 2p), without the final conditional
-// subtraction: valid for a * b < p * 2^32 (e.g. a < 2p, b < p), and its result
-// may feed one more such product as the operand below 2p.
-KB_HD uint32_t mul_lazy(uint32_t a, uint32_t b) {
-  const uint64_t t = (uint64_t)a * b;
-  const uint32_t lo = (uint32_t)t, hi = (uint32_t)(t >> 32);
-  return hi - mulhi(lo * P_INV, P) + P;
-}
-
 // Product by a constant w < p with Shoup's precomputed quotient (Shoup, NTL;
 // Harvey, "Faster arithmetic for number-theoretic transforms", 2014):
 // ws = floor(w * 2^32 / p), q = floor(a * ws / 2^32) <= floor(a * w / p) and

@@ -213,15 +213,4 @@ KB_HD void permute_canonical(uint32_t (&x)[T], const P2Consts& k) {
   for (int r = RF / 2; r < RF; r++) full_round<T>(x, k.ext_rc + r * T);
 }
 
-// The permutation on Montgomery-form values (the representation of every
-// field element stored on the device).
-template <int T, int RP>
-KB_HD void permute(uint32_t (&x)[T], const P2Consts& k) {
-#pragma unroll
-  for (int i = 0; i < T; i++) x[i] = kb::from_mont(x[i]);
-  permute_canonical<T, RP>(x, k);
-#pragma unroll
-  for (int i = 0; i < T; i++) x[i] = kb::to_mont(x[i]);
-}
-
 }  // namespace p2
