@@ -39,7 +39,9 @@ def test_every_dft_plan_matches_oracle(pkg, gpu_ctx, oracle, log_chunk, log_w, l
 
 LEAF_SHAPES = [(128, 0), (128, 8), (128, 16), (256, 0), (256, 4), (256, 8), (256, 16), (512, 0), (512, 2), (512, 4),
                (512, 8)]
-NODE_SHAPES = [(t, s, v) for v in (0, 1) for t, s in [(128, 0), (128, 8), (128, 16), (256, 0), (256, 8), (256, 16)]]
+# variant bit 0: top kernel (cooperative subtrees / one CTA); bit 1: the two-level
+# kernel's permutations one after the other
+NODE_SHAPES = [(t, s, v) for v in (0, 1, 2, 3) for t, s in [(128, 0), (128, 8), (128, 16), (256, 0), (256, 8), (256, 16)]]
 
 
 # 2^17 and 2^13 leaves: leaf-digest kernel, two-level launches and either top

@@ -998,41 +998,64 @@ __global__ void __launch_bounds__(CTA) k_leaf_digests(const uint32_t* __restrict
 
 // Two tree levels per launch: each thread compresses four nodes of level l
 // into two nodes of level l+1 (written out) and their parent at level l+2.
-template <int CTA>
+// SEQ = false keeps both level-(l+1) permutations in flight together (two
+// independent chains per thread, about 78 registers); SEQ = true runs them one
+// after the other (one chain, fewer registers, more resident warps).
+template <int CTA, bool SEQ>
 __global__ void __launch_bounds__(CTA) k_merkle_two_levels(uint32_t* __restrict__ digests, size_t in_off,
                                                             size_t in_count, const __grid_constant__ P2Consts comp) {
   const size_t out_count = in_count >> 2;
   const size_t mid_off = in_off + in_count, top_off = mid_off + (in_count >> 1);
   for (size_t j = (size_t)blockIdx.x * blockDim.x + threadIdx.x; j < out_count; j += (size_t)gridDim.x * blockDim.x) {
     const uint4* src = reinterpret_cast<const uint4*>(digests + (in_off + 4 * j) * 8);
-    uint32_t a[16], b[16];
-#pragma unroll
-    for (int q = 0; q < 4; q++) {
-      const uint4 va = src[q], vb = src[4 + q];
-      a[4 * q] = va.x; a[4 * q + 1] = va.y; a[4 * q + 2] = va.z; a[4 * q + 3] = va.w;
-      b[4 * q] = vb.x; b[4 * q + 1] = vb.y; b[4 * q + 2] = vb.z; b[4 * q + 3] = vb.w;
-    }
-#pragma unroll
-    for (int k = 0; k < 16; k++) {
-      a[k] = kb::from_mont(a[k]);
-      b[k] = kb::from_mont(b[k]);
-    }
-    p2::permute_canonical<16, p2::RP16>(a, comp);
-    p2::permute_canonical<16, p2::RP16>(b, comp);
-    // the parent's inputs stay canonical
-    uint32_t c[16], am[8], bm[8];
-#pragma unroll
-    for (int k = 0; k < 8; k++) {
-      c[k] = a[k];
-      c[8 + k] = b[k];
-      am[k] = kb::to_mont(a[k]);
-      bm[k] = kb::to_mont(b[k]);
-    }
     uint4* mid = reinterpret_cast<uint4*>(digests + (mid_off + 2 * j) * 8);
-    mid[0] = make_uint4(am[0], am[1], am[2], am[3]);
-    mid[1] = make_uint4(am[4], am[5], am[6], am[7]);
-    mid[2] = make_uint4(bm[0], bm[1], bm[2], bm[3]);
-    mid[3] = make_uint4(bm[4], bm[5], bm[6], bm[7]);
+    uint32_t c[16];  // the parent's inputs, canonical
+    if (SEQ) {
+#pragma unroll
+      for (int h = 0; h < 2; h++) {
+        uint32_t a[16];
+#pragma unroll
+        for (int q = 0; q < 4; q++) {
+          const uint4 v = src[4 * h + q];
+          a[4 * q] = kb::from_mont(v.x);
+          a[4 * q + 1] = kb::from_mont(v.y);
+          a[4 * q + 2] = kb::from_mont(v.z);
+          a[4 * q + 3] = kb::from_mont(v.w);
+        }
+        p2::permute_canonical<16, p2::RP16>(a, comp);
+#pragma unroll
+        for (int k = 0; k < 8; k++) c[8 * h + k] = a[k];
+        mid[2 * h] = make_uint4(kb::to_mont(a[0]), kb::to_mont(a[1]), kb::to_mont(a[2]), kb::to_mont(a[3]));
+        mid[2 * h + 1] = make_uint4(kb::to_mont(a[4]), kb::to_mont(a[5]), kb::to_mont(a[6]), kb::to_mont(a[7]));
+      }
+    } else {
+      uint32_t a[16], b[16];
+#pragma unroll
+      for (int q = 0; q < 4; q++) {
+        const uint4 va = src[q], vb = src[4 + q];
+        a[4 * q] = va.x; a[4 * q + 1] = va.y; a[4 * q + 2] = va.z; a[4 * q + 3] = va.w;
+        b[4 * q] = vb.x; b[4 * q + 1] = vb.y; b[4 * q + 2] = vb.z; b[4 * q + 3] = vb.w;
+      }
+#pragma unroll
+      for (int k = 0; k < 16; k++) {
+        a[k] = kb::from_mont(a[k]);
+        b[k] = kb::from_mont(b[k]);
+      }
+      p2::permute_canonical<16, p2::RP16>(a, comp);
+      p2::permute_canonical<16, p2::RP16>(b, comp);
+      uint32_t am[8], bm[8];
+#pragma unroll
+      for (int k = 0; k < 8; k++) {
+        c[k] = a[k];
+        c[8 + k] = b[k];
+        am[k] = kb::to_mont(a[k]);
+        bm[k] = kb::to_mont(b[k]);
+      }
+      mid[0] = make_uint4(am[0], am[1], am[2], am[3]);
+      mid[1] = make_uint4(am[4], am[5], am[6], am[7]);
+      mid[2] = make_uint4(bm[0], bm[1], bm[2], bm[3]);
+      mid[3] = make_uint4(bm[4], bm[5], bm[6], bm[7]);
+    }
     p2::permute_canonical<16, p2::RP16>(c, comp);
 #pragma unroll
     for (int k = 0; k < 8; k++) c[k] = kb::to_mont(c[k]);
@@ -1280,17 +1303,24 @@ cudaError_t merkle_upper(int log_h, uint32_t* digests, const P2Consts& p16, Shap
   if (posted) *posted = 0;
   const size_t h = (size_t)1 << log_h;
   size_t off = 0, cnt = h;
-  if (node.variant != 0 && node.variant != 1) return cudaErrorInvalidValue;
-  const size_t top = node.variant == 1 ? kCtaTop : kCoopTop;
+  // variant bit 0: the top kernel (0 cooperative subtrees, 1 one CTA); bit 1:
+  // the two-level kernel with its two permutations one after the other
+  if (node.variant < 0 || node.variant > 3) return cudaErrorInvalidValue;
+  const bool top_cta = (node.variant & 1) != 0, one_chain = (node.variant & 2) != 0;
+  const size_t top = top_cta ? kCtaTop : kCoopTop;
   if (h >= kLevelPairMin) {
     if ((node.threads != 128 && node.threads != 256) || node.per_sm < 0) return cudaErrorInvalidValue;
     while (cnt > top) {
       const size_t out = cnt >> 2;
       const unsigned blocks = grid_shape(out, node);
-      if (node.threads == 128)
-        k_merkle_two_levels<128><<<blocks, 128, 0, st>>>(digests, off, cnt, p16);
+      if (node.threads == 128 && one_chain)
+        k_merkle_two_levels<128, true><<<blocks, 128, 0, st>>>(digests, off, cnt, p16);
+      else if (node.threads == 128)
+        k_merkle_two_levels<128, false><<<blocks, 128, 0, st>>>(digests, off, cnt, p16);
+      else if (one_chain)
+        k_merkle_two_levels<256, true><<<blocks, 256, 0, st>>>(digests, off, cnt, p16);
       else
-        k_merkle_two_levels<256><<<blocks, 256, 0, st>>>(digests, off, cnt, p16);
+        k_merkle_two_levels<256, false><<<blocks, 256, 0, st>>>(digests, off, cnt, p16);
       count_launch();
       cudaError_t e = cudaGetLastError();
       if (e != cudaSuccess) return e;
@@ -1306,7 +1336,7 @@ cudaError_t merkle_upper(int log_h, uint32_t* digests, const P2Consts& p16, Shap
     }
   }
   if (cnt <= 1) return cudaSuccess;
-  if (node.variant == 1) {
+  if (top_cta) {
     k_merkle_top_cta<<<1, TOP1_CTA, 0, st>>>(digests, off, (int)cnt, p16, mail, seq);
   } else {
     // one launch: subtrees of 256 nodes, then the last CTA joins their roots

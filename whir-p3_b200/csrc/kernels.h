@@ -84,9 +84,10 @@ cudaError_t merkle_build(const uint32_t* rows, int log_h, int row_words, int lea
 // the two halves of merkle_build: leaf hashing with the CTA subtrees, then the
 // upper levels. `leaf` shapes the leaf-digest kernel of trees with at least
 // kMerkleLevelPairMin leaves (threads 128, 256 or 512), `node` the two-level
-// compression kernel (threads 128 or 256) and picks the top kernel (variant 0:
-// cooperative four-lane permutations in many CTAs; 1: one CTA, one
-// permutation per thread).
+// compression kernel (threads 128 or 256) and picks the top kernel (variant
+// bit 0 clear: cooperative four-lane permutations in many CTAs; set: one CTA,
+// one permutation per thread) and the two-level kernel's form (bit 1 set: its
+// two permutations one after the other, fewer registers).
 constexpr int kMerkleLevelPairMin = 1 << 12;
 Shape merkle_leaf_default();
 Shape merkle_node_default();

@@ -184,8 +184,11 @@ int tune_dft(whir_ctx* ctx, const Key& k, const uint32_t* in, uint32_t* out, uin
 
 const wk::Shape kLeafShapes[] = {{128, 0, 0},  {128, 8, 0}, {128, 16, 0}, {256, 0, 0}, {256, 4, 0}, {256, 8, 0},
                                  {256, 16, 0}, {512, 0, 0}, {512, 2, 0},  {512, 4, 0}, {512, 8, 0}};
+// variant: bit 0 the top kernel (cooperative subtrees / one CTA), bit 1 the
+// two-level kernel's permutations one after the other instead of together
 const wk::Shape kNodeShapes[] = {{128, 0, 0}, {128, 8, 0}, {128, 16, 0}, {256, 0, 0}, {256, 8, 0}, {256, 16, 0},
-                                 {128, 0, 1}, {128, 8, 1}, {128, 16, 1}, {256, 0, 1}, {256, 8, 1}, {256, 16, 1}};
+                                 {128, 0, 1}, {128, 8, 1}, {128, 16, 1}, {256, 0, 1}, {256, 8, 1}, {256, 16, 1},
+                                 {128, 0, 2}, {128, 16, 2}, {256, 0, 2}, {256, 16, 2}, {128, 0, 3}, {256, 0, 3}};
 const wk::Shape kFoldShapes[] = {{128, 0, 0},  {128, 16, 0}, {256, 0, 0}, {256, 4, 0}, {256, 8, 0},
                                  {256, 16, 0}, {512, 0, 0},  {512, 2, 0}, {512, 4, 0}, {512, 8, 0}};
 
