@@ -486,6 +486,8 @@ def main() -> None:
     # ---- end to end through the public API with host buffers ----
     host_poly = torch.from_numpy(poly).pin_memory()
     host_np = host_poly.numpy()
+    for _ in range(max(args.warmup, 1)):  # untimed: the pool takes the uploaded polynomial's size once
+        step(host_np)
     barrier()
     e2e_ms = 0.0
     for _ in range(args.steps):
