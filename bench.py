@@ -393,7 +393,7 @@ def main() -> None:
     ap.add_argument("--micro", default=None, choices=["all", "eq", "eval", "fold", "dft", "merkle", "grind"])
     ap.add_argument("--batch", action="store_true")
     ap.add_argument("--serve", action="store_true")
-    ap.add_argument("--workers", type=int, default=8)
+    ap.add_argument("--workers", type=int, default=16)
     ap.add_argument("--rates", default="10,50,100,200,500")
     ap.add_argument("--no-batch", action="store_true", help="skip the batch/serve summary in the default run")
     args = ap.parse_args()
