@@ -1128,54 +1128,48 @@ __device__ __forceinline__ void coop_permute16(uint32_t (&x)[4], int q, const P2
 // size in `digests` (advanced past the levels done).
 __device__ __forceinline__ void coop_levels(uint32_t* sh, int cnt, int levels, size_t base, size_t& off, size_t& lsz,
                                             uint32_t* __restrict__ digests, const P2Consts& comp) {
-  const int t = threadIdx.x, q = t & 3, groups = (int)blockDim.x >> 2;
+  const int t = threadIdx.x, g = t >> 2, q = t & 3;
   int cur = cnt;
   for (int l = 1; l <= levels; l++) {
     const int act = cur >> 1;
-    // pairs in passes of one per four-lane group; a pass writes its outputs
-    // below the inputs of every later pass (8 g < 16 g'), so in place is safe
-    for (int g0 = 0; g0 < act; g0 += groups) {
-      const int g = g0 + (t >> 2);
-      const bool on = g < act;
-      const int src = on ? 16 * g + 4 * q : 0;
-      uint32_t x[4];
+    const bool on = g < act;
+    const int src = on ? 16 * g + 4 * q : 0;
+    uint32_t x[4];
 #pragma unroll
-      for (int j = 0; j < 4; j++) x[j] = sh[src + j];
-      // a warp holds groups 8w .. 8w+7: warps with none of this level's pairs
-      // skip the permutation (warp-uniform, so its shuffles stay full-warp),
-      // which leaves the upper levels latency-bound rather than issue-bound
-      if (g0 + (t >> 5) * 8 < act) coop_permute16(x, q, comp);
-      __syncthreads();
-      if (on && q < 2) {
-        const size_t node = (base >> l) + g;
-#pragma unroll
-        for (int j = 0; j < 4; j++) {
-          sh[8 * g + 4 * q + j] = x[j];
-          digests[(off + lsz + node) * 8 + 4 * q + j] = x[j];
-        }
-      }
-      __syncthreads();
-    }
+    for (int j = 0; j < 4; j++) x[j] = sh[src + j];
+    // a warp holds groups 8w .. 8w+7: warps with none of this level's pairs
+    // skip the permutation (warp-uniform, so its shuffles stay full-warp),
+    // which leaves the upper levels latency-bound rather than issue-bound
+    if ((t >> 5) * 8 < act) coop_permute16(x, q, comp);
+    __syncthreads();
     off += lsz;
     lsz >>= 1;
+    if (on && q < 2) {
+      const size_t node = (base >> l) + g;
+#pragma unroll
+      for (int j = 0; j < 4; j++) {
+        sh[8 * g + 4 * q + j] = x[j];
+        digests[(off + node) * 8 + 4 * q + j] = x[j];
+      }
+    }
+    __syncthreads();
     cur = act;
   }
 }
 
 // Top of a tree: each CTA compresses up to 256 nodes of one level into a
 // subtree, one four-lane group per node pair, level by level in shared memory.
-// With several CTAs (at most TOP_JOIN), the last one to finish (atomic counter, no
+// With several CTAs (at most 256), the last one to finish (atomic counter, no
 // waiting) loads their subtree roots and compresses them to the root in the
 // same launch. With `mail` set, the root is posted to that mailbox.
 constexpr int TOP_CTA = 512;
 constexpr int TOP_NODES = 256;
-constexpr int TOP_JOIN = 512;  // subtree roots the last CTA can join
 __global__ void __launch_bounds__(TOP_CTA) k_merkle_top_coop(uint32_t* __restrict__ digests, size_t in_off,
                                                               size_t in_count, int levels,
                                                               const __grid_constant__ P2Consts comp,
                                                               unsigned* __restrict__ counter, uint32_t* mail,
                                                               uint32_t seq) {
-  __shared__ uint32_t sh[TOP_JOIN * 8];
+  __shared__ uint32_t sh[TOP_NODES * 8];
   __shared__ bool s_last;
   const int t = threadIdx.x;
   const size_t base = (size_t)blockIdx.x * TOP_NODES;
@@ -1248,11 +1242,11 @@ __global__ void __launch_bounds__(TOP1_CTA) k_merkle_top_cta(uint32_t* __restric
 // Trees with at least kLevelPairMin leaves are built as: leaf digests, then
 // two levels per launch while a level is wider than the top kernel takes, then
 // the top: either cooperative-permutation subtrees (k_merkle_top_coop, node
-// shape variant 0, from 2^17 nodes) or one CTA (k_merkle_top_cta, variant 1,
+// shape variant 0, from 2^15 nodes) or one CTA (k_merkle_top_cta, variant 1,
 // from 2^11 nodes). Smaller trees hash their leaves with in-CTA subtrees and
 // use the same top kernels above those.
 constexpr size_t kLevelPairMin = (size_t)kMerkleLevelPairMin;
-constexpr size_t kCoopTop = (size_t)1 << 17;
+constexpr size_t kCoopTop = (size_t)1 << 15;
 constexpr size_t kCtaTop = (size_t)2 * TOP1_CTA;
 
 // CTAs for `work` items at `threads` per CTA, capped at per_sm CTAs per SM
@@ -1348,7 +1342,7 @@ cudaError_t merkle_upper(int log_h, uint32_t* digests, const P2Consts& p16, Shap
     // one launch: subtrees of 256 nodes, then the last CTA joins their roots
     const int c2 = (int)(cnt < (size_t)TOP_NODES ? cnt : (size_t)TOP_NODES);
     const unsigned blocks2 = (unsigned)(cnt / c2);
-    if (blocks2 > (unsigned)TOP_JOIN || (blocks2 > 1 && !counter)) return cudaErrorInvalidValue;
+    if (blocks2 > (unsigned)TOP_NODES || (blocks2 > 1 && !counter)) return cudaErrorInvalidValue;
     k_merkle_top_coop<<<blocks2, TOP_CTA, 0, st>>>(digests, off, cnt, ilog2i((size_t)c2), p16, counter, mail, seq);
   }
   count_launch();
