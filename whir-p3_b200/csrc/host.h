@@ -95,7 +95,7 @@ struct whir_ctx {
   cudaStream_t stream = nullptr;
   bool own_stream = false;
   whir_poseidon2_params p16_params, p24_params;
-  p2::P2Consts p16, p24;  // Montgomery form
+  p2::P2Consts p16, p24;  // canonical round constants for the kernels
   wh::HostP16 hp16;       // canonical, for the host transcript
   uint32_t* tw_stage = nullptr;
   // twiddle tables of every height, built at creation so that proving never
