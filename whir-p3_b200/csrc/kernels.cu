@@ -1100,7 +1100,9 @@ __device__ __forceinline__ void coop_permute16(uint32_t (&x)[4], int q, const P2
   // which leaves S-box, one addition and the diagonal product of word 0 as
   // the round's dependent chain.
   uint32_t w0 = __shfl_sync(0xffffffffu, x[0], (threadIdx.x & 31) & ~3);
-#pragma unroll 1
+  // fully unrolled: round constants become immediate constant-bank operands,
+  // off the dependent chain of this latency-bound form
+#pragma unroll
   for (int r = 0; r < p2::RP16; r++) {
     uint32_t o = add(add(q == 0 ? 0u : x[0], x[1]), add(x[2], x[3]));
     o = add(o, __shfl_xor_sync(0xffffffffu, o, 1));
