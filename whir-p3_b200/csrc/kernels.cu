@@ -938,7 +938,11 @@ __global__ void __launch_bounds__(MERKLE_CTA) k_merkle_leaves(const uint32_t* __
         for (int k = 0; k < RATE; k++)
           if (k < take) s[k] = kb::from_mont(row[pos + k]);
       }
-      p2::permute_canonical<T, RP>(s, leaf);
+      const bool first = pos == 0, last = pos + RATE >= row_words;
+      if (first && last) p2::permute_sponge<T, RP, RATE, true, true>(s, leaf);
+      else if (first) p2::permute_sponge<T, RP, RATE, true, false>(s, leaf);
+      else if (last) p2::permute_sponge<T, RP, RATE, false, true>(s, leaf);
+      else p2::permute_sponge<T, RP, RATE, false, false>(s, leaf);
     }
 #pragma unroll
     for (int k = 0; k < 8; k++) {
@@ -986,7 +990,11 @@ __global__ void __launch_bounds__(CTA) k_leaf_digests(const uint32_t* __restrict
         for (int k = 0; k < RATE; k++)
           if (k < take) s[k] = kb::from_mont(row[pos + k]);
       }
-      p2::permute_canonical<T, RP>(s, leaf);
+      const bool first = pos == 0, last = pos + RATE >= row_words;
+      if (first && last) p2::permute_sponge<T, RP, RATE, true, true>(s, leaf);
+      else if (first) p2::permute_sponge<T, RP, RATE, true, false>(s, leaf);
+      else if (last) p2::permute_sponge<T, RP, RATE, false, true>(s, leaf);
+      else p2::permute_sponge<T, RP, RATE, false, false>(s, leaf);
     }
 #pragma unroll
     for (int k = 0; k < 8; k++) s[k] = kb::to_mont(s[k]);

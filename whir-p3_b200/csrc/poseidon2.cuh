@@ -213,4 +213,67 @@ KB_HD void permute_canonical(uint32_t (&x)[T], const P2Consts& k) {
   for (int r = RF / 2; r < RF; r++) full_round<T>(x, k.ext_rc + r * T);
 }
 
+// Sponge forms of the permutation (PaddingFreeSponge, overwrite mode). FIRST:
+// the capacity words (from RATE on) are zero on entry, so the initial external
+// layer skips their M4 blocks and sums; LAST: only the first 8 words (the
+// digest) of the output are read, so the final external layer forms only those.
+template <int T, int RATE>
+KB_HD void ext_layer_zero_capacity(uint32_t (&x)[T]) {
+  using namespace kb;
+#pragma unroll
+  for (int c = 0; c < RATE; c += 4) m4(x[c], x[c + 1], x[c + 2], x[c + 3]);
+  uint32_t s0 = x[0], s1 = x[1], s2 = x[2], s3 = x[3];
+#pragma unroll
+  for (int c = 4; c < RATE; c += 4) {
+    s0 = add(s0, x[c]);
+    s1 = add(s1, x[c + 1]);
+    s2 = add(s2, x[c + 2]);
+    s3 = add(s3, x[c + 3]);
+  }
+#pragma unroll
+  for (int c = 0; c < T; c += 4) {
+    x[c] = c < RATE ? add(x[c], s0) : s0;
+    x[c + 1] = c < RATE ? add(x[c + 1], s1) : s1;
+    x[c + 2] = c < RATE ? add(x[c + 2], s2) : s2;
+    x[c + 3] = c < RATE ? add(x[c + 3], s3) : s3;
+  }
+}
+template <int T>
+KB_HD void ext_layer_digest(uint32_t (&x)[T]) {
+  using namespace kb;
+#pragma unroll
+  for (int c = 0; c < T; c += 4) m4(x[c], x[c + 1], x[c + 2], x[c + 3]);
+  uint32_t s0 = x[0], s1 = x[1], s2 = x[2], s3 = x[3];
+#pragma unroll
+  for (int c = 4; c < T; c += 4) {
+    s0 = add(s0, x[c]);
+    s1 = add(s1, x[c + 1]);
+    s2 = add(s2, x[c + 2]);
+    s3 = add(s3, x[c + 3]);
+  }
+#pragma unroll
+  for (int c = 0; c < 8; c += 4) {
+    x[c] = add(x[c], s0);
+    x[c + 1] = add(x[c + 1], s1);
+    x[c + 2] = add(x[c + 2], s2);
+    x[c + 3] = add(x[c + 3], s3);
+  }
+}
+template <int T, int RP, int RATE, bool FIRST, bool LAST>
+KB_HD void permute_sponge(uint32_t (&x)[T], const P2Consts& k) {
+  if (FIRST) ext_layer_zero_capacity<T, RATE>(x);
+  else ext_layer<T>(x);
+#pragma unroll 1
+  for (int r = 0; r < RF / 2; r++) full_round<T>(x, k.ext_rc + r * T);
+#pragma unroll 1
+  for (int r = 0; r < RP; r++) partial_round<T>(x, k.int_rc[r]);
+#pragma unroll 1
+  for (int r = RF / 2; r < RF - 1; r++) full_round<T>(x, k.ext_rc + r * T);
+  const uint32_t* rc = k.ext_rc + (RF - 1) * T;
+#pragma unroll
+  for (int i = 0; i < T; i++) x[i] = cube(kb::add(x[i], rc[i]));
+  if (LAST) ext_layer_digest<T>(x);
+  else ext_layer<T>(x);
+}
+
 }  // namespace p2
