@@ -1096,7 +1096,7 @@ __device__ __forceinline__ void coop_permute16(uint32_t (&x)[4], int q, const P2
 #pragma unroll
   for (int j = 0; j < 4; j++) x[j] = from_mont(x[j]);
   coop_ext_layer(x);
-#pragma unroll 1
+#pragma unroll
   for (int r = 0; r < p2::RF / 2; r++) {
 #pragma unroll
     for (int j = 0; j < 4; j++) x[j] = p2::cube(add(x[j], k.ext_rc[r * 16 + 4 * q + j]));
@@ -1122,7 +1122,7 @@ __device__ __forceinline__ void coop_permute16(uint32_t (&x)[4], int q, const P2
     w0 = p2::diag_axpy(p2::diag_code(16, 0), s, y0);
     if (q == 0) x[0] = w0;
   }
-#pragma unroll 1
+#pragma unroll
   for (int r = p2::RF / 2; r < p2::RF; r++) {
 #pragma unroll
     for (int j = 0; j < 4; j++) x[j] = p2::cube(add(x[j], k.ext_rc[r * 16 + 4 * q + j]));
