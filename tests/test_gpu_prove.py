@@ -91,6 +91,32 @@ def test_split_commit_then_prove_matches(pkg, gpu_ctx):
     assert np.array_equal(ch.sample_algebra_element(), cp1)
 
 
+@pytest.mark.parametrize("n,k,rate", [(20, 4, 1), (18, 3, 2), (18, 5, 1)])
+def test_pipelined_upload_matches_device_resident(pkg, gpu_ctx, n, k, rate):
+    """A host polynomial goes up in eight chunk groups, each group's DFT first
+    pass queued behind its copy once the DFT plan of the shape is known; the
+    proof equals the one from a device-resident polynomial, and the launch
+    count shows the pipelined path ran (eight encodings and eight first-pass
+    launches in place of one encoding and one first pass)."""
+    rng = np.random.default_rng(n * 10 + k)
+    poly = rnd(rng, 1 << n)
+    pt = rnd(rng, 4 * n)
+    params = pkg.ProtocolParameters(90, 12, pkg.FoldingFactor.constant(k), pkg.SecurityAssumption.CapacityBound,
+                                    rate, 1)
+    dpoly = pkg.DeviceArray.from_host(gpu_ctx, poly)
+    ref, ref_cp, ref_ev = pkg.commit_and_prove(gpu_ctx, params, n, dpoly, pt)  # tunes the shapes
+    l0 = pkg.kernel_launches()
+    again = pkg.commit_and_prove(gpu_ctx, params, n, dpoly, pt)
+    dev_launches = pkg.kernel_launches() - l0
+    for _ in range(2):
+        l0 = pkg.kernel_launches()
+        proof, cp, ev = pkg.commit_and_prove(gpu_ctx, params, n, poly, pt)
+        host_launches = pkg.kernel_launches() - l0
+        assert np.array_equal(proof, ref) and np.array_equal(cp, ref_cp) and np.array_equal(ev, ref_ev)
+        assert host_launches == dev_launches + 15, (host_launches, dev_launches)
+    assert np.array_equal(again[0], ref)
+
+
 def test_e2e_headline_n24(pkg, gpu_ctx, oracle):
     """The reference's benchmark configuration (benches/whir.rs:34-120): n = 24,
     k = 4, rate 1/2, 100-bit CapacityBound, pow_bits 16, rs reduction 3, one

@@ -396,6 +396,11 @@ int whir_ctx_create(int32_t device, const whir_poseidon2_params* p16, const whir
   if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess)
     return wh::set_error("stream creation failed"), fail(WHIR_ERR_CUDA);
   c->own_stream = true;
+  if (cudaStreamCreateWithFlags(&c->copy_stream, cudaStreamNonBlocking) != cudaSuccess)
+    return wh::set_error("stream creation failed"), fail(WHIR_ERR_CUDA);
+  for (cudaEvent_t& e : c->up_ev)
+    if (cudaEventCreateWithFlags(&e, cudaEventDisableTiming) != cudaSuccess)
+      return wh::set_error("event creation failed"), fail(WHIR_ERR_CUDA);
   {
     // the context's own pool, keeping freed blocks cached between proofs
     cudaMemPoolProps props;
@@ -450,6 +455,12 @@ int whir_ctx_destroy(whir_ctx* c) {
     cudaEventDestroy(rec.second.second);
   }
   for (cudaEvent_t e : c->event_pool) cudaEventDestroy(e);
+  if (c->copy_stream) {
+    cudaStreamSynchronize(c->copy_stream);
+    cudaStreamDestroy(c->copy_stream);
+  }
+  for (cudaEvent_t e : c->up_ev)
+    if (e) cudaEventDestroy(e);
   cudaFree(c->tw_stage);
   cudaFree(c->d_partials);
   cudaFree(c->d_small);

@@ -87,6 +87,7 @@ enum Stage { kStDft = 0, kStLeaves, kStNodes, kStGrind, kStSumcheck, kStEval, kS
 // twiddle tables of one subgroup height: omega_H^e and omega_H^(e * 2^12), e < 2^12
 constexpr int kDftLogHeights = 25;  // heights 2^0 .. 2^24
 constexpr size_t kDftTableWords = 2 * 4096;
+constexpr int kUploadGroups = 8;  // chunk groups of a pipelined polynomial upload
 
 }  // namespace wh
 
@@ -120,6 +121,10 @@ struct whir_ctx {
   // allocator from reusing one stream's freed blocks on another stream (which
   // would make concurrent contexts wait on each other's queued work)
   cudaMemPool_t pool = nullptr;
+  // upload of a host polynomial in chunk groups on a stream of its own, each
+  // group's DFT first pass queued on `stream` behind the group's copy
+  cudaStream_t copy_stream = nullptr;
+  cudaEvent_t up_ev[wh::kUploadGroups + 1] = {};
   // stage timing
   bool profiling = false;
   std::vector<cudaEvent_t> event_pool;
@@ -160,6 +165,9 @@ int fetch_posted(whir_ctx* ctx, uint32_t seq, void* host, const void* dev, size_
 int dot_eq(whir_ctx* ctx, const uint32_t* d_f, int ext, int seg_bits, const kb::ef* z, int m_bits, uint32_t* posted);
 
 // Tuned launches (launch shapes chosen per shape on first use, process-wide)
+// The DFT plan run_dft would use for this shape, if it needs no tuning run
+// first (false: the tuner has not timed it yet).
+bool dft_plan_known(const whir_ctx* ctx, int log_chunk, int log_w, int log_blowup, int lanes, wk::DftPlan* plan);
 int run_dft(whir_ctx* ctx, const uint32_t* in, uint32_t* out, uint32_t* scratch, int log_chunk, int log_w,
             int log_blowup, int lanes, const wk::DftTables& t);
 int run_merkle_leaves(whir_ctx* ctx, const uint32_t* rows, int log_h, int row_words, int leaf_hash,

@@ -781,11 +781,19 @@ void dft_candidates(int log_chunk, int log_w, int log_blowup, int lanes, DftPlan
 
 cudaError_t dft_batch(const uint32_t* in, uint32_t* out, uint32_t* scratch, int log_chunk, int log_w,
                       int log_blowup, int lanes, const DftTables& t, const DftPlan& plan, int passes,
-                      cudaStream_t st) {
+                      cudaStream_t st, int col0, int ncols) {
   if (!dft_plan_ok(plan, log_chunk, log_w, log_blowup, lanes)) return cudaErrorInvalidValue;
   init_smem_attributes();
   const int log_h = log_chunk + log_blowup;
-  const int W = 1 << log_w;
+  int W = 1 << log_w;
+  if (ncols > 0) {
+    // a column range of pass 1 only: chunk j reads in + j * chunk and writes
+    // scratch + j * height, so the range is a pointer offset and a grid height
+    if (passes != 1 || plan.log_h2 == 0 || col0 < 0 || col0 + ncols > W) return cudaErrorInvalidValue;
+    in += ((size_t)col0 * lanes) << log_chunk;
+    scratch += ((size_t)col0 * lanes) << log_h;
+    W = ncols;
+  }
   if (plan.log_h2 == 0) {
     const int jt = 1 << plan.log_t1;
     const size_t smem = kDftTwBytes + dft_tile_bytes(plan.log_t1, log_chunk, lanes);

@@ -61,10 +61,12 @@ bool dft_plan_ok(const DftPlan& p, int log_chunk, int log_w, int log_blowup, int
 // transpose & pad & DFT: 2^log_w chunks of 2^log_chunk elements -> row-major
 // (2^(log_chunk+log_blowup)) x 2^log_w; `scratch` needs out-size elements.
 // `passes` selects the four-step passes to run (bit 0: pass 1, bit 1: pass 2;
-// 3 for the whole transform); only the tuner runs a single pass.
+// 3 for the whole transform). Pass 1 works column by column: with passes == 1
+// and ncols > 0 it runs only chunks [col0, col0 + ncols) (a four-step plan;
+// the tuner and the pipelined upload of a polynomial run single passes).
 cudaError_t dft_batch(const uint32_t* in, uint32_t* out, uint32_t* scratch, int log_chunk, int log_w,
                       int log_blowup, int lanes, const DftTables& t, const DftPlan& plan, int passes,
-                      cudaStream_t st);
+                      cudaStream_t st, int col0 = 0, int ncols = 0);
 
 // Grid shape of a streaming kernel: threads per CTA, a cap on CTAs per SM
 // (0: one CTA per `threads` work items, no cap) and a kernel variant where a

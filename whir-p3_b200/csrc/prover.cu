@@ -169,6 +169,10 @@ struct whir_witness {
   uint32_t* d_poly = nullptr;
   bool own_poly = false;
   Tree commit_tree;
+  // set when the upload already ran the commitment DFT's first pass (the
+  // tree's rows and digests are then allocated too)
+  uint32_t* pre_scratch = nullptr;
+  wk::DftPlan pre_plan;
   std::vector<Constraint> cons;
   std::vector<uint32_t> proof;
   bool proved = false;
@@ -183,27 +187,43 @@ void free_tree(whir_ctx* ctx, Tree& t) {
   t.digests = nullptr;
 }
 
-// DFT + Merkle commitment of 2^log_w contiguous chunks of 2^log_chunk elements
+// DFT + Merkle commitment of 2^log_w contiguous chunks of 2^log_chunk elements.
+// With `pass1` set, t->rows and t->digests are allocated and the DFT's first
+// pass already wrote *pre_scratch with that plan; this call frees the scratch
+// and clears *pre_scratch.
 int commit_matrix(whir_ctx* ctx, const uint32_t* d_src, int log_chunk, int log_w, int log_blowup, int ext,
-                  int leaf_hash, Tree* t, uint32_t* root_canon) {
+                  int leaf_hash, Tree* t, uint32_t* root_canon, const wk::DftPlan* pass1 = nullptr,
+                  uint32_t** pre_scratch = nullptr) {
   const int lanes = ext ? 4 : 1;
   t->log_h = log_chunk + log_blowup;
   t->row_words = lanes << log_w;
   t->ext = ext;
   const size_t h = (size_t)1 << t->log_h;
   const size_t words = h * (size_t)t->row_words;
-  WH_TRY_CUDA(wh::ctx_malloc(ctx, &t->rows, words * 4));
-  WH_TRY_CUDA(wh::ctx_malloc(ctx, &t->digests, (2 * h - 1) * 8 * 4));
+  if (!pass1) {
+    WH_TRY_CUDA(wh::ctx_malloc(ctx, &t->rows, words * 4));
+    WH_TRY_CUDA(wh::ctx_malloc(ctx, &t->digests, (2 * h - 1) * 8 * 4));
+  }
   wk::DftTables tab;
   WH_TRY(wh::ensure_dft_tables(ctx, t->log_h, &tab));
-  uint32_t* scratch = nullptr;
-  WH_TRY_CUDA(wh::ctx_malloc(ctx, &scratch, words * 4));
-  int s;
+  uint32_t* scratch = pass1 ? *pre_scratch : nullptr;
+  if (!pass1) WH_TRY_CUDA(wh::ctx_malloc(ctx, &scratch, words * 4));
+  int s = WHIR_OK;
   {
     wh::StageTimer timer(ctx, wh::kStDft);
-    s = wh::run_dft(ctx, d_src, t->rows, scratch, log_chunk, log_w, log_blowup, lanes, tab);
+    if (pass1) {
+      const cudaError_t ce =
+          wk::dft_batch(d_src, t->rows, scratch, log_chunk, log_w, log_blowup, lanes, tab, *pass1, 2, ctx->stream);
+      if (ce != cudaSuccess) {
+        wh::set_error(std::string("DFT second pass: ") + cudaGetErrorString(ce));
+        s = WHIR_ERR_CUDA;
+      }
+    } else {
+      s = wh::run_dft(ctx, d_src, t->rows, scratch, log_chunk, log_w, log_blowup, lanes, tab);
+    }
   }
   cudaFreeAsync(scratch, ctx->stream);
+  if (pass1) *pre_scratch = nullptr;
   WH_TRY(s);
   {
     wh::StageTimer timer(ctx, wh::kStLeaves);
@@ -339,7 +359,7 @@ int do_commit(whir_ctx* ctx, whir_witness* w, wh::Chal& ch, const uint32_t* user
   pf.push_back(1u);
   uint32_t root[8];
   WH_TRY(commit_matrix(ctx, w->d_poly, n - k0, k0, c.starting_log_inv_rate, 0, w->params.leaf_hash, &w->commit_tree,
-                       root));
+                       root, w->pre_scratch ? &w->pre_plan : nullptr, &w->pre_scratch));
   for (int i = 0; i < 8; i++) pf.push_back(root[i]);
   for (int i = 0; i < 8; i++) ch.observe(ctx->hp16, kb::to_mont(root[i]));
   pf.push_back((uint32_t)c.commitment_ood_samples);
@@ -557,6 +577,51 @@ int do_prove(whir_ctx* ctx, whir_witness* wit, wh::Chal& ch) {
   return WHIR_OK;
 }
 
+// Upload of a host polynomial overlapped with the commitment DFT's first pass.
+// Each of the 2^k0 columns of the committed matrix is one contiguous chunk of
+// the polynomial, and pass 1 transforms a column from its own chunk only; so
+// the chunks go up in kUploadGroups groups on the context's copy stream, and
+// each group's Montgomery encoding and pass 1 queue on the context's stream
+// behind that group's copy. Sets *done = false and queues nothing when the
+// shape does not allow it: fewer columns than groups, a one-pass plan, or a
+// shape the tuner has not timed yet (its first run tunes on the whole input).
+int upload_with_dft(whir_ctx* ctx, whir_witness* w, const uint32_t* poly, bool* done) {
+  *done = false;
+  const whir_config& c = w->cfg;
+  const int k0 = c.folding_factor_0, log_chunk = w->n - k0, log_blowup = c.starting_log_inv_rate;
+  const int W = 1 << k0, G = wh::kUploadGroups;
+  if (W < G || log_chunk < 12) return WHIR_OK;
+  wk::DftPlan plan;
+  if (!wh::dft_plan_known(ctx, log_chunk, k0, log_blowup, 1, &plan) || plan.log_h2 == 0) return WHIR_OK;
+  Tree& t = w->commit_tree;
+  const int log_h = log_chunk + log_blowup;
+  const size_t h = (size_t)1 << log_h, words = h << k0;
+  wk::DftTables tab;
+  WH_TRY(wh::ensure_dft_tables(ctx, log_h, &tab));
+  WH_TRY_CUDA(wh::ctx_malloc(ctx, &t.rows, words * 4));
+  WH_TRY_CUDA(wh::ctx_malloc(ctx, &t.digests, (2 * h - 1) * 8 * 4));
+  WH_TRY_CUDA(wh::ctx_malloc(ctx, &w->pre_scratch, words * 4));
+  // the copies start once the allocations are ordered on the context's stream
+  WH_TRY_CUDA(cudaEventRecord(ctx->up_ev[G], ctx->stream));
+  WH_TRY_CUDA(cudaStreamWaitEvent(ctx->copy_stream, ctx->up_ev[G], 0));
+  const int per = W / G;
+  const size_t group = (size_t)per << log_chunk;  // words per group
+  for (int g = 0; g < G; g++) {
+    WH_TRY_CUDA(cudaMemcpyAsync(w->d_poly + (size_t)g * group, poly + (size_t)g * group, group * 4,
+                                cudaMemcpyHostToDevice, ctx->copy_stream));
+    WH_TRY_CUDA(cudaEventRecord(ctx->up_ev[g], ctx->copy_stream));
+  }
+  for (int g = 0; g < G; g++) {
+    WH_TRY_CUDA(cudaStreamWaitEvent(ctx->stream, ctx->up_ev[g], 0));
+    WH_TRY_CUDA(wk::encode(w->d_poly + (size_t)g * group, group, ctx->stream));
+    WH_TRY_CUDA(wk::dft_batch(w->d_poly, t.rows, w->pre_scratch, log_chunk, k0, log_blowup, 1, tab, plan, 1,
+                              ctx->stream, g * per, per));
+  }
+  w->pre_plan = plan;
+  *done = true;
+  return WHIR_OK;
+}
+
 }  // namespace
 
 extern "C" {
@@ -598,8 +663,14 @@ int whir_commit(whir_ctx* ctx, const whir_protocol_params* params, int32_t n, co
       return WHIR_ERR_NOMEM;
     }
     w->own_poly = true;
-    if (cudaMemcpyAsync(w->d_poly, poly, N * 4, cudaMemcpyHostToDevice, ctx->stream) != cudaSuccess ||
-        wk::encode(w->d_poly, N, ctx->stream) != cudaSuccess) {
+    bool piped = false;
+    s = upload_with_dft(ctx, w, poly, &piped);
+    if (s != WHIR_OK) {
+      whir_witness_free(w);
+      return s;
+    }
+    if (!piped && (cudaMemcpyAsync(w->d_poly, poly, N * 4, cudaMemcpyHostToDevice, ctx->stream) != cudaSuccess ||
+                   wk::encode(w->d_poly, N, ctx->stream) != cudaSuccess)) {
       whir_witness_free(w);
       wh::set_error("polynomial upload failed");
       return WHIR_ERR_CUDA;
@@ -639,7 +710,11 @@ int whir_prove(whir_ctx* ctx, whir_witness* w, whir_challenger* chs, uint32_t* p
 int whir_witness_free(whir_witness* w) {
   if (!w) return WHIR_OK;
   whir_ctx* ctx = w->ctx;
+  // copies of a pipelined upload end before their buffers go back to the pool
+  // (and before the caller may reuse the host polynomial)
+  if (ctx->copy_stream) cudaStreamSynchronize(ctx->copy_stream);
   free_tree(ctx, w->commit_tree);
+  if (w->pre_scratch) cudaFreeAsync(w->pre_scratch, ctx->stream);
   if (w->own_poly && w->d_poly) cudaFreeAsync(w->d_poly, ctx->stream);
   cudaStreamSynchronize(ctx->stream);
   delete w;

@@ -258,6 +258,18 @@ int run_dft(whir_ctx* ctx, const uint32_t* in, uint32_t* out, uint32_t* scratch,
   return WHIR_OK;
 }
 
+bool dft_plan_known(const whir_ctx* ctx, int log_chunk, int log_w, int log_blowup, int lanes, wk::DftPlan* plan) {
+  const Key k{WHIR_TUNE_DFT, ctx->device, log_chunk, log_w, log_blowup, lanes};
+  whir_tune_entry e;
+  *plan = wk::dft_default_plan(log_chunk, log_w, log_blowup, lanes);
+  if (lookup(k, &e)) {
+    *plan = plan_of(e);
+    return true;
+  }
+  // mode 1 would tune this shape on its first run; other modes use the default
+  return g_mode.load() != 1 || !wk::dft_plan_ok(*plan, log_chunk, log_w, log_blowup, lanes);
+}
+
 int run_merkle_leaves(whir_ctx* ctx, const uint32_t* rows, int log_h, int row_words, int leaf_hash,
                       uint32_t* digests) {
   wk::Shape sh = wk::merkle_leaf_default();
