@@ -38,6 +38,7 @@ import os
 import pathlib
 import subprocess
 import sys
+import tempfile
 import time
 
 import numpy as np
@@ -92,7 +93,10 @@ class Clocks:
 
     def __init__(self, index: int):
         self.proc = None
-        self.path = ROOT / "gpurun_out" / f"clocks_rank{index}.csv"
+        # raw samples beside the run's other outputs when BENCH_OUT_DIR names a
+        # folder, else in the temporary directory; the JSON line summarises them
+        out_dir = os.environ.get("BENCH_OUT_DIR") or tempfile.gettempdir()
+        self.path = pathlib.Path(out_dir) / f"clocks_rank{index}.csv"
         try:
             self.path.parent.mkdir(exist_ok=True)
             q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
