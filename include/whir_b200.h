@@ -163,7 +163,8 @@ int whir_dft_plans(int32_t log_chunk, int32_t log_width, int32_t log_blowup, int
 /* whir_dft_batch / whir_merkle_commit / whir_fold_ext with an explicit launch
  * shape instead of the tuned one: plan = 7 words as above; Merkle shape =
  * {leaf threads, leaf CTAs per SM, node threads, node CTAs per SM, node variant (bit 0:
- * one-CTA top kernel, bit 1: sequential two-level kernel)}; fold
+ * one-CTA top kernel, bit 1: sequential two-level kernel, bit 2: cooperative last
+ * two-level step)}; fold
  * shape = {threads, CTAs per SM} (CTAs per SM 0: no cap). */
 int whir_dft_batch_plan(whir_ctx* ctx, const uint32_t* d_chunks, int32_t log_chunk, int32_t log_width,
                         int32_t log_blowup, int32_t ext, const int32_t* plan, uint32_t* d_out);

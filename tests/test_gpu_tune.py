@@ -40,8 +40,10 @@ def test_every_dft_plan_matches_oracle(pkg, gpu_ctx, oracle, log_chunk, log_w, l
 LEAF_SHAPES = [(128, 0), (128, 8), (128, 16), (256, 0), (256, 4), (256, 8), (256, 16), (512, 0), (512, 2), (512, 4),
                (512, 8)]
 # variant bit 0: top kernel (cooperative subtrees / one CTA); bit 1: the two-level
-# kernel's permutations one after the other
+# kernel's permutations one after the other; bit 2: the last two-level step with
+# four-lane cooperative permutations
 NODE_SHAPES = [(t, s, v) for v in (0, 1, 2, 3) for t, s in [(128, 0), (128, 8), (128, 16), (256, 0), (256, 8), (256, 16)]]
+NODE_SHAPES += [(256, 0, 4), (128, 16, 4), (128, 0, 5), (256, 8, 5), (256, 16, 6), (128, 0, 7)]
 
 
 # 2^17 and 2^13 leaves: leaf-digest kernel, two-level launches and either top

@@ -534,7 +534,7 @@ def dft_batch_plan(ctx: Context, chunks: DeviceArray, log_chunk: int, log_width:
 def merkle_commit_shaped(ctx: Context, rows: DeviceArray, log_height: int, row_words: int, leaf_hash: int,
                          shape, digests: DeviceArray) -> np.ndarray:
     """merkle_commit with shape = (leaf threads, leaf CTAs/SM, node threads, node CTAs/SM, node variant:
-    bit 0 one-CTA top kernel, bit 1 sequential two-level kernel)."""
+    bit 0 one-CTA top kernel, bit 1 sequential two-level kernel, bit 2 cooperative last two-level step)."""
     sh = np.ascontiguousarray(shape, dtype=np.int32)
     root = np.zeros(8, dtype=np.uint32)
     _check(lib().whir_merkle_commit_shaped(ctx.handle, rows.ptr, log_height, row_words, leaf_hash, sh.ctypes.data,

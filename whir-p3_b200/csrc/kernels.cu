@@ -1175,6 +1175,51 @@ __device__ __forceinline__ void coop_levels(uint32_t* sh, int cnt, int levels, s
   }
 }
 
+// Two tree levels with four-lane cooperative permutations: one group of four
+// lanes per output node (its two children, then the node), for the last,
+// narrow two-level step of a tree, where one thread per node leaves the
+// launch latency-bound (two dependent single-thread permutations). Lane q
+// holds words 4q .. 4q+3 of a state; a child's digest ends on lanes 0 and 1.
+// The loop runs per warp so all 32 lanes take every shuffle together.
+template <int CTA>
+__global__ void __launch_bounds__(CTA) k_merkle_two_levels_coop(uint32_t* __restrict__ digests, size_t in_off,
+                                                                 size_t in_count, const __grid_constant__ P2Consts comp) {
+  const size_t out_count = in_count >> 2;
+  const size_t mid_off = in_off + in_count, top_off = mid_off + (in_count >> 1);
+  const int lane = threadIdx.x & 31, q = lane & 3;
+  const size_t groups = (size_t)gridDim.x * (CTA / 4);
+  for (size_t base = (size_t)blockIdx.x * (CTA / 4) + (threadIdx.x >> 5) * 8; base < out_count; base += groups) {
+    const size_t jw = base + (lane >> 2);
+    const bool on = jw < out_count;
+    const size_t j = on ? jw : base;
+    uint32_t keep[4];
+#pragma unroll
+    for (int h = 0; h < 2; h++) {
+      // children 4j + 2h and 4j + 2h + 1: 16 consecutive words
+      const uint4 v = *reinterpret_cast<const uint4*>(digests + (in_off + 4 * j + 2 * h) * 8 + 4 * q);
+      uint32_t x[4] = {v.x, v.y, v.z, v.w};
+      coop_permute16(x, q, comp);
+      if (on && q < 2)
+        *reinterpret_cast<uint4*>(digests + (mid_off + 2 * j + h) * 8 + 4 * q) = make_uint4(x[0], x[1], x[2], x[3]);
+      // the parent's state: the first child's digest on lanes 0-1, the
+      // second's moved to lanes 2-3
+      if (h == 0) {
+#pragma unroll
+        for (int k = 0; k < 4; k++) keep[k] = x[k];
+      } else {
+#pragma unroll
+        for (int k = 0; k < 4; k++) {
+          const uint32_t from_b = __shfl_sync(0xffffffffu, x[k], (lane & ~3) | (q & 1));
+          if (q >= 2) keep[k] = from_b;
+        }
+      }
+    }
+    coop_permute16(keep, q, comp);
+    if (on && q < 2)
+      *reinterpret_cast<uint4*>(digests + (top_off + j) * 8 + 4 * q) = make_uint4(keep[0], keep[1], keep[2], keep[3]);
+  }
+}
+
 // Top of a tree: each CTA compresses up to 256 nodes of one level into a
 // subtree, one four-lane group per node pair, level by level in shared memory.
 // With several CTAs (at most 256), the last one to finish (atomic counter, no
@@ -1322,16 +1367,23 @@ cudaError_t merkle_upper(int log_h, uint32_t* digests, const P2Consts& p16, Shap
   const size_t h = (size_t)1 << log_h;
   size_t off = 0, cnt = h;
   // variant bit 0: the top kernel (0 cooperative subtrees, 1 one CTA); bit 1:
-  // the two-level kernel with its two permutations one after the other
-  if (node.variant < 0 || node.variant > 3) return cudaErrorInvalidValue;
-  const bool top_cta = (node.variant & 1) != 0, one_chain = (node.variant & 2) != 0;
+  // the two-level kernel with its two permutations one after the other; bit 2:
+  // the last two-level step with four-lane cooperative permutations
+  if (node.variant < 0 || node.variant > 7) return cudaErrorInvalidValue;
+  const bool top_cta = (node.variant & 1) != 0, one_chain = (node.variant & 2) != 0, coop_tail = (node.variant & 4) != 0;
   const size_t top = top_cta ? kCtaTop : kCoopTop;
   if (h >= kLevelPairMin) {
     if ((node.threads != 128 && node.threads != 256) || node.per_sm < 0) return cudaErrorInvalidValue;
     while (cnt > top) {
       const size_t out = cnt >> 2;
       const unsigned blocks = grid_shape(out, node);
-      if (node.threads == 128 && one_chain)
+      if (coop_tail && (cnt >> 2) <= top) {
+        const unsigned cblocks = grid_shape(out * 4, node);
+        if (node.threads == 128)
+          k_merkle_two_levels_coop<128><<<cblocks, 128, 0, st>>>(digests, off, cnt, p16);
+        else
+          k_merkle_two_levels_coop<256><<<cblocks, 256, 0, st>>>(digests, off, cnt, p16);
+      } else if (node.threads == 128 && one_chain)
         k_merkle_two_levels<128, true><<<blocks, 128, 0, st>>>(digests, off, cnt, p16);
       else if (node.threads == 128)
         k_merkle_two_levels<128, false><<<blocks, 128, 0, st>>>(digests, off, cnt, p16);

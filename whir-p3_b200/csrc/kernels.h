@@ -89,7 +89,8 @@ cudaError_t merkle_build(const uint32_t* rows, int log_h, int row_words, int lea
 // compression kernel (threads 128 or 256) and picks the top kernel (variant
 // bit 0 clear: cooperative four-lane permutations in many CTAs; set: one CTA,
 // one permutation per thread) and the two-level kernel's form (bit 1 set: its
-// two permutations one after the other, fewer registers).
+// two permutations one after the other, fewer registers; bit 2 set: the last,
+// narrow two-level step with four-lane cooperative permutations).
 constexpr int kMerkleLevelPairMin = 1 << 12;
 Shape merkle_leaf_default();
 Shape merkle_node_default();

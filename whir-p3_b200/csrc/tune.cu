@@ -185,10 +185,12 @@ int tune_dft(whir_ctx* ctx, const Key& k, const uint32_t* in, uint32_t* out, uin
 const wk::Shape kLeafShapes[] = {{128, 0, 0},  {128, 8, 0}, {128, 16, 0}, {256, 0, 0}, {256, 4, 0}, {256, 8, 0},
                                  {256, 16, 0}, {512, 0, 0}, {512, 2, 0},  {512, 4, 0}, {512, 8, 0}};
 // variant: bit 0 the top kernel (cooperative subtrees / one CTA), bit 1 the
-// two-level kernel's permutations one after the other instead of together
+// two-level kernel's permutations one after the other instead of together,
+// bit 2 the last two-level step with four-lane cooperative permutations
 const wk::Shape kNodeShapes[] = {{128, 0, 0}, {128, 8, 0}, {128, 16, 0}, {256, 0, 0}, {256, 8, 0}, {256, 16, 0},
                                  {128, 0, 1}, {128, 8, 1}, {128, 16, 1}, {256, 0, 1}, {256, 8, 1}, {256, 16, 1},
-                                 {128, 0, 2}, {128, 16, 2}, {256, 0, 2}, {256, 16, 2}, {128, 0, 3}, {256, 0, 3}};
+                                 {128, 0, 2}, {128, 16, 2}, {256, 0, 2}, {256, 16, 2}, {128, 0, 3}, {256, 0, 3},
+                                 {128, 0, 4}, {256, 0, 4}, {256, 16, 4}, {128, 0, 5}, {256, 0, 5}};
 const wk::Shape kFoldShapes[] = {{128, 0, 0},  {128, 16, 0}, {256, 0, 0}, {256, 4, 0}, {256, 8, 0},
                                  {256, 16, 0}, {512, 0, 0},  {512, 2, 0}, {512, 4, 0}, {512, 8, 0}};
 
