@@ -1466,51 +1466,6 @@ cudaError_t merkle_open(const uint32_t* rows, const uint32_t* digests, int log_h
 
 constexpr int GRIND_CTA = 256;
 
-// Entry i of column `slot` of the width-16 external matrix circ(2*M4, M4, M4, M4):
-// 2 * M4[i % 4][slot % 4] in the block of `slot`, M4[i % 4][slot % 4] elsewhere.
-__host__ __device__ constexpr int ext_col16(int slot, int i) {
-  const int m4[4][4] = {{5, 7, 1, 3}, {4, 6, 1, 1}, {1, 3, 5, 7}, {1, 1, 4, 6}};
-  return m4[i & 3][slot & 3] * ((i >> 2) == (slot >> 2) ? 2 : 1);
-}
-
-// The challenger's check of one candidate w: the Poseidon2-16 permutation of
-// the sponge state with w at position SLOT, and only output word 7 (the word
-// sample_bits reads). The initial external layer is linear, so it and the
-// first round's constants are folded into cp = ext(state with 0 at SLOT) + rc
-// (host-computed) plus w times a compile-time column of small integers; the
-// last external layer computes word 7 only.
-template <int SLOT>
-__device__ __forceinline__ uint32_t grind_word7(uint32_t w, const uint32_t (&cp)[16], const P2Consts& k) {
-  using namespace kb;
-  uint32_t wm[15];  // w * j mod p, j < 15
-  wm[0] = 0u;
-  wm[1] = w;
-#pragma unroll
-  for (int j = 2; j < 15; j++) wm[j] = add(wm[j - 1], w);
-  uint32_t x[16];
-#pragma unroll
-  for (int i = 0; i < 16; i++) x[i] = p2::cube(add(cp[i], wm[ext_col16(SLOT, i)]));
-  p2::ext_layer<16>(x);
-#pragma unroll 1
-  for (int r = 1; r < p2::RF / 2; r++) p2::full_round<16>(x, k.ext_rc + r * 16);
-#pragma unroll 1
-  for (int r = 0; r < p2::RP16; r++) p2::partial_round<16>(x, k.int_rc[r]);
-#pragma unroll 1
-  for (int r = p2::RF / 2; r < p2::RF - 1; r++) p2::full_round<16>(x, k.ext_rc + r * 16);
-  const uint32_t* rc = k.ext_rc + (p2::RF - 1) * 16;
-#pragma unroll
-  for (int i = 0; i < 16; i++) x[i] = p2::cube(add(x[i], rc[i]));
-  // word 7 of the external layer: row 3 of M4 ([1, 1, 4, 6]) of block 1, plus
-  // the sum of row 3 over all blocks (the M4 addition chain's x3 output)
-  uint32_t r3[4];
-#pragma unroll
-  for (int b = 0; b < 4; b++) {
-    const uint32_t t0 = add(x[4 * b], x[4 * b + 1]), t1 = add(x[4 * b + 2], x[4 * b + 3]);
-    r3[b] = add(dbl(dbl(t1)), add(dbl(x[4 * b + 3]), t0));
-  }
-  return add(r3[1], add(add(r3[0], r3[1]), add(r3[2], r3[3])));
-}
-
 // Each claim is GRIND_CTA consecutive candidates, one per thread.
 template <int SLOT>
 __global__ void __launch_bounds__(GRIND_CTA) k_grind(const __grid_constant__ P2Consts p16, uint4 st0, uint4 st1,
@@ -1550,7 +1505,7 @@ __global__ void __launch_bounds__(GRIND_CTA) k_grind(const __grid_constant__ P2C
       return;
     }
     const uint64_t w = start + threadIdx.x;
-    if (w < limit && (grind_word7<SLOT>((uint32_t)w, cp, p16) & mask) == 0u) atomicMin(result, (uint32_t)w);
+    if (w < limit && (p2::grind_word7<SLOT>((uint32_t)w, cp, p16) & mask) == 0u) atomicMin(result, (uint32_t)w);
   }
 }
 
@@ -1577,8 +1532,7 @@ cudaError_t grind(const uint32_t* state, const uint32_t* in, int in_len, int bit
   for (int i = 0; i < 16; i++) s[i] = kb::from_mont(state[i]);
   for (int i = 0; i < in_len; i++) s[i] = kb::from_mont(in[i]);
   s[in_len] = 0u;
-  p2::ext_layer<16>(s);
-  for (int i = 0; i < 16; i++) s[i] = kb::add(s[i], p16.ext_rc[i]);
+  p2::grind_fold(s, p16);
   // with a mailbox the previous search left the state reset (grind_reset
   // initialises it once per context)
   if (!mail) {

@@ -276,4 +276,53 @@ KB_HD void permute_sponge(uint32_t (&x)[T], const P2Consts& k) {
   else ext_layer<T>(x);
 }
 
+// Proof-of-work check of one candidate w (the duplex challenger's
+// check_witness): the width-16 permutation of the sponge state with w at
+// position SLOT, of which sample_bits reads only output word 7. The initial
+// external layer is linear, so it and the first round's constants fold into
+// cp = ext(state with 0 at SLOT) + rc (grind_fold, once per search) plus w
+// times column SLOT of circ(2*M4, M4, M4, M4), whose entries are small
+// integers; the last external layer forms word 7 only.
+KB_HD constexpr int ext_col16(int slot, int i) {
+  const int m[4][4] = {{5, 7, 1, 3}, {4, 6, 1, 1}, {1, 3, 5, 7}, {1, 1, 4, 6}};
+  return m[i & 3][slot & 3] * ((i >> 2) == (slot >> 2) ? 2 : 1);
+}
+// state (canonical, 0 at the witness position) -> cp
+KB_HD void grind_fold(uint32_t (&state)[16], const P2Consts& k) {
+  ext_layer<16>(state);
+#pragma unroll
+  for (int i = 0; i < 16; i++) state[i] = kb::add(state[i], k.ext_rc[i]);
+}
+template <int SLOT>
+KB_HD uint32_t grind_word7(uint32_t w, const uint32_t (&cp)[16], const P2Consts& k) {
+  using namespace kb;
+  uint32_t wm[15];  // w * j mod p, j < 15
+  wm[0] = 0u;
+  wm[1] = w;
+#pragma unroll
+  for (int j = 2; j < 15; j++) wm[j] = add(wm[j - 1], w);
+  uint32_t x[16];
+#pragma unroll
+  for (int i = 0; i < 16; i++) x[i] = cube(add(cp[i], wm[ext_col16(SLOT, i)]));
+  ext_layer<16>(x);
+#pragma unroll 1
+  for (int r = 1; r < RF / 2; r++) full_round<16>(x, k.ext_rc + r * 16);
+#pragma unroll 1
+  for (int r = 0; r < RP16; r++) partial_round<16>(x, k.int_rc[r]);
+#pragma unroll 1
+  for (int r = RF / 2; r < RF - 1; r++) full_round<16>(x, k.ext_rc + r * 16);
+  const uint32_t* rc = k.ext_rc + (RF - 1) * 16;
+#pragma unroll
+  for (int i = 0; i < 16; i++) x[i] = cube(add(x[i], rc[i]));
+  // word 7 of the external layer: row 3 of M4 ([1, 1, 4, 6]) of block 1, plus
+  // the sum of row 3 over all blocks (the M4 addition chain's x3 output)
+  uint32_t r3[4];
+#pragma unroll
+  for (int b = 0; b < 4; b++) {
+    const uint32_t t0 = add(x[4 * b], x[4 * b + 1]), t1 = add(x[4 * b + 2], x[4 * b + 3]);
+    r3[b] = add(dbl(dbl(t1)), add(dbl(x[4 * b + 3]), t0));
+  }
+  return add(r3[1], add(add(r3[0], r3[1]), add(r3[2], r3[3])));
+}
+
 }  // namespace p2
