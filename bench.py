@@ -5,7 +5,11 @@ Workload (the reference's own benchmark, benches/whir.rs:34-120 "prove"):
 KoalaBear / quartic extension, num_variables = 24, folding factor 4, rate 1/2,
 100-bit CapacityBound, pow_bits 16, rs_domain_initial_reduction_factor 3, one
 evaluation constraint, Poseidon2-24 leaf hashing, Poseidon2-16 compression and
-duplex challenger, DIGEST_ELEMS 32. Inputs are seeded synthetic data.
+duplex challenger, DIGEST_ELEMS 32. Inputs are drawn as the reference's
+benchmark draws them: SmallRng::seed_from_u64(0) yields the 2^24-element
+polynomial, then the constraint point; the Poseidon2 permutations are
+new_from_rng_128 on SmallRng::seed_from_u64(1) with Plonky3's KoalaBear
+external block.
 
 One step = one full commit + prove of one polynomial on each GPU (replicas:
 one independent proof per rank, no collective on the data path). Rank 0 prints
@@ -75,11 +79,14 @@ def job_value(max_total_ms: float, steps: int, world: int) -> tuple[float, float
     return step_ms, step_ms / world
 
 
-def inputs(rank: int, n: int):
-    rng = np.random.default_rng(1000 + rank)
-    poly = rng.integers(0, P, 1 << n, dtype=np.uint64).astype(np.uint32)
-    point = rng.integers(0, P, 4 * n, dtype=np.uint64).astype(np.uint32)
-    return poly, point
+def inputs(draw, rank: int, n: int):
+    """The benchmark's inputs as benches/whir.rs:92-100 draws them: 2^n base
+    elements, then n extension coordinates, from SmallRng::seed_from_u64(0)
+    (rank r of a replica run uses seed r). `draw(seed, count)` is the
+    product's whir_rng_koalabear or, on the CPU legs, the oracle's restatement
+    of the same generator."""
+    v = draw(rank, (1 << n) + 4 * n)
+    return v[: 1 << n], v[1 << n:]
 
 
 def oracle_params():
@@ -150,7 +157,7 @@ def run_reference(args) -> None:
 
     o = Oracle()
     prm = oracle_params()
-    poly, point = inputs(0, N_VARS)
+    poly, point = inputs(o.rng_fields, 0, N_VARS)
     cores = os.cpu_count() or 1
     # a CPU proof takes seconds: one warm-up proof, then at most as many timed
     # proofs as fit in about two and a half minutes (at least one), so the
@@ -168,7 +175,8 @@ def run_reference(args) -> None:
     ms = float(np.mean(times))
     line = {"metric": METRIC, "value": ms, "unit": UNIT, "n_gpus": args.gpus, "steps": len(times),
             "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": False, "scaling": "weak",
-            "vs_baseline": None, "dtype": "u32 (KoalaBear mod p)", "data": "synthetic (seeded)",
+            "vs_baseline": None, "dtype": "u32 (KoalaBear mod p)",
+            "data": "synthetic: the reference benchmark's SmallRng(0) polynomial and point",
             "config": dict(CONFIG, parallelism="cpu"), "impl": "reference",
             "cpu_baseline": {"value": ms, "unit": UNIT, "cores": cores, "kind": "port",
                              "sample": f"{len(times)} full n=24 commit+prove runs of the oracle port (OpenMP)"},
@@ -180,7 +188,7 @@ def cpu_baseline_sample() -> dict:
     from oracle.oracle import Oracle
 
     o = Oracle()
-    poly, point = inputs(0, N_VARS)
+    poly, point = inputs(o.rng_fields, 0, N_VARS)
     t0 = time.perf_counter()
     o.prove(oracle_params(), N_VARS, poly, point)
     ms = (time.perf_counter() - t0) * 1e3
@@ -451,7 +459,7 @@ def main() -> None:
     ctx.set_stream(stream.cuda_stream)
     params = pkg.ProtocolParameters(100, 16, pkg.FoldingFactor.constant(4), pkg.SecurityAssumption.CapacityBound, 1, 3,
                                     "poseidon2_24", 32)
-    poly, point = inputs(rank, N_VARS)
+    poly, point = inputs(pkg.rng_koalabear, rank, N_VARS)
     d_poly = pkg.DeviceArray.from_host(ctx, poly)  # resident in HBM, Montgomery form
     flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
 
@@ -568,7 +576,7 @@ def main() -> None:
         line = {"metric": METRIC, "value": round(value, 4), "unit": UNIT, "n_gpus": world, "steps": args.steps,
                 "warmup": max(args.warmup, 3), "ms_per_step": round(step_ms, 4), "higher_is_better": False,
                 "scaling": "weak", "vs_baseline": None, "dtype": "u32 (KoalaBear mod p, exact)",
-                "data": "synthetic (seeded)",
+                "data": "synthetic: the reference benchmark's SmallRng(0) polynomial and point",
                 "config": dict(CONFIG, parallelism=f"replicas x{world} (one proof per GPU per step)"),
                 "proofs_per_s": round(1e3 / value, 3), "proof_words": int(ref_proof.size),
                 "e2e": {"value": round(e2e_value, 4), "unit": UNIT, "h2d_bytes_per_step": h2d * world,

@@ -48,10 +48,15 @@ typedef struct whir_witness whir_witness;
 /* Poseidon2 permutation data (canonical values). Supported shapes: width 16
  * with 8 full + 20 partial rounds, width 24 with 8 full + 23 partial rounds.
  * Replaces p3-koala-bear Poseidon2KoalaBear<16>/<24> (src/bin/main.rs:31-32). */
+enum {
+  WHIR_P2_MDS_MAT4 = 0,  /* external 4x4 block circ(2,3,1,1): Plonky3's Monty-31 MDSMat4 (KoalaBear) */
+  WHIR_P2_HL_MAT4 = 1    /* the Poseidon2 paper's M4 [[5,7,1,3],[4,6,1,1],[1,3,5,7],[1,1,4,6]] (HLMDSMat4) */
+};
 typedef struct {
   uint32_t width;
   uint32_t rounds_f;
   uint32_t rounds_p;
+  uint32_t external_matrix; /* WHIR_P2_MDS_MAT4 or WHIR_P2_HL_MAT4; both widths of a context use the same */
   uint32_t ext_rc[8 * 24]; /* rounds_f rows of `width`: first half before, second half after the partial rounds */
   uint32_t int_rc[32];     /* one per partial round, added to lane 0 */
   uint32_t diag[24];       /* internal matrix = all-ones + diag(diag); fixed, as p3-koala-bear's internal
@@ -105,8 +110,21 @@ typedef struct {
 const char* whir_last_error(void);
 /* Number of CUDA kernels this library has enqueued in this process. */
 uint64_t whir_kernel_launches(void);
-/* The library's default Poseidon2 data (seeded stand-in, not Plonky3's). */
+/* The library's default Poseidon2 data: whir_poseidon2_params_from_rng(1,
+ * WHIR_P2_MDS_MAT4), the set-up of src/bin/main.rs:100-102 and
+ * benches/whir.rs:66-68 (Poseidon16 then Poseidon24 from one SmallRng seeded 1). */
 int whir_poseidon2_default_params(whir_poseidon2_params* p16, whir_poseidon2_params* p24);
+/* Poseidon2KoalaBear<16>::new_from_rng_128 followed by <24>::new_from_rng_128
+ * on one rand::rngs::SmallRng::seed_from_u64(seed) stream (p3-poseidon2
+ * new_from_rng: initial external rows, terminal external rows, then the
+ * internal constants), with the given external block. */
+int whir_poseidon2_params_from_rng(uint64_t seed, uint32_t external_matrix, whir_poseidon2_params* p16,
+                                   whir_poseidon2_params* p24);
+/* The first `count` KoalaBear elements (canonical) that `rng.random::<F>()`
+ * draws from rand::rngs::SmallRng::seed_from_u64(seed): the polynomial and
+ * constraint point of benches/whir.rs:92-100 (seed 0: 2^n base elements, then
+ * 4 per extension coordinate). Host only. */
+int whir_rng_koalabear(uint64_t seed, uint32_t* out, size_t count);
 int whir_ctx_create(int32_t device, const whir_poseidon2_params* p16, const whir_poseidon2_params* p24,
                     whir_ctx** out);
 int whir_ctx_destroy(whir_ctx* ctx);
@@ -171,6 +189,11 @@ int whir_dft_batch_plan(whir_ctx* ctx, const uint32_t* d_chunks, int32_t log_chu
 int whir_merkle_commit_shaped(whir_ctx* ctx, const uint32_t* d_rows, int32_t log_height, int32_t row_words,
                               int32_t leaf_hash, const int32_t* shape, uint32_t* d_digests, uint32_t* root);
 int whir_fold_ext_shaped(whir_ctx* ctx, uint32_t* d_evals, int32_t n, const uint32_t* r, const int32_t* shape);
+/* whir_sumcheck_coeffs with its reduction's block count capped at max_blocks
+ * (1 .. 4096): the launch shape whir_sumcheck_coeffs_noalloc uses at its cap of
+ * 2048, reachable at any cap for shape tests. */
+int whir_sumcheck_coeffs_shaped(whir_ctx* ctx, const uint32_t* d_f, const uint32_t* d_w, int32_t n,
+                                int32_t max_blocks, uint32_t* c0, uint32_t* c2);
 
 /* ---- parameters (WhirConfig::new, src/whir/parameters.rs:81-234) ----------- */
 int whir_config_new(const whir_protocol_params* params, int32_t num_variables, whir_config* out);

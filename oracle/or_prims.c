@@ -4,15 +4,27 @@
  *
  *   Poseidon2 ...... Grassi, Khovratovich, Schofnegger, "Poseidon2: A Faster
  *                    Version of the Poseidon Hash Function", eprint 2023/323.
- *                    S-box x^3, external matrix circ(2*M4, M4, ...) with the
- *                    paper's M4, internal matrix 1*1^T + diag(mu).
- *                    Round counts 8 full + 20 partial (width 16) and 8 + 23
- *                    (width 24) for the 31-bit field with x^3.
- *   Constants ...... SplitMix64 (Steele, Lea, Flood 2014) seeded with 1,
- *                    31-bit rejection sampling; the width-16 set is drawn
- *                    first, then the width-24 set, mirroring the reference's
- *                    one-RNG-two-permutations set-up (src/bin/main.rs:100-102).
- *                    The values themselves are not Plonky3's (parity unpinned).
+ *                    S-box x^3, external matrix circ(2*M, M, ...) for a 4x4
+ *                    block M, internal matrix 1*1^T + diag(mu). Round counts
+ *                    8 full + 20 partial (width 16) and 8 + 23 (width 24) for
+ *                    the 31-bit field with x^3. Block M: mat 0 is the circulant
+ *                    (2, 3, 1, 1) that Plonky3's Monty-31 external layer uses
+ *                    for Poseidon2KoalaBear (MDSMat4); mat 1 is the paper's M4
+ *                    (Plonky3's HLMDSMat4).
+ *   Constants ...... Poseidon2KoalaBear::new_from_rng_128 on
+ *                    rand::rngs::SmallRng::seed_from_u64(1), the width-16 set
+ *                    drawn first and the width-24 set after it on the same
+ *                    stream (src/bin/main.rs:100-102, benches/whir.rs:66-68).
+ *                    SmallRng = xoshiro256++ (Blackman, Vigna 2021) with its
+ *                    four state words from SplitMix64 (Steele, Lea, Flood
+ *                    2014) of the seed; next_u32 = high half of next_u64.
+ *                    KoalaBear sampling: v = next_u32 >> 1, rejected if
+ *                    v >= p, and v is the Montgomery word (value v / 2^32).
+ *                    Order (p3-poseidon2 new_from_rng): the 4 initial external
+ *                    rows, the 4 terminal external rows, then the internal
+ *                    constants. These are restated from the published
+ *                    algorithms and Plonky3's documented behaviour; no output
+ *                    of the reference pins them (parity unpinned).
  *                    The internal diagonal is fixed, not drawn: small integers
  *                    and signed powers of two, the form of p3-koala-bear's
  *                    internal layer (which takes only round constants).
@@ -34,33 +46,77 @@
 #include "or_field.h"
 
 /* ------------------------------------------------------------------------ */
-/* Poseidon2                                                                 */
+/* SmallRng and KoalaBear sampling                                           */
 /* ------------------------------------------------------------------------ */
 
-static uint64_t sm64_next(uint64_t* s) {
-  uint64_t z = (*s += 0x9e3779b97f4a7c15ull);
-  z = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ull;
-  z = (z ^ (z >> 27)) * 0x94d049bb133111ebull;
-  return z ^ (z >> 31);
-}
+typedef struct {
+  uint64_t s[4];
+} or_rng;
 
-static uint32_t sm64_field(uint64_t* s) {
-  for (;;) {
-    uint32_t v = (uint32_t)(sm64_next(s) >> 33);
-    if (v < OR_P) return v;
+static uint64_t rotl64(uint64_t x, int k) { return (x << k) | (x >> (64 - k)); }
+
+static void or_rng_seed(or_rng* g, uint64_t seed) {
+  for (int i = 0; i < 4; i++) {
+    uint64_t z = (seed += 0x9e3779b97f4a7c15ull);
+    z = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ull;
+    z = (z ^ (z >> 27)) * 0x94d049bb133111ebull;
+    g->s[i] = z ^ (z >> 31);
   }
 }
 
-static void p2_fill(or_p2_params* p, uint32_t width, uint32_t rp, uint64_t* s) {
+static uint64_t or_rng_next(or_rng* g) {
+  uint64_t* s = g->s;
+  const uint64_t out = rotl64(s[0] + s[3], 23) + s[0];
+  const uint64_t t = s[1] << 17;
+  s[2] ^= s[0];
+  s[3] ^= s[1];
+  s[1] ^= s[2];
+  s[0] ^= s[3];
+  s[2] ^= t;
+  s[3] = rotl64(s[3], 45);
+  return out;
+}
+
+/* canonical value of the next KoalaBear element */
+static uint32_t or_rng_field(or_rng* g) {
+  const uint32_t r_inv = 0x3f010000u; /* 2^-32 mod p */
+  for (;;) {
+    const uint32_t v = (uint32_t)(or_rng_next(g) >> 32) >> 1;
+    if (v < OR_P) return or_mul(v, r_inv);
+  }
+}
+
+void or_rng_fields(uint64_t seed, uint32_t* out, size_t count) {
+  or_rng g;
+  or_rng_seed(&g, seed);
+  for (size_t i = 0; i < count; i++) out[i] = or_rng_field(&g);
+}
+
+/* raw generator access for known-answer checks */
+void or_rng_seed_state(uint64_t seed, uint64_t* state4) {
+  or_rng g;
+  or_rng_seed(&g, seed);
+  memcpy(state4, g.s, sizeof(g.s));
+}
+void or_rng_u64_from_state(const uint64_t* state4, uint64_t* out, size_t count) {
+  or_rng g;
+  memcpy(g.s, state4, sizeof(g.s));
+  for (size_t i = 0; i < count; i++) out[i] = or_rng_next(&g);
+}
+
+/* ------------------------------------------------------------------------ */
+/* Poseidon2                                                                 */
+/* ------------------------------------------------------------------------ */
+
+static void p2_fill(or_p2_params* p, uint32_t width, uint32_t rp, uint32_t mat, or_rng* g) {
   memset(p, 0, sizeof(*p));
   p->width = width;
   p->rounds_f = 8;
   p->rounds_p = rp;
-  for (uint32_t r = 0; r < 4; r++)
-    for (uint32_t i = 0; i < width; i++) p->ext_rc[r * width + i] = sm64_field(s);
-  for (uint32_t r = 0; r < rp; r++) p->int_rc[r] = sm64_field(s);
-  for (uint32_t r = 4; r < 8; r++)
-    for (uint32_t i = 0; i < width; i++) p->ext_rc[r * width + i] = sm64_field(s);
+  p->mat = mat;
+  for (uint32_t r = 0; r < 8; r++)
+    for (uint32_t i = 0; i < width; i++) p->ext_rc[r * width + i] = or_rng_field(g);
+  for (uint32_t r = 0; r < rp; r++) p->int_rc[r] = or_rng_field(g);
   /* internal diagonal: fixed, drawn from no RNG. Entries are small integers
    * and signed powers of two: width 16
    *   -2, 1, 2, 1/2, 3, 4, -1/2, -3, -4, 2^-8, 2^-3, 2^-24, -2^-8, -2^-3, -2^-4, -2^-24
@@ -85,26 +141,31 @@ static void p2_fill(or_p2_params* p, uint32_t width, uint32_t rp, uint64_t* s) {
   }
 }
 
-void or_p2_default(or_p2_params* p16, or_p2_params* p24) {
-  uint64_t s = 1;
+void or_p2_from_rng(uint64_t seed, uint32_t mat, or_p2_params* p16, or_p2_params* p24) {
+  or_rng g;
+  or_rng_seed(&g, seed);
   or_p2_params t16, t24;
-  p2_fill(&t16, 16, 20, &s);
-  p2_fill(&t24, 24, 23, &s);
+  p2_fill(&t16, 16, 20, mat, &g);
+  p2_fill(&t24, 24, 23, mat, &g);
   if (p16) *p16 = t16;
   if (p24) *p24 = t24;
 }
 
-static void m4(uint32_t* x) {
-  /* M4 = [[5,7,1,3],[4,6,1,1],[1,3,5,7],[1,1,4,6]] (eprint 2023/323, sec. 5.1) */
-  uint64_t a = x[0], b = x[1], c = x[2], d = x[3];
-  x[0] = (uint32_t)((5 * a + 7 * b + 1 * c + 3 * d) % OR_P);
-  x[1] = (uint32_t)((4 * a + 6 * b + 1 * c + 1 * d) % OR_P);
-  x[2] = (uint32_t)((1 * a + 3 * b + 5 * c + 7 * d) % OR_P);
-  x[3] = (uint32_t)((1 * a + 1 * b + 4 * c + 6 * d) % OR_P);
+void or_p2_default(or_p2_params* p16, or_p2_params* p24) { or_p2_from_rng(1, 0, p16, p24); }
+
+static void m4(uint32_t* x, uint32_t mat) {
+  /* mat 0: circ(2, 3, 1, 1), row i = (2, 3, 1, 1) rotated right by i;
+   * mat 1: [[5,7,1,3],[4,6,1,1],[1,3,5,7],[1,1,4,6]] (eprint 2023/323, sec. 5.1) */
+  static const uint64_t circ[4][4] = {{2, 3, 1, 1}, {1, 2, 3, 1}, {1, 1, 2, 3}, {3, 1, 1, 2}};
+  static const uint64_t hl[4][4] = {{5, 7, 1, 3}, {4, 6, 1, 1}, {1, 3, 5, 7}, {1, 1, 4, 6}};
+  const uint64_t(*m)[4] = mat == 1 ? hl : circ;
+  uint64_t y[4];
+  for (int i = 0; i < 4; i++) y[i] = (m[i][0] * x[0] + m[i][1] * x[1] + m[i][2] * x[2] + m[i][3] * x[3]) % OR_P;
+  for (int i = 0; i < 4; i++) x[i] = (uint32_t)y[i];
 }
 
-static void ext_layer(uint32_t* x, uint32_t t) {
-  for (uint32_t c = 0; c < t; c += 4) m4(x + c);
+static void ext_layer(uint32_t* x, uint32_t t, uint32_t mat) {
+  for (uint32_t c = 0; c < t; c += 4) m4(x + c, mat);
   uint32_t s[4] = {0, 0, 0, 0};
   for (uint32_t c = 0; c < t; c += 4)
     for (int j = 0; j < 4; j++) s[j] = or_add(s[j], x[c + j]);
@@ -115,10 +176,10 @@ static inline uint32_t cube(uint32_t v) { return or_mul(or_mul(v, v), v); }
 
 void or_p2_permute(const or_p2_params* prm, uint32_t* x) {
   const uint32_t t = prm->width, hf = prm->rounds_f / 2;
-  ext_layer(x, t);
+  ext_layer(x, t, prm->mat);
   for (uint32_t r = 0; r < hf; r++) {
     for (uint32_t i = 0; i < t; i++) x[i] = cube(or_add(x[i], prm->ext_rc[r * t + i]));
-    ext_layer(x, t);
+    ext_layer(x, t, prm->mat);
   }
   for (uint32_t r = 0; r < prm->rounds_p; r++) {
     x[0] = cube(or_add(x[0], prm->int_rc[r]));
@@ -128,7 +189,7 @@ void or_p2_permute(const or_p2_params* prm, uint32_t* x) {
   }
   for (uint32_t r = hf; r < prm->rounds_f; r++) {
     for (uint32_t i = 0; i < t; i++) x[i] = cube(or_add(x[i], prm->ext_rc[r * t + i]));
-    ext_layer(x, t);
+    ext_layer(x, t, prm->mat);
   }
 }
 

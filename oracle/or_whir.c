@@ -284,6 +284,28 @@ typedef struct {
   or_p2_params p16, p24;
 } tr_t;
 
+static int g_p2_set = 0;
+static or_p2_params g_p16, g_p24;
+
+void or_p2_select(const or_p2_params* p16, const or_p2_params* p24) {
+  if (p16 && p24) {
+    g_p16 = *p16;
+    g_p24 = *p24;
+    g_p2_set = 1;
+  } else {
+    g_p2_set = 0;
+  }
+}
+
+static void p2_selected(or_p2_params* p16, or_p2_params* p24) {
+  if (g_p2_set) {
+    *p16 = g_p16;
+    *p24 = g_p24;
+  } else {
+    or_p2_default(p16, p24);
+  }
+}
+
 static or_ef sample_ef(tr_t* t) {
   or_ef r;
   for (int i = 0; i < 4; i++) r.c[i] = or_chal_sample(&t->ch, &t->p16);
@@ -481,7 +503,7 @@ int or_whir_prove(const or_params* prm, int n, const uint32_t* poly, const uint3
   int rc = or_config_new(prm, n, &cfg);
   if (rc) return rc;
   tr_t t;
-  or_p2_default(&t.p16, &t.p24);
+  p2_selected(&t.p16, &t.p24);
   or_chal_init(&t.ch);
   {
     int len = or_domain_separator(&cfg, prm->ds_digest_elems, NULL, 0);
@@ -808,7 +830,7 @@ int or_whir_verify(const or_params* prm, int n, const uint32_t* user_points, con
   int rc = or_config_new(prm, n, &cfg);
   if (rc) return rc;
   tr_t t;
-  or_p2_default(&t.p16, &t.p24);
+  p2_selected(&t.p16, &t.p24);
   or_chal_init(&t.ch);
   {
     int len = or_domain_separator(&cfg, prm->ds_digest_elems, NULL, 0);

@@ -7,12 +7,12 @@
  * product library (whir-p3_b200) never includes, links or calls it.
  *
  * Parity status: the whir-p3 protocol logic (src/) is restated line by line.
- * The Plonky3 primitives (rev c38eb05, not vendored in the reference) are
- * restated from their published algorithms; where the concrete constants come
- * from running Plonky3 code (Poseidon2 round constants drawn by
- * `new_from_rng_128(SmallRng::seed_from_u64(1))`, the RNG-drawn polynomial),
- * this restatement uses its own documented seeded generator instead, so those
- * values are "parity unpinned" against the reference.
+ * The Plonky3 primitives (rev c38eb05, not vendored in the reference) and the
+ * rand 0.10 generator behind `new_from_rng_128(SmallRng::seed_from_u64(1))`
+ * and the RNG-drawn inputs are restated from their published algorithms and
+ * documented behaviour. No output of the reference (roots, transcripts,
+ * proofs) exists to check them against, so those values are "parity
+ * unpinned" against the reference.
  *
  * All field elements at this interface are canonical uint32 values; an
  * extension element is 4 consecutive words (coefficients of 1, X, X^2, X^3).
@@ -32,12 +32,24 @@ typedef struct {
   uint32_t width;            /* 16 or 24 */
   uint32_t rounds_f;         /* full rounds (half before, half after the partial rounds) */
   uint32_t rounds_p;         /* partial rounds */
+  uint32_t mat;              /* external block: 0 circ(2,3,1,1) (Plonky3 MDSMat4), 1 the paper's M4 */
   uint32_t ext_rc[8 * 24];   /* rounds_f rows of `width` constants */
   uint32_t int_rc[32];       /* rounds_p constants, added to lane 0 */
   uint32_t diag[24];         /* internal matrix = all-ones + diag(diag) */
 } or_p2_params;
 
 void or_p2_default(or_p2_params* p16, or_p2_params* p24);
+/* new_from_rng_128 for width 16, then 24, on one SmallRng::seed_from_u64(seed) */
+void or_p2_from_rng(uint64_t seed, uint32_t mat, or_p2_params* p16, or_p2_params* p24);
+/* the permutations or_whir_prove / or_whir_verify use (NULL: or_p2_default) */
+void or_p2_select(const or_p2_params* p16, const or_p2_params* p24);
+/* the first `count` KoalaBear elements rng.random::<F>() draws from
+ * SmallRng::seed_from_u64(seed), canonical */
+void or_rng_fields(uint64_t seed, uint32_t* out, size_t count);
+/* the generator's state after seed_from_u64(seed), and raw next_u64 outputs
+ * from a given state (known-answer checks of xoshiro256++ and SplitMix64) */
+void or_rng_seed_state(uint64_t seed, uint64_t* state4);
+void or_rng_u64_from_state(const uint64_t* state4, uint64_t* out, size_t count);
 void or_p2_permute(const or_p2_params* prm, uint32_t* state);
 
 /* ---- Protocol parameters (ProtocolParameters, src/parameters/mod.rs:147-166) */

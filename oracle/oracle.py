@@ -30,6 +30,7 @@ class P2Params(C.Structure):
         ("width", C.c_uint32),
         ("rounds_f", C.c_uint32),
         ("rounds_p", C.c_uint32),
+        ("mat", C.c_uint32),
         ("ext_rc", C.c_uint32 * (8 * 24)),
         ("int_rc", C.c_uint32 * 32),
         ("diag", C.c_uint32 * 24),
@@ -100,10 +101,18 @@ _u32p = np.ctypeslib.ndpointer(dtype=np.uint32, flags="C_CONTIGUOUS")
 
 
 class Oracle:
-    def __init__(self, path: os.PathLike | None = None):
+    def __init__(self, path: os.PathLike | None = None, p2_seed: int = 1, p2_mat: int = 0):
+        """p2_seed, p2_mat: the Poseidon2 permutations, new_from_rng_128 on
+        SmallRng::seed_from_u64(p2_seed) with external block p2_mat (0: the
+        circulant (2, 3, 1, 1) of Plonky3's KoalaBear; 1: the paper's M4)."""
         self.lib = C.CDLL(str(path or build()))
         L = self.lib
         L.or_p2_default.argtypes = [C.POINTER(P2Params), C.POINTER(P2Params)]
+        L.or_p2_from_rng.argtypes = [C.c_uint64, C.c_uint32, C.POINTER(P2Params), C.POINTER(P2Params)]
+        L.or_p2_select.argtypes = [C.POINTER(P2Params), C.POINTER(P2Params)]
+        L.or_rng_fields.argtypes = [C.c_uint64, _u32p, C.c_size_t]
+        L.or_rng_seed_state.argtypes = [C.c_uint64, C.POINTER(C.c_uint64)]
+        L.or_rng_u64_from_state.argtypes = [C.POINTER(C.c_uint64), C.POINTER(C.c_uint64), C.c_size_t]
         L.or_p2_permute.argtypes = [C.POINTER(P2Params), _u32p]
         L.or_config_new.argtypes = [C.POINTER(Params), C.c_int, C.POINTER(Config)]
         L.or_config_new.restype = C.c_int
@@ -140,9 +149,15 @@ class Oracle:
         L.or_free.argtypes = [C.c_void_p]
         self.p16 = P2Params()
         self.p24 = P2Params()
-        L.or_p2_default(C.byref(self.p16), C.byref(self.p24))
+        L.or_p2_from_rng(p2_seed, p2_mat, C.byref(self.p16), C.byref(self.p24))
 
     # ---- primitives -------------------------------------------------------
+    def rng_fields(self, seed: int, count: int) -> np.ndarray:
+        """rng.random::<KoalaBear>() drawn `count` times from SmallRng::seed_from_u64(seed)."""
+        out = np.empty(count, dtype=np.uint32)
+        self.lib.or_rng_fields(seed, out, count)
+        return out
+
     def permute(self, state: np.ndarray) -> np.ndarray:
         s = np.ascontiguousarray(state, dtype=np.uint32).copy()
         self.lib.or_p2_permute(C.byref(self.p16 if len(s) == 16 else self.p24), s)
@@ -247,6 +262,7 @@ class Oracle:
         out = C.POINTER(C.c_uint32)()
         words = C.c_size_t()
         cp = np.zeros(4, dtype=np.uint32)
+        self.lib.or_p2_select(C.byref(self.p16), C.byref(self.p24))
         rc = self.lib.or_whir_prove(C.byref(params), n, poly, None if pts is None else pts.ctypes.data, npts,
                                     C.byref(out), C.byref(words), cp)
         if rc:
@@ -261,6 +277,7 @@ class Oracle:
         evs = None if npts == 0 else np.ascontiguousarray(evals, dtype=np.uint32)
         cp = np.zeros(4, dtype=np.uint32)
         proof = np.ascontiguousarray(proof, dtype=np.uint32)
+        self.lib.or_p2_select(C.byref(self.p16), C.byref(self.p24))
         rc = self.lib.or_whir_verify(C.byref(params), n, None if pts is None else pts.ctypes.data,
                                      None if evs is None else evs.ctypes.data, npts, proof, len(proof), cp)
         return rc, cp

@@ -1,7 +1,9 @@
 // Host build of the device Poseidon2 header (poseidon2.cuh) checking the
 // specialised forms the kernels use against the plain permutation, on the
 // same templates the GPU compiles (only the S-box's product method differs
-// between host and device):
+// between host and device), for both external blocks (MAT 0: the circulant
+// (2, 3, 1, 1); MAT 1: the paper's M4):
+//   - m4<MAT> and m4_row3<MAT> against the block's matrix entries;
 //   - grind_word7<slot> (folded initial layer, output word 7 only) for every
 //     witness position 0..7;
 //   - permute_sponge (zero-capacity first layer, digest-only last layer) for
@@ -53,7 +55,25 @@ bool fail(const char* what, int a, int b) {
   return false;
 }
 
-template <int SLOT>
+template <int MAT>
+bool check_m4() {
+  for (int t = 0; t < 400; t++) {
+    uint32_t x[4];
+    for (int i = 0; i < 4; i++) x[i] = pick(t < 6 ? t : (t < 30 ? (t + i) % 6 : 6));
+    uint32_t y[4] = {x[0], x[1], x[2], x[3]};
+    p2::m4<MAT>(y[0], y[1], y[2], y[3]);
+    for (int i = 0; i < 4; i++) {
+      uint64_t want = 0;
+      for (int j = 0; j < 4; j++) want += (uint64_t)p2::m4_entry<MAT>(i, j) * x[j];
+      if (y[i] != want % kb::P) return fail("m4", MAT, i);
+    }
+    if (p2::m4_row3<MAT>(x[0], x[1], x[2], x[3]) != y[3]) return fail("m4_row3", MAT, t);
+    g_checks++;
+  }
+  return true;
+}
+
+template <int SLOT, int MAT>
 bool check_grind(const p2::P2Consts& k) {
   for (int t = 0; t < 40; t++) {
     uint32_t st[16];
@@ -62,25 +82,25 @@ bool check_grind(const p2::P2Consts& k) {
     uint32_t full[16];
     memcpy(full, st, sizeof(full));
     full[SLOT] = w;
-    p2::permute_canonical<16, p2::RP16>(full, k);
+    p2::permute_canonical<16, p2::RP16, MAT>(full, k);
     uint32_t cp[16];
     memcpy(cp, st, sizeof(cp));
     cp[SLOT] = 0u;
-    p2::grind_fold(cp, k);
-    if (p2::grind_word7<SLOT>(w, cp, k) != full[7]) return fail("grind_word7", SLOT, t);
+    p2::grind_fold<MAT>(cp, k);
+    if (p2::grind_word7<SLOT, MAT>(w, cp, k) != full[7]) return fail("grind_word7", SLOT + 8 * MAT, t);
     g_checks++;
   }
   return true;
 }
 
-template <int T, int RP, int RATE, bool FIRST, bool LAST>
+template <int T, int RP, int RATE, bool FIRST, bool LAST, int MAT>
 bool check_sponge(const p2::P2Consts& k) {
   for (int t = 0; t < 40; t++) {
     uint32_t a[T], b[T];
     for (int i = 0; i < T; i++) a[i] = (FIRST && i >= RATE) ? 0u : pick(t == 0 ? i % 6 : 6);
     memcpy(b, a, sizeof(a));
-    p2::permute_canonical<T, RP>(a, k);
-    p2::permute_sponge<T, RP, RATE, FIRST, LAST>(b, k);
+    p2::permute_canonical<T, RP, MAT>(a, k);
+    p2::permute_sponge<T, RP, RATE, FIRST, LAST, MAT>(b, k);
     const int n = LAST ? 8 : T;
     for (int i = 0; i < n; i++)
       if (a[i] != b[i]) return fail("permute_sponge", T * 10 + (FIRST ? 1 : 0) + (LAST ? 2 : 0), i);
@@ -124,13 +144,24 @@ bool check_sum() {
 }
 }  // namespace
 
+template <int MAT>
+bool check_forms(const p2::P2Consts& k16, const p2::P2Consts& k24) {
+  bool ok = check_m4<MAT>();
+  ok = ok && check_grind<0, MAT>(k16) && check_grind<1, MAT>(k16) && check_grind<2, MAT>(k16) &&
+       check_grind<3, MAT>(k16) && check_grind<4, MAT>(k16) && check_grind<5, MAT>(k16) &&
+       check_grind<6, MAT>(k16) && check_grind<7, MAT>(k16);
+  ok = ok && check_sponge<24, p2::RP24, 16, true, true, MAT>(k24) &&
+       check_sponge<24, p2::RP24, 16, true, false, MAT>(k24) &&
+       check_sponge<24, p2::RP24, 16, false, true, MAT>(k24) &&
+       check_sponge<24, p2::RP24, 16, false, false, MAT>(k24);
+  ok = ok && check_sponge<16, p2::RP16, 8, true, true, MAT>(k16) &&
+       check_sponge<16, p2::RP16, 8, false, true, MAT>(k16);
+  return ok;
+}
+
 int main() {
   const p2::P2Consts k16 = consts(16), k24 = consts(24);
-  bool ok = check_grind<0>(k16) && check_grind<1>(k16) && check_grind<2>(k16) && check_grind<3>(k16) &&
-            check_grind<4>(k16) && check_grind<5>(k16) && check_grind<6>(k16) && check_grind<7>(k16);
-  ok = ok && check_sponge<24, p2::RP24, 16, true, true>(k24) && check_sponge<24, p2::RP24, 16, true, false>(k24) &&
-       check_sponge<24, p2::RP24, 16, false, true>(k24) && check_sponge<24, p2::RP24, 16, false, false>(k24);
-  ok = ok && check_sponge<16, p2::RP16, 8, true, true>(k16) && check_sponge<16, p2::RP16, 8, false, true>(k16);
+  bool ok = check_forms<p2::kMatMds>(k16, k24) && check_forms<p2::kMatHl>(k16, k24);
   ok = ok && check_diag() && check_sum();
   if (!ok) return 1;
   printf("ok %ld\n", g_checks);

@@ -29,7 +29,10 @@ def _rank_main(rank, world, port, out):
     local = 10.0 + 5.0 * rank  # rank 1 is slower
     mx = bench.reduce_over_ranks(local, dist, "cpu")
     step_ms, value = bench.job_value(mx, 5, world)
-    poly, point = bench.inputs(rank, 10)
+    import __graft_entry__
+
+    pkg = __graft_entry__.load_package()
+    poly, point = bench.inputs(pkg.rng_koalabear, rank, 10)
     polys = [None] * world
     dist.all_gather_object(polys, poly[:8].tolist())
     out[rank] = (mx, step_ms, value, polys)

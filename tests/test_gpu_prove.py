@@ -61,7 +61,10 @@ def test_e2e_hash_and_separator_choices(pkg, gpu_ctx, oracle, leaf, dig):
 
 def test_e2e_cli_default_shape_n18(pkg, gpu_ctx, oracle):
     """n = 18, k = 4, rate 1/2, 90-bit CapacityBound, pow_bits 16, rs reduction
-    3 (the reference CLI defaults, src/bin/main.rs:41-67), one constraint."""
+    3, one constraint: the CLI's security level, rate, pow_bits and rs
+    reduction defaults (src/bin/main.rs:41-67; its defaults for the variable
+    count and folding factor are 25 and 5), at a size the oracle proves in
+    about a second."""
     run_both(pkg, gpu_ctx, oracle, 18, 90, 16, 4, 4, 2, 1, 3, 0, 32, 1, 18)
 
 
@@ -120,8 +123,25 @@ def test_pipelined_upload_matches_device_resident(pkg, gpu_ctx, n, k, rate):
 def test_e2e_headline_n24(pkg, gpu_ctx, oracle):
     """The reference's benchmark configuration (benches/whir.rs:34-120): n = 24,
     k = 4, rate 1/2, 100-bit CapacityBound, pow_bits 16, rs reduction 3, one
-    constraint, Poseidon2-24 leaves, DIGEST_ELEMS 32."""
-    run_both(pkg, gpu_ctx, oracle, 24, 100, 16, 4, 4, 2, 1, 3, 0, 32, 1, 24)
+    constraint, Poseidon2-24 leaves, DIGEST_ELEMS 32, with the polynomial and
+    point drawn as the benchmark draws them (SmallRng::seed_from_u64(0))."""
+    n = 24
+    draw = pkg.rng_koalabear(0, (1 << n) + 4 * n)
+    poly, pts = draw[: 1 << n], draw[1 << n:]
+    params = pkg.ProtocolParameters(100, 16, pkg.FoldingFactor.constant(4), pkg.SecurityAssumption.CapacityBound, 1, 3,
+                                    "poseidon2_24", 32)
+    proof, cp, evals = pkg.commit_and_prove(gpu_ctx, params, n, poly, pts)
+    oprm = make_params(100, 16, 4, None, 2, 1, 3, 0, 32)
+    ref, ref_cp = oracle.prove(oprm, n, poly, pts)
+    assert np.array_equal(proof, ref) and np.array_equal(cp, ref_cp)
+    rc, vcp = oracle.verify(oprm, n, pts, evals, proof)
+    assert rc == 0 and np.array_equal(vcp, cp)
+
+
+def test_e2e_n26_four_constraints_word_identical(pkg, gpu_ctx, oracle):
+    """n = 26 with four constraints (the larger full-prove configuration),
+    rs reduction 3: proof words and checkpoint equal the oracle's."""
+    run_both(pkg, gpu_ctx, oracle, 26, 100, 16, 4, 4, 2, 1, 3, 0, 32, 4, 2626)
 
 
 def test_e2e_n26_verified(pkg, gpu_ctx, oracle):

@@ -55,6 +55,22 @@ def test_noalloc_matches_existing_entry_point_twice(pkg, gpu_ctx):
         assert np.array_equal(got[4:], c2)
 
 
+@pytest.mark.parametrize("max_blocks", [1, 7, 100, 2048])
+def test_capped_block_count_matches(pkg, gpu_ctx, max_blocks):
+    """The allocation-free entry point caps its reduction at 2048 blocks, above
+    the grid a B200 picks (8 CTAs per SM); the capped path, with caps below
+    the natural grid, gives the same coefficients as the uncapped one."""
+    rng = np.random.default_rng(900 + max_blocks)
+    for n in (19, 9):
+        f = rng.integers(0, P, 4 << n, dtype=np.uint64).astype(np.uint32)
+        w = rng.integers(0, P, 4 << n, dtype=np.uint64).astype(np.uint32)
+        d_f = pkg.DeviceArray.from_host(gpu_ctx, f)
+        d_w = pkg.DeviceArray.from_host(gpu_ctx, w)
+        want = pkg.sumcheck_coeffs(gpu_ctx, d_f, d_w, n)
+        got = pkg.sumcheck_coeffs_shaped(gpu_ctx, d_f, d_w, n, max_blocks)
+        assert np.array_equal(got[0], want[0]) and np.array_equal(got[1], want[1])
+
+
 def test_noalloc_rejects_sizes_beyond_the_maximum(pkg, gpu_ctx):
     fn = _entry(pkg)
     d = pkg.DeviceArray(gpu_ctx, 64)

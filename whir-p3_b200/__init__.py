@@ -38,9 +38,14 @@ class WhirError(RuntimeError):
         self.code = code
 
 
+# external 4x4 block of the Poseidon2 external layer
+P2_MDS_MAT4 = 0  # circ(2, 3, 1, 1): Plonky3's Monty-31 MDSMat4, the KoalaBear permutation
+P2_HL_MAT4 = 1   # the Poseidon2 paper's M4 (Plonky3's HLMDSMat4)
+
+
 class Poseidon2Params(C.Structure):
     _fields_ = [("width", C.c_uint32), ("rounds_f", C.c_uint32), ("rounds_p", C.c_uint32),
-                ("ext_rc", C.c_uint32 * (8 * 24)), ("int_rc", C.c_uint32 * 32), ("diag", C.c_uint32 * 24)]
+                ("external_matrix", C.c_uint32), ("ext_rc", C.c_uint32 * (8 * 24)), ("int_rc", C.c_uint32 * 32), ("diag", C.c_uint32 * 24)]
 
 
 class _Params(C.Structure):
@@ -88,6 +93,9 @@ _SIGS = {
     "whir_last_error": (C.c_char_p, []),
     "whir_kernel_launches": (C.c_uint64, []),
     "whir_poseidon2_default_params": (C.c_int, [C.POINTER(Poseidon2Params), C.POINTER(Poseidon2Params)]),
+    "whir_poseidon2_params_from_rng": (C.c_int, [C.c_uint64, C.c_uint32, C.POINTER(Poseidon2Params),
+                                                 C.POINTER(Poseidon2Params)]),
+    "whir_rng_koalabear": (C.c_int, [C.c_uint64, _vp, C.c_size_t]),
     "whir_ctx_create": (C.c_int, [_i32, C.POINTER(Poseidon2Params), C.POINTER(Poseidon2Params), C.POINTER(_vp)]),
     "whir_ctx_destroy": (C.c_int, [_vp]),
     "whir_ctx_set_stream": (C.c_int, [_vp, _vp]),
@@ -144,6 +152,7 @@ _SIGS = {
     "whir_dft_batch_plan": (C.c_int, [_vp, _vp, _i32, _i32, _i32, _i32, _vp, _vp]),
     "whir_merkle_commit_shaped": (C.c_int, [_vp, _vp, _i32, _i32, _i32, _vp, _vp, _u32]),
     "whir_fold_ext_shaped": (C.c_int, [_vp, _vp, _i32, _u32, _vp]),
+    "whir_sumcheck_coeffs_shaped": (C.c_int, [_vp, _vp, _vp, _i32, _i32, _u32, _u32]),
 }
 
 _lib = None
@@ -315,6 +324,23 @@ def default_poseidon2() -> tuple[Poseidon2Params, Poseidon2Params]:
     a, b = Poseidon2Params(), Poseidon2Params()
     _check(lib().whir_poseidon2_default_params(C.byref(a), C.byref(b)))
     return a, b
+
+
+def poseidon2_from_rng(seed: int, external_matrix: int = P2_MDS_MAT4) -> tuple[Poseidon2Params, Poseidon2Params]:
+    """Poseidon2KoalaBear<16>::new_from_rng_128 then <24>::new_from_rng_128 on
+    one SmallRng::seed_from_u64(seed) stream (src/bin/main.rs:100-102)."""
+    a, b = Poseidon2Params(), Poseidon2Params()
+    _check(lib().whir_poseidon2_params_from_rng(seed, external_matrix, C.byref(a), C.byref(b)))
+    return a, b
+
+
+def rng_koalabear(seed: int, count: int) -> np.ndarray:
+    """The first `count` KoalaBear elements (canonical uint32) that
+    `rng.random::<F>()` draws from SmallRng::seed_from_u64(seed)
+    (benches/whir.rs:92-100 draws the polynomial, then the point, this way)."""
+    out = np.empty(count, dtype=np.uint32)
+    _check(lib().whir_rng_koalabear(seed, out.ctypes.data, count))
+    return out
 
 
 class Context:
@@ -592,6 +618,15 @@ def sumcheck_coeffs(ctx: Context, f: DeviceArray, w: DeviceArray, n: int) -> tup
     c0 = np.zeros(4, dtype=np.uint32)
     c2 = np.zeros(4, dtype=np.uint32)
     _check(lib().whir_sumcheck_coeffs(ctx.handle, f.ptr, w.ptr, n, c0, c2))
+    return c0, c2
+
+
+def sumcheck_coeffs_shaped(ctx: Context, f: DeviceArray, w: DeviceArray, n: int,
+                           max_blocks: int) -> tuple[np.ndarray, np.ndarray]:
+    """sumcheck_coeffs with the reduction's block count capped at max_blocks."""
+    c0 = np.zeros(4, dtype=np.uint32)
+    c2 = np.zeros(4, dtype=np.uint32)
+    _check(lib().whir_sumcheck_coeffs_shaped(ctx.handle, f.ptr, w.ptr, n, max_blocks, c0, c2))
     return c0, c2
 
 

@@ -34,15 +34,23 @@ def build(force: bool = False, verbose: bool = False) -> pathlib.Path:
         return LIB
     LIB_DIR.mkdir(exist_ok=True)
     nvcc = os.environ.get("NVCC", "nvcc")
-    objs = []
+    cmds, objs = [], []
     for src in sources():
         obj = LIB_DIR / (src.stem + ".o")
-        cmd = [nvcc, *ARCH, "-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-dc" if False else "-c",
-               "-I", str(PKG.parent / "include"), str(src), "-o", str(obj)]
+        cmds.append([nvcc, *ARCH, "-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-c",
+                     "-I", str(PKG.parent / "include"), str(src), "-o", str(obj)])
+        objs.append(str(obj))
+    # one nvcc per translation unit, in parallel
+    import concurrent.futures
+
+    def run(cmd):
         if verbose:
             print(" ".join(cmd), file=sys.stderr)
         subprocess.run(cmd, check=True)
-        objs.append(str(obj))
+
+    with concurrent.futures.ThreadPoolExecutor(max_workers=max(1, min(len(cmds), os.cpu_count() or 1))) as ex:
+        for f in [ex.submit(run, c) for c in cmds]:
+            f.result()
     cmd = [nvcc, *ARCH, "-shared", "-o", str(LIB), *objs, "-lcudart"]
     subprocess.run(cmd, check=True)
     for o in objs:

@@ -96,7 +96,8 @@ void run_job(whir_ctx* ctx, whir_job* j) {
 
 void worker(whir_batch* b, int idx) {
   whir_ctx* ctx = b->ctxs[idx];
-  cudaSetDevice(b->device);
+  // a worker whose thread cannot select the device fails every job it takes
+  const cudaError_t dev_err = cudaSetDevice(b->device);
   for (;;) {
     whir_job* j = nullptr;
     {
@@ -110,7 +111,14 @@ void worker(whir_batch* b, int idx) {
       b->queue.pop_front();
       b->in_use += j->footprint_bytes;
     }
-    run_job(ctx, j);
+    if (dev_err == cudaSuccess) {
+      run_job(ctx, j);
+    } else {
+      j->t_start_ms = j->t_done_ms = now_ms();
+      j->status = WHIR_ERR_CUDA;
+      snprintf(j->error, sizeof(j->error), "cudaSetDevice failed on the worker thread: %s",
+               cudaGetErrorString(dev_err));
+    }
     {
       std::lock_guard<std::mutex> lk(b->mu);
       b->in_use -= j->footprint_bytes;

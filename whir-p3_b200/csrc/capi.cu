@@ -346,6 +346,20 @@ int whir_poseidon2_default_params(whir_poseidon2_params* p16, whir_poseidon2_par
   return WHIR_OK;
 }
 
+int whir_poseidon2_params_from_rng(uint64_t seed, uint32_t external_matrix, whir_poseidon2_params* p16,
+                                   whir_poseidon2_params* p24) {
+  WH_CHECK(external_matrix == WHIR_P2_MDS_MAT4 || external_matrix == WHIR_P2_HL_MAT4, "unknown external matrix");
+  wh::params_from_rng(seed, external_matrix, p16, p24);
+  return WHIR_OK;
+}
+
+int whir_rng_koalabear(uint64_t seed, uint32_t* out, size_t count) {
+  WH_CHECK(out || count == 0, "null output");
+  wh::SmallRng g(seed);
+  for (size_t i = 0; i < count; i++) out[i] = g.field();
+  return WHIR_OK;
+}
+
 int whir_ctx_create(int32_t device, const whir_poseidon2_params* p16, const whir_poseidon2_params* p24,
                     whir_ctx** out) {
   if (!out) return wh::set_error("null output"), WHIR_ERR_INVALID;
@@ -358,6 +372,8 @@ int whir_ctx_create(int32_t device, const whir_poseidon2_params* p16, const whir
     if (!p24) p24 = &d24;
     WH_TRY(wh::validate_params(*p16, 16));
     WH_TRY(wh::validate_params(*p24, 24));
+    WH_CHECK(p16->external_matrix == p24->external_matrix,
+             "the width-16 and width-24 permutations must use the same external matrix");
     whir_ctx* c = new whir_ctx();
     c->device = -1;
     c->p16_params = *p16;
@@ -381,6 +397,8 @@ int whir_ctx_create(int32_t device, const whir_poseidon2_params* p16, const whir
   if (!p24) p24 = &d24;
   WH_TRY(wh::validate_params(*p16, 16));
   WH_TRY(wh::validate_params(*p24, 24));
+  WH_CHECK(p16->external_matrix == p24->external_matrix,
+           "the width-16 and width-24 permutations must use the same external matrix");
   whir_ctx* c = new whir_ctx();
   c->device = device;
   c->p16_params = *p16;
@@ -528,7 +546,7 @@ int whir_poseidon2_permute(const whir_ctx* ctx, uint32_t* state, int32_t width) 
   } else {
     uint32_t s[24];
     for (int i = 0; i < 24; i++) s[i] = state[i];
-    p2::permute_canonical<24, p2::RP24>(s, ctx->p24);
+    p2::permute_canonical_rt<24, p2::RP24>(s, ctx->p24);
     for (int i = 0; i < 24; i++) state[i] = s[i];
   }
   return WHIR_OK;
@@ -775,6 +793,22 @@ int whir_sumcheck_coeffs(whir_ctx* ctx, const uint32_t* d_f, const uint32_t* d_w
 }
 
 
+
+int whir_sumcheck_coeffs_shaped(whir_ctx* ctx, const uint32_t* d_f, const uint32_t* d_w, int32_t n,
+                                int32_t max_blocks, uint32_t* c0, uint32_t* c2) {
+  WH_TRY(check_gpu(ctx));
+  WH_CHECK(d_f && d_w && c0 && c2 && n >= 1 && n <= 30, "bad sumcheck arguments");
+  // the partial sums take 2 * blocks of the context's 8192-entry buffer
+  WH_CHECK(max_blocks >= 1 && max_blocks <= 4096, "max_blocks must be in [1, 4096]");
+  WH_TRY_CUDA(wk::sumcheck_coeffs_capped(reinterpret_cast<const ef*>(d_f), reinterpret_cast<const ef*>(d_w),
+                                         (size_t)1 << (n - 1), ctx->d_partials, (unsigned)max_blocks,
+                                         ctx->d_small, ctx->stream));
+  ef r[2];
+  WH_TRY(wh::fetch(ctx, r, ctx->d_small, sizeof(r)));
+  store_ef_canon(c0, r[0]);
+  store_ef_canon(c2, r[1]);
+  return WHIR_OK;
+}
 
 int whir_combine_eq(whir_ctx* ctx, uint32_t* d_w, int32_t n, const uint32_t* points, int32_t m,
                     const uint32_t* gamma_pows) {

@@ -40,6 +40,18 @@ void set_error(const std::string& msg);
 
 p2::P2Consts to_consts(const whir_poseidon2_params& p);  // canonical -> Montgomery
 void default_params(whir_poseidon2_params* p16, whir_poseidon2_params* p24);
+void params_from_rng(uint64_t seed, uint32_t mat, whir_poseidon2_params* p16, whir_poseidon2_params* p24);
+
+// rand::rngs::SmallRng (xoshiro256++ seeded through SplitMix64) and
+// KoalaBear's StandardUniform sampler on it; field() returns canonical values.
+struct SmallRng {
+  uint64_t s[4];
+  explicit SmallRng(uint64_t seed);
+  static uint64_t rotl(uint64_t x, int k) { return (x << k) | (x >> (64 - k)); }
+  uint64_t next_u64();
+  uint32_t next_u32() { return (uint32_t)(next_u64() >> 32); }
+  uint32_t field();
+};
 int validate_params(const whir_poseidon2_params& p, uint32_t width);
 
 // WhirConfig::new restated (src/whir/parameters.rs:81-234); returns WHIR_OK or an error
@@ -58,6 +70,7 @@ struct HostP16 {
   uint32_t ext_rc[8 * 16];
   uint32_t int_rc[20];
   uint32_t diag[16];
+  uint32_t mat;  // WHIR_P2_MDS_MAT4 or WHIR_P2_HL_MAT4
 };
 HostP16 host_consts16(const whir_poseidon2_params& p);
 void host_permute16(uint32_t* state_canonical, const HostP16& k);

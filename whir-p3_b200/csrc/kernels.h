@@ -16,6 +16,15 @@ namespace wk {
 unsigned long long launches();
 void count_launch();
 
+// SM count of the current device (read once per device, thread-safe)
+int sm_count();
+
+#define LAUNCH_DONE()              \
+  do {                             \
+    count_launch();                \
+    return cudaGetLastError();     \
+  } while (0)
+
 // small device-side tables owned by the caller
 struct DftTables {
   const uint32_t* tw_stage;  // omega_{2^12}^k, k < 2^11 (Montgomery)
@@ -32,6 +41,15 @@ constexpr int kMailWords = 512;
 // copy `words` (<= kMailWords) device words into the mailbox, then (after a
 // system-wide fence) write `seq` to the flag
 cudaError_t publish(const uint32_t* src, int words, uint32_t* mail, uint32_t seq, cudaStream_t st);
+
+#ifdef __CUDACC__
+// Mailbox write by one thread: payload, a system-wide fence, then the flag.
+__device__ __forceinline__ void mail_post(volatile uint32_t* mail, const uint32_t* src, int words, uint32_t seq) {
+  for (int i = 0; i < words; i++) mail[i] = src[i];
+  __threadfence_system();
+  mail[kMailWords] = seq;
+}
+#endif
 
 cudaError_t encode(uint32_t* p, size_t n, cudaStream_t st);
 cudaError_t decode(uint32_t* p, size_t n, cudaStream_t st);
@@ -77,6 +95,18 @@ struct Shape {
   int variant;
 };
 
+// CTAs for `work` items at sh.threads per CTA, capped at sh.per_sm CTAs per SM
+// (per_sm 0: no cap)
+inline unsigned grid_shape(size_t work, Shape sh) {
+  size_t b = (work + sh.threads - 1) / sh.threads;
+  if (sh.per_sm > 0) {
+    const size_t cap = (size_t)sm_count() * sh.per_sm;
+    if (b > cap) b = cap;
+  }
+  if (b < 1) b = 1;
+  return (unsigned)b;
+}
+
 // Merkle tree: digests has (2h-1)*8 words, leaves first. leaf_hash 0: sponge
 // over Poseidon2-24 rate 16; 1: Poseidon2-16 rate 8. Compression: Poseidon2-16.
 // `counter` (device, one word, 0 before the first launch, left at 0) joins the
@@ -117,6 +147,20 @@ cudaError_t grind_reset(uint32_t* result, uint32_t* counter, uint32_t* done, cud
 cudaError_t grind(const uint32_t* state, const uint32_t* in, int in_len, int bits, uint64_t limit,
                   uint32_t* result, uint32_t* counter, uint32_t* done, uint32_t* mail, uint32_t seq,
                   const p2::P2Consts& p16, cudaStream_t st);
+
+// The Poseidon2 launchers above for one external block MAT (p2::kMatMds or
+// p2::kMatHl), each form built in its own translation unit; merkle_leaves,
+// merkle_upper and grind pick the form of their constants (P2Consts::mat).
+template <int MAT>
+cudaError_t merkle_leaves_m(const uint32_t* rows, int log_h, int row_words, int leaf_hash, uint32_t* digests,
+                            const p2::P2Consts& p16, const p2::P2Consts& p24, Shape leaf, cudaStream_t st);
+template <int MAT>
+cudaError_t merkle_upper_m(int log_h, uint32_t* digests, const p2::P2Consts& p16, Shape node, unsigned* counter,
+                           uint32_t* mail, uint32_t seq, int* posted, cudaStream_t st);
+template <int MAT>
+cudaError_t grind_m(const uint32_t* state, const uint32_t* in, int in_len, int bits, uint64_t limit,
+                    uint32_t* result, uint32_t* counter, uint32_t* done, uint32_t* mail, uint32_t seq,
+                    const p2::P2Consts& p16, cudaStream_t st);
 
 // eq table of `h` coordinates scaled by `scale`: out[x] = scale * prod eq(z_j, bit_j(x)), MSB <-> z[0].
 struct EqPoint {

@@ -1,0 +1,684 @@
+// Merkle tree and proof-of-work kernels, templated on the Poseidon2 external
+// block MAT (p2::kMatMds or p2::kMatHl). Each form is instantiated in its own
+// translation unit (merkle_mds.cu, merkle_hl.cu); kernels.cu dispatches on the
+// context's choice. The kernels have internal linkage in each unit; only the
+// launchers at the end are shared.
+#pragma once
+#include "kernels.h"
+
+namespace wk {
+namespace {
+
+using kb::ef;
+using p2::P2Consts;
+
+// ---------------------------------------------------------------------------
+// Merkle tree (MerkleTreeMmcs::commit_matrix, src/whir/committer/writer.rs:89
+// and src/whir/prover/mod.rs:182-184): one thread hashes one row with the
+// PaddingFreeSponge (overwrite mode), then the CTA compresses its subtree
+// level by level in shared memory with TruncatedPermutation<P16>.
+// ---------------------------------------------------------------------------
+
+constexpr int MERKLE_CTA = 128;
+
+// TruncatedPermutation<P16, 2, 8, 16> on Montgomery-form digests: the
+// permutation runs on canonical values, and only the kept half of the output
+// is converted back.
+template <int MAT>
+__device__ __forceinline__ void compress_mont(uint32_t (&s)[16], const P2Consts& k) {
+#pragma unroll
+  for (int i = 0; i < 16; i++) s[i] = kb::from_mont(s[i]);
+  p2::permute_canonical<16, p2::RP16, MAT>(s, k);
+#pragma unroll
+  for (int i = 0; i < 8; i++) s[i] = kb::to_mont(s[i]);
+}
+
+template <int MAT>
+__device__ __forceinline__ void compress16(const uint32_t* l, const uint32_t* r, uint32_t* out,
+                                           const P2Consts& k) {
+  uint32_t s[16];
+#pragma unroll
+  for (int i = 0; i < 8; i++) {
+    s[i] = l[i];
+    s[i + 8] = r[i];
+  }
+  compress_mont<MAT>(s, k);
+#pragma unroll
+  for (int i = 0; i < 8; i++) out[i] = s[i];
+}
+
+// Compress `levels` levels above the digests in sh[0 .. count*8), writing each
+// level to global; `node0` is this CTA's first node index at the input level.
+template <int MAT>
+__device__ __forceinline__ void subtree_up(uint32_t* sh, int count, int levels, size_t node0, uint32_t* level_base,
+                                           size_t level_size, const P2Consts& comp) {
+  size_t off = 0;
+  size_t lsz = level_size;
+  for (int l = 1; l <= levels; l++) {
+    const int act = count >> l;
+    uint32_t d[8];
+    const int t = threadIdx.x;
+    if (t < act) compress16<MAT>(sh + 2 * t * 8, sh + (2 * t + 1) * 8, d, comp);
+    __syncthreads();
+    off += lsz;
+    lsz >>= 1;
+    if (t < act) {
+      const size_t node = (node0 >> l) + t;
+#pragma unroll
+      for (int i = 0; i < 8; i++) {
+        sh[t * 8 + i] = d[i];
+        level_base[(off + node) * 8 + i] = d[i];
+      }
+    }
+    __syncthreads();
+  }
+}
+
+template <int T, int RP, int RATE, int MAT>
+__global__ void __launch_bounds__(MERKLE_CTA) k_merkle_leaves(const uint32_t* __restrict__ rows, int row_words,
+                                                               size_t h, int levels, uint32_t* __restrict__ digests,
+                                                               const __grid_constant__ P2Consts leaf,
+                                                               const __grid_constant__ P2Consts comp) {
+  __shared__ uint32_t sh[MERKLE_CTA * 8];
+  const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < h) {
+    uint32_t s[T];
+#pragma unroll
+    for (int k = 0; k < T; k++) s[k] = 0u;
+    const uint32_t* row = rows + i * (size_t)row_words;
+    for (int pos = 0; pos < row_words; pos += RATE) {
+      const int take = row_words - pos < RATE ? row_words - pos : RATE;
+      if (take == RATE && (row_words & 3) == 0) {
+#pragma unroll
+        for (int k = 0; k < RATE; k += 4) {
+          uint4 v = __ldg(reinterpret_cast<const uint4*>(row + pos + k));
+          s[k] = kb::from_mont(v.x);
+          s[k + 1] = kb::from_mont(v.y);
+          s[k + 2] = kb::from_mont(v.z);
+          s[k + 3] = kb::from_mont(v.w);
+        }
+      } else {
+#pragma unroll
+        for (int k = 0; k < RATE; k++)
+          if (k < take) s[k] = kb::from_mont(row[pos + k]);
+      }
+      const bool first = pos == 0, last = pos + RATE >= row_words;
+      if (first && last) p2::permute_sponge<T, RP, RATE, true, true, MAT>(s, leaf);
+      else if (first) p2::permute_sponge<T, RP, RATE, true, false, MAT>(s, leaf);
+      else if (last) p2::permute_sponge<T, RP, RATE, false, true, MAT>(s, leaf);
+      else p2::permute_sponge<T, RP, RATE, false, false, MAT>(s, leaf);
+    }
+#pragma unroll
+    for (int k = 0; k < 8; k++) {
+      s[k] = kb::to_mont(s[k]);
+      sh[threadIdx.x * 8 + k] = s[k];
+      digests[i * 8 + k] = s[k];
+    }
+  }
+  __syncthreads();
+  subtree_up<MAT>(sh, blockDim.x, levels, (size_t)blockIdx.x * blockDim.x, digests, h, comp);
+}
+
+static int ilog2i(size_t v) {
+  int r = -1;
+  while (v) {
+    r++;
+    v >>= 1;
+  }
+  return r;
+}
+
+// Leaf digests only (level 0): one thread per row, full occupancy, no barriers.
+template <int T, int RP, int RATE, int CTA, int MAT>
+__global__ void __launch_bounds__(CTA) k_leaf_digests(const uint32_t* __restrict__ rows, int row_words, size_t h,
+                                                       uint32_t* __restrict__ digests,
+                                                       const __grid_constant__ P2Consts leaf) {
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < h; i += (size_t)gridDim.x * blockDim.x) {
+    uint32_t s[T];
+#pragma unroll
+    for (int k = 0; k < T; k++) s[k] = 0u;
+    const uint32_t* row = rows + i * (size_t)row_words;
+    for (int pos = 0; pos < row_words; pos += RATE) {
+      const int take = row_words - pos < RATE ? row_words - pos : RATE;
+      if (take == RATE && (row_words & 3) == 0) {
+#pragma unroll
+        for (int k = 0; k < RATE; k += 4) {
+          uint4 v = __ldg(reinterpret_cast<const uint4*>(row + pos + k));
+          s[k] = kb::from_mont(v.x);
+          s[k + 1] = kb::from_mont(v.y);
+          s[k + 2] = kb::from_mont(v.z);
+          s[k + 3] = kb::from_mont(v.w);
+        }
+      } else {
+#pragma unroll
+        for (int k = 0; k < RATE; k++)
+          if (k < take) s[k] = kb::from_mont(row[pos + k]);
+      }
+      const bool first = pos == 0, last = pos + RATE >= row_words;
+      if (first && last) p2::permute_sponge<T, RP, RATE, true, true, MAT>(s, leaf);
+      else if (first) p2::permute_sponge<T, RP, RATE, true, false, MAT>(s, leaf);
+      else if (last) p2::permute_sponge<T, RP, RATE, false, true, MAT>(s, leaf);
+      else p2::permute_sponge<T, RP, RATE, false, false, MAT>(s, leaf);
+    }
+#pragma unroll
+    for (int k = 0; k < 8; k++) s[k] = kb::to_mont(s[k]);
+    uint4* d = reinterpret_cast<uint4*>(digests + i * 8);
+    d[0] = make_uint4(s[0], s[1], s[2], s[3]);
+    d[1] = make_uint4(s[4], s[5], s[6], s[7]);
+  }
+}
+
+// Two tree levels per launch: each thread compresses four nodes of level l
+// into two nodes of level l+1 (written out) and their parent at level l+2.
+// SEQ = false keeps both level-(l+1) permutations in flight together (two
+// independent chains per thread, about 78 registers); SEQ = true runs them one
+// after the other (one chain, fewer registers, more resident warps).
+template <int CTA, bool SEQ, int MAT>
+__global__ void __launch_bounds__(CTA) k_merkle_two_levels(uint32_t* __restrict__ digests, size_t in_off,
+                                                            size_t in_count, const __grid_constant__ P2Consts comp) {
+  const size_t out_count = in_count >> 2;
+  const size_t mid_off = in_off + in_count, top_off = mid_off + (in_count >> 1);
+  for (size_t j = (size_t)blockIdx.x * blockDim.x + threadIdx.x; j < out_count; j += (size_t)gridDim.x * blockDim.x) {
+    const uint4* src = reinterpret_cast<const uint4*>(digests + (in_off + 4 * j) * 8);
+    uint4* mid = reinterpret_cast<uint4*>(digests + (mid_off + 2 * j) * 8);
+    uint32_t c[16];  // the parent's inputs, canonical
+    if (SEQ) {
+#pragma unroll
+      for (int h = 0; h < 2; h++) {
+        uint32_t a[16];
+#pragma unroll
+        for (int q = 0; q < 4; q++) {
+          const uint4 v = src[4 * h + q];
+          a[4 * q] = kb::from_mont(v.x);
+          a[4 * q + 1] = kb::from_mont(v.y);
+          a[4 * q + 2] = kb::from_mont(v.z);
+          a[4 * q + 3] = kb::from_mont(v.w);
+        }
+        p2::permute_canonical<16, p2::RP16, MAT>(a, comp);
+#pragma unroll
+        for (int k = 0; k < 8; k++) c[8 * h + k] = a[k];
+        mid[2 * h] = make_uint4(kb::to_mont(a[0]), kb::to_mont(a[1]), kb::to_mont(a[2]), kb::to_mont(a[3]));
+        mid[2 * h + 1] = make_uint4(kb::to_mont(a[4]), kb::to_mont(a[5]), kb::to_mont(a[6]), kb::to_mont(a[7]));
+      }
+    } else {
+      uint32_t a[16], b[16];
+#pragma unroll
+      for (int q = 0; q < 4; q++) {
+        const uint4 va = src[q], vb = src[4 + q];
+        a[4 * q] = va.x; a[4 * q + 1] = va.y; a[4 * q + 2] = va.z; a[4 * q + 3] = va.w;
+        b[4 * q] = vb.x; b[4 * q + 1] = vb.y; b[4 * q + 2] = vb.z; b[4 * q + 3] = vb.w;
+      }
+#pragma unroll
+      for (int k = 0; k < 16; k++) {
+        a[k] = kb::from_mont(a[k]);
+        b[k] = kb::from_mont(b[k]);
+      }
+      p2::permute_canonical<16, p2::RP16, MAT>(a, comp);
+      p2::permute_canonical<16, p2::RP16, MAT>(b, comp);
+      uint32_t am[8], bm[8];
+#pragma unroll
+      for (int k = 0; k < 8; k++) {
+        c[k] = a[k];
+        c[8 + k] = b[k];
+        am[k] = kb::to_mont(a[k]);
+        bm[k] = kb::to_mont(b[k]);
+      }
+      mid[0] = make_uint4(am[0], am[1], am[2], am[3]);
+      mid[1] = make_uint4(am[4], am[5], am[6], am[7]);
+      mid[2] = make_uint4(bm[0], bm[1], bm[2], bm[3]);
+      mid[3] = make_uint4(bm[4], bm[5], bm[6], bm[7]);
+    }
+    p2::permute_canonical<16, p2::RP16, MAT>(c, comp);
+#pragma unroll
+    for (int k = 0; k < 8; k++) c[k] = kb::to_mont(c[k]);
+    uint4* top = reinterpret_cast<uint4*>(digests + (top_off + j) * 8);
+    top[0] = make_uint4(c[0], c[1], c[2], c[3]);
+    top[1] = make_uint4(c[4], c[5], c[6], c[7]);
+  }
+}
+
+// Width-16 Poseidon2 spread over four consecutive lanes (q = lane & 3 holds
+// state words 4q .. 4q+3). The M4 blocks are lane-local; the cross-chunk sums
+// of the external layer and the full sum of the internal layer take two
+// xor-shuffle steps. About four times the per-permutation latency saving of a
+// one-thread permutation, for the narrow top levels of a tree. All 32 lanes
+// of the warp must call it together.
+template <int MAT>
+__device__ __forceinline__ void coop_ext_layer(uint32_t (&x)[4]) {
+  using namespace kb;
+  p2::m4<MAT>(x[0], x[1], x[2], x[3]);
+  uint32_t s[4] = {x[0], x[1], x[2], x[3]};
+#pragma unroll
+  for (int m = 1; m <= 2; m <<= 1)
+#pragma unroll
+    for (int j = 0; j < 4; j++) s[j] = add(s[j], __shfl_xor_sync(0xffffffffu, s[j], m));
+#pragma unroll
+  for (int j = 0; j < 4; j++) x[j] = add(x[j], s[j]);
+}
+
+template <int MAT>
+__device__ __forceinline__ void coop_permute16(uint32_t (&x)[4], int q, const P2Consts& k) {
+  using namespace kb;
+#pragma unroll
+  for (int j = 0; j < 4; j++) x[j] = from_mont(x[j]);
+  coop_ext_layer<MAT>(x);
+#pragma unroll
+  for (int r = 0; r < p2::RF / 2; r++) {
+#pragma unroll
+    for (int j = 0; j < 4; j++) x[j] = p2::cube(add(x[j], k.ext_rc[r * 16 + 4 * q + j]));
+    coop_ext_layer<MAT>(x);
+  }
+  // Internal rounds with word 0 replicated in all four lanes (w0): every lane
+  // computes its S-box, so the result needs no broadcast, and the sum of the
+  // other fifteen words (lane-local, then two shuffles) is independent of it,
+  // which leaves S-box, one addition and the diagonal product of word 0 as
+  // the round's dependent chain.
+  uint32_t w0 = __shfl_sync(0xffffffffu, x[0], (threadIdx.x & 31) & ~3);
+  // fully unrolled: round constants become immediate constant-bank operands,
+  // off the dependent chain of this latency-bound form
+#pragma unroll
+  for (int r = 0; r < p2::RP16; r++) {
+    uint32_t o = add(add(q == 0 ? 0u : x[0], x[1]), add(x[2], x[3]));
+    o = add(o, __shfl_xor_sync(0xffffffffu, o, 1));
+    o = add(o, __shfl_xor_sync(0xffffffffu, o, 2));
+    const uint32_t y0 = p2::cube(add(w0, k.int_rc[r]));
+    const uint32_t s = add(o, y0);
+#pragma unroll
+    for (int j = 0; j < 4; j++) x[j] = add(s, mul_shoup(x[j], k.diag_c[4 * q + j], k.diag_s[4 * q + j]));
+    w0 = p2::diag_axpy(p2::diag_code(16, 0), s, y0);
+    if (q == 0) x[0] = w0;
+  }
+#pragma unroll
+  for (int r = p2::RF / 2; r < p2::RF; r++) {
+#pragma unroll
+    for (int j = 0; j < 4; j++) x[j] = p2::cube(add(x[j], k.ext_rc[r * 16 + 4 * q + j]));
+    coop_ext_layer<MAT>(x);
+  }
+#pragma unroll
+  for (int j = 0; j < 4; j++) x[j] = to_mont(x[j]);
+}
+
+// Compresses `levels` levels above the `cnt` nodes in sh (8 words each), one
+// four-lane group per node pair, writing every new level to global; `base` is
+// the first node's index in its level, `off` and `lsz` the level's offset and
+// size in `digests` (advanced past the levels done).
+template <int MAT>
+__device__ __forceinline__ void coop_levels(uint32_t* sh, int cnt, int levels, size_t base, size_t& off, size_t& lsz,
+                                            uint32_t* __restrict__ digests, const P2Consts& comp) {
+  const int t = threadIdx.x, g = t >> 2, q = t & 3;
+  int cur = cnt;
+  for (int l = 1; l <= levels; l++) {
+    const int act = cur >> 1;
+    const bool on = g < act;
+    const int src = on ? 16 * g + 4 * q : 0;
+    uint32_t x[4];
+#pragma unroll
+    for (int j = 0; j < 4; j++) x[j] = sh[src + j];
+    // a warp holds groups 8w .. 8w+7: warps with none of this level's pairs
+    // skip the permutation (warp-uniform, so its shuffles stay full-warp),
+    // which leaves the upper levels latency-bound rather than issue-bound
+    if ((t >> 5) * 8 < act) coop_permute16<MAT>(x, q, comp);
+    __syncthreads();
+    off += lsz;
+    lsz >>= 1;
+    if (on && q < 2) {
+      const size_t node = (base >> l) + g;
+#pragma unroll
+      for (int j = 0; j < 4; j++) {
+        sh[8 * g + 4 * q + j] = x[j];
+        digests[(off + node) * 8 + 4 * q + j] = x[j];
+      }
+    }
+    __syncthreads();
+    cur = act;
+  }
+}
+
+// Two tree levels with four-lane cooperative permutations: one group of four
+// lanes per output node (its two children, then the node), for the last,
+// narrow two-level step of a tree, where one thread per node leaves the
+// launch latency-bound (two dependent single-thread permutations). Lane q
+// holds words 4q .. 4q+3 of a state; a child's digest ends on lanes 0 and 1.
+// The loop runs per warp so all 32 lanes take every shuffle together.
+template <int CTA, int MAT>
+__global__ void __launch_bounds__(CTA) k_merkle_two_levels_coop(uint32_t* __restrict__ digests, size_t in_off,
+                                                                 size_t in_count, const __grid_constant__ P2Consts comp) {
+  const size_t out_count = in_count >> 2;
+  const size_t mid_off = in_off + in_count, top_off = mid_off + (in_count >> 1);
+  const int lane = threadIdx.x & 31, q = lane & 3;
+  const size_t groups = (size_t)gridDim.x * (CTA / 4);
+  for (size_t base = (size_t)blockIdx.x * (CTA / 4) + (threadIdx.x >> 5) * 8; base < out_count; base += groups) {
+    const size_t jw = base + (lane >> 2);
+    const bool on = jw < out_count;
+    const size_t j = on ? jw : base;
+    uint32_t keep[4];
+#pragma unroll
+    for (int h = 0; h < 2; h++) {
+      // children 4j + 2h and 4j + 2h + 1: 16 consecutive words
+      const uint4 v = *reinterpret_cast<const uint4*>(digests + (in_off + 4 * j + 2 * h) * 8 + 4 * q);
+      uint32_t x[4] = {v.x, v.y, v.z, v.w};
+      coop_permute16<MAT>(x, q, comp);
+      if (on && q < 2)
+        *reinterpret_cast<uint4*>(digests + (mid_off + 2 * j + h) * 8 + 4 * q) = make_uint4(x[0], x[1], x[2], x[3]);
+      // the parent's state: the first child's digest on lanes 0-1, the
+      // second's moved to lanes 2-3
+      if (h == 0) {
+#pragma unroll
+        for (int k = 0; k < 4; k++) keep[k] = x[k];
+      } else {
+#pragma unroll
+        for (int k = 0; k < 4; k++) {
+          const uint32_t from_b = __shfl_sync(0xffffffffu, x[k], (lane & ~3) | (q & 1));
+          if (q >= 2) keep[k] = from_b;
+        }
+      }
+    }
+    coop_permute16<MAT>(keep, q, comp);
+    if (on && q < 2)
+      *reinterpret_cast<uint4*>(digests + (top_off + j) * 8 + 4 * q) = make_uint4(keep[0], keep[1], keep[2], keep[3]);
+  }
+}
+
+// Top of a tree: each CTA compresses up to 256 nodes of one level into a
+// subtree, one four-lane group per node pair, level by level in shared memory.
+// With several CTAs (at most 256), the last one to finish (atomic counter, no
+// waiting) loads their subtree roots and compresses them to the root in the
+// same launch. With `mail` set, the root is posted to that mailbox.
+constexpr int TOP_CTA = 512;
+constexpr int TOP_NODES = 256;
+template <int MAT>
+__global__ void __launch_bounds__(TOP_CTA) k_merkle_top_coop(uint32_t* __restrict__ digests, size_t in_off,
+                                                              size_t in_count, int levels,
+                                                              const __grid_constant__ P2Consts comp,
+                                                              unsigned* __restrict__ counter, uint32_t* mail,
+                                                              uint32_t seq) {
+  __shared__ uint32_t sh[TOP_NODES * 8];
+  __shared__ bool s_last;
+  const int t = threadIdx.x;
+  const size_t base = (size_t)blockIdx.x * TOP_NODES;
+  const int cnt = (int)min((size_t)TOP_NODES, in_count - base);
+  for (int k = t; k < cnt * 8; k += blockDim.x) sh[k] = digests[(in_off + base) * 8 + k];
+  __syncthreads();
+  size_t off = in_off, lsz = in_count;
+  coop_levels<MAT>(sh, cnt, levels, base, off, lsz, digests, comp);
+  if (gridDim.x > 1) {
+    if (t == 0) {
+      __threadfence();
+      s_last = atomicAdd(counter, 1u) == gridDim.x - 1;
+    }
+    __syncthreads();
+    if (!s_last) return;
+    __threadfence();
+    const int n = (int)gridDim.x;  // subtree roots, level `off`
+    for (int k = t; k < n * 8; k += blockDim.x) sh[k] = __ldcg(digests + off * 8 + k);
+    __syncthreads();
+    int top = 0;
+    while ((1 << top) < n) top++;
+    coop_levels<MAT>(sh, n, top, 0, off, lsz, digests, comp);
+    if (t == 0) *counter = 0u;
+  }
+  if (t == 0 && mail) mail_post(mail, sh, 8, seq);
+}
+
+// Top of a tree in one CTA: a level of at most 2 * TOP1_CTA nodes is
+// compressed to the root, one thread (one whole permutation) per node pair,
+// each new level kept in shared memory for the next and written out.
+constexpr int TOP1_CTA = 1024;
+template <int MAT>
+__global__ void __launch_bounds__(TOP1_CTA) k_merkle_top_cta(uint32_t* __restrict__ digests, size_t in_off,
+                                                              int in_count, const __grid_constant__ P2Consts comp,
+                                                              uint32_t* mail, uint32_t seq) {
+  __shared__ uint4 sh[2 * TOP1_CTA];  // node i at sh[2i], sh[2i + 1]
+  const int t = threadIdx.x;
+  size_t off = in_off;
+  int cnt = in_count;
+  for (int level = 0; cnt > 1; level++) {
+    const int act = cnt >> 1;
+    uint32_t x[16];
+    if (t < act) {
+      const uint4* src = level == 0 ? reinterpret_cast<const uint4*>(digests + (off + 2 * (size_t)t) * 8) : sh + 4 * t;
+#pragma unroll
+      for (int q = 0; q < 4; q++) {
+        const uint4 v = src[q];
+        x[4 * q] = v.x;
+        x[4 * q + 1] = v.y;
+        x[4 * q + 2] = v.z;
+        x[4 * q + 3] = v.w;
+      }
+      compress_mont<MAT>(x, comp);
+    }
+    __syncthreads();
+    off += cnt;
+    if (t < act) {
+      const uint4 a = make_uint4(x[0], x[1], x[2], x[3]), b = make_uint4(x[4], x[5], x[6], x[7]);
+      sh[2 * t] = a;
+      sh[2 * t + 1] = b;
+      uint4* dst = reinterpret_cast<uint4*>(digests + (off + t) * 8);
+      dst[0] = a;
+      dst[1] = b;
+    }
+    __syncthreads();
+    cnt = act;
+  }
+  if (threadIdx.x == 0 && mail) mail_post(mail, reinterpret_cast<const uint32_t*>(sh), 8, seq);
+}
+
+// Trees with at least kLevelPairMin leaves are built as: leaf digests, then
+// two levels per launch while a level is wider than the top kernel takes, then
+// the top: either cooperative-permutation subtrees (k_merkle_top_coop, node
+// shape variant 0, from 2^15 nodes) or one CTA (k_merkle_top_cta, variant 1,
+// from 2^11 nodes). Smaller trees hash their leaves with in-CTA subtrees and
+// use the same top kernels above those.
+constexpr size_t kLevelPairMin = (size_t)kMerkleLevelPairMin;
+constexpr size_t kCoopTop = (size_t)1 << 15;
+constexpr size_t kCtaTop = (size_t)2 * TOP1_CTA;
+
+template <int T, int RP, int RATE, int MAT>
+void launch_leaf_digests(const uint32_t* rows, int row_words, size_t h, uint32_t* digests,
+                                const P2Consts& k, Shape sh, cudaStream_t st) {
+  const unsigned blocks = grid_shape(h, sh);
+  if (sh.threads == 128)
+    k_leaf_digests<T, RP, RATE, 128, MAT><<<blocks, 128, 0, st>>>(rows, row_words, h, digests, k);
+  else if (sh.threads == 512)
+    k_leaf_digests<T, RP, RATE, 512, MAT><<<blocks, 512, 0, st>>>(rows, row_words, h, digests, k);
+  else
+    k_leaf_digests<T, RP, RATE, 256, MAT><<<blocks, 256, 0, st>>>(rows, row_words, h, digests, k);
+}
+
+}  // namespace
+
+template <int MAT>
+cudaError_t merkle_leaves_m(const uint32_t* rows, int log_h, int row_words, int leaf_hash, uint32_t* digests,
+                            const P2Consts& p16, const P2Consts& p24, Shape leaf, cudaStream_t st) {
+  const size_t h = (size_t)1 << log_h;
+  if (h >= kLevelPairMin) {
+    if ((leaf.threads != 128 && leaf.threads != 256 && leaf.threads != 512) || leaf.per_sm < 0)
+      return cudaErrorInvalidValue;
+    if (leaf_hash == 0)
+      launch_leaf_digests<24, p2::RP24, 16, MAT>(rows, row_words, h, digests, p24, leaf, st);
+    else
+      launch_leaf_digests<16, p2::RP16, 8, MAT>(rows, row_words, h, digests, p16, leaf, st);
+    LAUNCH_DONE();
+  }
+  const int cta = (int)(h < (size_t)MERKLE_CTA ? h : (size_t)MERKLE_CTA);
+  const int lv = ilog2i((size_t)cta);
+  const unsigned blocks = (unsigned)(h / cta);
+  if (leaf_hash == 0)
+    k_merkle_leaves<24, p2::RP24, 16, MAT><<<blocks, cta, 0, st>>>(rows, row_words, h, lv, digests, p24, p16);
+  else
+    k_merkle_leaves<16, p2::RP16, 8, MAT><<<blocks, cta, 0, st>>>(rows, row_words, h, lv, digests, p16, p16);
+  LAUNCH_DONE();
+}
+
+template <int MAT>
+cudaError_t merkle_upper_m(int log_h, uint32_t* digests, const P2Consts& p16, Shape node, unsigned* counter,
+                           uint32_t* mail, uint32_t seq, int* posted, cudaStream_t st) {
+  if (posted) *posted = 0;
+  const size_t h = (size_t)1 << log_h;
+  size_t off = 0, cnt = h;
+  // variant bit 0: the top kernel (0 cooperative subtrees, 1 one CTA); bit 1:
+  // the two-level kernel with its two permutations one after the other; bit 2:
+  // the last two-level step with four-lane cooperative permutations
+  if (node.variant < 0 || node.variant > 7) return cudaErrorInvalidValue;
+  const bool top_cta = (node.variant & 1) != 0, one_chain = (node.variant & 2) != 0, coop_tail = (node.variant & 4) != 0;
+  const size_t top = top_cta ? kCtaTop : kCoopTop;
+  if (h >= kLevelPairMin) {
+    if ((node.threads != 128 && node.threads != 256) || node.per_sm < 0) return cudaErrorInvalidValue;
+    while (cnt > top) {
+      const size_t out = cnt >> 2;
+      const unsigned blocks = grid_shape(out, node);
+      if (coop_tail && (cnt >> 2) <= top) {
+        const unsigned cblocks = grid_shape(out * 4, node);
+        if (node.threads == 128)
+          k_merkle_two_levels_coop<128, MAT><<<cblocks, 128, 0, st>>>(digests, off, cnt, p16);
+        else
+          k_merkle_two_levels_coop<256, MAT><<<cblocks, 256, 0, st>>>(digests, off, cnt, p16);
+      } else if (node.threads == 128 && one_chain)
+        k_merkle_two_levels<128, true, MAT><<<blocks, 128, 0, st>>>(digests, off, cnt, p16);
+      else if (node.threads == 128)
+        k_merkle_two_levels<128, false, MAT><<<blocks, 128, 0, st>>>(digests, off, cnt, p16);
+      else if (one_chain)
+        k_merkle_two_levels<256, true, MAT><<<blocks, 256, 0, st>>>(digests, off, cnt, p16);
+      else
+        k_merkle_two_levels<256, false, MAT><<<blocks, 256, 0, st>>>(digests, off, cnt, p16);
+      count_launch();
+      cudaError_t e = cudaGetLastError();
+      if (e != cudaSuccess) return e;
+      off += cnt + (cnt >> 1);
+      cnt >>= 2;
+    }
+  } else {
+    const int cta = (int)(h < (size_t)MERKLE_CTA ? h : (size_t)MERKLE_CTA);
+    const int lv = ilog2i((size_t)cta);
+    for (int l = 0; l < lv; l++) {
+      off += cnt;
+      cnt >>= 1;
+    }
+  }
+  if (cnt <= 1) return cudaSuccess;
+  if (top_cta) {
+    k_merkle_top_cta<MAT><<<1, TOP1_CTA, 0, st>>>(digests, off, (int)cnt, p16, mail, seq);
+  } else {
+    // one launch: subtrees of 256 nodes, then the last CTA joins their roots
+    const int c2 = (int)(cnt < (size_t)TOP_NODES ? cnt : (size_t)TOP_NODES);
+    const unsigned blocks2 = (unsigned)(cnt / c2);
+    if (blocks2 > (unsigned)TOP_NODES || (blocks2 > 1 && !counter)) return cudaErrorInvalidValue;
+    k_merkle_top_coop<MAT><<<blocks2, TOP_CTA, 0, st>>>(digests, off, cnt, ilog2i((size_t)c2), p16, counter, mail, seq);
+  }
+  count_launch();
+  const cudaError_t e = cudaGetLastError();
+  if (e == cudaSuccess && posted && mail) *posted = 1;
+  return e;
+}
+
+// ---------------------------------------------------------------------------
+// Proof of work (GrindingChallenger::grind on DuplexChallenger, called at
+// src/whir/proof.rs:188 and src/whir/prover/mod.rs:224,363). Candidates are
+// claimed in increasing chunks; a CTA stops once every remaining chunk starts
+// above the best witness found, so the result is the smallest valid witness.
+// The loop is bounded by `limit` candidates.
+// ---------------------------------------------------------------------------
+
+namespace {
+constexpr int GRIND_CTA = 256;
+
+// Each claim is GRIND_CTA consecutive candidates, one per thread.
+template <int SLOT, int MAT>
+__global__ void __launch_bounds__(GRIND_CTA) k_grind(const __grid_constant__ P2Consts p16, uint4 st0, uint4 st1,
+                                                      uint4 st2, uint4 st3, int bits, uint64_t limit,
+                                                      uint32_t* result, uint32_t* counter, uint32_t* done,
+                                                      uint32_t* mail, uint32_t seq) {
+  __shared__ uint64_t s_start;
+  __shared__ int s_go;
+  const uint32_t mask = (1u << bits) - 1u;
+  const uint32_t cp[16] = {st0.x, st0.y, st0.z, st0.w, st1.x, st1.y, st1.z, st1.w,
+                           st2.x, st2.y, st2.z, st2.w, st3.x, st3.y, st3.z, st3.w};
+  for (;;) {
+    if (threadIdx.x == 0) {
+      const uint64_t start = (uint64_t)atomicAdd(counter, 1u) * GRIND_CTA;
+      s_start = start;
+      s_go = start < limit && start < (uint64_t)*(volatile uint32_t*)result;
+    }
+    __syncthreads();
+    const uint64_t start = s_start;
+    const int go = s_go;
+    __syncthreads();
+    if (!go) {
+      // every atomicMin of this CTA precedes the barriers above; the last CTA
+      // to stop holds the final result, posts it to the mailbox and resets
+      // the search state for the next search (every other CTA has finished
+      // with it), which then needs no initialising launch
+      if (threadIdx.x == 0 && mail) {
+        __threadfence();
+        if (atomicAdd(done, 1u) == gridDim.x - 1) {
+          const uint32_t r = atomicAdd(result, 0u);
+          mail_post(mail, &r, 1, seq);
+          *result = kb::P;
+          *counter = 0u;
+          *done = 0u;
+        }
+      }
+      return;
+    }
+    const uint64_t w = start + threadIdx.x;
+    if (w < limit && (p2::grind_word7<SLOT, MAT>((uint32_t)w, cp, p16) & mask) == 0u) atomicMin(result, (uint32_t)w);
+  }
+}
+
+}  // namespace
+
+template <int MAT>
+cudaError_t grind_m(const uint32_t* state, const uint32_t* in, int in_len, int bits, uint64_t limit,
+                    uint32_t* result, uint32_t* counter, uint32_t* done, uint32_t* mail, uint32_t seq,
+                    const P2Consts& p16, cudaStream_t st) {
+  if (in_len < 0 || in_len > 7 || bits < 0 || bits > 30) return cudaErrorInvalidValue;
+  if (limit > kb::P) limit = kb::P;
+  // the sponge state with the pending inputs, canonical (a witness w < p is
+  // its own canonical value), with 0 at the witness position; then its
+  // external layer plus the first round constants
+  uint32_t s[16];
+  for (int i = 0; i < 16; i++) s[i] = kb::from_mont(state[i]);
+  for (int i = 0; i < in_len; i++) s[i] = kb::from_mont(in[i]);
+  s[in_len] = 0u;
+  p2::grind_fold<MAT>(s, p16);
+  // with a mailbox the previous search left the state reset (grind_reset
+  // initialises it once per context)
+  if (!mail) {
+    const cudaError_t e = grind_reset(result, counter, done, st);
+    if (e != cudaSuccess) return e;
+  }
+  uint4 a = make_uint4(s[0], s[1], s[2], s[3]), b = make_uint4(s[4], s[5], s[6], s[7]);
+  uint4 c = make_uint4(s[8], s[9], s[10], s[11]), d = make_uint4(s[12], s[13], s[14], s[15]);
+  // Candidates in flight: once the smallest witness w is found, every claim
+  // already running still completes, so a search costs about w + W
+  // permutations for W in flight, while the rate grows with W. Expected cost
+  // (2^bits + W) / rate(W), minimised over CTAs per SM with the rates measured
+  // for Poseidon2-16 on B200 (relative to 8 CTAs of 256 per SM). Searches too
+  // small to fill the GPU keep about 2^(bits+1) candidates in flight.
+  static const int kPerSm[6] = {1, 2, 3, 4, 6, 8};
+  static const double kRate[6] = {0.892, 0.923, 0.946, 0.965, 0.986, 1.0};
+  const double expect = (double)(1ull << bits);
+  unsigned blocks = (unsigned)(((2ull << bits) + GRIND_CTA - 1) / GRIND_CTA);
+  if (blocks > (unsigned)sm_count()) {
+    double best = 0.0;
+    unsigned pick = (unsigned)sm_count();
+    for (int i = 0; i < 6; i++) {
+      const unsigned b = (unsigned)sm_count() * kPerSm[i];
+      const double cost = (expect + (double)b * GRIND_CTA) / kRate[i];
+      if (i == 0 || cost < best) {
+        best = cost;
+        pick = b;
+      }
+    }
+    if (pick < blocks) blocks = pick;
+  }
+  switch (in_len) {
+#define WK_GRIND(S) \
+  case S: k_grind<S, MAT><<<blocks, GRIND_CTA, 0, st>>>(p16, a, b, c, d, bits, limit, result, counter, done, mail, seq); break;
+    WK_GRIND(0) WK_GRIND(1) WK_GRIND(2) WK_GRIND(3) WK_GRIND(4) WK_GRIND(5) WK_GRIND(6) WK_GRIND(7)
+#undef WK_GRIND
+  }
+  LAUNCH_DONE();
+}
+
+}  // namespace wk

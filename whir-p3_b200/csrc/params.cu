@@ -21,6 +21,7 @@ p2::P2Consts to_consts(const whir_poseidon2_params& p) {
   k.width = p.width;
   k.rounds_f = p.rounds_f;
   k.rounds_p = p.rounds_p;
+  k.mat = p.external_matrix;
   memcpy(k.ext_rc, p.ext_rc, sizeof(k.ext_rc));
   memcpy(k.int_rc, p.int_rc, sizeof(k.int_rc));
   for (int i = 0; i < 24; i++) {
@@ -37,6 +38,8 @@ int validate_params(const whir_poseidon2_params& p, uint32_t width) {
               std::to_string(p.rounds_f) + "+" + std::to_string(p.rounds_p) + " (supported: 16 with 8+20, 24 with 8+23)");
     return WHIR_ERR_INVALID;
   }
+  if (p.external_matrix != WHIR_P2_MDS_MAT4 && p.external_matrix != WHIR_P2_HL_MAT4)
+    return set_error("unknown Poseidon2 external matrix " + std::to_string(p.external_matrix)), WHIR_ERR_INVALID;
   for (int i = 0; i < 8 * 24; i++)
     if (p.ext_rc[i] >= kb::P) return set_error("Poseidon2 constant out of range"), WHIR_ERR_INVALID;
   for (int i = 0; i < 32; i++)
@@ -53,46 +56,68 @@ int validate_params(const whir_poseidon2_params& p, uint32_t width) {
   return WHIR_OK;
 }
 
-// SplitMix64 (Steele, Lea, Flood, "Fast splittable pseudorandom number
-// generators", OOPSLA 2014), 31-bit rejection sampling into [0, p).
-namespace {
-struct SplitMix {
-  uint64_t s;
-  uint64_t next() {
-    uint64_t z = (s += 0x9e3779b97f4a7c15ull);
+// rand::rngs::SmallRng on 64-bit targets: xoshiro256++ (Blackman and Vigna,
+// "Scrambled linear pseudorandom number generators", 2021) whose
+// seed_from_u64 fills the four state words with SplitMix64 (Steele, Lea,
+// Flood, OOPSLA 2014) outputs; next_u32 is the high half of next_u64.
+// KoalaBear's StandardUniform draws next_u32() >> 1 and rejects values >= p;
+// the accepted value is the element's Montgomery representation (x * 2^32 mod
+// p), so its canonical value is that word reduced once.
+SmallRng::SmallRng(uint64_t seed) {
+  for (int i = 0; i < 4; i++) {
+    seed += 0x9e3779b97f4a7c15ull;
+    uint64_t z = seed;
     z = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ull;
     z = (z ^ (z >> 27)) * 0x94d049bb133111ebull;
-    return z ^ (z >> 31);
+    s[i] = z ^ (z >> 31);
   }
-  uint32_t field() {
-    for (;;) {
-      uint32_t v = (uint32_t)(next() >> 33);
-      if (v < kb::P) return v;
-    }
+}
+uint64_t SmallRng::next_u64() {
+  const uint64_t r = rotl(s[0] + s[3], 23) + s[0];
+  const uint64_t t = s[1] << 17;
+  s[2] ^= s[0];
+  s[3] ^= s[1];
+  s[1] ^= s[2];
+  s[0] ^= s[3];
+  s[2] ^= t;
+  s[3] = rotl(s[3], 45);
+  return r;
+}
+uint32_t SmallRng::field() {
+  for (;;) {
+    const uint32_t v = next_u32() >> 1;
+    if (v < kb::P) return kb::from_mont(v);
   }
-};
+}
 
-void fill(whir_poseidon2_params* p, uint32_t width, uint32_t rp, SplitMix& g) {
+namespace {
+// Poseidon2::new_from_rng: ExternalLayerConstants::new_from_rng (rounds_f / 2
+// initial rows, then rounds_f / 2 terminal rows, each row `width` elements in
+// order), then rounds_p internal constants.
+void fill(whir_poseidon2_params* p, uint32_t width, uint32_t rp, uint32_t mat, SmallRng& g) {
   memset(p, 0, sizeof(*p));
   p->width = width;
   p->rounds_f = p2::RF;
   p->rounds_p = rp;
-  for (uint32_t r = 0; r < 4; r++)
+  p->external_matrix = mat;
+  for (uint32_t r = 0; r < (uint32_t)p2::RF; r++)
     for (uint32_t i = 0; i < width; i++) p->ext_rc[r * width + i] = g.field();
   for (uint32_t r = 0; r < rp; r++) p->int_rc[r] = g.field();
-  for (uint32_t r = 4; r < 8; r++)
-    for (uint32_t i = 0; i < width; i++) p->ext_rc[r * width + i] = g.field();
   for (uint32_t i = 0; i < width; i++) p->diag[i] = p2::diag_value(p2::diag_code((int)width, (int)i));
 }
 }  // namespace
 
-void default_params(whir_poseidon2_params* p16, whir_poseidon2_params* p24) {
-  SplitMix g{1};
+void params_from_rng(uint64_t seed, uint32_t mat, whir_poseidon2_params* p16, whir_poseidon2_params* p24) {
+  SmallRng g(seed);
   whir_poseidon2_params a, b;
-  fill(&a, 16, p2::RP16, g);
-  fill(&b, 24, p2::RP24, g);
+  fill(&a, 16, p2::RP16, mat, g);
+  fill(&b, 24, p2::RP24, mat, g);
   if (p16) *p16 = a;
   if (p24) *p24 = b;
+}
+
+void default_params(whir_poseidon2_params* p16, whir_poseidon2_params* p24) {
+  params_from_rng(1, WHIR_P2_MDS_MAT4, p16, p24);
 }
 
 // ---------------------------------------------------------------------------
@@ -373,6 +398,7 @@ HostP16 host_consts16(const whir_poseidon2_params& p) {
   memcpy(k.ext_rc, p.ext_rc, sizeof(k.ext_rc));
   memcpy(k.int_rc, p.int_rc, sizeof(k.int_rc));
   memcpy(k.diag, p.diag, sizeof(k.diag));
+  k.mat = p.external_matrix;
   return k;
 }
 
@@ -382,17 +408,25 @@ inline uint64_t cube64(uint64_t v) {  // v < 2p: v^2 < 2^64, (v^2 mod p) * v < 2
   const uint64_t sq = (v * v) % P64;
   return (sq * v) % P64;
 }
-// external layer on canonical inputs: M4 outputs < 16p, chunk sums < 64p,
+// external layer on canonical inputs: block outputs < 16p, chunk sums < 64p,
 // results < 80p < 2^38, reduced once
-inline void ext_layer64(uint64_t* x) {
+inline void ext_layer64(uint64_t* x, uint32_t mat) {
   for (int c = 0; c < 16; c += 4) {
     const uint64_t a = x[c], b = x[c + 1], cc = x[c + 2], d = x[c + 3];
-    const uint64_t t0 = a + b, t1 = cc + d, t2 = 2 * b + t1, t3 = 2 * d + t0;
-    const uint64_t t4 = 4 * t1 + t3, t5 = 4 * t0 + t2;
-    x[c] = t3 + t5;
-    x[c + 1] = t5;
-    x[c + 2] = t2 + t4;
-    x[c + 3] = t4;
+    if (mat == WHIR_P2_HL_MAT4) {
+      const uint64_t t0 = a + b, t1 = cc + d, t2 = 2 * b + t1, t3 = 2 * d + t0;
+      const uint64_t t4 = 4 * t1 + t3, t5 = 4 * t0 + t2;
+      x[c] = t3 + t5;
+      x[c + 1] = t5;
+      x[c + 2] = t2 + t4;
+      x[c + 3] = t4;
+    } else {  // circ(2, 3, 1, 1)
+      const uint64_t s = a + b + cc + d;
+      x[c] = s + a + 2 * b;
+      x[c + 1] = s + b + 2 * cc;
+      x[c + 2] = s + cc + 2 * d;
+      x[c + 3] = s + d + 2 * a;
+    }
   }
   for (int j = 0; j < 4; j++) {
     const uint64_t s = x[j] + x[4 + j] + x[8 + j] + x[12 + j];
@@ -404,10 +438,10 @@ inline void ext_layer64(uint64_t* x) {
 void host_permute16(uint32_t* st, const HostP16& k) {
   uint64_t x[16];
   for (int i = 0; i < 16; i++) x[i] = st[i];
-  ext_layer64(x);
+  ext_layer64(x, k.mat);
   for (int r = 0; r < 4; r++) {
     for (int i = 0; i < 16; i++) x[i] = cube64(x[i] + k.ext_rc[r * 16 + i]);
-    ext_layer64(x);
+    ext_layer64(x, k.mat);
   }
   for (int r = 0; r < p2::RP16; r++) {
     x[0] = cube64(x[0] + k.int_rc[r]);
@@ -417,7 +451,7 @@ void host_permute16(uint32_t* st, const HostP16& k) {
   }
   for (int r = 4; r < 8; r++) {
     for (int i = 0; i < 16; i++) x[i] = cube64(x[i] + k.ext_rc[r * 16 + i]);
-    ext_layer64(x);
+    ext_layer64(x, k.mat);
   }
   for (int i = 0; i < 16; i++) st[i] = (uint32_t)x[i];
 }

@@ -3,8 +3,16 @@
 // Structure from the Poseidon2 paper (Grassi, Khovratovich, Schofnegger,
 // eprint 2023/323): an initial external linear layer, R_F/2 full rounds,
 // R_P partial rounds, R_F/2 full rounds. The external layer is
-// circ(2*M4, M4, ..., M4) with the paper's 4x4 matrix M4, evaluated with its
-// published 8-addition chain; the internal layer is 1*1^T + diag(mu).
+// circ(2*M, M, ..., M) for a 4x4 block M; the internal layer is
+// 1*1^T + diag(mu).
+//
+// Two choices of the block M (the template parameter MAT of every form below):
+//   MAT 0  the circulant [[2,3,1,1],[1,2,3,1],[1,1,2,3],[3,1,1,2]]: the block
+//          of Plonky3's Monty-31 external layer (`MDSMat4`), which
+//          `Poseidon2KoalaBear` applies;
+//   MAT 1  the paper's M4 [[5,7,1,3],[4,6,1,1],[1,3,5,7],[1,1,4,6]]
+//          (Plonky3's `HLMDSMat4`, the Horizen Labs form).
+// MAT 0 is the default of the library (the reference's permutation).
 //
 // Reference types this replaces: p3-koala-bear `Poseidon2KoalaBear<16>` and
 // `<24>` (src/bin/main.rs:31-32), used by PaddingFreeSponge (leaf hashing),
@@ -35,8 +43,13 @@ constexpr int RF = 8;
 constexpr int RP16 = 20;
 constexpr int RP24 = 23;
 
+// external 4x4 block choices
+constexpr int kMatMds = 0;  // Plonky3 MDSMat4 (circulant 2, 3, 1, 1)
+constexpr int kMatHl = 1;   // the paper's M4 (Plonky3 HLMDSMat4)
+
 struct P2Consts {
   uint32_t width, rounds_f, rounds_p;
+  uint32_t mat;             // kMatMds or kMatHl
   uint32_t ext_rc[8 * 24];  // canonical
   uint32_t int_rc[32];      // canonical
   uint32_t diag_c[24];      // the fixed diagonal, canonical (run-time indexed uses)
@@ -61,26 +74,65 @@ inline uint32_t diag_value(int code) {
   return code < 200 ? (uint32_t)v : (uint32_t)((kb::P - v) % kb::P);
 }
 
-// M4 = [[5,7,1,3],[4,6,1,1],[1,3,5,7],[1,1,4,6]] via the paper's addition chain.
-KB_HD void m4(uint32_t& x0, uint32_t& x1, uint32_t& x2, uint32_t& x3) {
-  using namespace kb;
-  const uint32_t t0 = add(x0, x1);
-  const uint32_t t1 = add(x2, x3);
-  const uint32_t t2 = add(dbl(x1), t1);
-  const uint32_t t3 = add(dbl(x3), t0);
-  const uint32_t t4 = add(dbl(dbl(t1)), t3);
-  const uint32_t t5 = add(dbl(dbl(t0)), t2);
-  x0 = add(t3, t5);
-  x1 = t5;
-  x2 = add(t2, t4);
-  x3 = t4;
+// Entry (i, j) of the block M.
+template <int MAT>
+KB_HD constexpr int m4_entry(int i, int j) {
+  const int hl[4][4] = {{5, 7, 1, 3}, {4, 6, 1, 1}, {1, 3, 5, 7}, {1, 1, 4, 6}};
+  const int circ[4] = {2, 3, 1, 1};  // row i is this row rotated right by i
+  return MAT == kMatHl ? hl[i][j] : circ[(j - i) & 3];
 }
 
-template <int T>
+// x <- M x.
+// MAT 0: with s = x0 + x1 + x2 + x3, a = s + x1 and b = s + x3, the rows are
+//   2x0 + 3x1 + x2 + x3 = a + (x0 + x1),   x0 + 2x1 + 3x2 + x3 = a + 2x2,
+//   x0 + x1 + 2x2 + 3x3 = b + (x2 + x3),   3x0 + x1 + x2 + 2x3 = b + 2x0:
+//   9 additions and 2 doublings.
+// MAT 1: the paper's addition chain (8 additions, 6 doublings).
+template <int MAT>
+KB_HD void m4(uint32_t& x0, uint32_t& x1, uint32_t& x2, uint32_t& x3) {
+  using namespace kb;
+  if (MAT == kMatHl) {
+    const uint32_t t0 = add(x0, x1);
+    const uint32_t t1 = add(x2, x3);
+    const uint32_t t2 = add(dbl(x1), t1);
+    const uint32_t t3 = add(dbl(x3), t0);
+    const uint32_t t4 = add(dbl(dbl(t1)), t3);
+    const uint32_t t5 = add(dbl(dbl(t0)), t2);
+    x0 = add(t3, t5);
+    x1 = t5;
+    x2 = add(t2, t4);
+    x3 = t4;
+  } else {
+    const uint32_t s01 = add(x0, x1), s23 = add(x2, x3);
+    const uint32_t s = add(s01, s23);
+    const uint32_t a = add(s, x1), b = add(s, x3);
+    const uint32_t y0 = add(a, s01), y1 = add(a, dbl(x2));
+    const uint32_t y2 = add(b, s23), y3 = add(b, dbl(x0));
+    x0 = y0;
+    x1 = y1;
+    x2 = y2;
+    x3 = y3;
+  }
+}
+
+// Row 3 of M applied to (x0, x1, x2, x3).
+template <int MAT>
+KB_HD uint32_t m4_row3(uint32_t x0, uint32_t x1, uint32_t x2, uint32_t x3) {
+  using namespace kb;
+  if (MAT == kMatHl) {  // x0 + x1 + 4x2 + 6x3
+    const uint32_t t0 = add(x0, x1), t1 = add(x2, x3);
+    return add(dbl(dbl(t1)), add(dbl(x3), t0));
+  } else {  // 3x0 + x1 + x2 + 2x3
+    const uint32_t s = add(add(x0, x1), add(x2, x3));
+    return add(add(s, x3), dbl(x0));
+  }
+}
+
+template <int T, int MAT>
 KB_HD void ext_layer(uint32_t (&x)[T]) {
   using namespace kb;
 #pragma unroll
-  for (int c = 0; c < T; c += 4) m4(x[c], x[c + 1], x[c + 2], x[c + 3]);
+  for (int c = 0; c < T; c += 4) m4<MAT>(x[c], x[c + 1], x[c + 2], x[c + 3]);
   uint32_t s0 = x[0], s1 = x[1], s2 = x[2], s3 = x[3];
 #pragma unroll
   for (int c = 4; c < T; c += 4) {
@@ -166,11 +218,11 @@ KB_HD uint32_t diag_axpy(int code, uint32_t s, uint32_t x) {
   }
 }
 
-template <int T>
+template <int T, int MAT>
 KB_HD void full_round(uint32_t (&x)[T], const uint32_t* rc) {
 #pragma unroll
   for (int i = 0; i < T; i++) x[i] = cube(kb::add(x[i], rc[i]));
-  ext_layer<T>(x);
+  ext_layer<T, MAT>(x);
 }
 
 // Sum of T canonical values mod p without a reduction per addition: pairs of
@@ -202,26 +254,33 @@ KB_HD void partial_round(uint32_t (&x)[T], uint32_t rc) {
 // unrolled width-24 permutation is about ten thousand instructions, more than
 // the instruction cache holds, while one round body is a few hundred. Round
 // constants are read by index.
-template <int T, int RP>
+template <int T, int RP, int MAT>
 KB_HD void permute_canonical(uint32_t (&x)[T], const P2Consts& k) {
-  ext_layer<T>(x);
+  ext_layer<T, MAT>(x);
 #pragma unroll 1
-  for (int r = 0; r < RF / 2; r++) full_round<T>(x, k.ext_rc + r * T);
+  for (int r = 0; r < RF / 2; r++) full_round<T, MAT>(x, k.ext_rc + r * T);
 #pragma unroll 1
   for (int r = 0; r < RP; r++) partial_round<T>(x, k.int_rc[r]);
 #pragma unroll 1
-  for (int r = RF / 2; r < RF; r++) full_round<T>(x, k.ext_rc + r * T);
+  for (int r = RF / 2; r < RF; r++) full_round<T, MAT>(x, k.ext_rc + r * T);
+}
+
+// The same with the block chosen at run time from k.mat (host-side callers).
+template <int T, int RP>
+inline void permute_canonical_rt(uint32_t (&x)[T], const P2Consts& k) {
+  if (k.mat == (uint32_t)kMatHl) permute_canonical<T, RP, kMatHl>(x, k);
+  else permute_canonical<T, RP, kMatMds>(x, k);
 }
 
 // Sponge forms of the permutation (PaddingFreeSponge, overwrite mode). FIRST:
 // the capacity words (from RATE on) are zero on entry, so the initial external
-// layer skips their M4 blocks and sums; LAST: only the first 8 words (the
+// layer skips their M blocks and sums; LAST: only the first 8 words (the
 // digest) of the output are read, so the final external layer forms only those.
-template <int T, int RATE>
+template <int T, int RATE, int MAT>
 KB_HD void ext_layer_zero_capacity(uint32_t (&x)[T]) {
   using namespace kb;
 #pragma unroll
-  for (int c = 0; c < RATE; c += 4) m4(x[c], x[c + 1], x[c + 2], x[c + 3]);
+  for (int c = 0; c < RATE; c += 4) m4<MAT>(x[c], x[c + 1], x[c + 2], x[c + 3]);
   uint32_t s0 = x[0], s1 = x[1], s2 = x[2], s3 = x[3];
 #pragma unroll
   for (int c = 4; c < RATE; c += 4) {
@@ -238,11 +297,11 @@ KB_HD void ext_layer_zero_capacity(uint32_t (&x)[T]) {
     x[c + 3] = c < RATE ? add(x[c + 3], s3) : s3;
   }
 }
-template <int T>
+template <int T, int MAT>
 KB_HD void ext_layer_digest(uint32_t (&x)[T]) {
   using namespace kb;
 #pragma unroll
-  for (int c = 0; c < T; c += 4) m4(x[c], x[c + 1], x[c + 2], x[c + 3]);
+  for (int c = 0; c < T; c += 4) m4<MAT>(x[c], x[c + 1], x[c + 2], x[c + 3]);
   uint32_t s0 = x[0], s1 = x[1], s2 = x[2], s3 = x[3];
 #pragma unroll
   for (int c = 4; c < T; c += 4) {
@@ -259,21 +318,21 @@ KB_HD void ext_layer_digest(uint32_t (&x)[T]) {
     x[c + 3] = add(x[c + 3], s3);
   }
 }
-template <int T, int RP, int RATE, bool FIRST, bool LAST>
+template <int T, int RP, int RATE, bool FIRST, bool LAST, int MAT>
 KB_HD void permute_sponge(uint32_t (&x)[T], const P2Consts& k) {
-  if (FIRST) ext_layer_zero_capacity<T, RATE>(x);
-  else ext_layer<T>(x);
+  if (FIRST) ext_layer_zero_capacity<T, RATE, MAT>(x);
+  else ext_layer<T, MAT>(x);
 #pragma unroll 1
-  for (int r = 0; r < RF / 2; r++) full_round<T>(x, k.ext_rc + r * T);
+  for (int r = 0; r < RF / 2; r++) full_round<T, MAT>(x, k.ext_rc + r * T);
 #pragma unroll 1
   for (int r = 0; r < RP; r++) partial_round<T>(x, k.int_rc[r]);
 #pragma unroll 1
-  for (int r = RF / 2; r < RF - 1; r++) full_round<T>(x, k.ext_rc + r * T);
+  for (int r = RF / 2; r < RF - 1; r++) full_round<T, MAT>(x, k.ext_rc + r * T);
   const uint32_t* rc = k.ext_rc + (RF - 1) * T;
 #pragma unroll
   for (int i = 0; i < T; i++) x[i] = cube(kb::add(x[i], rc[i]));
-  if (LAST) ext_layer_digest<T>(x);
-  else ext_layer<T>(x);
+  if (LAST) ext_layer_digest<T, MAT>(x);
+  else ext_layer<T, MAT>(x);
 }
 
 // Proof-of-work check of one candidate w (the duplex challenger's
@@ -281,47 +340,55 @@ KB_HD void permute_sponge(uint32_t (&x)[T], const P2Consts& k) {
 // position SLOT, of which sample_bits reads only output word 7. The initial
 // external layer is linear, so it and the first round's constants fold into
 // cp = ext(state with 0 at SLOT) + rc (grind_fold, once per search) plus w
-// times column SLOT of circ(2*M4, M4, M4, M4), whose entries are small
-// integers; the last external layer forms word 7 only.
+// times column SLOT of circ(2*M, M, M, M), whose entries are small integers;
+// the last external layer forms word 7 only.
+template <int MAT>
 KB_HD constexpr int ext_col16(int slot, int i) {
-  const int m[4][4] = {{5, 7, 1, 3}, {4, 6, 1, 1}, {1, 3, 5, 7}, {1, 1, 4, 6}};
-  return m[i & 3][slot & 3] * ((i >> 2) == (slot >> 2) ? 2 : 1);
+  return m4_entry<MAT>(i & 3, slot & 3) * ((i >> 2) == (slot >> 2) ? 2 : 1);
+}
+// the largest entry of circ(2*M, M, M, M), plus one
+template <int MAT>
+KB_HD constexpr int ext_col_bound() {
+  return MAT == kMatHl ? 15 : 7;
 }
 // state (canonical, 0 at the witness position) -> cp
+template <int MAT>
 KB_HD void grind_fold(uint32_t (&state)[16], const P2Consts& k) {
-  ext_layer<16>(state);
+  ext_layer<16, MAT>(state);
 #pragma unroll
   for (int i = 0; i < 16; i++) state[i] = kb::add(state[i], k.ext_rc[i]);
 }
-template <int SLOT>
+inline void grind_fold_rt(uint32_t (&state)[16], const P2Consts& k) {
+  if (k.mat == (uint32_t)kMatHl) grind_fold<kMatHl>(state, k);
+  else grind_fold<kMatMds>(state, k);
+}
+template <int SLOT, int MAT>
 KB_HD uint32_t grind_word7(uint32_t w, const uint32_t (&cp)[16], const P2Consts& k) {
   using namespace kb;
-  uint32_t wm[15];  // w * j mod p, j < 15
+  constexpr int kJ = ext_col_bound<MAT>();
+  uint32_t wm[kJ];  // w * j mod p, j < kJ
   wm[0] = 0u;
   wm[1] = w;
 #pragma unroll
-  for (int j = 2; j < 15; j++) wm[j] = add(wm[j - 1], w);
+  for (int j = 2; j < kJ; j++) wm[j] = add(wm[j - 1], w);
   uint32_t x[16];
 #pragma unroll
-  for (int i = 0; i < 16; i++) x[i] = cube(add(cp[i], wm[ext_col16(SLOT, i)]));
-  ext_layer<16>(x);
+  for (int i = 0; i < 16; i++) x[i] = cube(add(cp[i], wm[ext_col16<MAT>(SLOT, i)]));
+  ext_layer<16, MAT>(x);
 #pragma unroll 1
-  for (int r = 1; r < RF / 2; r++) full_round<16>(x, k.ext_rc + r * 16);
+  for (int r = 1; r < RF / 2; r++) full_round<16, MAT>(x, k.ext_rc + r * 16);
 #pragma unroll 1
   for (int r = 0; r < RP16; r++) partial_round<16>(x, k.int_rc[r]);
 #pragma unroll 1
-  for (int r = RF / 2; r < RF - 1; r++) full_round<16>(x, k.ext_rc + r * 16);
+  for (int r = RF / 2; r < RF - 1; r++) full_round<16, MAT>(x, k.ext_rc + r * 16);
   const uint32_t* rc = k.ext_rc + (RF - 1) * 16;
 #pragma unroll
   for (int i = 0; i < 16; i++) x[i] = cube(add(x[i], rc[i]));
-  // word 7 of the external layer: row 3 of M4 ([1, 1, 4, 6]) of block 1, plus
-  // the sum of row 3 over all blocks (the M4 addition chain's x3 output)
+  // word 7 of the external layer: row 3 of M on block 1, plus the sum of
+  // row 3 of M over all blocks
   uint32_t r3[4];
 #pragma unroll
-  for (int b = 0; b < 4; b++) {
-    const uint32_t t0 = add(x[4 * b], x[4 * b + 1]), t1 = add(x[4 * b + 2], x[4 * b + 3]);
-    r3[b] = add(dbl(dbl(t1)), add(dbl(x[4 * b + 3]), t0));
-  }
+  for (int b = 0; b < 4; b++) r3[b] = m4_row3<MAT>(x[4 * b], x[4 * b + 1], x[4 * b + 2], x[4 * b + 3]);
   return add(r3[1], add(add(r3[0], r3[1]), add(r3[2], r3[3])));
 }
 
