@@ -89,6 +89,39 @@ def inputs(draw, rank: int, n: int):
     return v[: 1 << n], v[1 << n:]
 
 
+def inputs_m(draw, rank: int, n: int, m: int):
+    """inputs() with m constraint points drawn after the polynomial, one after
+    the other (the loop of src/bin/main.rs:131-133)."""
+    v = draw(rank, (1 << n) + 4 * n * m)
+    return v[: 1 << n], v[1 << n:]
+
+
+def measure_config(pkg, ctx, stream, flush, n: int, m: int, steps: int, warmup: int) -> dict:
+    """Device-resident commit + prove of the benchmark's workload at n
+    variables with m constraints: ms per proof over `steps` timed proofs (CUDA
+    events on the context's stream, L2 flushed before each), after `warmup`."""
+    import torch
+
+    params = pkg.ProtocolParameters(100, 16, pkg.FoldingFactor.constant(4), pkg.SecurityAssumption.CapacityBound, 1, 3,
+                                    "poseidon2_24", 32)
+    poly, pts = inputs_m(pkg.rng_koalabear, 0, n, m)
+    d_poly = pkg.DeviceArray.from_host(ctx, poly)
+    for _ in range(max(warmup, 1)):
+        pkg.commit_and_prove(ctx, params, n, d_poly, pts)
+    total = 0.0
+    for _ in range(steps):
+        flush.zero_()
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record(stream)
+        pkg.commit_and_prove(ctx, params, n, d_poly, pts)
+        e.record(stream)
+        e.synchronize()
+        total += s.elapsed_time(e)
+    del d_poly
+    return {"num_variables": n, "constraints": m, "value": round(total / steps, 4), "unit": UNIT, "steps": steps,
+            "warmup": max(warmup, 1), "rs_domain_initial_reduction_factor": 3, "inputs": "SmallRng(0) draw"}
+
+
 def oracle_params():
     from oracle.oracle import make_params
 
@@ -145,6 +178,64 @@ class Clocks:
                     reasons.add(name)
         return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
                 "samples": len(sm)}
+
+
+# Warp instructions one warp issues for 32 permutations (one per thread) in
+# each Poseidon2 kernel, from ncu's smsp__inst_executed.sum divided by the
+# permutations of the captured launches, measured once on this build (Poseidon2
+# with Plonky3's KoalaBear external block). The issue ceiling is 4 warp
+# instructions per clock per SM at the SM clock sampled during the timed run.
+WARP_INST_PER_32_PERMS = {"grind": 5260, "merkle_leaves": 8550, "merkle_upper": 5535}
+
+
+def stage_rooflines(stages, work, steps, sm_mhz):
+    """One roofline entry per measured kernel stage. Poseidon2 stages (grinding,
+    leaf hashing, tree compression) are bound by instruction issue: achieved
+    = permutations per second (the stage's counted permutations over its live
+    CUDA-event time) times warp instructions per permutation, against SMs x 4
+    x the sampled SM clock. The DFT is bound by HBM: achieved = algorithmic
+    bytes (chunks read once, LDE written once) over its live time, against the
+    measured copy bandwidth."""
+    peaks = json.loads((ROOT / "MEASURED_PEAKS.json").read_text()) if (ROOT / "MEASURED_PEAKS.json").exists() else {}
+    hbm = float(peaks.get("hbm_gbs", 6650.0))
+    import torch
+
+    sms = torch.cuda.get_device_properties(torch.cuda.current_device()).multi_processor_count
+    issue_peak = sms * 4 * sm_mhz * 1e6 / 1e9  # G warp-instructions / s
+    names = {"grind": "k_grind (Poseidon2-16 proof-of-work search)",
+             "merkle_leaves": "k_leaf_digests (Poseidon2-24 leaf sponge)",
+             "merkle_upper": "k_merkle_two_levels / tree tops (Poseidon2-16 compression)",
+             "dft": "k_dft_cols_reg + k_dft_rows_reg / k_dft_coset (LDE)"}
+    out = []
+    for st, label in names.items():
+        ms, launches = stages[st]
+        units = work.get(st, 0)
+        if ms <= 0 or units <= 0:
+            continue
+        sec = ms * 1e-3
+        e = {"kernel": label, "stage": st, "ms_per_proof": round(ms / steps, 4),
+             "launches_per_proof": round(launches / steps, 2)}
+        if st == "dft":
+            gbs = units / sec / 1e9
+            e.update({"bound": "hbm", "achieved": round(gbs, 1), "peak": hbm, "unit": "GB/s",
+                      "frac": round(gbs / hbm, 4), "traffic": None,
+                      "algorithmic_bytes_per_proof": units // steps,
+                      "peak_source": "MEASURED_PEAKS.json hbm_gbs (measured)" if peaks else "fallback 6650 GB/s"})
+        else:
+            rate = units / sec
+            e.update({"permutations_per_proof": units // steps, "permutations_per_s": round(rate)})
+            ipp = WARP_INST_PER_32_PERMS.get(st)
+            if ipp:
+                ach = rate / 32.0 * ipp / 1e9
+                e.update({"bound": "issue", "achieved": round(ach, 2), "peak": round(issue_peak, 2),
+                          "unit": "G warp-instructions/s", "frac": round(ach / issue_peak, 4), "traffic": None,
+                          "warp_instructions_per_32_permutations": ipp,
+                          "peak_source": f"{sms} SMs x 4 issue slots x {sm_mhz:.0f} MHz sampled"})
+            else:
+                e.update({"bound": "issue", "achieved": None, "peak": round(issue_peak, 2),
+                          "unit": "G warp-instructions/s", "frac": None, "traffic": None})
+        out.append(e)
+    return out
 
 
 def run_reference(args) -> None:
@@ -213,9 +304,11 @@ def run_micro(args) -> None:
     reps = max(args.steps, 1)
 
     def timed(fn):
-        for _ in range(max(args.warmup, 1)):
+        for _ in range(max(args.warmup, 1)):  # the launch-shape tuner runs here, on first use
             fn()
         total = 0.0
+        # the timed launches only, for a profiler run with --profile-from-start off
+        torch.cuda.profiler.start()
         for _ in range(reps):
             flush.zero_()
             s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -224,6 +317,7 @@ def run_micro(args) -> None:
             e.record(stream)
             e.synchronize()
             total += s.elapsed_time(e)
+        torch.cuda.profiler.stop()
         return total / reps
 
     def emit(name, ms, alg_bytes=None, units=None, unit_name=None, extra=None):
@@ -273,13 +367,21 @@ def run_micro(args) -> None:
         ch = pkg.DuplexChallenger(ctx)
         seq = iter(range(1 << 30))
 
+        evaluated = []
+
         def grind():
             ch.observe(next(seq))
             ch.grind(bits)
+            evaluated.append(ctx.stage_work(reset=True)["grind"])
 
+        ctx.set_profiling(True)  # counts the candidates each search evaluated
         ms = timed(grind)
-        emit(f"grind {bits} bits", ms, units=float(1 << bits), unit_name="expected permutations/s",
-             extra={"note": "expected work 2^bits Poseidon2-16 permutations per grind"})
+        ctx.set_profiling(False)
+        ctx.stage_times(reset=True)
+        timed_evals = evaluated[-reps:]
+        emit(f"grind {bits} bits", ms, units=float(np.mean(timed_evals)), unit_name="permutations/s",
+             extra={"candidates_evaluated_per_call": [int(v) for v in evaluated],
+                    "note": "one Poseidon2-16 permutation per evaluated candidate; expected 2^bits per search"})
     ctx.close()
 
 
@@ -414,6 +516,9 @@ def main() -> None:
     ap.add_argument("--workers", type=int, default=16)
     ap.add_argument("--rates", default="10,50,100,200,500")
     ap.add_argument("--no-batch", action="store_true", help="skip the batch/serve summary in the default run")
+    ap.add_argument("--n", type=int, default=N_VARS, help="num_variables of the headline workload")
+    ap.add_argument("--constraints", type=int, default=1, help="evaluation constraints of the headline workload")
+    ap.add_argument("--no-extra", action="store_true", help="skip the n=26 / four-constraint lines")
     args = ap.parse_args()
     if args.micro:
         run_micro(args)
@@ -459,7 +564,8 @@ def main() -> None:
     ctx.set_stream(stream.cuda_stream)
     params = pkg.ProtocolParameters(100, 16, pkg.FoldingFactor.constant(4), pkg.SecurityAssumption.CapacityBound, 1, 3,
                                     "poseidon2_24", 32)
-    poly, point = inputs(pkg.rng_koalabear, rank, N_VARS)
+    n_vars = args.n
+    poly, point = inputs_m(pkg.rng_koalabear, rank, n_vars, args.constraints)
     d_poly = pkg.DeviceArray.from_host(ctx, poly)  # resident in HBM, Montgomery form
     flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
 
@@ -470,7 +576,7 @@ def main() -> None:
         torch.cuda.synchronize()
 
     def step(poly_arg):
-        return pkg.commit_and_prove(ctx, params, N_VARS, poly_arg, point)
+        return pkg.commit_and_prove(ctx, params, n_vars, poly_arg, point)
 
     for _ in range(max(args.warmup, 3)):
         step(d_poly)
@@ -521,70 +627,53 @@ def main() -> None:
     h2d = poly.nbytes + point.nbytes
     d2h = int(proof.size) * 4
 
-    # ---- per-stage device times and the dominant kernel, timed live with CUDA
-    # events on the context's stream over a second pass of the same steps ----
+    # ---- per-stage device times and work, timed live with CUDA events on the
+    # context's stream over a second pass of the same steps ----
     ctx.set_profiling(True)
     ctx.stage_times(reset=True)
+    ctx.stage_work(reset=True)
     for _ in range(args.steps):
         flush.zero_()
         step(d_poly)
     stages = ctx.stage_times(reset=True)
+    work = ctx.stage_work(reset=True)
     ctx.set_profiling(False)
     stages_ms = {k: round(v[0] / args.steps, 4) for k, v in stages.items()}
-    leaf_ms, leaf_launches = stages["merkle_leaves"]
-    cfg = pkg.WhirConfig(N_VARS, params)
-    trees = [(N_VARS + 1 - 4, 16)]  # (log height, row words): commitment, then one per round
-    for i, rc in enumerate(cfg.round_parameters):
-        new_dom = rc.domain_size >> (cfg.rs_reduction if i == 0 else 1)
-        trees.append((new_dom.bit_length() - 1 - 4, 64))
+    rooflines = stage_rooflines(stages, work, args.steps, clk.get("sm_mhz") or 1965.0)
+    primary = max(rooflines, key=lambda r: r["ms_per_proof"])
 
-    def leaf_bytes(log_h, words):
-        # rows read once, one 8-word digest written per leaf
-        h = 1 << log_h
-        return h * words * 4 + h * 32
-
-    per_proof_bytes = sum(leaf_bytes(*t) for t in trees)
-    launch_ms = leaf_ms / max(leaf_launches, 1)
-    per_launch_bytes = per_proof_bytes / len(trees)
-    achieved = per_launch_bytes / (launch_ms * 1e-3) / 1e9
-    perms = sum((1 << lh) * ((w + 15) // 16) for lh, w in trees)
-    peaks = json.loads((ROOT / "MEASURED_PEAKS.json").read_text()) if (ROOT / "MEASURED_PEAKS.json").exists() else {}
-    peak = float(peaks.get("hbm_gbs", 6650.0))
-    # DRAM traffic of the commitment-tree launch (ncu, 2^21 leaves x 16 words: 134.6 MB read + 38.0 MB
-    # written, profiles/poseidon2_grind_and_leaves_n24.md), scaled to the average launch by algorithmic bytes
-    traffic = 172.60e6 * per_launch_bytes / leaf_bytes(21, 16)
-    roofline = {"kernel": "k_leaf_digests (Poseidon2-24 leaf sponge, one row per thread)",
-                "bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
-                "frac": round(achieved / peak, 4), "traffic": round(traffic),
-                "peak_source": "MEASURED_PEAKS.json hbm_gbs" if peaks else "fallback 6650 GB/s",
-                "ms_per_launch": round(launch_ms, 4), "launches_per_proof": round(leaf_launches / args.steps, 2),
-                "algorithmic_bytes_per_launch": round(per_launch_bytes),
-                "compute_bound": {"leaf_permutations_per_s": round(perms / (leaf_ms / args.steps * 1e-3)),
-                                  "alu_pipe_busy": 0.779, "issue_active": 0.808,
-                                  "note": "integer-issue bound: ALU pipe 77.9% and issue 80.8% active, FMA-heavy "
-                                          "61.0%, FP64 11.2% (S-box quotients), DRAM 3.1% "
-                                          "(ncu, profiles/poseidon2_grind_and_leaves_n24.md)"}}
-
+    extra = None
+    if rank == 0 and world == 1 and not args.no_extra:
+        # the other sizes of the full-prove configuration: n = 24 and 26, one
+        # and four constraints
+        extra = [measure_config(pkg, ctx, stream, flush, n, m, 5, 2)
+                 for n, m in ((24, 1), (24, 4), (26, 1), (26, 4)) if (n, m) != (n_vars, args.constraints)]
     batch = serve = None
     if rank == 0 and world == 1 and not args.no_batch:
         batch = run_batch(pkg, ctx, batch_jobs(pkg, 64, 4), args.workers)
-        serve = run_serve(pkg, ctx, local, 200.0, args.workers, 120, 5)
+        serve = []
+        for rate in [float(x) for x in args.rates.split(",")]:
+            count = int(min(400, max(40, rate * 1.0)))
+            serve.append(run_serve(pkg, ctx, local, rate, args.workers, count, 5))
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline_sample()
     if rank == 0:
-        line = {"metric": METRIC, "value": round(value, 4), "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        metric = METRIC if n_vars == N_VARS else METRIC.replace("2^24", f"2^{n_vars}")
+        line = {"metric": metric, "value": round(value, 4), "unit": UNIT, "n_gpus": world, "steps": args.steps,
                 "warmup": max(args.warmup, 3), "ms_per_step": round(step_ms, 4), "higher_is_better": False,
                 "scaling": "weak", "vs_baseline": None, "dtype": "u32 (KoalaBear mod p, exact)",
                 "data": "synthetic: the reference benchmark's SmallRng(0) polynomial and point",
-                "config": dict(CONFIG, parallelism=f"replicas x{world} (one proof per GPU per step)"),
+                "config": dict(CONFIG, num_variables=n_vars, constraints=args.constraints,
+                               parallelism=f"replicas x{world} (one proof per GPU per step)"),
                 "proofs_per_s": round(1e3 / value, 3), "proof_words": int(ref_proof.size),
                 "e2e": {"value": round(e2e_value, 4), "unit": UNIT, "h2d_bytes_per_step": h2d * world,
                         "d2h_bytes_per_step": d2h * world},
-                "gpu_launches": int(launches), "roofline": roofline, "stages_ms_per_proof": stages_ms,
+                "gpu_launches": int(launches), "roofline": primary, "rooflines": rooflines,
+                "stages_ms_per_proof": stages_ms,
                 "autotune": autotune,
                 "cpu_baseline": cpu, "clocks": clk,
-                "batched": batch, "served": serve}
+                "extra": extra, "batched": batch, "served": serve}
         print(json.dumps(line), flush=True)
     ctx.close()
     if dist is not None:

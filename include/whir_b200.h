@@ -139,6 +139,12 @@ int whir_ctx_synchronize(whir_ctx* ctx);
  * min(8, cap) entries (milliseconds and scope counts); returns the stage count. */
 int whir_ctx_set_profiling(whir_ctx* ctx, int32_t enable);
 int whir_ctx_stage_times(whir_ctx* ctx, double* ms, uint64_t* counts, int32_t cap, int32_t reset);
+/* Work done per stage while profiling was on, in the stage's own unit: DFT
+ * algorithmic bytes (chunks read once, LDE written once), Merkle leaf
+ * permutations, Merkle compressions, grinding candidates evaluated (one
+ * Poseidon2-16 permutation each); other stages 0. Writes min(8, cap) entries;
+ * returns the stage count. */
+int whir_ctx_stage_work(whir_ctx* ctx, uint64_t* work, int32_t cap, int32_t reset);
 /* Host permutation with the context's data (width taken from the state length 16 or 24). */
 int whir_poseidon2_permute(const whir_ctx* ctx, uint32_t* state, int32_t width);
 
@@ -296,6 +302,18 @@ int whir_svo_partial_evals(whir_ctx* ctx, const uint32_t* d_poly, int32_t n, int
  * query    = kind (0 base, 1 ext), n_values, values, path_len, path[8*path_len]
  * This mirrors WhirProof (src/whir/proof.rs:17-121) field by field.
  */
+/* The bytes bincode::serialize gives for WhirProof (src/whir/proof.rs:11-141,
+ * src/bin/main.rs:221): bincode 1.3 default options (little-endian, fixed-width
+ * integers, u64 sequence lengths, one-byte Option tags), field elements as
+ * their Montgomery u32 words, extension elements / digests / Merkle path
+ * nodes as fixed arrays, Merkle proofs as Vec<[F; 8]>, and QueryOpening
+ * internally tagged ("type": "base" | "extension"). The Plonky3 serde forms
+ * are assumed, not checked against the reference. out may be NULL to get the
+ * length; WHIR_ERR_BUFFER if cap is too small (out_len holds the length). */
+int whir_proof_to_bincode(const uint32_t* words, size_t n_words, uint8_t* out, size_t cap, size_t* out_len);
+/* The inverse: bincode bytes to the flat stream; rejects malformed input and
+ * field words >= p. words may be NULL to get the length. */
+int whir_proof_from_bincode(const uint8_t* bytes, size_t len, uint32_t* words, size_t cap, size_t* n_words);
 /* InitialStatement::evaluate for each user point (src/whir/constraints/statement/initial.rs:143-152)
  * followed by CommitmentWriter::commit (src/whir/committer/writer.rs:56-109).
  * poly: 2^n values, host canonical (poly_on_device = 0) or device Montgomery

@@ -18,3 +18,36 @@ def test_specialised_poseidon2_forms_match_plain(tmp_path):
     assert out.returncode == 0, out.stdout + out.stderr
     words = out.stdout.split()
     assert words[0] == "ok" and int(words[1]) > 5000, out.stdout
+
+
+def test_device_sbox_method_on_unreduced_inputs():
+    """The device S-box (poseidon2.cuh `cube`) forms v^2 mod p and then
+    (v^2 mod p) * v mod p from a double-precision quotient estimate
+    q = round(a * fl(b / p)) (an FMA with 1.5 * 2^52) and r = a * b - q * p
+    modulo 2^32 with one signed correction. Its inputs are round-constant sums
+    that skip their reduction (below 2p), so it must hold for every v < 2^32.
+    Emulated here in IEEE double with an exactly rounded FMA."""
+    import random
+    import struct
+    from fractions import Fraction
+
+    p = 2**31 - 2**24 + 1
+    inv_p, magic = 1.0 / p, 6755399441055744.0
+
+    def mulmod_q(a, ad, bp, b):
+        q = float(Fraction(ad) * Fraction(bp) + Fraction(magic))
+        q_lo = struct.unpack("<Q", struct.pack("<d", q))[0] & 0xFFFFFFFF
+        r = (a * b - q_lo * p) & 0xFFFFFFFF
+        return min(r, (r + p) & 0xFFFFFFFF)
+
+    def cube(v):
+        vd = float(v)
+        vp = vd * inv_p
+        v2 = mulmod_q(v, vd, vp, v)
+        return mulmod_q(v2, float(v2), vp, v)
+
+    rng = random.Random(3)
+    vals = [0, 1, p - 1, p, p + 1, 2 * p - 2, 2**31 - 1, 2**31, 2**32 - 2, 2**32 - 1]
+    vals += [rng.randrange(2 * p) for _ in range(6000)] + [rng.randrange(2**32) for _ in range(6000)]
+    for v in vals:
+        assert cube(v) == pow(v, 3, p), v

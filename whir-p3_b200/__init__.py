@@ -96,6 +96,8 @@ _SIGS = {
     "whir_poseidon2_params_from_rng": (C.c_int, [C.c_uint64, C.c_uint32, C.POINTER(Poseidon2Params),
                                                  C.POINTER(Poseidon2Params)]),
     "whir_rng_koalabear": (C.c_int, [C.c_uint64, _vp, C.c_size_t]),
+    "whir_proof_to_bincode": (C.c_int, [_vp, C.c_size_t, _vp, C.c_size_t, C.POINTER(C.c_size_t)]),
+    "whir_proof_from_bincode": (C.c_int, [_vp, C.c_size_t, _vp, C.c_size_t, C.POINTER(C.c_size_t)]),
     "whir_ctx_create": (C.c_int, [_i32, C.POINTER(Poseidon2Params), C.POINTER(Poseidon2Params), C.POINTER(_vp)]),
     "whir_ctx_destroy": (C.c_int, [_vp]),
     "whir_ctx_set_stream": (C.c_int, [_vp, _vp]),
@@ -103,6 +105,7 @@ _SIGS = {
     "whir_poseidon2_permute": (C.c_int, [_vp, _u32, _i32]),
     "whir_ctx_set_profiling": (C.c_int, [_vp, _i32]),
     "whir_ctx_stage_times": (C.c_int, [_vp, _vp, _vp, _i32, _i32]),
+    "whir_ctx_stage_work": (C.c_int, [_vp, _vp, _i32, _i32]),
     "whir_config_new": (C.c_int, [C.POINTER(_Params), _i32, C.POINTER(_Config)]),
     "whir_domain_separator": (C.c_int, [C.POINTER(_Config), _i32, _vp, _i32]),
     "whir_challenger_init": (None, [C.POINTER(_Chal)]),
@@ -334,6 +337,31 @@ def poseidon2_from_rng(seed: int, external_matrix: int = P2_MDS_MAT4) -> tuple[P
     return a, b
 
 
+def proof_to_bincode(proof: np.ndarray) -> bytes:
+    """The flat proof stream as the bytes bincode::serialize gives for the
+    reference's WhirProof (src/whir/proof.rs:11-141)."""
+    w = np.ascontiguousarray(proof, dtype=np.uint32)
+    n = C.c_size_t(0)
+    rc = lib().whir_proof_to_bincode(w.ctypes.data, w.size, None, 0, C.byref(n))
+    if rc not in (0, -5):
+        _check(rc)
+    out = np.empty(n.value, dtype=np.uint8)
+    _check(lib().whir_proof_to_bincode(w.ctypes.data, w.size, out.ctypes.data, out.size, C.byref(n)))
+    return out.tobytes()
+
+
+def proof_from_bincode(data: bytes) -> np.ndarray:
+    """bincode bytes of a WhirProof back to the flat proof stream."""
+    b = np.frombuffer(data, dtype=np.uint8)
+    n = C.c_size_t(0)
+    rc = lib().whir_proof_from_bincode(b.ctypes.data, b.size, None, 0, C.byref(n))
+    if rc not in (0, -5):
+        _check(rc)
+    out = np.empty(n.value, dtype=np.uint32)
+    _check(lib().whir_proof_from_bincode(b.ctypes.data, b.size, out.ctypes.data, out.size, C.byref(n)))
+    return out
+
+
 def rng_koalabear(seed: int, count: int) -> np.ndarray:
     """The first `count` KoalaBear elements (canonical uint32) that
     `rng.random::<F>()` draws from SmallRng::seed_from_u64(seed)
@@ -386,6 +414,14 @@ class Context:
         cnt = np.zeros(8, dtype=np.uint64)
         _check(lib().whir_ctx_stage_times(self.handle, ms.ctypes.data, cnt.ctypes.data, 8, int(reset)))
         return {name: (float(m), int(c)) for name, m, c in zip(self.STAGES, ms, cnt)}
+
+    def stage_work(self, reset: bool = True) -> dict:
+        """Work per stage while profiling was on: DFT algorithmic bytes, Merkle
+        leaf permutations, Merkle compressions, grinding candidates (one
+        Poseidon2-16 permutation each)."""
+        w = np.zeros(8, dtype=np.uint64)
+        _check(lib().whir_ctx_stage_work(self.handle, w.ctypes.data, 8, int(reset)))
+        return {name: int(v) for name, v in zip(self.STAGES, w)}
 
     def permute(self, state) -> np.ndarray:
         s = _arr(state).copy()

@@ -61,8 +61,13 @@ int sync(whir_ctx* ctx) {
 // shared with prover.cu
 namespace wh {
 
-StageTimer::StageTimer(whir_ctx* c, int s) : ctx(c), stage(s) {
+void add_stage_work(whir_ctx* ctx, int stage, uint64_t work) {
+  if (ctx && ctx->profiling && stage >= 0 && stage < kStCount) ctx->stage_work[stage] += work;
+}
+
+StageTimer::StageTimer(whir_ctx* c, int s, uint64_t work) : ctx(c), stage(s) {
   if (!ctx || !ctx->profiling) return;
+  ctx->stage_work[s] += work;
   for (cudaEvent_t* e : {&a, &b}) {
     if (!ctx->event_pool.empty()) {
       *e = ctx->event_pool.back();
@@ -244,8 +249,12 @@ int grind(whir_ctx* ctx, Chal& ch, int bits, uint32_t* witness) {
     WH_TRY_CUDA(wk::grind(ch.st, ch.in, ch.in_len, bits, kb::P, ctx->d_words, ctx->d_words + 1, ctx->d_words + 2,
                           ctx->h_mail ? ctx->d_mail : nullptr, seq, ctx->p16, ctx->stream));
   }
-  uint32_t w = 0;
-  WH_TRY(fetch_posted(ctx, ctx->h_mail ? seq : 0u, &w, ctx->d_words, 4));
+  // with a mailbox the search posts its witness and the number of claims of
+  // 256 candidates it evaluated
+  uint32_t got[2] = {0u, 0u};
+  WH_TRY(fetch_posted(ctx, ctx->h_mail ? seq : 0u, got, ctx->d_words, ctx->h_mail ? 8 : 4));
+  const uint32_t w = got[0];
+  if (ctx->h_mail) add_stage_work(ctx, kStGrind, (uint64_t)got[1] * 256u);
   if (w >= kb::P) {
     set_error("proof-of-work search found no witness");
     return WHIR_ERR_NOT_FOUND;
@@ -534,6 +543,15 @@ int whir_ctx_stage_times(whir_ctx* ctx, double* ms, uint64_t* counts, int32_t ca
       ctx->stage_ms[i] = 0.;
       ctx->stage_launches[i] = 0;
     }
+  return wh::kStCount;
+}
+
+int whir_ctx_stage_work(whir_ctx* ctx, uint64_t* work, int32_t cap, int32_t reset) {
+  WH_TRY(check_ctx(ctx));
+  for (int i = 0; i < wh::kStCount && i < cap; i++)
+    if (work) work[i] = ctx->stage_work[i];
+  if (reset)
+    for (int i = 0; i < wh::kStCount; i++) ctx->stage_work[i] = 0;
   return wh::kStCount;
 }
 

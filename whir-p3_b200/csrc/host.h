@@ -144,6 +144,7 @@ struct whir_ctx {
   std::vector<std::pair<int, std::pair<cudaEvent_t, cudaEvent_t>>> stage_events;
   double stage_ms[wh::kStCount] = {};
   uint64_t stage_launches[wh::kStCount] = {};
+  uint64_t stage_work[wh::kStCount] = {};
 };
 
 namespace wh {
@@ -160,13 +161,18 @@ inline cudaError_t ctx_malloc(whir_ctx* ctx, void* p, size_t bytes) {
   return cudaMallocFromPoolAsync(reinterpret_cast<void**>(p), bytes, ctx->pool, ctx->stream);
 }
 // Records a CUDA event pair around a scope when the context is profiling.
+// Records CUDA events around a stage when profiling is on, and adds `work`
+// units to the stage's work count (DFT: algorithmic bytes; Merkle leaves and
+// upper levels: permutations; grinding adds its evaluated candidates after the
+// search, see add_stage_work).
 struct StageTimer {
   whir_ctx* ctx;
   int stage;
   cudaEvent_t a = nullptr, b = nullptr;
-  StageTimer(whir_ctx* c, int s);
+  StageTimer(whir_ctx* c, int s, uint64_t work = 0);
   ~StageTimer();
 };
+void add_stage_work(whir_ctx* ctx, int stage, uint64_t work);
 
 int ensure_dft_tables(whir_ctx* ctx, int log_h, wk::DftTables* t);
 int fetch(whir_ctx* ctx, void* host, const void* dev, size_t bytes);

@@ -265,7 +265,7 @@ __device__ __forceinline__ void coop_permute16(uint32_t (&x)[4], int q, const P2
 #pragma unroll
   for (int r = 0; r < p2::RF / 2; r++) {
 #pragma unroll
-    for (int j = 0; j < 4; j++) x[j] = p2::cube(add(x[j], k.ext_rc[r * 16 + 4 * q + j]));
+    for (int j = 0; j < 4; j++) x[j] = p2::cube_sum(x[j], k.ext_rc[r * 16 + 4 * q + j]);
     coop_ext_layer<MAT>(x);
   }
   // Internal rounds with word 0 replicated in all four lanes (w0): every lane
@@ -281,7 +281,7 @@ __device__ __forceinline__ void coop_permute16(uint32_t (&x)[4], int q, const P2
     uint32_t o = add(add(q == 0 ? 0u : x[0], x[1]), add(x[2], x[3]));
     o = add(o, __shfl_xor_sync(0xffffffffu, o, 1));
     o = add(o, __shfl_xor_sync(0xffffffffu, o, 2));
-    const uint32_t y0 = p2::cube(add(w0, k.int_rc[r]));
+    const uint32_t y0 = p2::cube_sum(w0, k.int_rc[r]);
     const uint32_t s = add(o, y0);
 #pragma unroll
     for (int j = 0; j < 4; j++) x[j] = add(s, mul_shoup(x[j], k.diag_c[4 * q + j], k.diag_s[4 * q + j]));
@@ -291,7 +291,7 @@ __device__ __forceinline__ void coop_permute16(uint32_t (&x)[4], int q, const P2
 #pragma unroll
   for (int r = p2::RF / 2; r < p2::RF; r++) {
 #pragma unroll
-    for (int j = 0; j < 4; j++) x[j] = p2::cube(add(x[j], k.ext_rc[r * 16 + 4 * q + j]));
+    for (int j = 0; j < 4; j++) x[j] = p2::cube_sum(x[j], k.ext_rc[r * 16 + 4 * q + j]);
     coop_ext_layer<MAT>(x);
   }
 #pragma unroll
@@ -605,14 +605,16 @@ __global__ void __launch_bounds__(GRIND_CTA) k_grind(const __grid_constant__ P2C
     __syncthreads();
     if (!go) {
       // every atomicMin of this CTA precedes the barriers above; the last CTA
-      // to stop holds the final result, posts it to the mailbox and resets
-      // the search state for the next search (every other CTA has finished
-      // with it), which then needs no initialising launch
+      // to stop holds the final result, posts it to the mailbox with the
+      // number of claims that were evaluated (every CTA made exactly one
+      // claim that it did not evaluate) and resets the search state for the
+      // next search (every other CTA has finished with it), which then needs
+      // no initialising launch
       if (threadIdx.x == 0 && mail) {
         __threadfence();
         if (atomicAdd(done, 1u) == gridDim.x - 1) {
-          const uint32_t r = atomicAdd(result, 0u);
-          mail_post(mail, &r, 1, seq);
+          const uint32_t post[2] = {atomicAdd(result, 0u), atomicAdd(counter, 0u) - gridDim.x};
+          mail_post(mail, post, 2, seq);
           *result = kb::P;
           *counter = 0u;
           *done = 0u;

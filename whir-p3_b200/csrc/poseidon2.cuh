@@ -28,7 +28,7 @@
 //
 // The permutation runs on canonical values. On the device the S-box products
 // take their quotient from a double-precision estimate (the floating-point
-// quotient method of Shoup's NTL MulMod): for a, b < 2^31,
+// quotient method of Shoup's NTL MulMod): for a * b < 2^64,
 // q = round(a * fl(b / p)) is within one of a * b / p, so r = a * b - q * p,
 // computed modulo 2^32, lies in (-p, p) and one signed correction gives the
 // residue. This moves the high halves of the products from the integer
@@ -155,9 +155,9 @@ KB_HD void ext_layer(uint32_t (&x)[T]) {
 // measured faster in this permutation than building 2^52 + a from its bit
 // pattern and subtracting 2^52 (one instruction instead of two moves and an add).
 __device__ __forceinline__ double exact_double(uint32_t a) { return __uint2double_rn(a); }
-// a * b mod p for a, b < 2^31, given a as a double and bp = fl(b / p): adding
-// 1.5 * 2^52 rounds the quotient estimate to an integer held in the low
-// mantissa bits, read back as the low word.
+// a * b mod p for a * b < 2^64 with a < 2^32, given a as a double and
+// bp = fl(b / p): adding 1.5 * 2^52 rounds the quotient estimate to an integer
+// held in the low mantissa bits, read back as the low word.
 __device__ __forceinline__ uint32_t mulmod_q(uint32_t a, double ad, double bp, uint32_t b) {
   const double q = fma(ad, bp, 6755399441055744.0);
   const uint32_t r = a * b - (uint32_t)__double2loint(q) * kb::P;
@@ -165,7 +165,11 @@ __device__ __forceinline__ uint32_t mulmod_q(uint32_t a, double ad, double bp, u
 }
 #endif
 
-// v^3 mod p, v canonical
+// v^3 mod p for any v < 2^32 (not necessarily reduced). On the device: with
+// v < 2^32 the estimate of v^2 / p is off by less than 2^-20 before rounding,
+// so q is within one of the quotient and v^2 - q p lies in (-p, p); the same
+// holds for the second product (v^2 mod p) * v. On the host both products fit
+// 64 bits.
 KB_HD uint32_t cube(uint32_t v) {
 #ifdef __CUDA_ARCH__
   constexpr double kInvP = 1.0 / 2130706433.0;
@@ -178,6 +182,10 @@ KB_HD uint32_t cube(uint32_t v) {
   return (uint32_t)(sq * v % kb::P);
 #endif
 }
+
+// (a + b)^3 mod p for canonical a, b: the sum is below 2p < 2^32 and goes
+// into the S-box unreduced.
+KB_HD uint32_t cube_sum(uint32_t a, uint32_t b) { return cube(a + b); }
 
 // x / 2, x canonical: (x + p) / 2 for odd x
 KB_HD uint32_t halve(uint32_t x) { return (x >> 1) + (x & 1u) * ((kb::P + 1) / 2); }
@@ -221,7 +229,7 @@ KB_HD uint32_t diag_axpy(int code, uint32_t s, uint32_t x) {
 template <int T, int MAT>
 KB_HD void full_round(uint32_t (&x)[T], const uint32_t* rc) {
 #pragma unroll
-  for (int i = 0; i < T; i++) x[i] = cube(kb::add(x[i], rc[i]));
+  for (int i = 0; i < T; i++) x[i] = cube_sum(x[i], rc[i]);
   ext_layer<T, MAT>(x);
 }
 
@@ -244,7 +252,7 @@ KB_HD uint32_t sum_mod(const uint32_t (&x)[T]) {
 template <int T>
 KB_HD void partial_round(uint32_t (&x)[T], uint32_t rc) {
   using namespace kb;
-  x[0] = cube(add(x[0], rc));
+  x[0] = cube_sum(x[0], rc);
   const uint32_t s = sum_mod<T>(x);
 #pragma unroll
   for (int i = 0; i < T; i++) x[i] = diag_axpy(diag_code(T, i), s, x[i]);
@@ -330,7 +338,7 @@ KB_HD void permute_sponge(uint32_t (&x)[T], const P2Consts& k) {
   for (int r = RF / 2; r < RF - 1; r++) full_round<T, MAT>(x, k.ext_rc + r * T);
   const uint32_t* rc = k.ext_rc + (RF - 1) * T;
 #pragma unroll
-  for (int i = 0; i < T; i++) x[i] = cube(kb::add(x[i], rc[i]));
+  for (int i = 0; i < T; i++) x[i] = cube_sum(x[i], rc[i]);
   if (LAST) ext_layer_digest<T, MAT>(x);
   else ext_layer<T, MAT>(x);
 }
@@ -373,7 +381,7 @@ KB_HD uint32_t grind_word7(uint32_t w, const uint32_t (&cp)[16], const P2Consts&
   for (int j = 2; j < kJ; j++) wm[j] = add(wm[j - 1], w);
   uint32_t x[16];
 #pragma unroll
-  for (int i = 0; i < 16; i++) x[i] = cube(add(cp[i], wm[ext_col16<MAT>(SLOT, i)]));
+  for (int i = 0; i < 16; i++) x[i] = cube_sum(cp[i], wm[ext_col16<MAT>(SLOT, i)]);
   ext_layer<16, MAT>(x);
 #pragma unroll 1
   for (int r = 1; r < RF / 2; r++) full_round<16, MAT>(x, k.ext_rc + r * 16);
@@ -383,7 +391,7 @@ KB_HD uint32_t grind_word7(uint32_t w, const uint32_t (&cp)[16], const P2Consts&
   for (int r = RF / 2; r < RF - 1; r++) full_round<16, MAT>(x, k.ext_rc + r * 16);
   const uint32_t* rc = k.ext_rc + (RF - 1) * 16;
 #pragma unroll
-  for (int i = 0; i < 16; i++) x[i] = cube(add(x[i], rc[i]));
+  for (int i = 0; i < 16; i++) x[i] = cube_sum(x[i], rc[i]);
   // word 7 of the external layer: row 3 of M on block 1, plus the sum of
   // row 3 of M over all blocks
   uint32_t r3[4];

@@ -210,7 +210,8 @@ int commit_matrix(whir_ctx* ctx, const uint32_t* d_src, int log_chunk, int log_w
   if (!pass1) WH_TRY_CUDA(wh::ctx_malloc(ctx, &scratch, words * 4));
   int s = WHIR_OK;
   {
-    wh::StageTimer timer(ctx, wh::kStDft);
+    // algorithmic bytes: the 2^log_w chunks read once, the LDE written once
+    wh::StageTimer timer(ctx, wh::kStDft, ((uint64_t)lanes << (log_chunk + log_w)) * 4 + (uint64_t)words * 4);
     if (pass1) {
       const cudaError_t ce =
           wk::dft_batch(d_src, t->rows, scratch, log_chunk, log_w, log_blowup, lanes, tab, *pass1, 2, ctx->stream);
@@ -226,12 +227,14 @@ int commit_matrix(whir_ctx* ctx, const uint32_t* d_src, int log_chunk, int log_w
   if (pass1) *pre_scratch = nullptr;
   WH_TRY(s);
   {
-    wh::StageTimer timer(ctx, wh::kStLeaves);
+    // one permutation per rate-sized chunk of each row (rate 16 for Poseidon2-24, 8 for Poseidon2-16)
+    const uint64_t rate = leaf_hash == 0 ? 16 : 8;
+    wh::StageTimer timer(ctx, wh::kStLeaves, (uint64_t)h * (((uint64_t)t->row_words + rate - 1) / rate));
     WH_TRY(wh::run_merkle_leaves(ctx, t->rows, t->log_h, t->row_words, leaf_hash, t->digests));
   }
   uint32_t posted = 0;
   {
-    wh::StageTimer timer(ctx, wh::kStNodes);
+    wh::StageTimer timer(ctx, wh::kStNodes, (uint64_t)h - 1);  // one compression per inner node
     WH_TRY(wh::run_merkle_upper(ctx, t->log_h, t->digests, &posted));
   }
   uint32_t r[8];
