@@ -341,10 +341,15 @@ int whir_commit_and_prove(whir_ctx* ctx, const whir_protocol_params* params, int
  * A pool of worker threads on one device, each with its own context and CUDA
  * stream, proves submitted jobs concurrently (the north star's batching and
  * serving patterns; no counterpart in the reference, which proves one
- * polynomial per call). Jobs are admitted in FIFO order when their device
- * footprint fits the HBM budget (a job larger than the whole budget runs
- * alone). Each job runs whir_commit_and_prove on its worker's context, so its
- * proof is identical to the one-at-a-time result. */
+ * polynomial per call). A job is admitted when the device memory the pool
+ * would then hold fits the HBM budget: every worker context's fixed
+ * allocations, plus per worker the larger of its stream-ordered pool's
+ * reservation and its running job's footprint. When nothing fits, idle
+ * workers' pools are trimmed first; the first queued job that fits starts (a
+ * job passed over more than twice the worker count is waited for), and with
+ * nothing running the oldest job runs alone even beyond the budget. Each job
+ * runs whir_commit_and_prove on its worker's context, so its proof is
+ * identical to the one-at-a-time result. */
 typedef struct whir_batch whir_batch;
 typedef struct {
   whir_protocol_params params;
@@ -370,6 +375,9 @@ int whir_job_footprint(const whir_protocol_params* params, int32_t n, int32_t po
 int whir_batch_create(int32_t device, int32_t workers, const whir_poseidon2_params* p16,
                       const whir_poseidon2_params* p24, uint64_t hbm_budget_bytes, whir_batch** out);
 int whir_batch_destroy(whir_batch* b);
+/* The admission accounting now: fixed device bytes of all worker contexts and
+ * the bytes their memory pools reserve. */
+int whir_batch_memory(whir_batch* b, uint64_t* fixed_bytes, uint64_t* pool_reserved_bytes);
 /* Enqueue (non-blocking). The job and its buffers must stay valid until it is done. */
 int whir_batch_submit(whir_batch* b, whir_job* job);
 /* Wait for one job (timeout_ms < 0: no limit); returns the job's status. */

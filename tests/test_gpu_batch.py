@@ -62,6 +62,69 @@ def test_admission_budget_limits_concurrency(pkg, gpu_ctx):
     check_against_single(pkg, gpu_ctx, jobs, reqs)
 
 
+def test_device_memory_stays_within_budget(pkg, gpu_ctx):
+    """A tight HBM budget with mixed sizes: the device memory in use
+    (cudaMemGetInfo, sampled every half millisecond while the pool runs) never
+    exceeds the budget by more than 64 MiB, jobs still run concurrently, and
+    every proof equals the one-at-a-time result."""
+    import threading
+
+    import torch
+
+    jobs = make_jobs(pkg, 24, 5, 14, 19)
+    workers = 6
+    with pkg.Batch(0, workers=1) as probe:
+        per_ctx = probe.memory()[0]
+    biggest = max(pkg.job_footprint(p, n) for p, n, _, _ in jobs)
+    budget = workers * per_ctx + int(2.5 * biggest)
+    torch.cuda.synchronize()
+    base = torch.cuda.mem_get_info()
+    base_used = base[1] - base[0]
+    peak = [0]
+    stop = threading.Event()
+
+    def sample():
+        while not stop.is_set():
+            free, total = torch.cuda.mem_get_info()
+            peak[0] = max(peak[0], total - free - base_used)
+            time.sleep(0.0005)
+
+    reqs = [pkg.ProofRequest(p, n, poly, pts if pts.size else None) for p, n, poly, pts in jobs]
+    th = threading.Thread(target=sample)
+    th.start()
+    try:
+        with pkg.Batch(0, workers=workers, hbm_budget_bytes=budget) as b:
+            b.run(reqs)
+            fixed, _ = b.memory()
+    finally:
+        stop.set()
+        th.join()
+    assert fixed == workers * per_ctx
+    assert peak[0] <= budget + (64 << 20), (peak[0], budget)
+    spans = sorted((r.job.t_start_ms, r.job.t_done_ms) for r in reqs)
+    overlapped = any(s1 < e0 for (s0, e0), (s1, e1) in zip(spans, spans[1:]))
+    assert overlapped, "the budget leaves room for two jobs, yet none ran concurrently"
+    check_against_single(pkg, gpu_ctx, jobs, reqs)
+
+
+def test_small_jobs_pass_a_large_waiting_one(pkg, gpu_ctx):
+    """First-fit admission: with a large job waiting for memory, a small job
+    queued behind it starts before it."""
+    big = make_jobs(pkg, 2, 11, 19, 19)
+    small = make_jobs(pkg, 1, 12, 12, 12)
+    jobs = [big[0], big[1], small[0]]
+    with pkg.Batch(0, workers=1) as probe:
+        per_ctx = probe.memory()[0]
+    fp_big = pkg.job_footprint(big[0][0], big[0][1])
+    fp_small = pkg.job_footprint(small[0][0], small[0][1])
+    budget = 3 * per_ctx + fp_big + 4 * fp_small  # one big job at a time, small ones beside it
+    reqs = [pkg.ProofRequest(p, n, poly, pts if pts.size else None) for p, n, poly, pts in jobs]
+    with pkg.Batch(0, workers=3, hbm_budget_bytes=budget) as b:
+        b.run(reqs)
+    assert reqs[2].job.t_start_ms < reqs[1].job.t_start_ms
+    check_against_single(pkg, gpu_ctx, jobs, reqs)
+
+
 def test_serving_requests_arriving_in_the_mix(pkg, gpu_ctx):
     """Requests submitted while others are on the GPU: each result is the
     same as proving it alone."""

@@ -143,6 +143,7 @@ _SIGS = {
     "whir_batch_create": (C.c_int, [_i32, _i32, C.POINTER(Poseidon2Params), C.POINTER(Poseidon2Params), C.c_uint64,
                                     C.POINTER(_vp)]),
     "whir_batch_destroy": (C.c_int, [_vp]),
+    "whir_batch_memory": (C.c_int, [_vp, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]),
     "whir_batch_submit": (C.c_int, [_vp, C.POINTER(Job)]),
     "whir_batch_wait": (C.c_int, [_vp, C.POINTER(Job), _i32]),
     "whir_batch_wait_all": (C.c_int, [_vp]),
@@ -849,6 +850,12 @@ class Batch:
 
     def submit(self, req: ProofRequest) -> None:
         _check(lib().whir_batch_submit(self.handle, C.byref(req.job)))
+
+    def memory(self) -> tuple[int, int]:
+        """(fixed device bytes of the worker contexts, bytes their pools reserve)."""
+        f, r = C.c_uint64(0), C.c_uint64(0)
+        _check(lib().whir_batch_memory(self.handle, C.byref(f), C.byref(r)))
+        return f.value, r.value
 
     def wait(self, req: ProofRequest, timeout_ms: int = -1) -> None:
         _check(lib().whir_batch_wait(self.handle, C.byref(req.job), timeout_ms))

@@ -1,15 +1,27 @@
 // Batched and served proving: a pool of worker threads, each owning one
 // context (one CUDA stream) on the same device, takes commit+prove jobs from
-// a FIFO queue. A job is admitted only when its device-memory footprint fits
-// the remaining HBM budget, so requests that arrive while others are running
+// a queue. A job is admitted only when the device memory the pool would then
+// hold fits the HBM budget, so requests that arrive while others are running
 // start as soon as a worker and memory free up, and their kernels overlap on
 // the device with the proofs already in flight. Every job runs the same code
 // path as whir_commit_and_prove, so each proof is identical to the one the
 // job would produce alone.
+//
+// Memory accounting. Each worker holds its context's fixed allocations
+// (tables, scratch, arena) and its stream-ordered pool, which keeps what it
+// has reserved between jobs. A worker counts as max(pool reservation,
+// footprint of its running job); admitting job j on worker w needs
+//   fixed(all workers) + sum over other workers + max(reserved(w), fp(j)) <= budget.
+// When that fails, idle workers' pools are trimmed (their cached blocks go
+// back to the driver) and the check is repeated. The first queued job that
+// fits is taken; a job passed over more than twice the worker count is
+// waited for (no job behind it starts first). With nothing running, the
+// oldest job starts even if it exceeds the budget on its own.
 #include <stdio.h>
 
 #include <chrono>
 #include <condition_variable>
+#include <algorithm>
 #include <deque>
 #include <mutex>
 #include <thread>
@@ -37,7 +49,9 @@ int ilog2u(uint64_t v) {
 struct whir_batch {
   int device = 0;
   size_t budget = 0;
-  size_t in_use = 0;
+  size_t fixed = 0;                 // fixed device bytes of all worker contexts
+  std::vector<size_t> running_fp;   // per worker: footprint of its running job, 0 when idle
+  uint32_t head_skips = 0;          // times the oldest job was passed over
   std::vector<whir_ctx*> ctxs;
   std::vector<std::thread> threads;
   std::mutex mu;
@@ -94,6 +108,49 @@ void run_job(whir_ctx* ctx, whir_job* j) {
   j->t_done_ms = now_ms();
 }
 
+uint64_t reserved(whir_ctx* c) {
+  uint64_t v = 0;
+  if (c->pool && cudaMemPoolGetAttribute(c->pool, cudaMemPoolAttrReservedMemCurrent, &v) != cudaSuccess) v = 0;
+  return v;
+}
+
+// Bytes the pool holds apart from worker `idx`'s pool reservation; called
+// with b->mu held.
+size_t others(whir_batch* b, int idx) {
+  size_t total = b->fixed;
+  for (size_t w = 0; w < b->ctxs.size(); w++)
+    if ((int)w != idx) total += std::max((size_t)reserved(b->ctxs[w]), b->running_fp[w]);
+  return total;
+}
+
+whir_job* take(whir_batch* b, size_t i) {
+  whir_job* j = b->queue[i];
+  b->queue.erase(b->queue.begin() + (std::ptrdiff_t)i);
+  b->head_skips = i == 0 ? 0 : b->head_skips + 1;
+  return j;
+}
+
+// The job worker `idx` takes next, or null; called with b->mu held.
+whir_job* pick(whir_batch* b, int idx) {
+  if (b->queue.empty()) return nullptr;
+  bool any_running = false;
+  for (size_t v : b->running_fp) any_running |= v != 0;
+  const bool head_only = b->head_skips > 2 * b->ctxs.size();
+  for (int attempt = 0; attempt < 2; attempt++) {
+    const size_t base = others(b, idx), mine = (size_t)reserved(b->ctxs[idx]);
+    for (size_t i = 0; i < b->queue.size() && (i == 0 || !head_only); i++)
+      if (base + std::max(mine, (size_t)b->queue[i]->footprint_bytes) <= b->budget) return take(b, i);
+    if (attempt == 0) {
+      // make room: idle workers (this one included) hand their cached
+      // blocks back to the driver
+      for (size_t w = 0; w < b->ctxs.size(); w++)
+        if (b->running_fp[w] == 0 && b->ctxs[w]->pool) cudaMemPoolTrimTo(b->ctxs[w]->pool, 0);
+    }
+  }
+  // nothing fits and nothing runs: the oldest job runs alone
+  return any_running ? nullptr : take(b, 0);
+}
+
 void worker(whir_batch* b, int idx) {
   whir_ctx* ctx = b->ctxs[idx];
   // a worker whose thread cannot select the device fails every job it takes
@@ -102,14 +159,13 @@ void worker(whir_batch* b, int idx) {
     whir_job* j = nullptr;
     {
       std::unique_lock<std::mutex> lk(b->mu);
-      b->cv_work.wait(lk, [&] {
-        return b->stop || (!b->queue.empty() && (b->in_use + b->queue.front()->footprint_bytes <= b->budget ||
-                                                 b->in_use == 0));
-      });
-      if (b->stop && b->queue.empty()) return;
-      j = b->queue.front();
-      b->queue.pop_front();
-      b->in_use += j->footprint_bytes;
+      for (;;) {
+        if (b->stop && b->queue.empty()) return;
+        j = pick(b, idx);
+        if (j) break;
+        b->cv_work.wait(lk);
+      }
+      b->running_fp[idx] = std::max<size_t>(j->footprint_bytes, 1);
     }
     if (dev_err == cudaSuccess) {
       run_job(ctx, j);
@@ -121,7 +177,7 @@ void worker(whir_batch* b, int idx) {
     }
     {
       std::lock_guard<std::mutex> lk(b->mu);
-      b->in_use -= j->footprint_bytes;
+      b->running_fp[idx] = 0;
       j->done = 1;
       b->pending--;
     }
@@ -158,9 +214,21 @@ int whir_batch_create(int32_t device, int32_t workers, const whir_poseidon2_para
       return s;
     }
     b->ctxs.push_back(c);
+    b->fixed += c->fixed_device_bytes;
   }
+  b->running_fp.assign((size_t)workers, 0);
   for (int i = 0; i < workers; i++) b->threads.emplace_back(worker, b, i);
   *out = b;
+  return WHIR_OK;
+}
+
+int whir_batch_memory(whir_batch* b, uint64_t* fixed_bytes, uint64_t* pool_reserved_bytes) {
+  WH_CHECK(b, "null batch");
+  std::lock_guard<std::mutex> lk(b->mu);
+  uint64_t r = 0;
+  for (whir_ctx* c : b->ctxs) r += reserved(c);
+  if (fixed_bytes) *fixed_bytes = b->fixed;
+  if (pool_reserved_bytes) *pool_reserved_bytes = r;
   return WHIR_OK;
 }
 

@@ -464,6 +464,12 @@ int whir_ctx_create(int32_t device, const whir_poseidon2_params* p16, const whir
       return wh::set_error("DFT table build failed"), fail(WHIR_ERR_CUDA);
   }
   if (cudaStreamSynchronize(c->stream) != cudaSuccess) return wh::set_error("initial sync failed"), fail(WHIR_ERR_CUDA);
+  {
+    const size_t gran = (size_t)2 << 20;
+    auto up = [gran](size_t b) { return (b + gran - 1) / gran * gran; };
+    c->fixed_device_bytes = up(wk::kDftStageTableWords * 4) + up(8192 * sizeof(ef)) + up(256 * sizeof(ef)) + up(64) +
+                            up(kArenaBytes) + up((size_t)wh::kDftLogHeights * wh::kDftTableWords * 4);
+  }
   *out = c;
   return WHIR_OK;
 }

@@ -121,6 +121,9 @@ struct whir_ctx {
   uint32_t* d_words = nullptr;   // 16 words: grind result, claim and done counters (0-2), sumcheck round (8),
                                  // dot product (9) and tree-top (10) counters, streamed-dot wait flag (11)
   void* d_arena = nullptr;       // general scratch (tables, gathers)
+  // device bytes the context holds outside its memory pool (tables, scratch,
+  // arena), each allocation rounded up to the driver's 2 MiB granularity
+  size_t fixed_device_bytes = 0;
   size_t arena_bytes = 0;
   void* h_pinned = nullptr;      // staging for small transfers
   size_t pinned_bytes = 0;
