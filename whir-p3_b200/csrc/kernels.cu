@@ -406,8 +406,11 @@ __host__ __device__ constexpr int bitrev(int x, int bits) {
 }
 
 // In-place DIF DFT of length 2^L <= 64 over registers: natural order in,
-// a[r] = X[bitrev_L(r)] out.
-template <int L>
+// a[r] = X[bitrev_L(r)] out. A difference that goes on to a twiddle product
+// stays unreduced (u - v + p < 2p): the Shoup product takes any 32-bit input.
+// ZERO_HIGH: the upper half of the input is zero, so the first stage is
+// a[j + M/2] = a[j] * omega^j with a[j] unchanged.
+template <int L, bool ZERO_HIGH = false>
 __device__ __forceinline__ void dif(uint32_t (&a)[1 << L]) {
   constexpr int M = 1 << L;
 #pragma unroll
@@ -416,11 +419,14 @@ __device__ __forceinline__ void dif(uint32_t (&a)[1 << L]) {
     for (int start = 0; start < M; start += 2 * half) {
 #pragma unroll
       for (int j = 0; j < half; j++) {
-        const uint32_t u = a[start + j], v = a[start + j + half];
-        a[start + j] = kb::add(u, v);
-        const uint32_t d = kb::sub(u, v);
         const int tj = j * (32 / half);  // omega_{2*half}^j = omega_64^(j * 32 / half)
-        a[start + j + half] = tj == 0 ? d : kb::mul_shoup(d, c_tw64.w[tj], c_tw64.s[tj]);
+        const uint32_t u = a[start + j], v = a[start + j + half];
+        if (ZERO_HIGH && half == M / 2) {
+          a[start + j + half] = tj == 0 ? u : kb::mul_shoup(u, c_tw64.w[tj], c_tw64.s[tj]);
+          continue;
+        }
+        a[start + j] = kb::add(u, v);
+        a[start + j + half] = tj == 0 ? kb::sub(u, v) : kb::mul_shoup(u - v + kb::P, c_tw64.w[tj], c_tw64.s[tj]);
       }
     }
   }
@@ -458,12 +464,24 @@ __global__ void __launch_bounds__(1 << (LG + LT))
   {
     uint32_t a[E];
     const uint32_t* xj = x + (size_t)j * L + i2_0 + t;
+    if (2 * L1 <= N) {
+      // a low-degree extension: the upper half of every column is padding
 #pragma unroll
-    for (int e = 0; e < E; e++) {
-      const int i1 = g + G * e;
-      a[e] = i1 < L1 ? __ldg(xj + (size_t)i1 * H2) : 0u;
+      for (int e = 0; e < E / 2; e++) {
+        const int i1 = g + G * e;
+        a[e] = i1 < L1 ? __ldg(xj + (size_t)i1 * H2) : 0u;
+      }
+#pragma unroll
+      for (int e = E / 2; e < E; e++) a[e] = 0u;
+      dftreg::dif<LE, true>(a);
+    } else {
+#pragma unroll
+      for (int e = 0; e < E; e++) {
+        const int i1 = g + G * e;
+        a[e] = i1 < L1 ? __ldg(xj + (size_t)i1 * H2) : 0u;
+      }
+      dftreg::dif<LE>(a);
     }
-    dftreg::dif<LE>(a);
 #pragma unroll
     for (int r = 0; r < E; r++) {
       constexpr int kshift = 12 - LE - LG;

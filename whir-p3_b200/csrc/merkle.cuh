@@ -298,6 +298,57 @@ __device__ __forceinline__ void coop_permute16(uint32_t (&x)[4], int q, const P2
   for (int j = 0; j < 4; j++) x[j] = to_mont(x[j]);
 }
 
+// The same permutation on Montgomery words (x * 2^32 mod p) in and out, for
+// latency-bound uses. Every linear step is the same on Montgomery words, the
+// round constants come in Montgomery form, and the S-box is two Montgomery
+// products (x^3 in Montgomery form): an integer-only dependent chain with no
+// conversion at either end. The internal rounds also take the cross-lane sum
+// off the dependent chain: with p_j = mu_j x_j the words after a round are
+// s + p_j, so the next round's sum of words 1..15 is 15 s + sum_{j>=1} p_j,
+// and that sum of products (two shuffles) runs beside the S-box; a round's
+// chain is S-box, one addition and the product by 15.
+__device__ __forceinline__ uint32_t cube_m(uint32_t a) { return kb::mul(kb::mul(a, a), a); }
+template <int MAT>
+__device__ __forceinline__ void coop_permute16_m(uint32_t (&x)[4], int q, const P2Consts& k) {
+  using namespace kb;
+  constexpr uint32_t k15s = (uint32_t)((15ull << 32) / P);  // Shoup constant of 15
+  coop_ext_layer<MAT>(x);
+#pragma unroll
+  for (int r = 0; r < p2::RF / 2; r++) {
+#pragma unroll
+    for (int j = 0; j < 4; j++) x[j] = cube_m(add(x[j], k.ext_rc_m[r * 16 + 4 * q + j]));
+    coop_ext_layer<MAT>(x);
+  }
+  // word 0 lives in w0 on every lane; lane 0's x[0] is not read again until
+  // the internal rounds end
+  uint32_t w0 = __shfl_sync(0xffffffffu, x[0], (threadIdx.x & 31) & ~3);
+  uint32_t o = add(add(q == 0 ? 0u : x[0], x[1]), add(x[2], x[3]));  // sum of words 1..15
+  o = add(o, __shfl_xor_sync(0xffffffffu, o, 1));
+  o = add(o, __shfl_xor_sync(0xffffffffu, o, 2));
+#pragma unroll
+  for (int r = 0; r < p2::RP16; r++) {
+    uint32_t pj[4];
+#pragma unroll
+    for (int j = 0; j < 4; j++) pj[j] = mul_shoup(x[j], k.diag_c[4 * q + j], k.diag_s[4 * q + j]);
+    uint32_t d = add(add(q == 0 ? 0u : pj[0], pj[1]), add(pj[2], pj[3]));  // sum of p_j, j >= 1
+    d = add(d, __shfl_xor_sync(0xffffffffu, d, 1));
+    d = add(d, __shfl_xor_sync(0xffffffffu, d, 2));
+    const uint32_t y0 = cube_m(add(w0, k.int_rc_m[r]));
+    const uint32_t s = add(o, y0);
+#pragma unroll
+    for (int j = 0; j < 4; j++) x[j] = add(s, pj[j]);
+    w0 = p2::diag_axpy(p2::diag_code(16, 0), s, y0);
+    o = add(mul_shoup(s, 15u, k15s), d);
+  }
+  if (q == 0) x[0] = w0;
+#pragma unroll
+  for (int r = p2::RF / 2; r < p2::RF; r++) {
+#pragma unroll
+    for (int j = 0; j < 4; j++) x[j] = cube_m(add(x[j], k.ext_rc_m[r * 16 + 4 * q + j]));
+    coop_ext_layer<MAT>(x);
+  }
+}
+
 // Compresses `levels` levels above the `cnt` nodes in sh (8 words each), one
 // four-lane group per node pair, writing every new level to global; `base` is
 // the first node's index in its level, `off` and `lsz` the level's offset and
@@ -623,7 +674,12 @@ __global__ void __launch_bounds__(GRIND_CTA) k_grind(const __grid_constant__ P2C
       return;
     }
     const uint64_t w = start + threadIdx.x;
-    if (w < limit && (p2::grind_word7<SLOT, MAT>((uint32_t)w, cp, p16) & mask) == 0u) atomicMin(result, (uint32_t)w);
+    // a witness below this claim's first candidate makes the claim useless, so
+    // its threads may stop early; they read the same condition (up to a
+    // witness landing between their reads), and a stopped candidate is never
+    // one the smallest witness could be
+    const auto stop = [result, start] { return (uint64_t)*(volatile uint32_t*)result < start; };
+    if (w < limit && (p2::grind_word7<SLOT, MAT>((uint32_t)w, cp, p16, stop) & mask) == 0u) atomicMin(result, (uint32_t)w);
   }
 }
 

@@ -28,6 +28,8 @@ p2::P2Consts to_consts(const whir_poseidon2_params& p) {
     k.diag_c[i] = p.diag[i];
     k.diag_s[i] = kb::shoup_const(p.diag[i]);
   }
+  for (int i = 0; i < 8 * 24; i++) k.ext_rc_m[i] = kb::to_mont(p.ext_rc[i]);
+  for (int i = 0; i < 32; i++) k.int_rc_m[i] = kb::to_mont(p.int_rc[i]);
   return k;
 }
 

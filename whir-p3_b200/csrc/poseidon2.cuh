@@ -54,6 +54,8 @@ struct P2Consts {
   uint32_t int_rc[32];      // canonical
   uint32_t diag_c[24];      // the fixed diagonal, canonical (run-time indexed uses)
   uint32_t diag_s[24];      // kb::shoup_const(diag_c)
+  uint32_t ext_rc_m[8 * 24];  // ext_rc in Montgomery form (permutations run on Montgomery words)
+  uint32_t int_rc_m[32];      // int_rc in Montgomery form
 };
 
 // Internal diagonal codes: an integer v in [-4, 4] \ {0} is v itself;
@@ -370,8 +372,14 @@ inline void grind_fold_rt(uint32_t (&state)[16], const P2Consts& k) {
   if (k.mat == (uint32_t)kMatHl) grind_fold<kMatHl>(state, k);
   else grind_fold<kMatMds>(state, k);
 }
-template <int SLOT, int MAT>
-KB_HD uint32_t grind_word7(uint32_t w, const uint32_t (&cp)[16], const P2Consts& k) {
+// `stop()` is asked twice, after the first full rounds and after the partial
+// rounds; when it answers true the search no longer needs this candidate and
+// the form returns 0xffffffff (nonzero in any low bits) without finishing.
+struct NeverStop {
+  KB_HD bool operator()() const { return false; }
+};
+template <int SLOT, int MAT, typename Stop = NeverStop>
+KB_HD uint32_t grind_word7(uint32_t w, const uint32_t (&cp)[16], const P2Consts& k, Stop stop = Stop()) {
   using namespace kb;
   constexpr int kJ = ext_col_bound<MAT>();
   uint32_t wm[kJ];  // w * j mod p, j < kJ
@@ -385,8 +393,10 @@ KB_HD uint32_t grind_word7(uint32_t w, const uint32_t (&cp)[16], const P2Consts&
   ext_layer<16, MAT>(x);
 #pragma unroll 1
   for (int r = 1; r < RF / 2; r++) full_round<16, MAT>(x, k.ext_rc + r * 16);
+  if (stop()) return 0xffffffffu;
 #pragma unroll 1
   for (int r = 0; r < RP16; r++) partial_round<16>(x, k.int_rc[r]);
+  if (stop()) return 0xffffffffu;
 #pragma unroll 1
   for (int r = RF / 2; r < RF - 1; r++) full_round<16, MAT>(x, k.ext_rc + r * 16);
   const uint32_t* rc = k.ext_rc + (RF - 1) * 16;
