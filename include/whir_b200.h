@@ -145,6 +145,14 @@ int whir_ctx_stage_times(whir_ctx* ctx, double* ms, uint64_t* counts, int32_t ca
  * Poseidon2-16 permutation each); other stages 0. Writes min(8, cap) entries;
  * returns the stage count. */
 int whir_ctx_stage_work(whir_ctx* ctx, uint64_t* work, int32_t cap, int32_t reset);
+/* Where the transcript steps of a sumcheck stage run (the folding rounds of
+ * Prover::round, src/whir/prover/mod.rs:305-325, and the final sumcheck):
+ * enable = 1 queues each stage's coefficient kernels, challenger steps
+ * (DuplexChallenger observe / sample / grind on the device) and folds without
+ * the host in between, then replays the stage's log on the host challenger;
+ * enable = 0 (default) makes one host round trip per step. Proofs are the
+ * same either way. */
+int whir_ctx_set_device_transcript(whir_ctx* ctx, int32_t enable);
 /* Host permutation with the context's data (width taken from the state length 16 or 24). */
 int whir_poseidon2_permute(const whir_ctx* ctx, uint32_t* state, int32_t width);
 
@@ -344,10 +352,14 @@ int whir_commit_and_prove(whir_ctx* ctx, const whir_protocol_params* params, int
  * polynomial per call). A job is admitted when the device memory the pool
  * would then hold fits the HBM budget: every worker context's fixed
  * allocations, plus per worker the larger of its stream-ordered pool's
- * reservation and its running job's footprint. When nothing fits, idle
+ * reservation and its running job's charge (footprint plus one 32 MiB pool
+ * chunk, the granule in which the pool reserves memory). When nothing fits, idle
  * workers' pools are trimmed first; the first queued job that fits starts (a
  * job passed over more than twice the worker count is waited for), and with
- * nothing running the oldest job runs alone even beyond the budget. Each job
+ * nothing running the oldest job runs alone even beyond the budget. The first
+ * proof of a new shape also tunes its launch shapes (whir_tune_set_mode) on
+ * scratch arrays outside the footprint; a server that must stay within its
+ * budget proves each shape once before taking traffic. Each job
  * runs whir_commit_and_prove on its worker's context, so its proof is
  * identical to the one-at-a-time result. */
 typedef struct whir_batch whir_batch;

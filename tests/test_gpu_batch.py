@@ -73,9 +73,19 @@ def test_device_memory_stays_within_budget(pkg, gpu_ctx):
 
     jobs = make_jobs(pkg, 24, 5, 14, 19)
     workers = 6
+    # the first proof of a shape tunes its launch shapes on scratch arrays
+    # outside the job's footprint: tune every shape first, as a server warms up
+    seen = set()
+    for p, n, poly, pts in jobs:
+        key = (p.folding_factor.rest, p.starting_log_inv_rate, p.rs_domain_initial_reduction_factor, n)
+        if key not in seen:
+            seen.add(key)
+            pkg.commit_and_prove(gpu_ctx, p, n, poly, pts if pts.size else None)
     with pkg.Batch(0, workers=1) as probe:
         per_ctx = probe.memory()[0]
-    biggest = max(pkg.job_footprint(p, n) for p, n, _, _ in jobs)
+    # a job is charged its footprint plus one 32 MiB pool chunk: room for two
+    # of the largest
+    biggest = max(pkg.job_footprint(p, n) for p, n, _, _ in jobs) + (32 << 20)
     budget = workers * per_ctx + int(2.5 * biggest)
     torch.cuda.synchronize()
     base = torch.cuda.mem_get_info()
@@ -110,14 +120,17 @@ def test_device_memory_stays_within_budget(pkg, gpu_ctx):
 def test_small_jobs_pass_a_large_waiting_one(pkg, gpu_ctx):
     """First-fit admission: with a large job waiting for memory, a small job
     queued behind it starts before it."""
-    big = make_jobs(pkg, 2, 11, 19, 19)
+    big = make_jobs(pkg, 2, 11, 21, 21)
     small = make_jobs(pkg, 1, 12, 12, 12)
     jobs = [big[0], big[1], small[0]]
+    for p, n, poly, pts in (big[0], small[0]):  # tune both shapes first
+        pkg.commit_and_prove(gpu_ctx, p, n, poly, pts if pts.size else None)
     with pkg.Batch(0, workers=1) as probe:
         per_ctx = probe.memory()[0]
-    fp_big = pkg.job_footprint(big[0][0], big[0][1])
-    fp_small = pkg.job_footprint(small[0][0], small[0][1])
-    budget = 3 * per_ctx + fp_big + 4 * fp_small  # one big job at a time, small ones beside it
+    # charges: footprint plus one 32 MiB pool chunk
+    fp_big = max(pkg.job_footprint(p, n) for p, n, _, _ in big) + (32 << 20)
+    fp_small = pkg.job_footprint(small[0][0], small[0][1]) + (32 << 20)
+    budget = 3 * per_ctx + fp_big + fp_small + fp_small // 2  # one big job at a time, a small one beside it
     reqs = [pkg.ProofRequest(p, n, poly, pts if pts.size else None) for p, n, poly, pts in jobs]
     with pkg.Batch(0, workers=3, hbm_budget_bytes=budget) as b:
         b.run(reqs)

@@ -161,3 +161,25 @@ def test_e2e_n26_verified(pkg, gpu_ctx, oracle):
     assert rc == 0 and np.array_equal(vcp, cp)
     for i in range(4):
         assert np.array_equal(evals[4 * i:4 * i + 4], oracle.eval_base(poly, pts[4 * n * i:4 * n * (i + 1)]))
+
+
+@pytest.mark.parametrize("n,f,rs,pw", [(12, 3, 1, 10), (18, 4, 3, 16), (20, 4, 1, 16)])
+def test_device_transcript_matches_host_round_trips(pkg, gpu_ctx, oracle, n, f, rs, pw):
+    """Sumcheck stages with the transcript on the device and with one host
+    round trip per step (the default) give the same proof, equal to the
+    oracle's."""
+    rng = np.random.default_rng(4400 + n)
+    poly = rnd(rng, 1 << n)
+    pts = rnd(rng, 4 * n)
+    params = pkg.ProtocolParameters(100, pw, pkg.FoldingFactor.constant(f), pkg.SecurityAssumption.CapacityBound, 1,
+                                    rs, "poseidon2_24", 32)
+    out = []
+    for device in (False, True):
+        gpu_ctx.set_device_transcript(device)
+        try:
+            out.append(pkg.commit_and_prove(gpu_ctx, params, n, poly, pts))
+        finally:
+            gpu_ctx.set_device_transcript(False)
+    assert np.array_equal(out[0][0], out[1][0]) and np.array_equal(out[0][1], out[1][1])
+    ref, ref_cp = oracle.prove(make_params(100, pw, f, None, 2, 1, rs, 0, 32), n, poly, pts)
+    assert np.array_equal(out[1][0], ref) and np.array_equal(out[1][1], ref_cp)

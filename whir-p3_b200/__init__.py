@@ -106,6 +106,7 @@ _SIGS = {
     "whir_ctx_set_profiling": (C.c_int, [_vp, _i32]),
     "whir_ctx_stage_times": (C.c_int, [_vp, _vp, _vp, _i32, _i32]),
     "whir_ctx_stage_work": (C.c_int, [_vp, _vp, _i32, _i32]),
+    "whir_ctx_set_device_transcript": (C.c_int, [_vp, _i32]),
     "whir_config_new": (C.c_int, [C.POINTER(_Params), _i32, C.POINTER(_Config)]),
     "whir_domain_separator": (C.c_int, [C.POINTER(_Config), _i32, _vp, _i32]),
     "whir_challenger_init": (None, [C.POINTER(_Chal)]),
@@ -415,6 +416,11 @@ class Context:
         cnt = np.zeros(8, dtype=np.uint64)
         _check(lib().whir_ctx_stage_times(self.handle, ms.ctypes.data, cnt.ctypes.data, 8, int(reset)))
         return {name: (float(m), int(c)) for name, m, c in zip(self.STAGES, ms, cnt)}
+
+    def set_device_transcript(self, enable: bool) -> None:
+        """Sumcheck stages with their transcript steps on the device, or with
+        one host round trip per step (default); the proofs are the same."""
+        _check(lib().whir_ctx_set_device_transcript(self.handle, int(enable)))
 
     def stage_work(self, reset: bool = True) -> dict:
         """Work per stage while profiling was on: DFT algorithmic bytes, Merkle

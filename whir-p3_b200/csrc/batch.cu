@@ -9,9 +9,11 @@
 //
 // Memory accounting. Each worker holds its context's fixed allocations
 // (tables, scratch, arena) and its stream-ordered pool, which keeps what it
-// has reserved between jobs. A worker counts as max(pool reservation,
-// footprint of its running job); admitting job j on worker w needs
-//   fixed(all workers) + sum over other workers + max(reserved(w), fp(j)) <= budget.
+// has reserved between jobs. The pools reserve memory in chunks (32 MiB on
+// B200, measured), so a job is charged its footprint plus one chunk. A worker
+// counts as max(pool reservation, charge of its running job); admitting job j
+// on worker w needs
+//   fixed(all workers) + sum over other workers + max(reserved(w), charge(j)) <= budget.
 // When that fails, idle workers' pools are trimmed (their cached blocks go
 // back to the driver) and the check is repeated. The first queued job that
 // fits is taken; a job passed over more than twice the worker count is
@@ -50,7 +52,7 @@ struct whir_batch {
   int device = 0;
   size_t budget = 0;
   size_t fixed = 0;                 // fixed device bytes of all worker contexts
-  std::vector<size_t> running_fp;   // per worker: footprint of its running job, 0 when idle
+  std::vector<size_t> running_fp;   // per worker: charge of its running job, 0 when idle
   uint32_t head_skips = 0;          // times the oldest job was passed over
   std::vector<whir_ctx*> ctxs;
   std::vector<std::thread> threads;
@@ -108,6 +110,11 @@ void run_job(whir_ctx* ctx, whir_job* j) {
   j->t_done_ms = now_ms();
 }
 
+// the pool's reservation granule: a job may grow its worker's pool by up to
+// one chunk beyond its footprint
+constexpr size_t kPoolChunk = (size_t)32 << 20;
+size_t charge(const whir_job* j) { return (size_t)j->footprint_bytes + kPoolChunk; }
+
 uint64_t reserved(whir_ctx* c) {
   uint64_t v = 0;
   if (c->pool && cudaMemPoolGetAttribute(c->pool, cudaMemPoolAttrReservedMemCurrent, &v) != cudaSuccess) v = 0;
@@ -139,7 +146,7 @@ whir_job* pick(whir_batch* b, int idx) {
   for (int attempt = 0; attempt < 2; attempt++) {
     const size_t base = others(b, idx), mine = (size_t)reserved(b->ctxs[idx]);
     for (size_t i = 0; i < b->queue.size() && (i == 0 || !head_only); i++)
-      if (base + std::max(mine, (size_t)b->queue[i]->footprint_bytes) <= b->budget) return take(b, i);
+      if (base + std::max(mine, charge(b->queue[i])) <= b->budget) return take(b, i);
     if (attempt == 0) {
       // make room: idle workers (this one included) hand their cached
       // blocks back to the driver
@@ -165,7 +172,7 @@ void worker(whir_batch* b, int idx) {
         if (j) break;
         b->cv_work.wait(lk);
       }
-      b->running_fp[idx] = std::max<size_t>(j->footprint_bytes, 1);
+      b->running_fp[idx] = charge(j);
     }
     if (dev_err == cudaSuccess) {
       run_job(ctx, j);

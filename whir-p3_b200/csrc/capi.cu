@@ -456,6 +456,8 @@ int whir_ctx_create(int32_t device, const whir_poseidon2_params* p16, const whir
     return wh::set_error("mapped allocation failed"), fail(WHIR_ERR_NOMEM);
   memset(c->h_mail, 0, (wk::kMailWords + 32) * 4);
   // twiddle tables of every subgroup height (the stage tables come with them)
+  if (cudaMalloc(&c->d_tr, wh::kDevTrWords * 4) != cudaSuccess)
+    return wh::set_error("device allocation failed"), fail(WHIR_ERR_NOMEM);
   if (cudaMalloc(&c->tw_heights, wh::kDftLogHeights * wh::kDftTableWords * 4) != cudaSuccess)
     return wh::set_error("device allocation failed"), fail(WHIR_ERR_NOMEM);
   for (int lh = 0; lh < wh::kDftLogHeights; lh++) {
@@ -468,7 +470,8 @@ int whir_ctx_create(int32_t device, const whir_poseidon2_params* p16, const whir
     const size_t gran = (size_t)2 << 20;
     auto up = [gran](size_t b) { return (b + gran - 1) / gran * gran; };
     c->fixed_device_bytes = up(wk::kDftStageTableWords * 4) + up(8192 * sizeof(ef)) + up(256 * sizeof(ef)) + up(64) +
-                            up(kArenaBytes) + up((size_t)wh::kDftLogHeights * wh::kDftTableWords * 4);
+                            up(kArenaBytes) + up((size_t)wh::kDftLogHeights * wh::kDftTableWords * 4) +
+                            up(wh::kDevTrWords * 4);
   }
   *out = c;
   return WHIR_OK;
@@ -483,6 +486,7 @@ int whir_ctx_destroy(whir_ctx* c) {
   cudaSetDevice(c->device);
   if (c->stream) cudaStreamSynchronize(c->stream);
   cudaFree(c->tw_heights);
+  cudaFree(c->d_tr);
   for (auto& rec : c->stage_events) {
     cudaEventDestroy(rec.second.first);
     cudaEventDestroy(rec.second.second);
@@ -550,6 +554,12 @@ int whir_ctx_stage_times(whir_ctx* ctx, double* ms, uint64_t* counts, int32_t ca
       ctx->stage_launches[i] = 0;
     }
   return wh::kStCount;
+}
+
+int whir_ctx_set_device_transcript(whir_ctx* ctx, int32_t enable) {
+  WH_TRY(check_ctx(ctx));
+  ctx->device_transcript = enable != 0;
+  return WHIR_OK;
 }
 
 int whir_ctx_stage_work(whir_ctx* ctx, uint64_t* work, int32_t cap, int32_t reset) {

@@ -101,6 +101,13 @@ enum Stage { kStDft = 0, kStLeaves, kStNodes, kStGrind, kStSumcheck, kStEval, kS
 constexpr int kDftLogHeights = 25;  // heights 2^0 .. 2^24
 constexpr size_t kDftTableWords = 2 * 4096;
 constexpr int kUploadGroups = 8;  // chunk groups of a pipelined polynomial upload
+// device transcript area: DevChal at word 0, the search's folded state at
+// kTrCp, the error word at kTrErr, then per sumcheck round (kTrRound words):
+// c0 and c2 (8 words), the witness and its evaluated-claim count (2), the
+// sampled challenge (4 words, at offset 12)
+constexpr int kDevTrWords = 1024;
+constexpr int kTrCp = 40, kTrErr = 64, kTrLog = 68, kTrRound = 16;
+constexpr int kTrMaxRounds = (kDevTrWords - kTrLog) / kTrRound;
 
 }  // namespace wh
 
@@ -121,6 +128,10 @@ struct whir_ctx {
   uint32_t* d_words = nullptr;   // 16 words: grind result, claim and done counters (0-2), sumcheck round (8),
                                  // dot product (9) and tree-top (10) counters, streamed-dot wait flag (11)
   void* d_arena = nullptr;       // general scratch (tables, gathers)
+  // device transcript area (kDevTrWords words): the device challenger, the
+  // folded state of the next search, an error word and per-round logs of a
+  // sumcheck stage run with the transcript on the device
+  uint32_t* d_tr = nullptr;
   // device bytes the context holds outside its memory pool (tables, scratch,
   // arena), each allocation rounded up to the driver's 2 MiB granularity
   size_t fixed_device_bytes = 0;
@@ -143,6 +154,9 @@ struct whir_ctx {
   cudaEvent_t up_ev[wh::kUploadGroups + 1] = {};
   // stage timing
   bool profiling = false;
+  // run a sumcheck stage's transcript steps on the device (see
+  // whir_ctx_set_device_transcript); off: each step round-trips to the host
+  bool device_transcript = false;
   std::vector<cudaEvent_t> event_pool;
   std::vector<std::pair<int, std::pair<cudaEvent_t, cudaEvent_t>>> stage_events;
   double stage_ms[wh::kStCount] = {};

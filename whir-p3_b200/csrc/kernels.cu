@@ -676,6 +676,7 @@ constexpr size_t kDftTwBytes = 2048 * 4;
 constexpr size_t kDftTileMax = 128 * 1024;
 constexpr size_t kDftSmemMax = kDftTwBytes + kDftTileMax;
 constexpr size_t kSelectSmemMax = 160 * 1024;
+template <int R>
 __global__ void k_add_select(ef* __restrict__ w, size_t N, int lo_bits, const uint32_t* __restrict__ pow_lo,
                              const uint32_t* __restrict__ pow_hi, const ef* __restrict__ g, int m, int hi_bits);
 static std::once_flag g_attr_once;
@@ -687,7 +688,8 @@ static void init_smem_attributes() {
     cudaFuncSetAttribute(k_dft_rows<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kDftSmemMax);
     cudaFuncSetAttribute(k_dft_coset<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kDftSmemMax);
     cudaFuncSetAttribute(k_dft_coset<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kDftSmemMax);
-    cudaFuncSetAttribute(k_add_select, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSelectSmemMax);
+    cudaFuncSetAttribute(k_add_select<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSelectSmemMax);
+    cudaFuncSetAttribute(k_add_select<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSelectSmemMax);
   });
 }
 
@@ -907,10 +909,34 @@ cudaError_t grind_reset(uint32_t* result, uint32_t* counter, uint32_t* done, cud
 
 cudaError_t grind(const uint32_t* state, const uint32_t* in, int in_len, int bits, uint64_t limit,
                   uint32_t* result, uint32_t* counter, uint32_t* done, uint32_t* mail, uint32_t seq,
-                  const P2Consts& p16, cudaStream_t st) {
+                  const P2Consts& p16, cudaStream_t st, const uint32_t* cp_dev, uint32_t* res_out) {
   if (p16.mat == (uint32_t)p2::kMatHl)
-    return grind_m<p2::kMatHl>(state, in, in_len, bits, limit, result, counter, done, mail, seq, p16, st);
-  return grind_m<p2::kMatMds>(state, in, in_len, bits, limit, result, counter, done, mail, seq, p16, st);
+    return grind_m<p2::kMatHl>(state, in, in_len, bits, limit, result, counter, done, mail, seq, p16, st, cp_dev,
+                               res_out);
+  return grind_m<p2::kMatMds>(state, in, in_len, bits, limit, result, counter, done, mail, seq, p16, st, cp_dev,
+                              res_out);
+}
+
+__global__ void k_chal_set(DevChal* ch, const __grid_constant__ DevChal init, uint32_t* err) {
+  *ch = init;
+  *err = 0u;
+}
+
+cudaError_t chal_set(DevChal* ch, const DevChal& init, uint32_t* err, cudaStream_t st) {
+  k_chal_set<<<1, 1, 0, st>>>(ch, init, err);
+  LAUNCH_DONE();
+}
+
+cudaError_t chal_coeffs(DevChal* ch, const ef* coeffs, int grind_next, uint32_t* cp_out, ef* r_out,
+                        const P2Consts& p16, cudaStream_t st) {
+  if (p16.mat == (uint32_t)p2::kMatHl) return chal_coeffs_m<p2::kMatHl>(ch, coeffs, grind_next, cp_out, r_out, p16, st);
+  return chal_coeffs_m<p2::kMatMds>(ch, coeffs, grind_next, cp_out, r_out, p16, st);
+}
+
+cudaError_t chal_witness(DevChal* ch, const uint32_t* w_res, int bits, ef* r_out, uint32_t* err, const P2Consts& p16,
+                         cudaStream_t st) {
+  if (p16.mat == (uint32_t)p2::kMatHl) return chal_witness_m<p2::kMatHl>(ch, w_res, bits, r_out, err, p16, st);
+  return chal_witness_m<p2::kMatMds>(ch, w_res, bits, r_out, err, p16, st);
 }
 
 cudaError_t merkle_build(const uint32_t* rows, int log_h, int row_words, int leaf_hash, uint32_t* digests,
@@ -1465,9 +1491,11 @@ cudaError_t sumcheck_coeffs(const ef* f, const ef* w, size_t half, ef* partials,
 template <bool FOLD>
 __global__ void __launch_bounds__(256) k_sumcheck_round(ef* __restrict__ f, ef* __restrict__ w, size_t q, ef r,
                                                          ef* __restrict__ partials, unsigned* __restrict__ counter,
-                                                         ef* __restrict__ out, uint32_t* mail, uint32_t seq) {
+                                                         ef* __restrict__ out, uint32_t* mail, uint32_t seq,
+                                                         const ef* __restrict__ r_dev) {
   __shared__ ef sh[2][32];
   __shared__ bool s_last;
+  if (FOLD && r_dev) r = ld_ef(r_dev);
   ef v[2] = {kb::ef_zero(), kb::ef_zero()};
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < q; i += (size_t)gridDim.x * blockDim.x) {
     ef el, eh, wl, wh;
@@ -1518,13 +1546,13 @@ __global__ void __launch_bounds__(256) k_sumcheck_round(ef* __restrict__ f, ef* 
 }
 
 cudaError_t sumcheck_round(ef* f, ef* w, size_t q, int fold, ef r, ef* partials, unsigned* counter, ef* out,
-                           uint32_t* mail, uint32_t seq, cudaStream_t st) {
+                           uint32_t* mail, uint32_t seq, cudaStream_t st, const ef* r_dev) {
   if (q == 0) return cudaErrorInvalidValue;
   const unsigned b = grid_for(q, 256, 8);
   if (fold)
-    k_sumcheck_round<true><<<b, 256, 0, st>>>(f, w, q, r, partials, counter, out, mail, seq);
+    k_sumcheck_round<true><<<b, 256, 0, st>>>(f, w, q, r, partials, counter, out, mail, seq, r_dev);
   else
-    k_sumcheck_round<false><<<b, 256, 0, st>>>(f, w, q, r, partials, counter, out, mail, seq);
+    k_sumcheck_round<false><<<b, 256, 0, st>>>(f, w, q, r, partials, counter, out, mail, seq, r_dev);
   LAUNCH_DONE();
 }
 
@@ -1588,43 +1616,58 @@ cudaError_t select_tables(const uint32_t* vars, int m, int n, int lo_bits, uint3
   LAUNCH_DONE();
 }
 
-// Each CTA covers whole runs of 2^lo_bits >= blockDim consecutive x, so all its
-// threads share xh and the per-constraint factor g[s]*pow_hi[s][xh] is formed
-// once per CTA in shared memory.
+// W[x] += sum_s g[s] * v_s^x with x = xh * 2^lo_bits + xl and
+// v_s^x = v_s^(xh * 2^lo_bits) * v_s^xl. A tile is R consecutive xh by blockDim
+// consecutive xl: the CTA forms the R x m factors g[s] * pow_hi[s][xh] once in
+// shared memory, and each thread loads the low power pow_lo[s][xl] once per
+// constraint for its R outputs (R-fold fewer table loads than one output per
+// thread).
+template <int R>
 __global__ void k_add_select(ef* __restrict__ w, size_t N, int lo_bits, const uint32_t* __restrict__ pow_lo,
                              const uint32_t* __restrict__ pow_hi, const ef* __restrict__ g, int m, int hi_bits) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  ef* cs = reinterpret_cast<ef*>(smem_raw);
+  ef* cs = reinterpret_cast<ef*>(smem_raw);  // [R][m]
   const size_t Lc = (size_t)1 << lo_bits, Hc = (size_t)1 << hi_bits;
-  for (size_t x0 = (size_t)blockIdx.x * blockDim.x; x0 < N; x0 += (size_t)gridDim.x * blockDim.x) {
-    const size_t xh = x0 >> lo_bits;
+  const size_t col_tiles = Lc / blockDim.x, tiles = (Hc / R) * col_tiles;
+  for (size_t tile = blockIdx.x; tile < tiles; tile += gridDim.x) {
+    const size_t xh0 = (tile / col_tiles) * R, xl = (tile % col_tiles) * blockDim.x + threadIdx.x;
     __syncthreads();
-    for (int s = threadIdx.x; s < m; s += blockDim.x)
-      cs[s] = kb::ef_mul_base(ld_ef(g + s), __ldg(pow_hi + s * Hc + xh));
+    for (int i = threadIdx.x; i < R * m; i += blockDim.x) {
+      const int r = i / m, s = i - r * m;
+      cs[i] = kb::ef_mul_base(ld_ef(g + s), __ldg(pow_hi + s * Hc + xh0 + r));
+    }
     __syncthreads();
-    const size_t x = x0 + threadIdx.x;
-    const size_t xl = x & (Lc - 1);
-    ef acc = ld_ef(w + x);
-    // four constraints per step: their loads are issued together, then the
-    // four products (< 4p^2 < 2^64 per coefficient) are summed and reduced once
+    ef acc[R];
+#pragma unroll
+    for (int r = 0; r < R; r++) acc[r] = ld_ef(w + (xh0 + r) * Lc + xl);
+    // four constraints per step: the products of a coefficient (< 4p^2 < 2^64)
+    // are summed and reduced once
     int s = 0;
     const uint32_t* pp = pow_lo + xl;  // row s of the power table at pp
     for (; s + 4 <= m; s += 4, pp += 4 * Lc) {
       uint32_t pv[4];
 #pragma unroll
       for (int u = 0; u < 4; u++) pv[u] = __ldg(pp + u * Lc);
-      uint64_t t[4] = {0, 0, 0, 0};
 #pragma unroll
-      for (int u = 0; u < 4; u++) {
-        const ef c = cs[s + u];
+      for (int r = 0; r < R; r++) {
+        uint64_t tq[4] = {0, 0, 0, 0};
 #pragma unroll
-        for (int q = 0; q < 4; q++) t[q] += (uint64_t)c.c[q] * pv[u];
+        for (int u = 0; u < 4; u++) {
+          const ef c = cs[r * m + s + u];
+#pragma unroll
+          for (int q = 0; q < 4; q++) tq[q] += (uint64_t)c.c[q] * pv[u];
+        }
+        acc[r] = kb::ef_add(acc[r], ef{{kb::reduce_wide(tq[0]), kb::reduce_wide(tq[1]), kb::reduce_wide(tq[2]),
+                                        kb::reduce_wide(tq[3])}});
       }
-      acc = kb::ef_add(acc, ef{{kb::reduce_wide(t[0]), kb::reduce_wide(t[1]), kb::reduce_wide(t[2]),
-                                kb::reduce_wide(t[3])}});
     }
-    for (; s < m; s++) acc = kb::ef_add(acc, kb::ef_mul_base(cs[s], __ldg(pow_lo + (size_t)s * Lc + xl)));
-    st_ef(w + x, acc);
+    for (; s < m; s++) {
+      const uint32_t pv = __ldg(pow_lo + (size_t)s * Lc + xl);
+#pragma unroll
+      for (int r = 0; r < R; r++) acc[r] = kb::ef_add(acc[r], kb::ef_mul_base(cs[r * m + s], pv));
+    }
+#pragma unroll
+    for (int r = 0; r < R; r++) st_ef(w + (xh0 + r) * Lc + xl, acc[r]);
   }
 }
 
@@ -1633,11 +1676,19 @@ cudaError_t add_select(ef* w, int n, const uint32_t* pow_lo, const uint32_t* pow
   if (m <= 0) return cudaSuccess;
   const size_t N = (size_t)1 << n;
   const int threads = (int)(N < 256 ? N : 256);
-  if (((size_t)1 << lo_bits) < (size_t)threads) return cudaErrorInvalidValue;
-  const size_t smem = (size_t)m * sizeof(ef);
-  if (smem > kSelectSmemMax) return cudaErrorInvalidValue;
+  if (((size_t)1 << lo_bits) < (size_t)threads || lo_bits > n) return cudaErrorInvalidValue;
+  const size_t Hc = (size_t)1 << (n - lo_bits);
   init_smem_attributes();
-  k_add_select<<<grid_for(N, threads), threads, smem, st>>>(w, N, lo_bits, pow_lo, pow_hi, g, m, n - lo_bits);
+  if (Hc >= 4) {
+    const size_t smem = (size_t)4 * m * sizeof(ef);
+    if (smem > kSelectSmemMax) return cudaErrorInvalidValue;
+    k_add_select<4><<<grid_for(N / 4, threads), threads, smem, st>>>(w, N, lo_bits, pow_lo, pow_hi, g, m,
+                                                                       n - lo_bits);
+  } else {
+    const size_t smem = (size_t)m * sizeof(ef);
+    if (smem > kSelectSmemMax) return cudaErrorInvalidValue;
+    k_add_select<1><<<grid_for(N, threads), threads, smem, st>>>(w, N, lo_bits, pow_lo, pow_hi, g, m, n - lo_bits);
+  }
   LAUNCH_DONE();
 }
 

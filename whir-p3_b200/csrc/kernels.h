@@ -144,9 +144,41 @@ cudaError_t merkle_open(const uint32_t* rows, const uint32_t* digests, int log_h
 // Search state (result = p, counters 0) before the first search with a
 // mailbox on these words; each such search leaves it reset for the next.
 cudaError_t grind_reset(uint32_t* result, uint32_t* counter, uint32_t* done, cudaStream_t st);
+// With `cp_dev` set, the folded initial state (16 canonical words, see
+// p2::grind_fold) is read from device memory instead of being formed from
+// `state` and `in` on the host (in_len still selects the witness position);
+// with `res_out` set, the last CTA to stop writes the witness and the number of
+// evaluated claims there (2 words) and resets the search state, and no
+// initialising launch precedes the search.
 cudaError_t grind(const uint32_t* state, const uint32_t* in, int in_len, int bits, uint64_t limit,
                   uint32_t* result, uint32_t* counter, uint32_t* done, uint32_t* mail, uint32_t seq,
-                  const p2::P2Consts& p16, cudaStream_t st);
+                  const p2::P2Consts& p16, cudaStream_t st, const uint32_t* cp_dev = nullptr,
+                  uint32_t* res_out = nullptr);
+
+// Duplex challenger on the device (DuplexChallenger<F, Poseidon2-16, 16, 8>),
+// Montgomery words, laid out like the host's challenger: sponge state, pending
+// inputs, buffered outputs. The steps below run in one warp with the four-lane
+// permutation, so a chain of sumcheck rounds, searches and challenges can be
+// queued without the host in between.
+struct DevChal {
+  uint32_t st[16];
+  uint32_t in[8];
+  int32_t in_len;
+  uint32_t out[8];
+  int32_t out_len;
+};
+// set the device challenger to `init` and clear *err (no host synchronisation)
+cudaError_t chal_set(DevChal* ch, const DevChal& init, uint32_t* err, cudaStream_t st);
+// observe coeffs[0], coeffs[1] (c0 then c2, 8 words); then, with grind_next,
+// write the folded initial state of the next proof-of-work search (16
+// canonical words) to cp_out; otherwise sample an extension element into r_out
+cudaError_t chal_coeffs(DevChal* ch, const kb::ef* coeffs, int grind_next, uint32_t* cp_out, kb::ef* r_out,
+                        const p2::P2Consts& p16, cudaStream_t st);
+// observe the witness w_res[0] (canonical; p means none was found), check
+// that sample_bits(bits) is 0, then sample an extension element into r_out;
+// a failed check sets bit 0 (no witness) or bit 1 (check failed) of *err
+cudaError_t chal_witness(DevChal* ch, const uint32_t* w_res, int bits, kb::ef* r_out, uint32_t* err,
+                         const p2::P2Consts& p16, cudaStream_t st);
 
 // The Poseidon2 launchers above for one external block MAT (p2::kMatMds or
 // p2::kMatHl), each form built in its own translation unit; merkle_leaves,
@@ -160,7 +192,13 @@ cudaError_t merkle_upper_m(int log_h, uint32_t* digests, const p2::P2Consts& p16
 template <int MAT>
 cudaError_t grind_m(const uint32_t* state, const uint32_t* in, int in_len, int bits, uint64_t limit,
                     uint32_t* result, uint32_t* counter, uint32_t* done, uint32_t* mail, uint32_t seq,
-                    const p2::P2Consts& p16, cudaStream_t st);
+                    const p2::P2Consts& p16, cudaStream_t st, const uint32_t* cp_dev, uint32_t* res_out);
+template <int MAT>
+cudaError_t chal_coeffs_m(DevChal* ch, const kb::ef* coeffs, int grind_next, uint32_t* cp_out, kb::ef* r_out,
+                          const p2::P2Consts& p16, cudaStream_t st);
+template <int MAT>
+cudaError_t chal_witness_m(DevChal* ch, const uint32_t* w_res, int bits, kb::ef* r_out, uint32_t* err,
+                           const p2::P2Consts& p16, cudaStream_t st);
 
 // eq table of `h` coordinates scaled by `scale`: out[x] = scale * prod eq(z_j, bit_j(x)), MSB <-> z[0].
 struct EqPoint {
@@ -211,8 +249,10 @@ cudaError_t sumcheck_coeffs(const kb::ef* f, const kb::ef* w, size_t half, kb::e
 // `counter` (device, one word) must hold 0 before the first launch; the
 // kernel leaves it at 0. With `mail` set, (c0, c2) are also posted to that
 // mailbox with flag `seq`.
+// With r_dev set, the fold's challenge is read from device memory (r_dev[0])
+// instead of `r`.
 cudaError_t sumcheck_round(kb::ef* f, kb::ef* w, size_t q, int fold, kb::ef r, kb::ef* partials, unsigned* counter,
-                           kb::ef* out, uint32_t* mail, uint32_t seq, cudaStream_t st);
+                           kb::ef* out, uint32_t* mail, uint32_t seq, cudaStream_t st, const kb::ef* r_dev = nullptr);
 
 // The same reduction with the block count capped at max_blocks, so that the
 // partials fit a fixed-size buffer (2 * max_blocks entries).

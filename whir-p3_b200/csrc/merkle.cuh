@@ -240,9 +240,10 @@ __global__ void __launch_bounds__(CTA) k_merkle_two_levels(uint32_t* __restrict_
 // Width-16 Poseidon2 spread over four consecutive lanes (q = lane & 3 holds
 // state words 4q .. 4q+3). The M4 blocks are lane-local; the cross-chunk sums
 // of the external layer and the full sum of the internal layer take two
-// xor-shuffle steps. About four times the per-permutation latency saving of a
-// one-thread permutation, for the narrow top levels of a tree. All 32 lanes
-// of the warp must call it together.
+// xor-shuffle steps. For the narrow top levels of a tree, where one
+// permutation's latency sets the time (measured on B200: 6.5 thousand cycles
+// for the canonical-value form of this layout against 12 thousand for a
+// one-thread permutation). All 32 lanes of the warp must call it together.
 template <int MAT>
 __device__ __forceinline__ void coop_ext_layer(uint32_t (&x)[4]) {
   using namespace kb;
@@ -256,64 +257,24 @@ __device__ __forceinline__ void coop_ext_layer(uint32_t (&x)[4]) {
   for (int j = 0; j < 4; j++) x[j] = add(x[j], s[j]);
 }
 
-template <int MAT>
-__device__ __forceinline__ void coop_permute16(uint32_t (&x)[4], int q, const P2Consts& k) {
-  using namespace kb;
-#pragma unroll
-  for (int j = 0; j < 4; j++) x[j] = from_mont(x[j]);
-  coop_ext_layer<MAT>(x);
-#pragma unroll
-  for (int r = 0; r < p2::RF / 2; r++) {
-#pragma unroll
-    for (int j = 0; j < 4; j++) x[j] = p2::cube_sum(x[j], k.ext_rc[r * 16 + 4 * q + j]);
-    coop_ext_layer<MAT>(x);
-  }
-  // Internal rounds with word 0 replicated in all four lanes (w0): every lane
-  // computes its S-box, so the result needs no broadcast, and the sum of the
-  // other fifteen words (lane-local, then two shuffles) is independent of it,
-  // which leaves S-box, one addition and the diagonal product of word 0 as
-  // the round's dependent chain.
-  uint32_t w0 = __shfl_sync(0xffffffffu, x[0], (threadIdx.x & 31) & ~3);
-  // fully unrolled: round constants become immediate constant-bank operands,
-  // off the dependent chain of this latency-bound form
-#pragma unroll
-  for (int r = 0; r < p2::RP16; r++) {
-    uint32_t o = add(add(q == 0 ? 0u : x[0], x[1]), add(x[2], x[3]));
-    o = add(o, __shfl_xor_sync(0xffffffffu, o, 1));
-    o = add(o, __shfl_xor_sync(0xffffffffu, o, 2));
-    const uint32_t y0 = p2::cube_sum(w0, k.int_rc[r]);
-    const uint32_t s = add(o, y0);
-#pragma unroll
-    for (int j = 0; j < 4; j++) x[j] = add(s, mul_shoup(x[j], k.diag_c[4 * q + j], k.diag_s[4 * q + j]));
-    w0 = p2::diag_axpy(p2::diag_code(16, 0), s, y0);
-    if (q == 0) x[0] = w0;
-  }
-#pragma unroll
-  for (int r = p2::RF / 2; r < p2::RF; r++) {
-#pragma unroll
-    for (int j = 0; j < 4; j++) x[j] = p2::cube_sum(x[j], k.ext_rc[r * 16 + 4 * q + j]);
-    coop_ext_layer<MAT>(x);
-  }
-#pragma unroll
-  for (int j = 0; j < 4; j++) x[j] = to_mont(x[j]);
-}
-
-// The same permutation on Montgomery words (x * 2^32 mod p) in and out, for
-// latency-bound uses. Every linear step is the same on Montgomery words, the
+// The permutation runs on Montgomery words (x * 2^32 mod p) in and out, the
+// form the digests are stored in. Every linear step is the same on Montgomery words, the
 // round constants come in Montgomery form, and the S-box is two Montgomery
 // products (x^3 in Montgomery form): an integer-only dependent chain with no
 // conversion at either end. The internal rounds also take the cross-lane sum
 // off the dependent chain: with p_j = mu_j x_j the words after a round are
 // s + p_j, so the next round's sum of words 1..15 is 15 s + sum_{j>=1} p_j,
 // and that sum of products (two shuffles) runs beside the S-box; a round's
-// chain is S-box, one addition and the product by 15.
+// chain is S-box, one addition and the product by 15. ROLLED keeps the round
+// loops rolled: a kernel that permutes once or twice (the challenger steps)
+// would otherwise spend its time fetching the unrolled code.
 __device__ __forceinline__ uint32_t cube_m(uint32_t a) { return kb::mul(kb::mul(a, a), a); }
-template <int MAT>
+template <int MAT, bool ROLLED = false>
 __device__ __forceinline__ void coop_permute16_m(uint32_t (&x)[4], int q, const P2Consts& k) {
   using namespace kb;
   constexpr uint32_t k15s = (uint32_t)((15ull << 32) / P);  // Shoup constant of 15
   coop_ext_layer<MAT>(x);
-#pragma unroll
+#pragma unroll(ROLLED ? 1 : p2::RF / 2)
   for (int r = 0; r < p2::RF / 2; r++) {
 #pragma unroll
     for (int j = 0; j < 4; j++) x[j] = cube_m(add(x[j], k.ext_rc_m[r * 16 + 4 * q + j]));
@@ -325,7 +286,7 @@ __device__ __forceinline__ void coop_permute16_m(uint32_t (&x)[4], int q, const 
   uint32_t o = add(add(q == 0 ? 0u : x[0], x[1]), add(x[2], x[3]));  // sum of words 1..15
   o = add(o, __shfl_xor_sync(0xffffffffu, o, 1));
   o = add(o, __shfl_xor_sync(0xffffffffu, o, 2));
-#pragma unroll
+#pragma unroll(ROLLED ? 1 : p2::RP16)
   for (int r = 0; r < p2::RP16; r++) {
     uint32_t pj[4];
 #pragma unroll
@@ -341,7 +302,7 @@ __device__ __forceinline__ void coop_permute16_m(uint32_t (&x)[4], int q, const 
     o = add(mul_shoup(s, 15u, k15s), d);
   }
   if (q == 0) x[0] = w0;
-#pragma unroll
+#pragma unroll(ROLLED ? 1 : p2::RF / 2)
   for (int r = p2::RF / 2; r < p2::RF; r++) {
 #pragma unroll
     for (int j = 0; j < 4; j++) x[j] = cube_m(add(x[j], k.ext_rc_m[r * 16 + 4 * q + j]));
@@ -368,7 +329,7 @@ __device__ __forceinline__ void coop_levels(uint32_t* sh, int cnt, int levels, s
     // a warp holds groups 8w .. 8w+7: warps with none of this level's pairs
     // skip the permutation (warp-uniform, so its shuffles stay full-warp),
     // which leaves the upper levels latency-bound rather than issue-bound
-    if ((t >> 5) * 8 < act) coop_permute16<MAT>(x, q, comp);
+    if ((t >> 5) * 8 < act) coop_permute16_m<MAT>(x, q, comp);
     __syncthreads();
     off += lsz;
     lsz >>= 1;
@@ -408,7 +369,7 @@ __global__ void __launch_bounds__(CTA) k_merkle_two_levels_coop(uint32_t* __rest
       // children 4j + 2h and 4j + 2h + 1: 16 consecutive words
       const uint4 v = *reinterpret_cast<const uint4*>(digests + (in_off + 4 * j + 2 * h) * 8 + 4 * q);
       uint32_t x[4] = {v.x, v.y, v.z, v.w};
-      coop_permute16<MAT>(x, q, comp);
+      coop_permute16_m<MAT>(x, q, comp);
       if (on && q < 2)
         *reinterpret_cast<uint4*>(digests + (mid_off + 2 * j + h) * 8 + 4 * q) = make_uint4(x[0], x[1], x[2], x[3]);
       // the parent's state: the first child's digest on lanes 0-1, the
@@ -424,7 +385,7 @@ __global__ void __launch_bounds__(CTA) k_merkle_two_levels_coop(uint32_t* __rest
         }
       }
     }
-    coop_permute16<MAT>(keep, q, comp);
+    coop_permute16_m<MAT>(keep, q, comp);
     if (on && q < 2)
       *reinterpret_cast<uint4*>(digests + (top_off + j) * 8 + 4 * q) = make_uint4(keep[0], keep[1], keep[2], keep[3]);
   }
@@ -638,12 +599,17 @@ template <int SLOT, int MAT>
 __global__ void __launch_bounds__(GRIND_CTA) k_grind(const __grid_constant__ P2Consts p16, uint4 st0, uint4 st1,
                                                       uint4 st2, uint4 st3, int bits, uint64_t limit,
                                                       uint32_t* result, uint32_t* counter, uint32_t* done,
-                                                      uint32_t* mail, uint32_t seq) {
+                                                      uint32_t* mail, uint32_t seq, const uint32_t* cp_dev,
+                                                      uint32_t* res_out) {
   __shared__ uint64_t s_start;
   __shared__ int s_go;
   const uint32_t mask = (1u << bits) - 1u;
-  const uint32_t cp[16] = {st0.x, st0.y, st0.z, st0.w, st1.x, st1.y, st1.z, st1.w,
-                           st2.x, st2.y, st2.z, st2.w, st3.x, st3.y, st3.z, st3.w};
+  uint32_t cp[16] = {st0.x, st0.y, st0.z, st0.w, st1.x, st1.y, st1.z, st1.w,
+                     st2.x, st2.y, st2.z, st2.w, st3.x, st3.y, st3.z, st3.w};
+  if (cp_dev) {
+#pragma unroll
+    for (int i = 0; i < 16; i++) cp[i] = __ldcg(cp_dev + i);
+  }
   for (;;) {
     if (threadIdx.x == 0) {
       const uint64_t start = (uint64_t)atomicAdd(counter, 1u) * GRIND_CTA;
@@ -661,11 +627,15 @@ __global__ void __launch_bounds__(GRIND_CTA) k_grind(const __grid_constant__ P2C
       // claim that it did not evaluate) and resets the search state for the
       // next search (every other CTA has finished with it), which then needs
       // no initialising launch
-      if (threadIdx.x == 0 && mail) {
+      if (threadIdx.x == 0 && (mail || res_out)) {
         __threadfence();
         if (atomicAdd(done, 1u) == gridDim.x - 1) {
           const uint32_t post[2] = {atomicAdd(result, 0u), atomicAdd(counter, 0u) - gridDim.x};
-          mail_post(mail, post, 2, seq);
+          if (mail) mail_post(mail, post, 2, seq);
+          if (res_out) {
+            res_out[0] = post[0];
+            res_out[1] = post[1];
+          }
           *result = kb::P;
           *counter = 0u;
           *done = 0u;
@@ -688,20 +658,23 @@ __global__ void __launch_bounds__(GRIND_CTA) k_grind(const __grid_constant__ P2C
 template <int MAT>
 cudaError_t grind_m(const uint32_t* state, const uint32_t* in, int in_len, int bits, uint64_t limit,
                     uint32_t* result, uint32_t* counter, uint32_t* done, uint32_t* mail, uint32_t seq,
-                    const P2Consts& p16, cudaStream_t st) {
+                    const P2Consts& p16, cudaStream_t st, const uint32_t* cp_dev, uint32_t* res_out) {
   if (in_len < 0 || in_len > 7 || bits < 0 || bits > 30) return cudaErrorInvalidValue;
   if (limit > kb::P) limit = kb::P;
   // the sponge state with the pending inputs, canonical (a witness w < p is
   // its own canonical value), with 0 at the witness position; then its
-  // external layer plus the first round constants
-  uint32_t s[16];
-  for (int i = 0; i < 16; i++) s[i] = kb::from_mont(state[i]);
-  for (int i = 0; i < in_len; i++) s[i] = kb::from_mont(in[i]);
-  s[in_len] = 0u;
-  p2::grind_fold<MAT>(s, p16);
-  // with a mailbox the previous search left the state reset (grind_reset
-  // initialises it once per context)
-  if (!mail) {
+  // external layer plus the first round constants (read from cp_dev instead
+  // when the device challenger prepared them)
+  uint32_t s[16] = {0u};
+  if (!cp_dev) {
+    for (int i = 0; i < 16; i++) s[i] = kb::from_mont(state[i]);
+    for (int i = 0; i < in_len; i++) s[i] = kb::from_mont(in[i]);
+    s[in_len] = 0u;
+    p2::grind_fold<MAT>(s, p16);
+  }
+  // with a mailbox or a result slot the previous search left the state reset
+  // (grind_reset initialises it once per context)
+  if (!mail && !res_out) {
     const cudaError_t e = grind_reset(result, counter, done, st);
     if (e != cudaSuccess) return e;
   }
@@ -732,10 +705,146 @@ cudaError_t grind_m(const uint32_t* state, const uint32_t* in, int in_len, int b
   }
   switch (in_len) {
 #define WK_GRIND(S) \
-  case S: k_grind<S, MAT><<<blocks, GRIND_CTA, 0, st>>>(p16, a, b, c, d, bits, limit, result, counter, done, mail, seq); break;
+  case S:                                                                                                      \
+    k_grind<S, MAT><<<blocks, GRIND_CTA, 0, st>>>(p16, a, b, c, d, bits, limit, result, counter, done, mail, seq, \
+                                                  cp_dev, res_out);                                             \
+    break;
     WK_GRIND(0) WK_GRIND(1) WK_GRIND(2) WK_GRIND(3) WK_GRIND(4) WK_GRIND(5) WK_GRIND(6) WK_GRIND(7)
 #undef WK_GRIND
   }
+  LAUNCH_DONE();
+}
+
+// ---------------------------------------------------------------------------
+// Duplex challenger steps on the device (DuplexChallenger observe / sample /
+// sample_bits, the transcript calls of SumcheckData::observe_and_sample,
+// src/whir/proof.rs:163-193). One warp runs each step: lane 0 keeps the input
+// and output buffers in shared memory, and a duplexing permutes the sponge
+// state with the four-lane permutation (every four-lane group computes it;
+// group 0's result is kept). The state is Montgomery words, as the host's.
+// ---------------------------------------------------------------------------
+
+namespace {
+
+template <int MAT>
+__device__ void dc_duplex(DevChal& c, const P2Consts& k) {
+  const int lane = threadIdx.x & 31, q = lane & 3;
+  __syncwarp();
+  if (lane == 0) {
+    for (int i = 0; i < c.in_len; i++) c.st[i] = c.in[i];
+    c.in_len = 0;
+  }
+  __syncwarp();
+  uint32_t x[4];
+#pragma unroll
+  for (int j = 0; j < 4; j++) x[j] = c.st[4 * q + j];
+  __syncwarp();
+  coop_permute16_m<MAT, true>(x, q, k);
+  if (lane < 4) {
+#pragma unroll
+    for (int j = 0; j < 4; j++) c.st[4 * lane + j] = x[j];
+  }
+  __syncwarp();
+  if (lane == 0) {
+    for (int i = 0; i < 8; i++) c.out[i] = c.st[i];
+    c.out_len = 8;
+  }
+  __syncwarp();
+}
+
+template <int MAT>
+__device__ void dc_observe(DevChal& c, uint32_t v, const P2Consts& k) {
+  __syncwarp();
+  if ((threadIdx.x & 31) == 0) {
+    c.out_len = 0;
+    c.in[c.in_len++] = v;
+  }
+  __syncwarp();
+  if (c.in_len == 8) dc_duplex<MAT>(c, k);
+}
+
+template <int MAT>
+__device__ uint32_t dc_sample(DevChal& c, const P2Consts& k) {
+  __syncwarp();
+  if (c.in_len > 0 || c.out_len == 0) dc_duplex<MAT>(c, k);
+  const uint32_t v = c.out[c.out_len - 1];
+  __syncwarp();
+  if ((threadIdx.x & 31) == 0) c.out_len--;
+  __syncwarp();
+  return v;
+}
+
+__device__ void dc_load(DevChal& c, const DevChal* g) {
+  const uint32_t* src = reinterpret_cast<const uint32_t*>(g);
+  uint32_t* dst = reinterpret_cast<uint32_t*>(&c);
+  for (int i = threadIdx.x & 31; i < (int)(sizeof(DevChal) / 4); i += 32) dst[i] = __ldcg(src + i);
+  __syncwarp();
+}
+__device__ void dc_store(const DevChal& c, DevChal* g) {
+  __syncwarp();
+  const uint32_t* src = reinterpret_cast<const uint32_t*>(&c);
+  uint32_t* dst = reinterpret_cast<uint32_t*>(g);
+  for (int i = threadIdx.x & 31; i < (int)(sizeof(DevChal) / 4); i += 32) dst[i] = src[i];
+}
+
+template <int MAT>
+__global__ void __launch_bounds__(32) k_chal_coeffs(DevChal* ch, const ef* coeffs, int grind_next, uint32_t* cp_out,
+                                                     ef* r_out, const __grid_constant__ P2Consts k) {
+  __shared__ DevChal c;
+  dc_load(c, ch);
+  for (int i = 0; i < 8; i++) dc_observe<MAT>(c, __ldcg(coeffs[i >> 2].c + (i & 3)), k);
+  if (grind_next) {
+    // the sponge state with the pending inputs and 0 at the witness position,
+    // canonical, through the initial external layer plus the first constants
+    if ((threadIdx.x & 31) == 0) {
+      uint32_t s[16];
+      for (int i = 0; i < 16; i++) s[i] = kb::from_mont(c.st[i]);
+      for (int i = 0; i < c.in_len; i++) s[i] = kb::from_mont(c.in[i]);
+      s[c.in_len] = 0u;
+      p2::grind_fold<MAT>(s, k);
+      for (int i = 0; i < 16; i++) cp_out[i] = s[i];
+    }
+  } else {
+    ef r;
+    for (int i = 0; i < 4; i++) r.c[i] = dc_sample<MAT>(c, k);
+    if ((threadIdx.x & 31) == 0) *r_out = r;
+  }
+  dc_store(c, ch);
+}
+
+template <int MAT>
+__global__ void __launch_bounds__(32) k_chal_witness(DevChal* ch, const uint32_t* w_res, int bits, ef* r_out,
+                                                      uint32_t* err, const __grid_constant__ P2Consts k) {
+  __shared__ DevChal c;
+  dc_load(c, ch);
+  const uint32_t w = __ldcg(w_res);
+  if (w >= kb::P) {  // no witness: leave the transcript as it is
+    if ((threadIdx.x & 31) == 0) atomicOr(err, 1u);
+    return;
+  }
+  dc_observe<MAT>(c, kb::to_mont(w), k);
+  const uint32_t v = kb::from_mont(dc_sample<MAT>(c, k));
+  if ((v & ((1u << bits) - 1u)) != 0u && (threadIdx.x & 31) == 0) atomicOr(err, 2u);
+  ef r;
+  for (int i = 0; i < 4; i++) r.c[i] = dc_sample<MAT>(c, k);
+  if ((threadIdx.x & 31) == 0) *r_out = r;
+  dc_store(c, ch);
+}
+
+}  // namespace
+
+template <int MAT>
+cudaError_t chal_coeffs_m(DevChal* ch, const ef* coeffs, int grind_next, uint32_t* cp_out, ef* r_out,
+                          const P2Consts& p16, cudaStream_t st) {
+  k_chal_coeffs<MAT><<<1, 32, 0, st>>>(ch, coeffs, grind_next, cp_out, r_out, p16);
+  LAUNCH_DONE();
+}
+
+template <int MAT>
+cudaError_t chal_witness_m(DevChal* ch, const uint32_t* w_res, int bits, ef* r_out, uint32_t* err,
+                           const P2Consts& p16, cudaStream_t st) {
+  if (bits < 1 || bits > 30) return cudaErrorInvalidValue;
+  k_chal_witness<MAT><<<1, 32, 0, st>>>(ch, w_res, bits, r_out, err, p16);
   LAUNCH_DONE();
 }
 

@@ -9,5 +9,10 @@ template cudaError_t merkle_leaves_m<p2::kMatMds>(const uint32_t*, int, int, int
 template cudaError_t merkle_upper_m<p2::kMatMds>(int, uint32_t*, const p2::P2Consts&, Shape, unsigned*, uint32_t*,
                                                  uint32_t, int*, cudaStream_t);
 template cudaError_t grind_m<p2::kMatMds>(const uint32_t*, const uint32_t*, int, int, uint64_t, uint32_t*, uint32_t*,
-                                          uint32_t*, uint32_t*, uint32_t, const p2::P2Consts&, cudaStream_t);
+                                          uint32_t*, uint32_t*, uint32_t, const p2::P2Consts&, cudaStream_t,
+                                          const uint32_t*, uint32_t*);
+template cudaError_t chal_coeffs_m<p2::kMatMds>(DevChal*, const kb::ef*, int, uint32_t*, kb::ef*, const p2::P2Consts&,
+                                          cudaStream_t);
+template cudaError_t chal_witness_m<p2::kMatMds>(DevChal*, const uint32_t*, int, kb::ef*, uint32_t*, const p2::P2Consts&,
+                                           cudaStream_t);
 }  // namespace wk

@@ -322,6 +322,119 @@ int sumcheck_round(whir_ctx* ctx, wh::Chal& ch, Sumcheck& sd, ef* d_f, ef* d_w, 
   return WHIR_OK;
 }
 
+// The rounds of one sumcheck stage (k rounds over arrays of 2^m0 entries,
+// pending fold included) with every transcript step on the device: each
+// round's coefficients kernel is followed by a one-warp challenger kernel that
+// observes (c0, c2) and either samples the folding challenge or prepares the
+// proof-of-work search, whose last CTA hands the witness to a second
+// challenger kernel that observes it, checks it and samples the challenge; the
+// next round's kernel folds by that challenge from device memory. The host
+// queues the whole stage without waiting, tracking only the challenger's
+// buffer lengths (they do not depend on values, and they select the search's
+// witness position), then fetches the stage's log once and replays it on its
+// own challenger, which must sample the same challenges.
+int sumcheck_stage_device(whir_ctx* ctx, wh::Chal& ch, Sumcheck& sd, ef* d_f, ef* d_w, int m0, int k, ef* sum,
+                          int pow_bits, std::vector<ef>* rs, PendingFold& pend) {
+  wk::DevChal* dch = reinterpret_cast<wk::DevChal*>(ctx->d_tr);
+  uint32_t* cp = ctx->d_tr + wh::kTrCp;
+  uint32_t* err = ctx->d_tr + wh::kTrErr;
+  auto log_c = [&](int j) { return reinterpret_cast<ef*>(ctx->d_tr + wh::kTrLog + wh::kTrRound * j); };
+  auto log_w = [&](int j) { return ctx->d_tr + wh::kTrLog + wh::kTrRound * j + 8; };
+  auto log_r = [&](int j) { return reinterpret_cast<ef*>(ctx->d_tr + wh::kTrLog + wh::kTrRound * j + 12); };
+  static_assert(sizeof(wk::DevChal) == sizeof(uint32_t) * 34 && sizeof(wk::DevChal) <= 4 * wh::kTrCp, "layout");
+  wk::DevChal init;
+  memcpy(init.st, ch.st, sizeof(init.st));
+  memcpy(init.in, ch.in, sizeof(init.in));
+  init.in_len = ch.in_len;
+  memcpy(init.out, ch.out, sizeof(init.out));
+  init.out_len = ch.out_len;
+  WH_TRY_CUDA(wk::chal_set(dch, init, err, ctx->stream));
+  int in_len = ch.in_len, out_len = ch.out_len;  // the challenger's buffer lengths as the device runs
+  auto observed = [&] {
+    out_len = 0;
+    if (++in_len == 8) {
+      in_len = 0;
+      out_len = 8;
+    }
+  };
+  auto sampled = [&] {
+    if (in_len > 0 || out_len == 0) {
+      in_len = 0;
+      out_len = 8;
+    }
+    out_len--;
+  };
+  for (int j = 0; j < k; j++) {
+    const size_t half = (size_t)1 << (m0 - j - 1);
+    const bool fold = j > 0 || pend.on;
+    WH_CHECK(j > 0 || !pend.on || pend.half == 2 * half, "pending fold does not match the round size");
+    {
+      wh::StageTimer timer(ctx, wh::kStSumcheck);
+      WH_TRY_CUDA(wk::sumcheck_round(d_f, d_w, half, fold ? 1 : 0, j == 0 && pend.on ? pend.r : kb::ef_zero(),
+                                     ctx->d_partials, round_counter(ctx), log_c(j), nullptr, 0u, ctx->stream,
+                                     j > 0 ? log_r(j - 1) : nullptr));
+    }
+    for (int i = 0; i < 8; i++) observed();
+    WH_TRY_CUDA(wk::chal_coeffs(dch, log_c(j), pow_bits > 0, cp, log_r(j), ctx->p16, ctx->stream));
+    if (pow_bits > 0) {
+      {
+        wh::StageTimer timer(ctx, wh::kStGrind);
+        WH_TRY_CUDA(wk::grind(nullptr, nullptr, in_len, pow_bits, kb::P, ctx->d_words, ctx->d_words + 1,
+                              ctx->d_words + 2, nullptr, 0u, ctx->p16, ctx->stream, cp, log_w(j)));
+      }
+      observed();
+      sampled();
+      WH_TRY_CUDA(wk::chal_witness(dch, log_w(j), pow_bits, log_r(j), err, ctx->p16, ctx->stream));
+    }
+    for (int i = 0; i < 4; i++) sampled();
+  }
+  std::vector<uint32_t> lg((size_t)(wh::kTrLog - wh::kTrErr) + (size_t)wh::kTrRound * k);
+  WH_TRY(wh::fetch(ctx, lg.data(), err, lg.size() * 4));
+  if (lg[0] != 0u) {
+    wh::set_error(lg[0] & 1u ? "proof-of-work search found no witness" : "device grinding returned an invalid witness");
+    return (lg[0] & 1u) ? WHIR_ERR_NOT_FOUND : WHIR_ERR_CUDA;
+  }
+  for (int j = 0; j < k; j++) {
+    const uint32_t* rec = lg.data() + (wh::kTrLog - wh::kTrErr) + wh::kTrRound * j;
+    const ef c0{{rec[0], rec[1], rec[2], rec[3]}}, c2{{rec[4], rec[5], rec[6], rec[7]}};
+    const ef rd{{rec[12], rec[13], rec[14], rec[15]}};
+    sd.polys.push_back(c0);
+    sd.polys.push_back(c2);
+    sd.npolys++;
+    ch.observe_ef(ctx->hp16, c0);
+    ch.observe_ef(ctx->hp16, c2);
+    if (pow_bits > 0) {
+      const uint32_t w = rec[8];
+      wh::add_stage_work(ctx, wh::kStGrind, (uint64_t)rec[9] * 256u);
+      ch.observe(ctx->hp16, kb::to_mont(w));
+      if (ch.sample_bits(ctx->hp16, pow_bits) != 0) return wh::set_error("device grinding returned an invalid witness"), WHIR_ERR_CUDA;
+      sd.pows.push_back(w);
+    }
+    const ef r = ch.sample_ef(ctx->hp16);
+    if (!kb::ef_eq(r, rd)) return wh::set_error("device transcript diverged from the host's"), WHIR_ERR_CUDA;
+    *sum = extrapolate_012(c0, kb::ef_sub(*sum, c0), c2, r);
+    if (rs) rs->push_back(r);
+    pend.on = true;
+    pend.r = r;
+    pend.half = (size_t)1 << (m0 - j - 1);
+  }
+  return WHIR_OK;
+}
+
+// The rounds of one sumcheck stage: on the device when the context allows it,
+// else one host round trip per transcript step (sumcheck_round).
+int sumcheck_stage(whir_ctx* ctx, wh::Chal& ch, Sumcheck& sd, ef* d_f, ef* d_w, int m0, int k, ef* sum, int pow_bits,
+                   std::vector<ef>* rs, PendingFold& pend) {
+  if (ctx->device_transcript && ctx->d_tr && k >= 1 && k <= wh::kTrMaxRounds)
+    return sumcheck_stage_device(ctx, ch, sd, d_f, d_w, m0, k, sum, pow_bits, rs, pend);
+  for (int j = 0; j < k; j++) {
+    ef r;
+    WH_TRY(sumcheck_round(ctx, ch, sd, d_f, d_w, m0 - j, sum, pow_bits, &r, pend));
+    if (rs) rs->push_back(r);
+  }
+  return WHIR_OK;
+}
+
 // InitialStatement::evaluate for the split strategy: partial evaluations over
 // the first k0 variables, then the full evaluation.
 int evaluate_constraint(whir_ctx* ctx, whir_witness* w, const std::vector<ef>& point, Constraint* out) {
@@ -534,11 +647,7 @@ int do_prove(whir_ctx* ctx, whir_witness* wit, wh::Chal& ch) {
     WH_TRY(wh::add_select_vars(ctx, d_w, nv, svars, spow));
     Sumcheck sd;
     fold_rs.clear();
-    for (int j = 0; j < ffn; j++) {
-      ef r;
-      WH_TRY(sumcheck_round(ctx, ch, sd, d_f, d_w, nv - j, &sum, rc.folding_pow_bits, &r, pend));
-      fold_rs.push_back(r);
-    }
+    WH_TRY(sumcheck_stage(ctx, ch, sd, d_f, d_w, nv, ffn, &sum, rc.folding_pow_bits, &fold_rs, pend));
     sd.emit(pf);
     nv -= ffn;
     if (prev_owned) free_tree(ctx, prev);
@@ -566,10 +675,8 @@ int do_prove(whir_ctx* ctx, whir_witness* wit, wh::Chal& ch) {
     WH_TRY(open_queries(ctx, prev, idx, pf, rows));
     if (c.final_sumcheck_rounds > 0) {
       Sumcheck sd;
-      for (int j = 0; j < c.final_sumcheck_rounds; j++) {
-        ef r;
-        WH_TRY(sumcheck_round(ctx, ch, sd, d_f, d_w, nv - j, &sum, c.final_folding_pow_bits, &r, pend));
-      }
+      WH_TRY(sumcheck_stage(ctx, ch, sd, d_f, d_w, nv, c.final_sumcheck_rounds, &sum, c.final_folding_pow_bits,
+                            nullptr, pend));
       pf.push_back(1u);
       sd.emit(pf);
     } else {
