@@ -390,6 +390,9 @@ int whir_batch_destroy(whir_batch* b);
 /* The admission accounting now: fixed device bytes of all worker contexts and
  * the bytes their memory pools reserve. */
 int whir_batch_memory(whir_batch* b, uint64_t* fixed_bytes, uint64_t* pool_reserved_bytes);
+/* whir_ctx_set_device_transcript on every worker context; jobs that start
+ * afterwards use the setting (jobs already running keep theirs). */
+int whir_batch_set_device_transcript(whir_batch* b, int32_t enable);
 /* Enqueue (non-blocking). The job and its buffers must stay valid until it is done. */
 int whir_batch_submit(whir_batch* b, whir_job* job);
 /* Wait for one job (timeout_ms < 0: no limit); returns the job's status. */

@@ -137,7 +137,9 @@ bool check_sum() {
       y[i] = x[i];
       ref16 += y[i];
     }
-    if (p2::sum_mod<24>(x) != ref % kb::P || p2::sum_mod<16>(y) != ref16 % kb::P) return fail("sum_mod", t, 0);
+    // sum_rest leaves out word 0
+    if (p2::sum_rest<24>(x) != (ref - x[0]) % kb::P || p2::sum_rest<16>(y) != (ref16 - y[0]) % kb::P)
+      return fail("sum_rest", t, 0);
     g_checks++;
   }
   return true;

@@ -21,12 +21,12 @@ def test_specialised_poseidon2_forms_match_plain(tmp_path):
 
 
 def test_device_sbox_method_on_unreduced_inputs():
-    """The device S-box (poseidon2.cuh `cube`) forms v^2 mod p and then
-    (v^2 mod p) * v mod p from a double-precision quotient estimate
-    q = round(a * fl(b / p)) (an FMA with 1.5 * 2^52) and r = a * b - q * p
-    modulo 2^32 with one signed correction. Its inputs are round-constant sums
-    that skip their reduction (below 2p), so it must hold for every v < 2^32.
-    Emulated here in IEEE double with an exactly rounded FMA."""
+    """The device S-box (poseidon2.cuh `cube`) forms t = v^2 - q p with
+    q = round(v * fl(v / p)) (an FMA with 1.5 * 2^52), t in (-p, p) kept
+    signed, then r = t * v - q' p with q' = round(t * fl(v / p)) and one
+    correction of r, all products modulo 2^32. Its inputs are round-constant
+    sums that skip their reduction (below 2p), so it must hold for every
+    v < 2^32. Emulated here in IEEE double with an exactly rounded FMA."""
     import random
     import struct
     from fractions import Fraction
@@ -34,17 +34,18 @@ def test_device_sbox_method_on_unreduced_inputs():
     p = 2**31 - 2**24 + 1
     inv_p, magic = 1.0 / p, 6755399441055744.0
 
-    def mulmod_q(a, ad, bp, b):
+    def low_word(ad, bp):
         q = float(Fraction(ad) * Fraction(bp) + Fraction(magic))
-        q_lo = struct.unpack("<Q", struct.pack("<d", q))[0] & 0xFFFFFFFF
-        r = (a * b - q_lo * p) & 0xFFFFFFFF
-        return min(r, (r + p) & 0xFFFFFFFF)
+        return struct.unpack("<Q", struct.pack("<d", q))[0] & 0xFFFFFFFF
 
     def cube(v):
         vd = float(v)
         vp = vd * inv_p
-        v2 = mulmod_q(v, vd, vp, v)
-        return mulmod_q(v2, float(v2), vp, v)
+        t = (v * v - low_word(vd, vp) * p) & 0xFFFFFFFF
+        ts = t - (1 << 32) if t >= 1 << 31 else t
+        assert -p < ts < p
+        r = (t * v - low_word(float(ts), vp) * p) & 0xFFFFFFFF
+        return min(r, (r + p) & 0xFFFFFFFF)
 
     rng = random.Random(3)
     vals = [0, 1, p - 1, p, p + 1, 2 * p - 2, 2**31 - 1, 2**31, 2**32 - 2, 2**32 - 1]

@@ -145,6 +145,7 @@ _SIGS = {
                                     C.POINTER(_vp)]),
     "whir_batch_destroy": (C.c_int, [_vp]),
     "whir_batch_memory": (C.c_int, [_vp, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]),
+    "whir_batch_set_device_transcript": (C.c_int, [_vp, _i32]),
     "whir_batch_submit": (C.c_int, [_vp, C.POINTER(Job)]),
     "whir_batch_wait": (C.c_int, [_vp, C.POINTER(Job), _i32]),
     "whir_batch_wait_all": (C.c_int, [_vp]),
@@ -862,6 +863,10 @@ class Batch:
         f, r = C.c_uint64(0), C.c_uint64(0)
         _check(lib().whir_batch_memory(self.handle, C.byref(f), C.byref(r)))
         return f.value, r.value
+
+    def set_device_transcript(self, enable: bool) -> None:
+        """Context.set_device_transcript on every worker (jobs started later)."""
+        _check(lib().whir_batch_set_device_transcript(self.handle, int(enable)))
 
     def wait(self, req: ProofRequest, timeout_ms: int = -1) -> None:
         _check(lib().whir_batch_wait(self.handle, C.byref(req.job), timeout_ms))

@@ -239,6 +239,13 @@ int whir_batch_memory(whir_batch* b, uint64_t* fixed_bytes, uint64_t* pool_reser
   return WHIR_OK;
 }
 
+int whir_batch_set_device_transcript(whir_batch* b, int32_t enable) {
+  WH_CHECK(b, "null batch");
+  std::lock_guard<std::mutex> lk(b->mu);
+  for (whir_ctx* c : b->ctxs) WH_TRY(whir_ctx_set_device_transcript(c, enable));
+  return WHIR_OK;
+}
+
 int whir_batch_destroy(whir_batch* b) {
   if (!b) return WHIR_OK;
   {

@@ -254,7 +254,7 @@ int grind(whir_ctx* ctx, Chal& ch, int bits, uint32_t* witness) {
   uint32_t got[2] = {0u, 0u};
   WH_TRY(fetch_posted(ctx, ctx->h_mail ? seq : 0u, got, ctx->d_words, ctx->h_mail ? 8 : 4));
   const uint32_t w = got[0];
-  if (ctx->h_mail) add_stage_work(ctx, kStGrind, (uint64_t)got[1] * 256u);
+  if (ctx->h_mail) add_stage_work(ctx, kStGrind, (uint64_t)got[1] * wk::kGrindClaim);
   if (w >= kb::P) {
     set_error("proof-of-work search found no witness");
     return WHIR_ERR_NOT_FOUND;

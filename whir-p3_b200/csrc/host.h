@@ -3,6 +3,7 @@
 #pragma once
 #include <cuda_runtime.h>
 
+#include <atomic>
 #include <map>
 #include <string>
 #include <vector>
@@ -155,8 +156,9 @@ struct whir_ctx {
   // stage timing
   bool profiling = false;
   // run a sumcheck stage's transcript steps on the device (see
-  // whir_ctx_set_device_transcript); off: each step round-trips to the host
-  bool device_transcript = false;
+  // whir_ctx_set_device_transcript); off: each step round-trips to the host.
+  // Atomic: a batch may switch it while its worker proves.
+  std::atomic<bool> device_transcript{false};
   std::vector<cudaEvent_t> event_pool;
   std::vector<std::pair<int, std::pair<cudaEvent_t, cudaEvent_t>>> stage_events;
   double stage_ms[wh::kStCount] = {};

@@ -149,7 +149,8 @@ cudaError_t grind_reset(uint32_t* result, uint32_t* counter, uint32_t* done, cud
 // `state` and `in` on the host (in_len still selects the witness position);
 // with `res_out` set, the last CTA to stop writes the witness and the number of
 // evaluated claims there (2 words) and resets the search state, and no
-// initialising launch precedes the search.
+// initialising launch precedes the search. A claim is kGrindClaim candidates.
+constexpr int kGrindClaim = 128;
 cudaError_t grind(const uint32_t* state, const uint32_t* in, int in_len, int bits, uint64_t limit,
                   uint32_t* result, uint32_t* counter, uint32_t* done, uint32_t* mail, uint32_t seq,
                   const p2::P2Consts& p16, cudaStream_t st, const uint32_t* cp_dev = nullptr,

