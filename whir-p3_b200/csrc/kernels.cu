@@ -12,7 +12,7 @@
 #include <atomic>
 #include <mutex>
 
-#include "kernels.h"
+#include "devutil.cuh"
 
 using kb::ef;
 using p2::P2Consts;
@@ -47,13 +47,6 @@ static inline unsigned grid_for(size_t work, int threads, int per_sm = 8) {
   return (unsigned)b;
 }
 
-__device__ __forceinline__ ef ld_ef(const ef* p) {
-  uint4 v = __ldg(reinterpret_cast<const uint4*>(p));
-  return ef{{v.x, v.y, v.z, v.w}};
-}
-__device__ __forceinline__ void st_ef(ef* p, const ef& v) {
-  *reinterpret_cast<uint4*>(p) = make_uint4(v.c[0], v.c[1], v.c[2], v.c[3]);
-}
 
 // ---------------------------------------------------------------------------
 // Representation conversion
@@ -82,33 +75,6 @@ cudaError_t decode(uint32_t* p, size_t n, cudaStream_t st) {
 // Reductions
 // ---------------------------------------------------------------------------
 
-__device__ __forceinline__ ef warp_sum(ef v) {
-#pragma unroll
-  for (int off = 16; off; off >>= 1) {
-#pragma unroll
-    for (int c = 0; c < 4; c++) v.c[c] = kb::add(v.c[c], __shfl_down_sync(0xffffffffu, v.c[c], off));
-  }
-  return v;
-}
-
-// Block-wide sum of K extension values; thread 0 gets the result.
-template <int K>
-__device__ __forceinline__ void block_sum(ef (&v)[K], ef (&sh)[K][32]) {
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
-#pragma unroll
-  for (int k = 0; k < K; k++) v[k] = warp_sum(v[k]);
-  if (lane == 0)
-#pragma unroll
-    for (int k = 0; k < K; k++) sh[k][warp] = v[k];
-  __syncthreads();
-  if (warp == 0) {
-#pragma unroll
-    for (int k = 0; k < K; k++) {
-      v[k] = lane < nw ? sh[k][lane] : kb::ef_zero();
-      v[k] = warp_sum(v[k]);
-    }
-  }
-}
 
 __global__ void k_publish(const uint32_t* __restrict__ src, int words, volatile uint32_t* mail, uint32_t seq) {
   for (int i = threadIdx.x; i < words; i += blockDim.x) mail[i] = src[i];
@@ -909,34 +875,23 @@ cudaError_t grind_reset(uint32_t* result, uint32_t* counter, uint32_t* done, cud
 
 cudaError_t grind(const uint32_t* state, const uint32_t* in, int in_len, int bits, uint64_t limit,
                   uint32_t* result, uint32_t* counter, uint32_t* done, uint32_t* mail, uint32_t seq,
-                  const P2Consts& p16, cudaStream_t st, const uint32_t* cp_dev, uint32_t* res_out) {
+                  const P2Consts& p16, cudaStream_t st, const uint32_t* cp_dev, uint32_t* res_out, DevChal* ch,
+                  ef* r_out, uint32_t* err) {
   if (p16.mat == (uint32_t)p2::kMatHl)
     return grind_m<p2::kMatHl>(state, in, in_len, bits, limit, result, counter, done, mail, seq, p16, st, cp_dev,
-                               res_out);
+                               res_out, ch, r_out, err);
   return grind_m<p2::kMatMds>(state, in, in_len, bits, limit, result, counter, done, mail, seq, p16, st, cp_dev,
-                              res_out);
+                              res_out, ch, r_out, err);
 }
 
-__global__ void k_chal_set(DevChal* ch, const __grid_constant__ DevChal init, uint32_t* err) {
-  *ch = init;
-  *err = 0u;
-}
-
-cudaError_t chal_set(DevChal* ch, const DevChal& init, uint32_t* err, cudaStream_t st) {
-  k_chal_set<<<1, 1, 0, st>>>(ch, init, err);
-  LAUNCH_DONE();
-}
-
-cudaError_t chal_coeffs(DevChal* ch, const ef* coeffs, int grind_next, uint32_t* cp_out, ef* r_out,
-                        const P2Consts& p16, cudaStream_t st) {
-  if (p16.mat == (uint32_t)p2::kMatHl) return chal_coeffs_m<p2::kMatHl>(ch, coeffs, grind_next, cp_out, r_out, p16, st);
-  return chal_coeffs_m<p2::kMatMds>(ch, coeffs, grind_next, cp_out, r_out, p16, st);
-}
-
-cudaError_t chal_witness(DevChal* ch, const uint32_t* w_res, int bits, ef* r_out, uint32_t* err, const P2Consts& p16,
-                         cudaStream_t st) {
-  if (p16.mat == (uint32_t)p2::kMatHl) return chal_witness_m<p2::kMatHl>(ch, w_res, bits, r_out, err, p16, st);
-  return chal_witness_m<p2::kMatMds>(ch, w_res, bits, r_out, err, p16, st);
+cudaError_t sumcheck_round_tr(ef* f, ef* w, size_t q, int fold, ef r, ef* partials, unsigned* counter, ef* out,
+                              const ef* r_dev, DevChal* ch, const DevChal* init, uint32_t* err, int grind_next,
+                              uint32_t* cp_out, ef* r_out, const P2Consts& p16, cudaStream_t st) {
+  if (p16.mat == (uint32_t)p2::kMatHl)
+    return sumcheck_round_tr_m<p2::kMatHl>(f, w, q, fold, r, partials, counter, out, r_dev, ch, init, err, grind_next,
+                                           cp_out, r_out, p16, st);
+  return sumcheck_round_tr_m<p2::kMatMds>(f, w, q, fold, r, partials, counter, out, r_dev, ch, init, err, grind_next,
+                                          cp_out, r_out, p16, st);
 }
 
 cudaError_t merkle_build(const uint32_t* rows, int log_h, int row_words, int leaf_hash, uint32_t* digests,
@@ -1481,13 +1436,9 @@ cudaError_t sumcheck_coeffs(const ef* f, const ef* w, size_t half, ef* partials,
   LAUNCH_DONE();
 }
 
-// One launch per sumcheck round in the prover: optionally the previous
-// round's fold (FOLD: f, w hold 4q entries; f'(i) = f(i) + r (f(i + 2q) - f(i))
-// for i < 2q, in place, each thread owning i, i + q, i + 2q, i + 3q), then the
-// round's coefficients over the pairs (i, i + q) of the (folded) arrays. Each
-// CTA writes its two partial sums; the last CTA to finish (atomic counter, no
-// waiting) adds them up, writes out[0] = c0 and out[1] = c2, and re-arms the
-// counter, so no second launch is needed.
+// One launch per sumcheck round in the prover (sumcheck_round_body); the last
+// CTA also posts (c0, c2) to the mailbox when one is given, so no second
+// launch is needed.
 template <bool FOLD>
 __global__ void __launch_bounds__(256) k_sumcheck_round(ef* __restrict__ f, ef* __restrict__ w, size_t q, ef r,
                                                          ef* __restrict__ partials, unsigned* __restrict__ counter,
@@ -1495,60 +1446,17 @@ __global__ void __launch_bounds__(256) k_sumcheck_round(ef* __restrict__ f, ef* 
                                                          const ef* __restrict__ r_dev) {
   __shared__ ef sh[2][32];
   __shared__ bool s_last;
-  if (FOLD && r_dev) r = ld_ef(r_dev);
-  ef v[2] = {kb::ef_zero(), kb::ef_zero()};
-  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < q; i += (size_t)gridDim.x * blockDim.x) {
-    ef el, eh, wl, wh;
-    if (FOLD) {
-      const ef fa = ld_ef(f + i), fb = ld_ef(f + i + 2 * q), fc = ld_ef(f + i + q), fd = ld_ef(f + i + 3 * q);
-      const ef wa = ld_ef(w + i), wb = ld_ef(w + i + 2 * q), wc = ld_ef(w + i + q), wd = ld_ef(w + i + 3 * q);
-      el = kb::ef_add(fa, kb::ef_mul(kb::ef_sub(fb, fa), r));
-      eh = kb::ef_add(fc, kb::ef_mul(kb::ef_sub(fd, fc), r));
-      wl = kb::ef_add(wa, kb::ef_mul(kb::ef_sub(wb, wa), r));
-      wh = kb::ef_add(wc, kb::ef_mul(kb::ef_sub(wd, wc), r));
-      st_ef(f + i, el);
-      st_ef(f + i + q, eh);
-      st_ef(w + i, wl);
-      st_ef(w + i + q, wh);
-    } else {
-      el = ld_ef(f + i);
-      eh = ld_ef(f + i + q);
-      wl = ld_ef(w + i);
-      wh = ld_ef(w + i + q);
-    }
-    v[0] = kb::ef_add(v[0], kb::ef_mul(el, wl));
-    v[1] = kb::ef_add(v[1], kb::ef_mul(kb::ef_sub(kb::ef_dbl(eh), el), kb::ef_sub(kb::ef_dbl(wh), wl)));
-  }
-  block_sum<2>(v, sh);
-  if (threadIdx.x == 0) {
-    partials[blockIdx.x] = v[0];
-    partials[gridDim.x + blockIdx.x] = v[1];
-    __threadfence();
-    s_last = atomicAdd(counter, 1u) == gridDim.x - 1;
-  }
-  __syncthreads();
-  if (!s_last) return;
-  __threadfence();
-  ef a[2] = {kb::ef_zero(), kb::ef_zero()};
-  for (unsigned b = threadIdx.x; b < gridDim.x; b += blockDim.x) {
-    const uint4 x0 = __ldcg(reinterpret_cast<const uint4*>(partials + b));
-    const uint4 x1 = __ldcg(reinterpret_cast<const uint4*>(partials + gridDim.x + b));
-    a[0] = kb::ef_add(a[0], ef{{x0.x, x0.y, x0.z, x0.w}});
-    a[1] = kb::ef_add(a[1], ef{{x1.x, x1.y, x1.z, x1.w}});
-  }
-  block_sum<2>(a, sh);
-  if (threadIdx.x == 0) {
-    out[0] = a[0];
-    out[1] = a[1];
-    *counter = 0u;
-    if (mail) mail_post(mail, a[0].c, 8, seq);
-  }
+  ef res[2];
+  if (!sumcheck_round_body<FOLD>(f, w, q, r, partials, counter, out, r_dev, res, sh, s_last)) return;
+  if (threadIdx.x == 0 && mail) mail_post(mail, res[0].c, 8, seq);
 }
+
+unsigned sumcheck_round_blocks(size_t q) { return grid_for(q, 256, 8); }
 
 cudaError_t sumcheck_round(ef* f, ef* w, size_t q, int fold, ef r, ef* partials, unsigned* counter, ef* out,
                            uint32_t* mail, uint32_t seq, cudaStream_t st, const ef* r_dev) {
   if (q == 0) return cudaErrorInvalidValue;
-  const unsigned b = grid_for(q, 256, 8);
+  const unsigned b = sumcheck_round_blocks(q);
   if (fold)
     k_sumcheck_round<true><<<b, 256, 0, st>>>(f, w, q, r, partials, counter, out, mail, seq, r_dev);
   else

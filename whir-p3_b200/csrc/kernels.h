@@ -150,17 +150,24 @@ cudaError_t grind_reset(uint32_t* result, uint32_t* counter, uint32_t* done, cud
 // with `res_out` set, the last CTA to stop writes the witness and the number of
 // evaluated claims there (2 words) and resets the search state, and no
 // initialising launch precedes the search. A claim is kGrindClaim candidates.
+// With `ch` set (res_out, r_out and err too), the search's last CTA also runs
+// the transcript step after it on the device challenger: observe the witness,
+// check that sample_bits(bits) is 0, sample the round's challenge into r_out
+// (a failed check sets bit 0, no witness, or bit 1, check failed, of *err).
 constexpr int kGrindClaim = 128;
+struct DevChal;
 cudaError_t grind(const uint32_t* state, const uint32_t* in, int in_len, int bits, uint64_t limit,
                   uint32_t* result, uint32_t* counter, uint32_t* done, uint32_t* mail, uint32_t seq,
                   const p2::P2Consts& p16, cudaStream_t st, const uint32_t* cp_dev = nullptr,
-                  uint32_t* res_out = nullptr);
+                  uint32_t* res_out = nullptr, DevChal* ch = nullptr, kb::ef* r_out = nullptr,
+                  uint32_t* err = nullptr);
 
 // Duplex challenger on the device (DuplexChallenger<F, Poseidon2-16, 16, 8>),
 // Montgomery words, laid out like the host's challenger: sponge state, pending
-// inputs, buffered outputs. The steps below run in one warp with the four-lane
-// permutation, so a chain of sumcheck rounds, searches and challenges can be
-// queued without the host in between.
+// inputs, buffered outputs. Its steps run in one warp with the four-lane
+// permutation, in the tails of the kernels whose results they observe, so a
+// chain of sumcheck rounds, searches and challenges can be queued without the
+// host in between.
 struct DevChal {
   uint32_t st[16];
   uint32_t in[8];
@@ -168,18 +175,15 @@ struct DevChal {
   uint32_t out[8];
   int32_t out_len;
 };
-// set the device challenger to `init` and clear *err (no host synchronisation)
-cudaError_t chal_set(DevChal* ch, const DevChal& init, uint32_t* err, cudaStream_t st);
-// observe coeffs[0], coeffs[1] (c0 then c2, 8 words); then, with grind_next,
-// write the folded initial state of the next proof-of-work search (16
-// canonical words) to cp_out; otherwise sample an extension element into r_out
-cudaError_t chal_coeffs(DevChal* ch, const kb::ef* coeffs, int grind_next, uint32_t* cp_out, kb::ef* r_out,
-                        const p2::P2Consts& p16, cudaStream_t st);
-// observe the witness w_res[0] (canonical; p means none was found), check
-// that sample_bits(bits) is 0, then sample an extension element into r_out;
-// a failed check sets bit 0 (no witness) or bit 1 (check failed) of *err
-cudaError_t chal_witness(DevChal* ch, const uint32_t* w_res, int bits, kb::ef* r_out, uint32_t* err,
-                         const p2::P2Consts& p16, cudaStream_t st);
+// sumcheck_round followed, in its last CTA, by the round's transcript step on
+// the device challenger `ch` (set from *init first and *err cleared when init
+// is not null): observe c0, c2; then with grind_next write the folded initial
+// state of the next proof-of-work search (16 canonical words, see
+// p2::grind_fold) to cp_out, otherwise sample the round's challenge into r_out.
+cudaError_t sumcheck_round_tr(kb::ef* f, kb::ef* w, size_t q, int fold, kb::ef r, kb::ef* partials,
+                              unsigned* counter, kb::ef* out, const kb::ef* r_dev, DevChal* ch, const DevChal* init,
+                              uint32_t* err, int grind_next, uint32_t* cp_out, kb::ef* r_out,
+                              const p2::P2Consts& p16, cudaStream_t st);
 
 // The Poseidon2 launchers above for one external block MAT (p2::kMatMds or
 // p2::kMatHl), each form built in its own translation unit; merkle_leaves,
@@ -193,13 +197,13 @@ cudaError_t merkle_upper_m(int log_h, uint32_t* digests, const p2::P2Consts& p16
 template <int MAT>
 cudaError_t grind_m(const uint32_t* state, const uint32_t* in, int in_len, int bits, uint64_t limit,
                     uint32_t* result, uint32_t* counter, uint32_t* done, uint32_t* mail, uint32_t seq,
-                    const p2::P2Consts& p16, cudaStream_t st, const uint32_t* cp_dev, uint32_t* res_out);
+                    const p2::P2Consts& p16, cudaStream_t st, const uint32_t* cp_dev, uint32_t* res_out,
+                    DevChal* ch, kb::ef* r_out, uint32_t* err);
 template <int MAT>
-cudaError_t chal_coeffs_m(DevChal* ch, const kb::ef* coeffs, int grind_next, uint32_t* cp_out, kb::ef* r_out,
-                          const p2::P2Consts& p16, cudaStream_t st);
-template <int MAT>
-cudaError_t chal_witness_m(DevChal* ch, const uint32_t* w_res, int bits, kb::ef* r_out, uint32_t* err,
-                           const p2::P2Consts& p16, cudaStream_t st);
+cudaError_t sumcheck_round_tr_m(kb::ef* f, kb::ef* w, size_t q, int fold, kb::ef r, kb::ef* partials,
+                                unsigned* counter, kb::ef* out, const kb::ef* r_dev, DevChal* ch, const DevChal* init,
+                                uint32_t* err, int grind_next, uint32_t* cp_out, kb::ef* r_out,
+                                const p2::P2Consts& p16, cudaStream_t st);
 
 // eq table of `h` coordinates scaled by `scale`: out[x] = scale * prod eq(z_j, bit_j(x)), MSB <-> z[0].
 struct EqPoint {
@@ -252,6 +256,9 @@ cudaError_t sumcheck_coeffs(const kb::ef* f, const kb::ef* w, size_t half, kb::e
 // mailbox with flag `seq`.
 // With r_dev set, the fold's challenge is read from device memory (r_dev[0])
 // instead of `r`.
+// grid size of sumcheck_round (and of sumcheck_round_tr): partial sums of
+// this many CTAs
+unsigned sumcheck_round_blocks(size_t q);
 cudaError_t sumcheck_round(kb::ef* f, kb::ef* w, size_t q, int fold, kb::ef r, kb::ef* partials, unsigned* counter,
                            kb::ef* out, uint32_t* mail, uint32_t seq, cudaStream_t st, const kb::ef* r_dev = nullptr);
 

@@ -4,7 +4,7 @@
 // context's choice. The kernels have internal linkage in each unit; only the
 // launchers at the end are shared.
 #pragma once
-#include "kernels.h"
+#include "devutil.cuh"
 
 namespace wk {
 namespace {
@@ -584,148 +584,15 @@ cudaError_t merkle_upper_m(int log_h, uint32_t* digests, const P2Consts& p16, Sh
 }
 
 // ---------------------------------------------------------------------------
-// Proof of work (GrindingChallenger::grind on DuplexChallenger, called at
-// src/whir/proof.rs:188 and src/whir/prover/mod.rs:224,363). Candidates are
-// claimed in increasing chunks; a CTA stops once every remaining chunk starts
-// above the best witness found, so the result is the smallest valid witness.
-// The loop is bounded by `limit` candidates.
-// ---------------------------------------------------------------------------
-
-namespace {
-constexpr int GRIND_CTA = kGrindClaim;  // 128: one warp per SM sub-partition
-
-// Each claim is GRIND_CTA consecutive candidates, one per thread.
-template <int SLOT, int MAT>
-__global__ void __launch_bounds__(GRIND_CTA) k_grind(const __grid_constant__ P2Consts p16, uint4 st0, uint4 st1,
-                                                      uint4 st2, uint4 st3, int bits, uint64_t limit,
-                                                      uint32_t* result, uint32_t* counter, uint32_t* done,
-                                                      uint32_t* mail, uint32_t seq, const uint32_t* cp_dev,
-                                                      uint32_t* res_out) {
-  __shared__ uint64_t s_start;
-  __shared__ int s_go;
-  const uint32_t mask = (1u << bits) - 1u;
-  uint32_t cp[16] = {st0.x, st0.y, st0.z, st0.w, st1.x, st1.y, st1.z, st1.w,
-                     st2.x, st2.y, st2.z, st2.w, st3.x, st3.y, st3.z, st3.w};
-  if (cp_dev) {
-#pragma unroll
-    for (int i = 0; i < 16; i++) cp[i] = __ldcg(cp_dev + i);
-  }
-  for (;;) {
-    if (threadIdx.x == 0) {
-      const uint64_t start = (uint64_t)atomicAdd(counter, 1u) * GRIND_CTA;
-      s_start = start;
-      s_go = start < limit && start < (uint64_t)*(volatile uint32_t*)result;
-    }
-    __syncthreads();
-    const uint64_t start = s_start;
-    const int go = s_go;
-    __syncthreads();
-    if (!go) {
-      // every atomicMin of this CTA precedes the barriers above; the last CTA
-      // to stop holds the final result, posts it to the mailbox with the
-      // number of claims that were evaluated (every CTA made exactly one
-      // claim that it did not evaluate) and resets the search state for the
-      // next search (every other CTA has finished with it), which then needs
-      // no initialising launch
-      if (threadIdx.x == 0 && (mail || res_out)) {
-        __threadfence();
-        if (atomicAdd(done, 1u) == gridDim.x - 1) {
-          const uint32_t post[2] = {atomicAdd(result, 0u), atomicAdd(counter, 0u) - gridDim.x};
-          if (mail) mail_post(mail, post, 2, seq);
-          if (res_out) {
-            res_out[0] = post[0];
-            res_out[1] = post[1];
-          }
-          *result = kb::P;
-          *counter = 0u;
-          *done = 0u;
-        }
-      }
-      return;
-    }
-    const uint64_t w = start + threadIdx.x;
-    // a witness below this claim's first candidate makes the claim useless, so
-    // its threads may stop early; they read the same condition (up to a
-    // witness landing between their reads), and a stopped candidate is never
-    // one the smallest witness could be
-    const auto stop = [result, start] { return (uint64_t)*(volatile uint32_t*)result < start; };
-    if (w < limit && (p2::grind_word7<SLOT, MAT>((uint32_t)w, cp, p16, stop) & mask) == 0u) atomicMin(result, (uint32_t)w);
-  }
-}
-
-}  // namespace
-
-template <int MAT>
-cudaError_t grind_m(const uint32_t* state, const uint32_t* in, int in_len, int bits, uint64_t limit,
-                    uint32_t* result, uint32_t* counter, uint32_t* done, uint32_t* mail, uint32_t seq,
-                    const P2Consts& p16, cudaStream_t st, const uint32_t* cp_dev, uint32_t* res_out) {
-  if (in_len < 0 || in_len > 7 || bits < 0 || bits > 30) return cudaErrorInvalidValue;
-  if (limit > kb::P) limit = kb::P;
-  // the sponge state with the pending inputs, canonical (a witness w < p is
-  // its own canonical value), with 0 at the witness position; then its
-  // external layer plus the first round constants (read from cp_dev instead
-  // when the device challenger prepared them)
-  uint32_t s[16] = {0u};
-  if (!cp_dev) {
-    for (int i = 0; i < 16; i++) s[i] = kb::from_mont(state[i]);
-    for (int i = 0; i < in_len; i++) s[i] = kb::from_mont(in[i]);
-    s[in_len] = 0u;
-    p2::grind_fold<MAT>(s, p16);
-  }
-  // with a mailbox or a result slot the previous search left the state reset
-  // (grind_reset initialises it once per context)
-  if (!mail && !res_out) {
-    const cudaError_t e = grind_reset(result, counter, done, st);
-    if (e != cudaSuccess) return e;
-  }
-  uint4 a = make_uint4(s[0], s[1], s[2], s[3]), b = make_uint4(s[4], s[5], s[6], s[7]);
-  uint4 c = make_uint4(s[8], s[9], s[10], s[11]), d = make_uint4(s[12], s[13], s[14], s[15]);
-  // Candidates in flight: once the smallest witness w is found, every claim
-  // already running still completes, so a search costs about w + W
-  // permutations for W in flight, while the rate grows with W. Expected cost
-  // (2^bits + W) / rate(W), minimised over CTAs per SM with the rates measured
-  // for Poseidon2-16 on B200, relative to 16 CTAs of 128 per SM (one CTA per
-  // SM: one warp per sub-partition, about 7 us per permutation, 47 % of the
-  // full rate; the kernel's registers allow 10 resident CTAs). A search too
-  // small to fill the GPU runs one CTA per SM with about 2^(bits+3)
-  // candidates in flight: the first pass then holds a witness with
-  // probability 1 - e^-8, and the pass costs no more than a narrower one.
-  static const int kPerSm[7] = {1, 2, 3, 4, 6, 8, 10};
-  static const double kRate[7] = {0.467, 0.703, 0.811, 0.865, 0.911, 0.948, 0.965};
-  const double expect = (double)(1ull << bits);
-  unsigned blocks = (unsigned)(((8ull << bits) + GRIND_CTA - 1) / GRIND_CTA);
-  if (blocks > (unsigned)sm_count()) {
-    double best = 0.0;
-    unsigned pick = (unsigned)sm_count();
-    for (int i = 0; i < 7; i++) {
-      const unsigned b = (unsigned)sm_count() * kPerSm[i];
-      const double cost = (expect + (double)b * GRIND_CTA) / kRate[i];
-      if (i == 0 || cost < best) {
-        best = cost;
-        pick = b;
-      }
-    }
-    if (pick < blocks) blocks = pick;
-  }
-  switch (in_len) {
-#define WK_GRIND(S) \
-  case S:                                                                                                      \
-    k_grind<S, MAT><<<blocks, GRIND_CTA, 0, st>>>(p16, a, b, c, d, bits, limit, result, counter, done, mail, seq, \
-                                                  cp_dev, res_out);                                             \
-    break;
-    WK_GRIND(0) WK_GRIND(1) WK_GRIND(2) WK_GRIND(3) WK_GRIND(4) WK_GRIND(5) WK_GRIND(6) WK_GRIND(7)
-#undef WK_GRIND
-  }
-  LAUNCH_DONE();
-}
-
-// ---------------------------------------------------------------------------
 // Duplex challenger steps on the device (DuplexChallenger observe / sample /
 // sample_bits, the transcript calls of SumcheckData::observe_and_sample,
-// src/whir/proof.rs:163-193). One warp runs each step: lane 0 keeps the input
-// and output buffers in shared memory, and a duplexing permutes the sponge
-// state with the four-lane permutation (every four-lane group computes it;
-// group 0's result is kept). The state is Montgomery words, as the host's.
+// src/whir/proof.rs:163-193). One warp runs them: lane 0 keeps the input and
+// output buffers in shared memory, and a duplexing permutes the sponge state
+// with the four-lane permutation (every four-lane group computes it; group
+// 0's result is kept). The state is Montgomery words, as the host's. The
+// steps run in the tails of the kernels whose results they observe (the last
+// CTA of a sumcheck round, the last CTA of a proof-of-work search), so a
+// sumcheck stage needs no launch of its own for its transcript.
 // ---------------------------------------------------------------------------
 
 namespace {
@@ -791,12 +658,14 @@ __device__ void dc_store(const DevChal& c, DevChal* g) {
   for (int i = threadIdx.x & 31; i < (int)(sizeof(DevChal) / 4); i += 32) dst[i] = src[i];
 }
 
+// Observe a round's coefficients c0, c2 (8 words, word i in lane i of cw);
+// then, with grind_next, write the folded initial state of the next
+// proof-of-work search (16 canonical words) to cp_out, else sample the
+// round's challenge into r_out.
 template <int MAT>
-__global__ void __launch_bounds__(32) k_chal_coeffs(DevChal* ch, const ef* coeffs, int grind_next, uint32_t* cp_out,
-                                                     ef* r_out, const __grid_constant__ P2Consts k) {
-  __shared__ DevChal c;
-  dc_load(c, ch);
-  for (int i = 0; i < 8; i++) dc_observe<MAT>(c, __ldcg(coeffs[i >> 2].c + (i & 3)), k);
+__device__ void dc_coeffs_step(DevChal& c, uint32_t cw, int grind_next, uint32_t* cp_out, ef* r_out,
+                               const P2Consts& k) {
+  for (int i = 0; i < 8; i++) dc_observe<MAT>(c, __shfl_sync(0xffffffffu, cw, i), k);
   if (grind_next) {
     // the sponge state with the pending inputs and 0 at the witness position,
     // canonical, through the initial external layer plus the first constants
@@ -813,18 +682,17 @@ __global__ void __launch_bounds__(32) k_chal_coeffs(DevChal* ch, const ef* coeff
     for (int i = 0; i < 4; i++) r.c[i] = dc_sample<MAT>(c, k);
     if ((threadIdx.x & 31) == 0) *r_out = r;
   }
-  dc_store(c, ch);
 }
 
+// Observe the witness w (canonical; p means none was found), check that
+// sample_bits(bits) is 0, then sample the round's challenge into r_out. A
+// failed check sets bit 0 (no witness) or bit 1 (check failed) of *err;
+// returns false, leaving the transcript as it is, when there is no witness.
 template <int MAT>
-__global__ void __launch_bounds__(32) k_chal_witness(DevChal* ch, const uint32_t* w_res, int bits, ef* r_out,
-                                                      uint32_t* err, const __grid_constant__ P2Consts k) {
-  __shared__ DevChal c;
-  dc_load(c, ch);
-  const uint32_t w = __ldcg(w_res);
-  if (w >= kb::P) {  // no witness: leave the transcript as it is
+__device__ bool dc_witness_step(DevChal& c, uint32_t w, int bits, ef* r_out, uint32_t* err, const P2Consts& k) {
+  if (w >= kb::P) {
     if ((threadIdx.x & 31) == 0) atomicOr(err, 1u);
-    return;
+    return false;
   }
   dc_observe<MAT>(c, kb::to_mont(w), k);
   const uint32_t v = kb::from_mont(dc_sample<MAT>(c, k));
@@ -832,23 +700,229 @@ __global__ void __launch_bounds__(32) k_chal_witness(DevChal* ch, const uint32_t
   ef r;
   for (int i = 0; i < 4; i++) r.c[i] = dc_sample<MAT>(c, k);
   if ((threadIdx.x & 31) == 0) *r_out = r;
+  return true;
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// Proof of work (GrindingChallenger::grind on DuplexChallenger, called at
+// src/whir/proof.rs:188 and src/whir/prover/mod.rs:224,363). Candidates are
+// claimed in increasing chunks; a CTA stops once every remaining chunk starts
+// above the best witness found, so the result is the smallest valid witness.
+// The loop is bounded by `limit` candidates.
+// ---------------------------------------------------------------------------
+
+namespace {
+constexpr int GRIND_CTA = kGrindClaim;  // 128: one warp per SM sub-partition
+
+// Each claim is GRIND_CTA consecutive candidates, one per thread; CTA b's
+// first claim is chunk b, later claims come from the counter (chunks
+// gridDim.x, gridDim.x + 1, ...). With `ch` set (and res_out), the last CTA's
+// first warp also runs the transcript step that follows the search on the
+// device challenger (dc_witness_step).
+template <int SLOT, int MAT>
+__global__ void __launch_bounds__(GRIND_CTA, 10) k_grind(const __grid_constant__ P2Consts p16, uint4 st0, uint4 st1,
+                                                      uint4 st2, uint4 st3, int bits, uint64_t limit,
+                                                      uint32_t* result, uint32_t* counter, uint32_t* done,
+                                                      uint32_t* mail, uint32_t seq, const uint32_t* cp_dev,
+                                                      uint32_t* res_out, DevChal* ch, ef* r_out, uint32_t* err) {
+  __shared__ uint64_t s_start;
+  __shared__ int s_go;
+  __shared__ bool s_last;
+  __shared__ uint32_t s_w;
+  __shared__ DevChal c;
+  const uint32_t mask = (1u << bits) - 1u;
+  uint32_t cp[16] = {st0.x, st0.y, st0.z, st0.w, st1.x, st1.y, st1.z, st1.w,
+                     st2.x, st2.y, st2.z, st2.w, st3.x, st3.y, st3.z, st3.w};
+  if (cp_dev) {
+#pragma unroll
+    for (int i = 0; i < 16; i++) cp[i] = __ldcg(cp_dev + i);
+  }
+  for (bool first = true;; first = false) {
+    if (threadIdx.x == 0) {
+      const uint64_t chunk = first ? (uint64_t)blockIdx.x : (uint64_t)gridDim.x + atomicAdd(counter, 1u);
+      const uint64_t start = chunk * GRIND_CTA;
+      s_start = start;
+      s_go = start < limit && start < (uint64_t)*(volatile uint32_t*)result;
+    }
+    __syncthreads();
+    const uint64_t start = s_start;
+    const int go = s_go;
+    __syncthreads();
+    if (!go) {
+      // every atomicMin of this CTA precedes the barriers above; the last CTA
+      // to stop holds the final result, posts it to the mailbox with the
+      // number of claims that were evaluated (the counter's claims: every CTA
+      // evaluated its first claim and made exactly one claim that it did not
+      // evaluate) and resets the search state for the next search (every
+      // other CTA has finished with it), which then needs no initialising
+      // launch
+      if (threadIdx.x == 0) {
+        s_last = false;
+        if (mail || res_out) {
+          __threadfence();
+          if (atomicAdd(done, 1u) == gridDim.x - 1) {
+            const uint32_t post[2] = {atomicAdd(result, 0u), atomicAdd(counter, 0u)};
+            if (mail) mail_post(mail, post, 2, seq);
+            if (res_out) {
+              res_out[0] = post[0];
+              res_out[1] = post[1];
+            }
+            *result = kb::P;
+            *counter = 0u;
+            *done = 0u;
+            s_w = post[0];
+            s_last = true;
+          }
+        }
+      }
+      if (!ch) return;
+      __syncthreads();
+      if (!s_last || threadIdx.x >= 32) return;
+      dc_load(c, ch);
+      if (dc_witness_step<MAT>(c, s_w, bits, r_out, err, p16)) dc_store(c, ch);
+      return;
+    }
+    const uint64_t w = start + threadIdx.x;
+    // a witness below this claim's first candidate makes the claim useless, so
+    // its threads may stop early; they read the same condition (up to a
+    // witness landing between their reads), and a stopped candidate is never
+    // one the smallest witness could be
+    const auto stop = [result, start] { return (uint64_t)*(volatile uint32_t*)result < start; };
+    if (w < limit && (p2::grind_word7<SLOT, MAT>((uint32_t)w, cp, p16, stop) & mask) == 0u) atomicMin(result, (uint32_t)w);
+  }
+}
+
+}  // namespace
+
+template <int MAT>
+cudaError_t grind_m(const uint32_t* state, const uint32_t* in, int in_len, int bits, uint64_t limit,
+                    uint32_t* result, uint32_t* counter, uint32_t* done, uint32_t* mail, uint32_t seq,
+                    const P2Consts& p16, cudaStream_t st, const uint32_t* cp_dev, uint32_t* res_out, DevChal* ch,
+                    ef* r_out, uint32_t* err) {
+  if (in_len < 0 || in_len > 7 || bits < 0 || bits > 30) return cudaErrorInvalidValue;
+  if (ch && (!res_out || !r_out || !err || bits < 1)) return cudaErrorInvalidValue;
+  if (limit > kb::P) limit = kb::P;
+  // the sponge state with the pending inputs, canonical (a witness w < p is
+  // its own canonical value), with 0 at the witness position; then its
+  // external layer plus the first round constants (read from cp_dev instead
+  // when the device challenger prepared them)
+  uint32_t s[16] = {0u};
+  if (!cp_dev) {
+    for (int i = 0; i < 16; i++) s[i] = kb::from_mont(state[i]);
+    for (int i = 0; i < in_len; i++) s[i] = kb::from_mont(in[i]);
+    s[in_len] = 0u;
+    p2::grind_fold<MAT>(s, p16);
+  }
+  // with a mailbox or a result slot the previous search left the state reset
+  // (grind_reset initialises it once per context)
+  if (!mail && !res_out) {
+    const cudaError_t e = grind_reset(result, counter, done, st);
+    if (e != cudaSuccess) return e;
+  }
+  uint4 a = make_uint4(s[0], s[1], s[2], s[3]), b = make_uint4(s[4], s[5], s[6], s[7]);
+  uint4 c = make_uint4(s[8], s[9], s[10], s[11]), d = make_uint4(s[12], s[13], s[14], s[15]);
+  // Candidates in flight: once the smallest witness w is found, every claim
+  // already running still completes, so a search costs about w + W
+  // permutations for W in flight, while the rate grows with W. Expected cost
+  // (2^bits + W) / rate(W), minimised over CTAs per SM with the rates measured
+  // for Poseidon2-16 on B200, relative to 16 CTAs of 128 per SM (one CTA per
+  // SM: one warp per sub-partition, about 7 us per permutation, 47 % of the
+  // full rate; the kernel's registers allow 10 resident CTAs). A search too
+  // small to fill the GPU runs one CTA per SM with about 2^(bits+3)
+  // candidates in flight: the first pass then holds a witness with
+  // probability 1 - e^-8, and the pass costs no more than a narrower one.
+  static const int kPerSm[7] = {1, 2, 3, 4, 6, 8, 10};
+  static const double kRate[7] = {0.467, 0.703, 0.811, 0.865, 0.911, 0.948, 0.965};
+  const double expect = (double)(1ull << bits);
+  unsigned blocks = (unsigned)(((8ull << bits) + GRIND_CTA - 1) / GRIND_CTA);
+  if (blocks > (unsigned)sm_count()) {
+    double best = 0.0;
+    unsigned pick = (unsigned)sm_count();
+    for (int i = 0; i < 7; i++) {
+      const unsigned b = (unsigned)sm_count() * kPerSm[i];
+      const double cost = (expect + (double)b * GRIND_CTA) / kRate[i];
+      if (i == 0 || cost < best) {
+        best = cost;
+        pick = b;
+      }
+    }
+    if (pick < blocks) blocks = pick;
+  }
+  switch (in_len) {
+#define WK_GRIND(S) \
+  case S:                                                                                                      \
+    k_grind<S, MAT><<<blocks, GRIND_CTA, 0, st>>>(p16, a, b, c, d, bits, limit, result, counter, done, mail, seq, \
+                                                  cp_dev, res_out, ch, r_out, err);                             \
+    break;
+    WK_GRIND(0) WK_GRIND(1) WK_GRIND(2) WK_GRIND(3) WK_GRIND(4) WK_GRIND(5) WK_GRIND(6) WK_GRIND(7)
+#undef WK_GRIND
+  }
+  LAUNCH_DONE();
+}
+
+// ---------------------------------------------------------------------------
+// A sumcheck round with its transcript step (sumcheck_round_body, then
+// dc_coeffs_step in the first warp of the last CTA): the round's coefficients
+// are observed on the device challenger in the same launch. With use_init the
+// challenger starts from `init` (the host's challenger at the start of a
+// sumcheck stage) and *err is cleared.
+// ---------------------------------------------------------------------------
+
+namespace {
+
+template <bool FOLD, int MAT>
+__global__ void __launch_bounds__(256) k_sumcheck_round_tr(ef* __restrict__ f, ef* __restrict__ w, size_t q, ef r,
+                                                            ef* __restrict__ partials, unsigned* __restrict__ counter,
+                                                            ef* __restrict__ out, const ef* __restrict__ r_dev,
+                                                            DevChal* ch, const __grid_constant__ DevChal init,
+                                                            int use_init, uint32_t* err, int grind_next,
+                                                            uint32_t* cp_out, ef* r_out,
+                                                            const __grid_constant__ P2Consts k) {
+  __shared__ ef sh[2][32];
+  __shared__ bool s_last;
+  __shared__ ef s_co[2];
+  __shared__ DevChal c;
+  ef res[2];
+  if (!sumcheck_round_body<FOLD>(f, w, q, r, partials, counter, out, r_dev, res, sh, s_last)) return;
+  if (threadIdx.x == 0) {
+    s_co[0] = res[0];
+    s_co[1] = res[1];
+  }
+  __syncthreads();
+  if (threadIdx.x >= 32) return;
+  const int lane = threadIdx.x;
+  const uint32_t cw = lane < 8 ? s_co[lane >> 2].c[lane & 3] : 0u;
+  if (use_init) {
+    const uint32_t* src = reinterpret_cast<const uint32_t*>(&init);
+    uint32_t* dst = reinterpret_cast<uint32_t*>(&c);
+    for (int i = lane; i < (int)(sizeof(DevChal) / 4); i += 32) dst[i] = src[i];
+    if (lane == 0) *err = 0u;
+    __syncwarp();
+  } else {
+    dc_load(c, ch);
+  }
+  dc_coeffs_step<MAT>(c, cw, grind_next, cp_out, r_out, k);
   dc_store(c, ch);
 }
 
 }  // namespace
 
 template <int MAT>
-cudaError_t chal_coeffs_m(DevChal* ch, const ef* coeffs, int grind_next, uint32_t* cp_out, ef* r_out,
-                          const P2Consts& p16, cudaStream_t st) {
-  k_chal_coeffs<MAT><<<1, 32, 0, st>>>(ch, coeffs, grind_next, cp_out, r_out, p16);
-  LAUNCH_DONE();
-}
-
-template <int MAT>
-cudaError_t chal_witness_m(DevChal* ch, const uint32_t* w_res, int bits, ef* r_out, uint32_t* err,
-                           const P2Consts& p16, cudaStream_t st) {
-  if (bits < 1 || bits > 30) return cudaErrorInvalidValue;
-  k_chal_witness<MAT><<<1, 32, 0, st>>>(ch, w_res, bits, r_out, err, p16);
+cudaError_t sumcheck_round_tr_m(ef* f, ef* w, size_t q, int fold, ef r, ef* partials, unsigned* counter, ef* out,
+                                const ef* r_dev, DevChal* ch, const DevChal* init, uint32_t* err, int grind_next,
+                                uint32_t* cp_out, ef* r_out, const P2Consts& p16, cudaStream_t st) {
+  if (q == 0 || !ch || !err || !out || (grind_next ? !cp_out : !r_out)) return cudaErrorInvalidValue;
+  DevChal iv{};
+  if (init) iv = *init;
+  const unsigned b = sumcheck_round_blocks(q);
+  if (fold)
+    k_sumcheck_round_tr<true, MAT><<<b, 256, 0, st>>>(f, w, q, r, partials, counter, out, r_dev, ch, iv, init ? 1 : 0,
+                                                       err, grind_next, cp_out, r_out, p16);
+  else
+    k_sumcheck_round_tr<false, MAT><<<b, 256, 0, st>>>(f, w, q, r, partials, counter, out, r_dev, ch, iv, init ? 1 : 0,
+                                                        err, grind_next, cp_out, r_out, p16);
   LAUNCH_DONE();
 }
 

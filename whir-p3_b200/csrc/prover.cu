@@ -323,12 +323,11 @@ int sumcheck_round(whir_ctx* ctx, wh::Chal& ch, Sumcheck& sd, ef* d_f, ef* d_w, 
 }
 
 // The rounds of one sumcheck stage (k rounds over arrays of 2^m0 entries,
-// pending fold included) with every transcript step on the device: each
-// round's coefficients kernel is followed by a one-warp challenger kernel that
-// observes (c0, c2) and either samples the folding challenge or prepares the
-// proof-of-work search, whose last CTA hands the witness to a second
-// challenger kernel that observes it, checks it and samples the challenge; the
-// next round's kernel folds by that challenge from device memory. The host
+// pending fold included) with every transcript step on the device: the last
+// CTA of each round's kernel observes (c0, c2) on the device challenger and
+// either samples the folding challenge or prepares the proof-of-work search,
+// whose last CTA observes the witness, checks it and samples the challenge;
+// the next round's kernel folds by that challenge from device memory. The host
 // queues the whole stage without waiting, tracking only the challenger's
 // buffer lengths (they do not depend on values, and they select the search's
 // witness position), then fetches the stage's log once and replays it on its
@@ -348,7 +347,6 @@ int sumcheck_stage_device(whir_ctx* ctx, wh::Chal& ch, Sumcheck& sd, ef* d_f, ef
   init.in_len = ch.in_len;
   memcpy(init.out, ch.out, sizeof(init.out));
   init.out_len = ch.out_len;
-  WH_TRY_CUDA(wk::chal_set(dch, init, err, ctx->stream));
   int in_len = ch.in_len, out_len = ch.out_len;  // the challenger's buffer lengths as the device runs
   auto observed = [&] {
     out_len = 0;
@@ -369,22 +367,23 @@ int sumcheck_stage_device(whir_ctx* ctx, wh::Chal& ch, Sumcheck& sd, ef* d_f, ef
     const bool fold = j > 0 || pend.on;
     WH_CHECK(j > 0 || !pend.on || pend.half == 2 * half, "pending fold does not match the round size");
     {
+      // the round, then its coefficients observed on the device challenger
+      // (set from the host's at the stage's first round)
       wh::StageTimer timer(ctx, wh::kStSumcheck);
-      WH_TRY_CUDA(wk::sumcheck_round(d_f, d_w, half, fold ? 1 : 0, j == 0 && pend.on ? pend.r : kb::ef_zero(),
-                                     ctx->d_partials, round_counter(ctx), log_c(j), nullptr, 0u, ctx->stream,
-                                     j > 0 ? log_r(j - 1) : nullptr));
+      WH_TRY_CUDA(wk::sumcheck_round_tr(d_f, d_w, half, fold ? 1 : 0, j == 0 && pend.on ? pend.r : kb::ef_zero(),
+                                        ctx->d_partials, round_counter(ctx), log_c(j), j > 0 ? log_r(j - 1) : nullptr,
+                                        dch, j == 0 ? &init : nullptr, err, pow_bits > 0 ? 1 : 0, cp, log_r(j),
+                                        ctx->p16, ctx->stream));
     }
     for (int i = 0; i < 8; i++) observed();
-    WH_TRY_CUDA(wk::chal_coeffs(dch, log_c(j), pow_bits > 0, cp, log_r(j), ctx->p16, ctx->stream));
     if (pow_bits > 0) {
-      {
-        wh::StageTimer timer(ctx, wh::kStGrind);
-        WH_TRY_CUDA(wk::grind(nullptr, nullptr, in_len, pow_bits, kb::P, ctx->d_words, ctx->d_words + 1,
-                              ctx->d_words + 2, nullptr, 0u, ctx->p16, ctx->stream, cp, log_w(j)));
-      }
+      // the search, then the witness observed, checked and the challenge
+      // sampled in its last CTA
+      wh::StageTimer timer(ctx, wh::kStGrind);
+      WH_TRY_CUDA(wk::grind(nullptr, nullptr, in_len, pow_bits, kb::P, ctx->d_words, ctx->d_words + 1,
+                            ctx->d_words + 2, nullptr, 0u, ctx->p16, ctx->stream, cp, log_w(j), dch, log_r(j), err));
       observed();
       sampled();
-      WH_TRY_CUDA(wk::chal_witness(dch, log_w(j), pow_bits, log_r(j), err, ctx->p16, ctx->stream));
     }
     for (int i = 0; i < 4; i++) sampled();
   }
