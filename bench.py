@@ -181,11 +181,16 @@ class Clocks:
 
 
 # Warp instructions one warp issues for 32 permutations (one per thread) in
-# each Poseidon2 kernel, from ncu's smsp__inst_executed.sum divided by the
+# each Poseidon2 stage, from ncu's smsp__inst_executed.sum divided by the
 # permutations of the captured launches, measured once on this build (Poseidon2
-# with Plonky3's KoalaBear external block). The issue ceiling is 4 warp
-# instructions per clock per SM at the SM clock sampled during the timed run.
-WARP_INST_PER_32_PERMS = {"grind": 5260, "merkle_leaves": 8550, "merkle_upper": 5535}
+# with Plonky3's KoalaBear external block): the grind from an 18-bit search,
+# leaves and tree levels from the n = 24 proof's launches (the tree stage mixes
+# one-thread and four-lane permutations). The DFT stage's instructions per
+# algorithmic byte come from the same proof's DFT launches. The issue ceiling
+# is 4 warp instructions per clock per SM at the SM clock sampled during the
+# timed run.
+WARP_INST_PER_32_PERMS = {"grind": 4810, "merkle_leaves": 8270, "merkle_upper": 5540}
+DFT_WARP_INST_PER_BYTE = 0.7064
 
 
 def stage_rooflines(stages, work, steps, sm_mhz):
@@ -195,7 +200,8 @@ def stage_rooflines(stages, work, steps, sm_mhz):
     CUDA-event time) times warp instructions per permutation, against SMs x 4
     x the sampled SM clock. The DFT is bound by HBM: achieved = algorithmic
     bytes (chunks read once, LDE written once) over its live time, against the
-    measured copy bandwidth."""
+    measured copy bandwidth; its instruction issue is reported beside it (the
+    passes run below the HBM limit because they are issue-bound)."""
     peaks = json.loads((ROOT / "MEASURED_PEAKS.json").read_text()) if (ROOT / "MEASURED_PEAKS.json").exists() else {}
     hbm = float(peaks.get("hbm_gbs", 6650.0))
     import torch
@@ -221,6 +227,10 @@ def stage_rooflines(stages, work, steps, sm_mhz):
                       "frac": round(gbs / hbm, 4), "traffic": None,
                       "algorithmic_bytes_per_proof": units // steps,
                       "peak_source": "MEASURED_PEAKS.json hbm_gbs (measured)" if peaks else "fallback 6650 GB/s"})
+            ach = units * DFT_WARP_INST_PER_BYTE / sec / 1e9
+            e["issue"] = {"achieved": round(ach, 2), "peak": round(issue_peak, 2), "unit": "G warp-instructions/s",
+                          "frac": round(ach / issue_peak, 4), "warp_instructions_per_algorithmic_byte":
+                          DFT_WARP_INST_PER_BYTE}
         else:
             rate = units / sec
             e.update({"permutations_per_proof": units // steps, "permutations_per_s": round(rate)})
