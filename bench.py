@@ -529,6 +529,8 @@ def main() -> None:
     ap.add_argument("--n", type=int, default=N_VARS, help="num_variables of the headline workload")
     ap.add_argument("--constraints", type=int, default=1, help="evaluation constraints of the headline workload")
     ap.add_argument("--no-extra", action="store_true", help="skip the n=26 / four-constraint lines")
+    ap.add_argument("--device-transcript", action="store_true",
+                    help="run the sumcheck stages' transcript steps on the device (Context.set_device_transcript)")
     args = ap.parse_args()
     if args.micro:
         run_micro(args)
@@ -572,6 +574,7 @@ def main() -> None:
     ctx = pkg.Context(local)
     stream = torch.cuda.current_stream()
     ctx.set_stream(stream.cuda_stream)
+    ctx.set_device_transcript(args.device_transcript)
     params = pkg.ProtocolParameters(100, 16, pkg.FoldingFactor.constant(4), pkg.SecurityAssumption.CapacityBound, 1, 3,
                                     "poseidon2_24", 32)
     n_vars = args.n
@@ -677,7 +680,8 @@ def main() -> None:
                 "scaling": "weak", "vs_baseline": None, "dtype": "u32 (KoalaBear mod p, exact)",
                 "data": "synthetic: the reference benchmark's SmallRng(0) polynomial and point",
                 "config": dict(CONFIG, num_variables=n_vars, constraints=args.constraints,
-                               parallelism=f"replicas x{world} (one proof per GPU per step)"),
+                               parallelism=f"replicas x{world} (one proof per GPU per step)",
+                               transcript="device" if args.device_transcript else "host"),
                 "proofs_per_s": round(1e3 / value, 3), "proof_words": int(ref_proof.size),
                 "e2e": {"value": round(e2e_value, 4), "unit": UNIT, "h2d_bytes_per_step": h2d * world,
                         "d2h_bytes_per_step": d2h * world},

@@ -280,6 +280,22 @@ void or_merkle_build(const or_p2_params* p16, const or_p2_params* p24, int leaf_
                      const uint32_t* rows, int log_height, int row_words, uint32_t* digests,
                      uint32_t* root) {
   const size_t h = (size_t)1 << log_height;
+  if (leaf_hash == 2) {
+    /* Keccak MMCS (or_keccak.c) */
+#pragma omp parallel for schedule(static)
+    for (size_t i = 0; i < h; i++) or_keccak_leaf(rows + i * row_words, row_words, digests + i * 8);
+    uint32_t* prev = digests;
+    size_t n = h;
+    while (n > 1) {
+      uint32_t* cur = prev + n * 8;
+#pragma omp parallel for schedule(static)
+      for (size_t j = 0; j < n / 2; j++) or_keccak_compress(prev + 2 * j * 8, prev + (2 * j + 1) * 8, cur + j * 8);
+      prev = cur;
+      n /= 2;
+    }
+    memcpy(root, prev, 32);
+    return;
+  }
 #pragma omp parallel for schedule(static)
   for (size_t i = 0; i < h; i++) {
     if (leaf_hash == 0)

@@ -282,7 +282,26 @@ int or_domain_separator(const or_config* c, int digest_elems, uint32_t* out, int
 typedef struct {
   or_chal ch;
   or_p2_params p16, p24;
+  int keccak;   /* leaf_hash 2: Keccak MMCS with SerializingChallenger32 */
+  or_kchal kc;
 } tr_t;
+
+/* the transcript's challenger: DuplexChallenger over Poseidon2-16, or the
+ * Keccak SerializingChallenger32 of the Keccak configuration */
+static void t_obs(tr_t* t, uint32_t v) {
+  if (t->keccak) or_kchal_observe(&t->kc, v);
+  else or_chal_observe(&t->ch, &t->p16, v);
+}
+static uint32_t t_smp(tr_t* t) { return t->keccak ? or_kchal_sample(&t->kc) : or_chal_sample(&t->ch, &t->p16); }
+static uint64_t t_bits(tr_t* t, int bits) {
+  return t->keccak ? or_kchal_sample_bits(&t->kc, bits) : or_chal_sample_bits(&t->ch, &t->p16, bits);
+}
+static uint32_t t_grind(tr_t* t, int bits) {
+  return t->keccak ? or_kchal_grind(&t->kc, bits) : or_chal_grind(&t->ch, &t->p16, bits);
+}
+static int t_check(tr_t* t, int bits, uint32_t w) {
+  return t->keccak ? or_kchal_check_witness(&t->kc, bits, w) : or_chal_check_witness(&t->ch, &t->p16, bits, w);
+}
 
 static int g_p2_set = 0;
 static or_p2_params g_p16, g_p24;
@@ -308,14 +327,14 @@ static void p2_selected(or_p2_params* p16, or_p2_params* p24) {
 
 static or_ef sample_ef(tr_t* t) {
   or_ef r;
-  for (int i = 0; i < 4; i++) r.c[i] = or_chal_sample(&t->ch, &t->p16);
+  for (int i = 0; i < 4; i++) r.c[i] = t_smp(t);
   return r;
 }
 static void observe_ef(tr_t* t, or_ef v) {
-  for (int i = 0; i < 4; i++) or_chal_observe(&t->ch, &t->p16, v.c[i]);
+  for (int i = 0; i < 4; i++) t_obs(t, v.c[i]);
 }
 static void observe_digest(tr_t* t, const uint32_t* d) {
-  for (int i = 0; i < 8; i++) or_chal_observe(&t->ch, &t->p16, d[i]);
+  for (int i = 0; i < 8; i++) t_obs(t, d[i]);
 }
 
 /* get_challenge_stir_queries (src/whir/utils.rs:24-145); returns count after sort+dedup */
@@ -326,7 +345,7 @@ static int stir_queries(tr_t* t, uint64_t domain_size, int ff, int nq, uint64_t*
   int total = nq * bits;
   int cnt = 0;
   if (total <= max_bits) {
-    uint64_t all = or_chal_sample_bits(&t->ch, &t->p16, total);
+    uint64_t all = t_bits(t, total);
     uint64_t mask = (1ull << bits) - 1;
     for (int i = 0; i < nq; i++) { out[cnt++] = (all & mask) % folded; all >>= bits; }
   } else {
@@ -336,12 +355,12 @@ static int stir_queries(tr_t* t, uint64_t domain_size, int ff, int nq, uint64_t*
       uint64_t mask = (1ull << bits) - 1;
       while (rem > 0) {
         int b = rem < per ? rem : per;
-        uint64_t all = or_chal_sample_bits(&t->ch, &t->p16, b * bits);
+        uint64_t all = t_bits(t, b * bits);
         for (int i = 0; i < b; i++) { out[cnt++] = (all & mask) % folded; all >>= bits; }
         rem -= b;
       }
     } else {
-      for (int i = 0; i < nq; i++) out[cnt++] = or_chal_sample_bits(&t->ch, &t->p16, bits);
+      for (int i = 0; i < nq; i++) out[cnt++] = t_bits(t, bits);
     }
   }
   /* sort_unstable + dedup */
@@ -452,7 +471,7 @@ static or_ef observe_and_sample(tr_t* t, sc_data* d, or_ef c0, or_ef c2, int pow
   sc_push(d, c0, c2);
   observe_ef(t, c0);
   observe_ef(t, c2);
-  if (pow_bits > 0) sc_pow(d, or_chal_grind(&t->ch, &t->p16, pow_bits));
+  if (pow_bits > 0) sc_pow(d, t_grind(t, pow_bits));
   return sample_ef(t);
 }
 
@@ -505,11 +524,13 @@ int or_whir_prove(const or_params* prm, int n, const uint32_t* poly, const uint3
   tr_t t;
   p2_selected(&t.p16, &t.p24);
   or_chal_init(&t.ch);
+  t.keccak = prm->leaf_hash == 2;
+  or_kchal_init(&t.kc);
   {
     int len = or_domain_separator(&cfg, prm->ds_digest_elems, NULL, 0);
     uint32_t* pat = (uint32_t*)malloc((size_t)len * 4);
     or_domain_separator(&cfg, prm->ds_digest_elems, pat, len);
-    for (int i = 0; i < len; i++) or_chal_observe(&t.ch, &t.p16, pat[i]);
+    for (int i = 0; i < len; i++) t_obs(&t, pat[i]);
     free(pat);
   }
   const size_t N = (size_t)1 << n;
@@ -623,9 +644,9 @@ int or_whir_prove(const or_params* prm, int n, const uint32_t* poly, const uint3
       bw_ef(&b, oevs[i]);
     }
     uint32_t pw = 0;
-    if (rp->pow_bits > 0) pw = or_chal_grind(&t.ch, &t.p16, rp->pow_bits);
+    if (rp->pow_bits > 0) pw = t_grind(&t, rp->pow_bits);
     bw(&b, pw);
-    (void)or_chal_sample(&t.ch, &t.p16);
+    (void)t_smp(&t);
     int nq = stir_queries(&t, rp->domain_size, cfg_ff(&cfg, round), rp->num_queries, idx);
     uint32_t* svars = (uint32_t*)malloc(sizeof(uint32_t) * (nq + 1));
     or_ef* sevs = (or_ef*)malloc(sizeof(or_ef) * (nq + 1));
@@ -676,7 +697,7 @@ int or_whir_prove(const or_params* prm, int n, const uint32_t* poly, const uint3
       bw_ef(&b, v);
     }
     uint32_t pw = 0;
-    if (cfg.final_pow_bits > 0) pw = or_chal_grind(&t.ch, &t.p16, cfg.final_pow_bits);
+    if (cfg.final_pow_bits > 0) pw = t_grind(&t, cfg.final_pow_bits);
     bw(&b, pw);
     or_round_cfg fc = final_round_config(&cfg);
     int nq = stir_queries(&t, fc.domain_size, cfg_ff(&cfg, cfg.n_rounds), cfg.final_queries, idx);
@@ -745,7 +766,7 @@ static int verify_sc(tr_t* t, rd_t* r, or_ef* claimed, int pow_bits, or_ef* rs_o
     observe_ef(t, polys[2 * i]);
     observe_ef(t, polys[2 * i + 1]);
     if (pow_bits > 0) {
-      if (i >= npow || !or_chal_check_witness(&t->ch, &t->p16, pow_bits, pows[i])) {
+      if (i >= npow || !t_check(t, pow_bits, pows[i])) {
         free(polys); free(pows); return -12;
       }
     }
@@ -763,6 +784,16 @@ static int verify_path(tr_t* t, int leaf_hash, const uint32_t* root, uint64_t id
   uint32_t cur[8], tmp[16];
   uint32_t st[24];
   memset(st, 0, sizeof(st));
+  if (leaf_hash == 2) {
+    /* Keccak MMCS: leaf hash and compression of or_keccak.c */
+    or_keccak_leaf(row, row_words, cur);
+    for (int l = 0; l < path_len; l++) {
+      const uint32_t* sib = path + 8 * l;
+      if ((idx >> l) & 1) or_keccak_compress(sib, cur, cur);
+      else or_keccak_compress(cur, sib, cur);
+    }
+    return memcmp(cur, root, 32) == 0;
+  }
   /* leaf digest via the same sponge as the builder */
   {
     const or_p2_params* p = leaf_hash == 0 ? &t->p24 : &t->p16;
@@ -791,8 +822,8 @@ static int verify_stir(tr_t* t, rd_t* r, const or_params* prm, const or_round_cf
                        or_ef** folds_out, int* nq_out) {
   /* the opened tree has domain_size >> folding_factor leaves */
   const int expect_height_log = ilog2_u64(rp->domain_size) - rp->folding_factor;
-  if (rp->pow_bits > 0 && !or_chal_check_witness(&t->ch, &t->p16, rp->pow_bits, pow_w)) return -20;
-  if (!is_final_round) (void)or_chal_sample(&t->ch, &t->p16);
+  if (rp->pow_bits > 0 && !t_check(t, rp->pow_bits, pow_w)) return -20;
+  if (!is_final_round) (void)t_smp(t);
   uint64_t idx[4096];
   int nq = stir_queries(t, rp->domain_size, rp->folding_factor, rp->num_queries, idx);
   int got = (int)rd(r);
@@ -832,11 +863,13 @@ int or_whir_verify(const or_params* prm, int n, const uint32_t* user_points, con
   tr_t t;
   p2_selected(&t.p16, &t.p24);
   or_chal_init(&t.ch);
+  t.keccak = prm->leaf_hash == 2;
+  or_kchal_init(&t.kc);
   {
     int len = or_domain_separator(&cfg, prm->ds_digest_elems, NULL, 0);
     uint32_t* pat = (uint32_t*)malloc((size_t)len * 4);
     or_domain_separator(&cfg, prm->ds_digest_elems, pat, len);
-    for (int i = 0; i < len; i++) or_chal_observe(&t.ch, &t.p16, pat[i]);
+    for (int i = 0; i < len; i++) t_obs(&t, pat[i]);
     free(pat);
   }
   rd_t r = {proof, proof_words, 0, 0};

@@ -61,7 +61,8 @@ typedef struct {
   int32_t soundness;             /* 0 UniqueDecoding, 1 JohnsonBound, 2 CapacityBound */
   int32_t starting_log_inv_rate;
   int32_t rs_reduction;          /* rs_domain_initial_reduction_factor */
-  int32_t leaf_hash;             /* 0: PaddingFreeSponge<P24,24,16,8>; 1: PaddingFreeSponge<P16,16,8,8> */
+  int32_t leaf_hash;             /* 0: PaddingFreeSponge<P24,24,16,8>; 1: PaddingFreeSponge<P16,16,8,8>;
+                                  * 2: the Keccak MMCS and SerializingChallenger32 (or_keccak.c) */
   int32_t ds_digest_elems;       /* DIGEST_ELEMS const used in DomainSeparator (32 in main/bench, 8 in tests) */
 } or_params;
 
@@ -98,6 +99,35 @@ uint32_t or_chal_sample(or_chal* c, const or_p2_params* p16);
 uint64_t or_chal_sample_bits(or_chal* c, const or_p2_params* p16, int bits);
 uint32_t or_chal_grind(or_chal* c, const or_p2_params* p16, int bits);
 int or_chal_check_witness(or_chal* c, const or_p2_params* p16, int bits, uint32_t w);
+/* ---- Keccak family (or_keccak.c) --------------------------------------- */
+void or_keccak_f1600(uint64_t* lanes25);
+typedef struct {
+  uint64_t st[25];
+  uint32_t pos; /* bytes absorbed into the current 136-byte block */
+} or_k256;
+void or_k256_init(or_k256* k);
+void or_k256_update(or_k256* k, const uint8_t* in, size_t len);
+void or_k256_final(const or_k256* k, uint8_t out[32]);
+void or_keccak256(const uint8_t* in, size_t len, uint8_t out[32]);
+/* leaf digest of a row (canonical values) and 2-to-1 compression, digests as
+ * 8 words (little-endian halves of [u64; 4]) */
+void or_keccak_leaf(const uint32_t* row, int words, uint32_t out8[8]);
+void or_keccak_compress(const uint32_t* l8, const uint32_t* r8, uint32_t out8[8]);
+/* SerializingChallenger32<F, HashChallenger<u8, Keccak256Hash, 32>>; the
+ * input buffer is held as an absorbing Keccak-256 state */
+typedef struct {
+  or_k256 in;
+  uint8_t out[32];
+  int32_t out_len;
+} or_kchal;
+void or_kchal_init(or_kchal* c);
+void or_kchal_observe(or_kchal* c, uint32_t v); /* a canonical value, or a raw digest word */
+void or_kchal_observe_bytes(or_kchal* c, const uint8_t* b, size_t n);
+uint32_t or_kchal_sample(or_kchal* c);
+uint64_t or_kchal_sample_bits(or_kchal* c, int bits);
+int or_kchal_check_witness(or_kchal* c, int bits, uint32_t w);
+uint32_t or_kchal_grind(or_kchal* c, int bits);
+
 /* domain separator pattern of DomainSeparator::commit_statement + add_whir_proof */
 int or_domain_separator(const or_config* cfg, int digest_elems, uint32_t* out, int cap);
 

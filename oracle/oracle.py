@@ -147,11 +147,25 @@ class Oracle:
                                      C.c_size_t, _u32p]
         L.or_whir_verify.restype = C.c_int
         L.or_free.argtypes = [C.c_void_p]
+        L.or_keccak256.argtypes = [C.c_char_p, C.c_size_t, C.c_void_p]
+        L.or_keccak_f1600.argtypes = [C.c_void_p]
         self.p16 = P2Params()
         self.p24 = P2Params()
         L.or_p2_from_rng(p2_seed, p2_mat, C.byref(self.p16), C.byref(self.p24))
 
     # ---- primitives -------------------------------------------------------
+    def keccak256(self, data: bytes) -> bytes:
+        """Keccak-256 (original Keccak padding, as p3-keccak's Keccak256Hash)."""
+        out = (C.c_uint8 * 32)()
+        self.lib.or_keccak256(data, len(data), out)
+        return bytes(out)
+
+    def keccak_f1600(self, lanes: np.ndarray) -> np.ndarray:
+        """Keccak-f[1600] on 25 64-bit lanes (lane x + 5y)."""
+        st = np.ascontiguousarray(lanes, dtype=np.uint64).copy()
+        self.lib.or_keccak_f1600(st.ctypes.data)
+        return st
+
     def rng_fields(self, seed: int, count: int) -> np.ndarray:
         """rng.random::<KoalaBear>() drawn `count` times from SmallRng::seed_from_u64(seed)."""
         out = np.empty(count, dtype=np.uint32)
