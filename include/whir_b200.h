@@ -64,6 +64,25 @@ typedef struct {
                             * (small integers and signed powers of two), else WHIR_ERR_INVALID */
 } whir_poseidon2_params;
 
+/* Hash family of the Merkle commitments and the transcript:
+ *   WHIR_LEAF_P24: leaves PaddingFreeSponge<P24, 24, 16, 8>, nodes
+ *     TruncatedPermutation<P16, 2, 8, 16>, DuplexChallenger<F, P16, 16, 8>
+ *     (src/bin/main.rs:34-39, benches/whir.rs);
+ *   WHIR_LEAF_P16: leaves PaddingFreeSponge<P16, 16, 8, 8>, otherwise the same
+ *     (src/whir/mod.rs:39 tests);
+ *   WHIR_LEAF_KECCAK: MerkleTreeMmcs<F, u64, SerializingHasher<
+ *     PaddingFreeSponge<KeccakF, 25, 17, 4>>, CompressionFunctionFromHasher<
+ *     .., 2, 4>, 4> with SerializingChallenger32<F, HashChallenger<u8,
+ *     Keccak256Hash, 32>> (src/whir/mod.rs:236-383). Digests are [u64; 4],
+ *     held and returned as 8 words (little-endian halves of each u64), never
+ *     converted; field elements enter the hash and the challenger as their
+ *     canonical values (Plonky3's serialisation, assumed). Runs through
+ *     whir_commit_and_prove (the split commit / prove API carries the duplex
+ *     challenger's state). */
+#define WHIR_LEAF_P24 0
+#define WHIR_LEAF_P16 1
+#define WHIR_LEAF_KECCAK 2
+
 /* ProtocolParameters (src/parameters/mod.rs:147-166) plus the hash and
  * domain-separator choices of the caller's set-up (src/bin/main.rs:34-39,178-180). */
 typedef struct {
@@ -74,7 +93,7 @@ typedef struct {
   int32_t soundness;             /* 0 UniqueDecoding, 1 JohnsonBound, 2 CapacityBound */
   int32_t starting_log_inv_rate;
   int32_t rs_reduction;          /* rs_domain_initial_reduction_factor */
-  int32_t leaf_hash;             /* 0: PaddingFreeSponge<P24,24,16,8>; 1: PaddingFreeSponge<P16,16,8,8> */
+  int32_t leaf_hash;             /* WHIR_LEAF_P24, WHIR_LEAF_P16 or WHIR_LEAF_KECCAK */
   int32_t ds_digest_elems;       /* DIGEST_ELEMS constant given to DomainSeparator::commit_statement */
 } whir_protocol_params;
 
@@ -244,11 +263,19 @@ int whir_monty_decode(whir_ctx* ctx, uint32_t* d_words, size_t n);
 int whir_dft_batch(whir_ctx* ctx, const uint32_t* d_chunks, int32_t log_chunk, int32_t log_width,
                    int32_t log_blowup, int32_t ext, uint32_t* d_out);
 /* Mmcs::commit_matrix (MerkleTreeMmcs, writer.rs:89, prover/mod.rs:182-184).
- * d_digests: (2 * 2^log_height - 1) * 8 words, leaf digests first; root (host) canonical. */
+ * d_digests: (2 * 2^log_height - 1) * 8 words, leaf digests first; root (host)
+ * canonical (Poseidon2 families) or the raw words of the Keccak digest. */
 int whir_merkle_commit(whir_ctx* ctx, const uint32_t* d_rows, int32_t log_height, int32_t row_words,
                        int32_t leaf_hash, uint32_t* d_digests, uint32_t* root);
 /* Mmcs::open_batch (prover/mod.rs:248-300): row (row_words) and sibling path
  * (log_height digests, leaf level first) for `index`, canonical, to host. */
+/* the same for a tree of hash family leaf_hash (Keccak path words are raw) */
+int whir_merkle_open_ex(whir_ctx* ctx, const uint32_t* d_rows, const uint32_t* d_digests, int32_t log_height,
+                        int32_t row_words, int32_t leaf_hash, uint64_t index, uint32_t* row_out,
+                        uint32_t* path_out);
+/* Keccak256Hash (p3-keccak; Keccak-256 with the original padding) of n bytes,
+ * on the host */
+int whir_keccak256(const uint8_t* data, size_t n, uint8_t* out32);
 int whir_merkle_open(whir_ctx* ctx, const uint32_t* d_rows, const uint32_t* d_digests, int32_t log_height,
                      int32_t row_words, uint64_t index, uint32_t* row_out, uint32_t* path_out);
 

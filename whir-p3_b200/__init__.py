@@ -124,6 +124,8 @@ _SIGS = {
     "whir_dft_batch": (C.c_int, [_vp, _vp, _i32, _i32, _i32, _i32, _vp]),
     "whir_merkle_commit": (C.c_int, [_vp, _vp, _i32, _i32, _i32, _vp, _u32]),
     "whir_merkle_open": (C.c_int, [_vp, _vp, _vp, _i32, _i32, C.c_uint64, _u32, _u32]),
+    "whir_merkle_open_ex": (C.c_int, [_vp, _vp, _vp, _i32, _i32, _i32, C.c_uint64, _u32, _u32]),
+    "whir_keccak256": (C.c_int, [C.c_char_p, C.c_size_t, _vp]),
     "whir_eq_table": (C.c_int, [_vp, _vp, _i32, _u32, _vp]),
     "whir_eval_base": (C.c_int, [_vp, _vp, _i32, _vp, _u32]),
     "whir_eval_ext": (C.c_int, [_vp, _vp, _i32, _vp, _u32]),
@@ -227,7 +229,9 @@ class FoldingFactor:
         return self.first if r == 0 else self.rest
 
 
-LEAF_HASH = {"poseidon2_24": 0, "poseidon2_16": 1}
+# hash families (whir_b200.h WHIR_LEAF_*): "keccak" is the Keccak MMCS with the
+# SerializingChallenger32 of src/whir/mod.rs:236-383 (commit_and_prove only)
+LEAF_HASH = {"poseidon2_24": 0, "poseidon2_16": 1, "keccak": 2}
 
 
 @dataclass
@@ -238,7 +242,7 @@ class ProtocolParameters:
     soundness_type: SecurityAssumption = SecurityAssumption.CapacityBound
     starting_log_inv_rate: int = 1
     rs_domain_initial_reduction_factor: int = 1
-    leaf_hash: str = "poseidon2_24"   # PaddingFreeSponge<P24,24,16,8>; "poseidon2_16" = <P16,16,8,8>
+    leaf_hash: str = "poseidon2_24"   # PaddingFreeSponge<P24,24,16,8>; "poseidon2_16" = <P16,16,8,8>; "keccak"
     ds_digest_elems: int = 32          # DIGEST_ELEMS given to DomainSeparator::commit_statement
 
     def _c(self) -> _Params:
@@ -618,11 +622,19 @@ def fold_ext_shaped(ctx: Context, evals: DeviceArray, n: int, r, shape) -> None:
 
 
 def merkle_open(ctx: Context, rows: DeviceArray, digests: DeviceArray, log_height: int, row_words: int,
-                index: int) -> tuple[np.ndarray, np.ndarray]:
+                index: int, leaf_hash: int = 0) -> tuple[np.ndarray, np.ndarray]:
     row = np.zeros(row_words, dtype=np.uint32)
     path = np.zeros(max(log_height, 1) * 8, dtype=np.uint32)
-    _check(lib().whir_merkle_open(ctx.handle, rows.ptr, digests.ptr, log_height, row_words, index, row, path))
+    _check(lib().whir_merkle_open_ex(ctx.handle, rows.ptr, digests.ptr, log_height, row_words, leaf_hash, index,
+                                     row, path))
     return row, path[: log_height * 8]
+
+
+def keccak256(data: bytes) -> bytes:
+    """Keccak256Hash (p3-keccak): Keccak-256 with the original padding, on the host."""
+    out = (C.c_uint8 * 32)()
+    _check(lib().whir_keccak256(data, len(data), out))
+    return bytes(out)
 
 
 def eq_table(ctx: Context, point, scale, out: DeviceArray) -> DeviceArray:

@@ -246,11 +246,15 @@ int grind(whir_ctx* ctx, Chal& ch, int bits, uint32_t* witness) {
   const uint32_t seq = ctx->h_mail ? mail_next(ctx) : 0u;
   {
     StageTimer t(ctx, kStGrind);
-    WH_TRY_CUDA(wk::grind(ch.st, ch.in, ch.in_len, bits, kb::P, ctx->d_words, ctx->d_words + 1, ctx->d_words + 2,
-                          ctx->h_mail ? ctx->d_mail : nullptr, seq, ctx->p16, ctx->stream));
+    if (ch.family == kChalKeccak)
+      WH_TRY_CUDA(wk::keccak_grind(ch.kin, bits, kb::P, ctx->d_words, ctx->d_words + 1, ctx->d_words + 2,
+                                   ctx->h_mail ? ctx->d_mail : nullptr, seq, ctx->stream));
+    else
+      WH_TRY_CUDA(wk::grind(ch.st, ch.in, ch.in_len, bits, kb::P, ctx->d_words, ctx->d_words + 1, ctx->d_words + 2,
+                            ctx->h_mail ? ctx->d_mail : nullptr, seq, ctx->p16, ctx->stream));
   }
   // with a mailbox the search posts its witness and the number of claims of
-  // 256 candidates it evaluated
+  // kGrindClaim candidates it evaluated
   uint32_t got[2] = {0u, 0u};
   WH_TRY(fetch_posted(ctx, ctx->h_mail ? seq : 0u, got, ctx->d_words, ctx->h_mail ? 8 : 4));
   const uint32_t w = got[0];
@@ -717,22 +721,39 @@ int whir_merkle_commit(whir_ctx* ctx, const uint32_t* d_rows, int32_t log_height
                        int32_t leaf_hash, uint32_t* d_digests, uint32_t* root) {
   WH_TRY(check_gpu(ctx));
   WH_CHECK(d_rows && d_digests && log_height >= 0 && log_height <= 30 && row_words > 0 &&
-               (leaf_hash == 0 || leaf_hash == 1),
+               (leaf_hash == WHIR_LEAF_P24 || leaf_hash == WHIR_LEAF_P16 || leaf_hash == WHIR_LEAF_KECCAK),
            "bad Merkle arguments");
   WH_TRY(wh::run_merkle_leaves(ctx, d_rows, log_height, row_words, leaf_hash, d_digests));
   uint32_t posted = 0;
-  WH_TRY(wh::run_merkle_upper(ctx, log_height, d_digests, root ? &posted : nullptr));
+  WH_TRY(wh::run_merkle_upper(ctx, log_height, leaf_hash, d_digests, root ? &posted : nullptr));
   if (root) {
     const size_t h = (size_t)1 << log_height;
     uint32_t r[8];
     WH_TRY(wh::fetch_posted(ctx, posted, r, d_digests + (2 * h - 2) * 8, 32));
-    for (int i = 0; i < 8; i++) root[i] = kb::from_mont(r[i]);
+    for (int i = 0; i < 8; i++) root[i] = wh::digest_word_out(leaf_hash, r[i]);
   }
+  return WHIR_OK;
+}
+
+int whir_keccak256(const uint8_t* data, size_t n, uint8_t* out32) {
+  WH_CHECK((data || n == 0) && out32, "null argument");
+  kk::K256 k;
+  kk::k256_init(k);
+  kk::k256_update(k, data, n);
+  uint8_t out[32];
+  kk::k256_final(k, out);
+  memcpy(out32, out, 32);
   return WHIR_OK;
 }
 
 int whir_merkle_open(whir_ctx* ctx, const uint32_t* d_rows, const uint32_t* d_digests, int32_t log_height,
                      int32_t row_words, uint64_t index, uint32_t* row_out, uint32_t* path_out) {
+  return whir_merkle_open_ex(ctx, d_rows, d_digests, log_height, row_words, WHIR_LEAF_P24, index, row_out, path_out);
+}
+
+int whir_merkle_open_ex(whir_ctx* ctx, const uint32_t* d_rows, const uint32_t* d_digests, int32_t log_height,
+                        int32_t row_words, int32_t leaf_hash, uint64_t index, uint32_t* row_out,
+                        uint32_t* path_out) {
   WH_TRY(check_gpu(ctx));
   WH_CHECK(d_rows && d_digests && row_out && path_out && index < (1ull << log_height) && row_words > 0,
            "bad opening arguments");
@@ -744,7 +765,7 @@ int whir_merkle_open(whir_ctx* ctx, const uint32_t* d_rows, const uint32_t* d_di
   std::vector<uint32_t> tmp((size_t)row_words + (size_t)log_height * 8);
   WH_TRY(wh::fetch(ctx, tmp.data(), d_row, tmp.size() * 4));
   for (int i = 0; i < row_words; i++) row_out[i] = kb::from_mont(tmp[i]);
-  for (int i = 0; i < log_height * 8; i++) path_out[i] = kb::from_mont(tmp[row_words + i]);
+  for (int i = 0; i < log_height * 8; i++) path_out[i] = wh::digest_word_out(leaf_hash, tmp[row_words + i]);
   return WHIR_OK;
 }
 

@@ -77,22 +77,43 @@ HostP16 host_consts16(const whir_poseidon2_params& p);
 void host_permute16(uint32_t* state_canonical, const HostP16& k);
 
 // DuplexChallenger with Montgomery-form state
+// The transcript's challenger. Family 0: DuplexChallenger<F, Poseidon2-16,
+// 16, 8> (st / in / out). Family 1: SerializingChallenger32<F,
+// HashChallenger<u8, Keccak256Hash, 32>> of the Keccak configuration, its
+// input buffer held as an absorbing Keccak-256 state (kin; a flush hashes it,
+// and the 32 output bytes both fill kout and start the next input buffer).
+// Values in and out are Montgomery words either way.
+constexpr int kChalDuplex = 0, kChalKeccak = 1;
 struct Chal {
   uint32_t st[16];
   uint32_t in[8];
   int in_len;
   uint32_t out[8];
   int out_len;
+  int family;
+  kk::K256 kin;
+  uint8_t kout[32];
+  int kout_len;
   void init();
+  void init_keccak();
   void duplex(const HostP16& k);
   void observe(const HostP16& k, uint32_t v);  // Montgomery value
   uint32_t sample(const HostP16& k);           // Montgomery value
   uint64_t sample_bits(const HostP16& k, int bits);
   kb::ef sample_ef(const HostP16& k);
   void observe_ef(const HostP16& k, const kb::ef& v);
+  // a Merkle root: Poseidon2 digests as 8 canonical field elements, Keccak
+  // digests as their 32 little-endian bytes
+  void observe_digest(const HostP16& k, const uint32_t* words8);
   void load(const whir_challenger& c);   // canonical -> internal
   void store(whir_challenger& c) const;  // internal -> canonical
 };
+
+// A digest word as the API returns it: Poseidon2 digests are held in
+// Montgomery form and returned canonical; Keccak digest words are raw bytes.
+inline uint32_t digest_word_out(int leaf_hash, uint32_t w) {
+  return leaf_hash == WHIR_LEAF_KECCAK ? w : kb::from_mont(w);
+}
 
 // Per-stage device timing (CUDA events on the context's stream), on when
 // profiling is enabled for the context.
@@ -212,6 +233,6 @@ int run_merkle_leaves(whir_ctx* ctx, const uint32_t* rows, int log_h, int row_wo
                       uint32_t* digests);
 // with posted_seq set, the root goes to the mailbox: *posted_seq receives the
 // sequence to wait for (0 when nothing was posted)
-int run_merkle_upper(whir_ctx* ctx, int log_h, uint32_t* digests, uint32_t* posted_seq);
+int run_merkle_upper(whir_ctx* ctx, int log_h, int leaf_hash, uint32_t* digests, uint32_t* posted_seq);
 int run_fold(whir_ctx* ctx, kb::ef* a, kb::ef* b, size_t half, const kb::ef& r);
 }  // namespace wh

@@ -8,6 +8,7 @@
 #include <stdint.h>
 
 #include "kb.cuh"
+#include "keccak.cuh"
 #include "poseidon2.cuh"
 
 namespace wk {
@@ -161,6 +162,17 @@ cudaError_t grind(const uint32_t* state, const uint32_t* in, int in_len, int bit
                   const p2::P2Consts& p16, cudaStream_t st, const uint32_t* cp_dev = nullptr,
                   uint32_t* res_out = nullptr, DevChal* ch = nullptr, kb::ef* r_out = nullptr,
                   uint32_t* err = nullptr);
+
+// Keccak family (keccak.cu): the Keccak MMCS's leaf digests (rows in
+// Montgomery form, hashed as canonical values) and tree levels, digests laid
+// out as for Poseidon2 (8 words per node, 2^log_h leaves first); and the
+// proof-of-work search on the Keccak challenger whose input buffer is `in`
+// (same result, counter and done words and mailbox convention as `grind`,
+// without a mailbox the search state is reset first by its own launch).
+cudaError_t keccak_leaves(const uint32_t* rows, int log_h, int row_words, uint32_t* digests, cudaStream_t st);
+cudaError_t keccak_upper(int log_h, uint32_t* digests, uint32_t* mail, uint32_t seq, int* posted, cudaStream_t st);
+cudaError_t keccak_grind(const kk::K256& in, int bits, uint64_t limit, uint32_t* result, uint32_t* counter,
+                         uint32_t* done, uint32_t* mail, uint32_t seq, cudaStream_t st);
 
 // Duplex challenger on the device (DuplexChallenger<F, Poseidon2-16, 16, 8>),
 // Montgomery words, laid out like the host's challenger: sponge state, pending

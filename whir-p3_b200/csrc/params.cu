@@ -216,7 +216,8 @@ int config_new(const whir_protocol_params& p, int n, whir_config* out) {
   WH_CHECK(n >= 1 && n <= 30, "num_variables out of range");
   WH_CHECK(p.starting_log_inv_rate >= 0 && p.starting_log_inv_rate <= 16, "starting_log_inv_rate out of range");
   WH_CHECK(p.security_level >= 0 && p.pow_bits >= 0, "negative security parameter");
-  WH_CHECK(p.leaf_hash == 0 || p.leaf_hash == 1, "leaf_hash must be 0 or 1");
+  WH_CHECK(p.leaf_hash == WHIR_LEAF_P24 || p.leaf_hash == WHIR_LEAF_P16 || p.leaf_hash == WHIR_LEAF_KECCAK,
+           "leaf_hash must be WHIR_LEAF_P24, WHIR_LEAF_P16 or WHIR_LEAF_KECCAK");
   const Sec S{p.soundness};
   const int sec = p.security_level, fb = kFieldBits;
   const int psl = sec > p.pow_bits ? sec - p.pow_bits : 0;
@@ -459,6 +460,11 @@ void host_permute16(uint32_t* st, const HostP16& k) {
 }
 
 void Chal::init() { memset(this, 0, sizeof(*this)); }
+void Chal::init_keccak() {
+  init();
+  family = kChalKeccak;
+  kk::k256_init(kin);
+}
 void Chal::duplex(const HostP16& k) {
   for (int i = 0; i < in_len; i++) st[i] = in[i];
   in_len = 0;
@@ -470,17 +476,57 @@ void Chal::duplex(const HostP16& k) {
   out_len = 8;
 }
 void Chal::observe(const HostP16& k, uint32_t v) {
+  if (family == kChalKeccak) {
+    // the 4 little-endian bytes of the canonical value
+    kout_len = 0;
+    kk::k256_word(kin, kb::from_mont(v));
+    return;
+  }
   out_len = 0;
   in[in_len++] = v;
   if (in_len == 8) duplex(k);
 }
+namespace {
+// HashChallenger::sample on the Keccak challenger: pop a byte from the end of
+// the output, hashing the input buffer first when the output is empty
+uint8_t keccak_byte(Chal& c) {
+  if (c.kout_len == 0) {
+    kk::k256_final(c.kin, c.kout);
+    c.kout_len = 32;
+    kk::k256_init(c.kin);
+    kk::k256_update(c.kin, c.kout, 32);
+  }
+  return c.kout[--c.kout_len];
+}
+uint32_t keccak_u32(Chal& c) {
+  uint32_t v = 0;
+  for (int i = 0; i < 4; i++) v |= (uint32_t)keccak_byte(c) << (8 * i);
+  return v;
+}
+}  // namespace
 uint32_t Chal::sample(const HostP16& k) {
+  if (family == kChalKeccak) {
+    // 4 bytes little-endian, masked to 31 bits, rejected while >= p
+    for (;;) {
+      const uint32_t v = keccak_u32(*this) & 0x7fffffffu;
+      if (v < kb::P) return kb::to_mont(v);
+    }
+  }
   if (in_len > 0 || out_len == 0) duplex(k);
   return out[--out_len];
 }
 uint64_t Chal::sample_bits(const HostP16& k, int bits) {
+  if (family == kChalKeccak) return (uint64_t)keccak_u32(*this) & ((1ull << bits) - 1);
   const uint32_t v = kb::from_mont(sample(k));
   return (uint64_t)v & ((1ull << bits) - 1);
+}
+void Chal::observe_digest(const HostP16& k, const uint32_t* words8) {
+  if (family == kChalKeccak) {
+    kout_len = 0;
+    for (int i = 0; i < 8; i++) kk::k256_word(kin, words8[i]);
+    return;
+  }
+  for (int i = 0; i < 8; i++) observe(k, kb::to_mont(words8[i]));
 }
 kb::ef Chal::sample_ef(const HostP16& k) {
   kb::ef r;
@@ -491,6 +537,7 @@ void Chal::observe_ef(const HostP16& k, const kb::ef& v) {
   for (int i = 0; i < 4; i++) observe(k, v.c[i]);
 }
 void Chal::load(const whir_challenger& c) {
+  init();
   for (int i = 0; i < 16; i++) st[i] = kb::to_mont(c.state[i]);
   for (int i = 0; i < 8; i++) in[i] = kb::to_mont(c.input[i]);
   for (int i = 0; i < 8; i++) out[i] = kb::to_mont(c.output[i]);

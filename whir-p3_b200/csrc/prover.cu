@@ -38,6 +38,7 @@ struct Tree {
   int log_h = 0;
   int row_words = 0;
   int ext = 0;
+  int leaf_hash = 0;  // hash family (WHIR_LEAF_*)
 };
 
 struct Constraint {
@@ -198,6 +199,7 @@ int commit_matrix(whir_ctx* ctx, const uint32_t* d_src, int log_chunk, int log_w
   t->log_h = log_chunk + log_blowup;
   t->row_words = lanes << log_w;
   t->ext = ext;
+  t->leaf_hash = leaf_hash;
   const size_t h = (size_t)1 << t->log_h;
   const size_t words = h * (size_t)t->row_words;
   if (!pass1) {
@@ -227,19 +229,20 @@ int commit_matrix(whir_ctx* ctx, const uint32_t* d_src, int log_chunk, int log_w
   if (pass1) *pre_scratch = nullptr;
   WH_TRY(s);
   {
-    // one permutation per rate-sized chunk of each row (rate 16 for Poseidon2-24, 8 for Poseidon2-16)
-    const uint64_t rate = leaf_hash == 0 ? 16 : 8;
+    // one permutation per rate-sized chunk of each row (rate 16 for Poseidon2-24, 8 for Poseidon2-16,
+    // 34 words for the Keccak sponge's 17 lanes)
+    const uint64_t rate = leaf_hash == WHIR_LEAF_P24 ? 16 : leaf_hash == WHIR_LEAF_P16 ? 8 : 34;
     wh::StageTimer timer(ctx, wh::kStLeaves, (uint64_t)h * (((uint64_t)t->row_words + rate - 1) / rate));
     WH_TRY(wh::run_merkle_leaves(ctx, t->rows, t->log_h, t->row_words, leaf_hash, t->digests));
   }
   uint32_t posted = 0;
   {
     wh::StageTimer timer(ctx, wh::kStNodes, (uint64_t)h - 1);  // one compression per inner node
-    WH_TRY(wh::run_merkle_upper(ctx, t->log_h, t->digests, &posted));
+    WH_TRY(wh::run_merkle_upper(ctx, t->log_h, leaf_hash, t->digests, &posted));
   }
   uint32_t r[8];
   WH_TRY(wh::fetch_posted(ctx, posted, r, t->digests + (2 * h - 2) * 8, 32));
-  for (int i = 0; i < 8; i++) root_canon[i] = kb::from_mont(r[i]);
+  for (int i = 0; i < 8; i++) root_canon[i] = wh::digest_word_out(leaf_hash, r[i]);
   return WHIR_OK;
 }
 
@@ -269,7 +272,8 @@ int open_queries(whir_ctx* ctx, const Tree& t, const std::vector<uint64_t>& idx,
     proof.push_back((uint32_t)nvals);
     for (int i = 0; i < t.row_words; i++) proof.push_back(kb::from_mont(rows[(size_t)k * t.row_words + i]));
     proof.push_back((uint32_t)t.log_h);
-    for (int i = 0; i < t.log_h * 8; i++) proof.push_back(kb::from_mont(paths[(size_t)k * t.log_h * 8 + i]));
+    for (int i = 0; i < t.log_h * 8; i++)
+      proof.push_back(wh::digest_word_out(t.leaf_hash, paths[(size_t)k * t.log_h * 8 + i]));
   }
   return WHIR_OK;
 }
@@ -424,7 +428,7 @@ int sumcheck_stage_device(whir_ctx* ctx, wh::Chal& ch, Sumcheck& sd, ef* d_f, ef
 // else one host round trip per transcript step (sumcheck_round).
 int sumcheck_stage(whir_ctx* ctx, wh::Chal& ch, Sumcheck& sd, ef* d_f, ef* d_w, int m0, int k, ef* sum, int pow_bits,
                    std::vector<ef>* rs, PendingFold& pend) {
-  if (ctx->device_transcript && ctx->d_tr && k >= 1 && k <= wh::kTrMaxRounds)
+  if (ctx->device_transcript && ctx->d_tr && ch.family == wh::kChalDuplex && k >= 1 && k <= wh::kTrMaxRounds)
     return sumcheck_stage_device(ctx, ch, sd, d_f, d_w, m0, k, sum, pow_bits, rs, pend);
   for (int j = 0; j < k; j++) {
     ef r;
@@ -476,7 +480,7 @@ int do_commit(whir_ctx* ctx, whir_witness* w, wh::Chal& ch, const uint32_t* user
   WH_TRY(commit_matrix(ctx, w->d_poly, n - k0, k0, c.starting_log_inv_rate, 0, w->params.leaf_hash, &w->commit_tree,
                        root, w->pre_scratch ? &w->pre_plan : nullptr, &w->pre_scratch));
   for (int i = 0; i < 8; i++) pf.push_back(root[i]);
-  for (int i = 0; i < 8; i++) ch.observe(ctx->hp16, kb::to_mont(root[i]));
+  ch.observe_digest(ctx->hp16, root);
   pf.push_back((uint32_t)c.commitment_ood_samples);
   for (int i = 0; i < c.commitment_ood_samples; i++) {
     const ef z = ch.sample_ef(ctx->hp16);
@@ -586,7 +590,7 @@ int do_prove(whir_ctx* ctx, whir_witness* wit, wh::Chal& ch) {
     WH_TRY(flush_fold(ctx, d_f, d_w, pend));
     WH_TRY(commit_matrix(ctx, reinterpret_cast<const uint32_t*>(d_f), nv - ffn, ffn, log_blowup, 1,
                          wit->params.leaf_hash, &nt, root));
-    for (int i = 0; i < 8; i++) ch.observe(ctx->hp16, kb::to_mont(root[i]));
+    ch.observe_digest(ctx->hp16, root);
     for (int i = 0; i < 8; i++) pf.push_back(root[i]);
     // OOD samples
     std::vector<std::vector<ef>> opts;
@@ -733,13 +737,13 @@ int upload_with_dft(whir_ctx* ctx, whir_witness* w, const uint32_t* poly, bool* 
 
 }  // namespace
 
-extern "C" {
+namespace {
 
-int whir_commit(whir_ctx* ctx, const whir_protocol_params* params, int32_t n, const uint32_t* poly,
+// whir_commit on the transcript's challenger `ch` (either family)
+int commit_with(whir_ctx* ctx, const whir_protocol_params* params, int32_t n, const uint32_t* poly,
                 int32_t poly_on_device, const uint32_t* user_points, int32_t num_points, uint32_t* user_evals_out,
-                whir_challenger* chs, whir_witness** out) {
-  WH_CHECK(ctx && params && poly && chs && out && num_points >= 0 && (num_points == 0 || user_points),
-           "null argument");
+                wh::Chal& ch, whir_witness** out) {
+  WH_CHECK(ctx && params && poly && out && num_points >= 0 && (num_points == 0 || user_points), "null argument");
   *out = nullptr;
   whir_witness* w = new whir_witness();
   w->ctx = ctx;
@@ -785,28 +789,23 @@ int whir_commit(whir_ctx* ctx, const whir_protocol_params* params, int32_t n, co
       return WHIR_ERR_CUDA;
     }
   }
-  wh::Chal ch;
-  ch.load(*chs);
   s = do_commit(ctx, w, ch, user_points, num_points, user_evals_out);
   if (s != WHIR_OK) {
     whir_witness_free(w);
     return s;
   }
-  ch.store(*chs);
   *out = w;
   return WHIR_OK;
 }
 
-int whir_prove(whir_ctx* ctx, whir_witness* w, whir_challenger* chs, uint32_t* proof_out, size_t cap_words,
+// whir_prove on the transcript's challenger `ch`
+int prove_with(whir_ctx* ctx, whir_witness* w, wh::Chal& ch, uint32_t* proof_out, size_t cap_words,
                size_t* proof_words) {
-  WH_CHECK(ctx && w && chs && proof_words && w->ctx == ctx, "bad argument");
+  WH_CHECK(ctx && w && proof_words && w->ctx == ctx, "bad argument");
   WH_CHECK(!w->proved, "witness already proved");
   cudaSetDevice(ctx->device);
-  wh::Chal ch;
-  ch.load(*chs);
   WH_TRY(do_prove(ctx, w, ch));
   w->proved = true;
-  ch.store(*chs);
   *proof_words = w->proof.size();
   if (!proof_out || cap_words < w->proof.size()) {
     wh::set_error("proof buffer too small");
@@ -814,6 +813,35 @@ int whir_prove(whir_ctx* ctx, whir_witness* w, whir_challenger* chs, uint32_t* p
   }
   memcpy(proof_out, w->proof.data(), w->proof.size() * 4);
   return WHIR_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+// The split API carries the duplex challenger's state (whir_challenger); the
+// Keccak configuration, whose challenger state is a hash input buffer, runs
+// through whir_commit_and_prove.
+int whir_commit(whir_ctx* ctx, const whir_protocol_params* params, int32_t n, const uint32_t* poly,
+                int32_t poly_on_device, const uint32_t* user_points, int32_t num_points, uint32_t* user_evals_out,
+                whir_challenger* chs, whir_witness** out) {
+  WH_CHECK(params && chs, "null argument");
+  WH_CHECK(params->leaf_hash != WHIR_LEAF_KECCAK, "the Keccak configuration runs through whir_commit_and_prove");
+  wh::Chal ch;
+  ch.load(*chs);
+  WH_TRY(commit_with(ctx, params, n, poly, poly_on_device, user_points, num_points, user_evals_out, ch, out));
+  ch.store(*chs);
+  return WHIR_OK;
+}
+
+int whir_prove(whir_ctx* ctx, whir_witness* w, whir_challenger* chs, uint32_t* proof_out, size_t cap_words,
+               size_t* proof_words) {
+  WH_CHECK(w && chs, "bad argument");
+  wh::Chal ch;
+  ch.load(*chs);
+  const int s = prove_with(ctx, w, ch, proof_out, cap_words, proof_words);
+  if (s == WHIR_OK || s == WHIR_ERR_BUFFER) ch.store(*chs);
+  return s;
 }
 
 int whir_witness_free(whir_witness* w) {
@@ -837,16 +865,18 @@ int whir_commit_and_prove(whir_ctx* ctx, const whir_protocol_params* params, int
   WH_CHECK(ctx && params && proof_words, "null argument");
   whir_config cfg;
   WH_TRY(wh::config_new(*params, n, &cfg));
-  whir_challenger chs;
-  whir_challenger_init(&chs);
-  const std::vector<uint32_t> ds = wh::domain_separator(cfg, params->ds_digest_elems);
-  WH_TRY(whir_challenger_observe(ctx, &chs, ds.data(), ds.size()));
+  WH_CHECK(ctx->device >= 0, "host-only context (device -1) cannot run device work");
+  wh::Chal ch;
+  if (params->leaf_hash == WHIR_LEAF_KECCAK) ch.init_keccak();
+  else ch.init();
+  for (uint32_t v : wh::domain_separator(cfg, params->ds_digest_elems)) ch.observe(ctx->hp16, kb::to_mont(v));
   whir_witness* w = nullptr;
-  WH_TRY(whir_commit(ctx, params, n, poly, poly_on_device, user_points, num_points, user_evals_out, &chs, &w));
-  int s = whir_prove(ctx, w, &chs, proof_out, cap_words, proof_words);
+  WH_TRY(commit_with(ctx, params, n, poly, poly_on_device, user_points, num_points, user_evals_out, ch, &w));
+  int s = prove_with(ctx, w, ch, proof_out, cap_words, proof_words);
   whir_witness_free(w);
   if (s != WHIR_OK) return s;
-  if (checkpoint) WH_TRY(whir_challenger_sample(ctx, &chs, checkpoint, 4));
+  if (checkpoint)
+    for (int i = 0; i < 4; i++) checkpoint[i] = kb::from_mont(ch.sample(ctx->hp16));
   return WHIR_OK;
 }
 

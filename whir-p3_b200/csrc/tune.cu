@@ -274,6 +274,10 @@ bool dft_plan_known(const whir_ctx* ctx, int log_chunk, int log_w, int log_blowu
 
 int run_merkle_leaves(whir_ctx* ctx, const uint32_t* rows, int log_h, int row_words, int leaf_hash,
                       uint32_t* digests) {
+  if (leaf_hash == WHIR_LEAF_KECCAK) {
+    WH_TRY_CUDA(wk::keccak_leaves(rows, log_h, row_words, digests, ctx->stream));
+    return WHIR_OK;
+  }
   wk::Shape sh = wk::merkle_leaf_default();
   if (((size_t)1 << log_h) >= (size_t)wk::kMerkleLevelPairMin) {
     const Key k{WHIR_TUNE_MERKLE_LEAVES, ctx->device, log_h, row_words, leaf_hash, 0};
@@ -288,7 +292,14 @@ int run_merkle_leaves(whir_ctx* ctx, const uint32_t* rows, int log_h, int row_wo
   return WHIR_OK;
 }
 
-int run_merkle_upper(whir_ctx* ctx, int log_h, uint32_t* digests, uint32_t* posted_seq) {
+int run_merkle_upper(whir_ctx* ctx, int log_h, int leaf_hash, uint32_t* digests, uint32_t* posted_seq) {
+  if (leaf_hash == WHIR_LEAF_KECCAK) {
+    const uint32_t seq = posted_seq && ctx->h_mail ? mail_next(ctx) : 0u;
+    int posted = 0;
+    WH_TRY_CUDA(wk::keccak_upper(log_h, digests, seq ? ctx->d_mail : nullptr, seq, &posted, ctx->stream));
+    if (posted_seq) *posted_seq = posted ? seq : 0u;
+    return WHIR_OK;
+  }
   unsigned* counter = reinterpret_cast<unsigned*>(ctx->d_words) + 10;
   wk::Shape sh = wk::merkle_node_default();
   // the two-level kernel runs only on levels wider than 2^15 nodes
