@@ -460,10 +460,14 @@ class DeviceArray:
         return d
 
     def to_host(self, words: int | None = None) -> np.ndarray:
+        return mont_decode(self.raw(words))
+
+    def raw(self, words: int | None = None) -> np.ndarray:
+        """The words as stored (Keccak digests are raw bytes, not field words)."""
         w = self.words if words is None else words
         out = np.zeros(w, dtype=np.uint32)
         _check(lib().whir_memcpy_d2h(self.ctx.handle, out.ctypes.data, self.ptr, w * 4))
-        return mont_decode(out)
+        return out
 
     def free(self) -> None:
         if self.ptr:
