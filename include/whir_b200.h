@@ -172,6 +172,11 @@ int whir_ctx_stage_work(whir_ctx* ctx, uint64_t* work, int32_t cap, int32_t rese
  * enable = 0 (default) makes one host round trip per step. Proofs are the
  * same either way. */
 int whir_ctx_set_device_transcript(whir_ctx* ctx, int32_t enable);
+/* A wait for a small device result (a root, coefficients, a witness) polls a
+ * flag in mapped host memory: it spins for `microseconds` (default 30), then
+ * polls with a yield between checks. 0 yields from the start (less host CPU
+ * per waiting context, e.g. many batch workers on few cores). */
+int whir_ctx_set_wait_spin(whir_ctx* ctx, int32_t microseconds);
 /* Host permutation with the context's data (width taken from the state length 16 or 24). */
 int whir_poseidon2_permute(const whir_ctx* ctx, uint32_t* state, int32_t width);
 
@@ -420,6 +425,8 @@ int whir_batch_memory(whir_batch* b, uint64_t* fixed_bytes, uint64_t* pool_reser
 /* whir_ctx_set_device_transcript on every worker context; jobs that start
  * afterwards use the setting (jobs already running keep theirs). */
 int whir_batch_set_device_transcript(whir_batch* b, int32_t enable);
+/* whir_ctx_set_wait_spin on every worker context */
+int whir_batch_set_wait_spin(whir_batch* b, int32_t microseconds);
 /* Enqueue (non-blocking). The job and its buffers must stay valid until it is done. */
 int whir_batch_submit(whir_batch* b, whir_job* job);
 /* Wait for one job (timeout_ms < 0: no limit); returns the job's status. */

@@ -148,6 +148,8 @@ _SIGS = {
     "whir_batch_destroy": (C.c_int, [_vp]),
     "whir_batch_memory": (C.c_int, [_vp, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]),
     "whir_batch_set_device_transcript": (C.c_int, [_vp, _i32]),
+    "whir_batch_set_wait_spin": (C.c_int, [_vp, _i32]),
+    "whir_ctx_set_wait_spin": (C.c_int, [_vp, _i32]),
     "whir_batch_submit": (C.c_int, [_vp, C.POINTER(Job)]),
     "whir_batch_wait": (C.c_int, [_vp, C.POINTER(Job), _i32]),
     "whir_batch_wait_all": (C.c_int, [_vp]),
@@ -421,6 +423,10 @@ class Context:
         cnt = np.zeros(8, dtype=np.uint64)
         _check(lib().whir_ctx_stage_times(self.handle, ms.ctypes.data, cnt.ctypes.data, 8, int(reset)))
         return {name: (float(m), int(c)) for name, m, c in zip(self.STAGES, ms, cnt)}
+
+    def set_wait_spin(self, microseconds: int) -> None:
+        """How long a wait for a small device result spins before yielding."""
+        _check(lib().whir_ctx_set_wait_spin(self.handle, int(microseconds)))
 
     def set_device_transcript(self, enable: bool) -> None:
         """Sumcheck stages with their transcript steps on the device, or with
@@ -879,6 +885,10 @@ class Batch:
         f, r = C.c_uint64(0), C.c_uint64(0)
         _check(lib().whir_batch_memory(self.handle, C.byref(f), C.byref(r)))
         return f.value, r.value
+
+    def set_wait_spin(self, microseconds: int) -> None:
+        """Context.set_wait_spin on every worker."""
+        _check(lib().whir_batch_set_wait_spin(self.handle, int(microseconds)))
 
     def set_device_transcript(self, enable: bool) -> None:
         """Context.set_device_transcript on every worker (jobs started later)."""

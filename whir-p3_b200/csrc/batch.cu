@@ -246,6 +246,13 @@ int whir_batch_set_device_transcript(whir_batch* b, int32_t enable) {
   return WHIR_OK;
 }
 
+int whir_batch_set_wait_spin(whir_batch* b, int32_t microseconds) {
+  WH_CHECK(b, "null batch");
+  std::lock_guard<std::mutex> lk(b->mu);
+  for (whir_ctx* c : b->ctxs) WH_TRY(whir_ctx_set_wait_spin(c, microseconds));
+  return WHIR_OK;
+}
+
 int whir_batch_destroy(whir_batch* b) {
   if (!b) return WHIR_OK;
   {

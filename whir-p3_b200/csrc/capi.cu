@@ -172,12 +172,13 @@ int mail_wait(whir_ctx* ctx, uint32_t seq, void* host, size_t bytes) {
   // is posted, not when the work queued behind its producer is done.
   using clk = std::chrono::steady_clock;
   const auto t0 = clk::now();
-  bool spinning = true;
+  const auto spin = std::chrono::microseconds(ctx->wait_spin_us.load(std::memory_order_relaxed));
+  bool spinning = spin.count() > 0;
   auto next_query = t0;
   for (uint64_t n = 1; *flag != seq; n++) {
     if (spinning) {
       cpu_relax();
-      if ((n & 255) == 0 && clk::now() - t0 > std::chrono::microseconds(30)) spinning = false;
+      if ((n & 255) == 0 && clk::now() - t0 > spin) spinning = false;
       continue;
     }
     std::this_thread::yield();
@@ -558,6 +559,13 @@ int whir_ctx_stage_times(whir_ctx* ctx, double* ms, uint64_t* counts, int32_t ca
       ctx->stage_launches[i] = 0;
     }
   return wh::kStCount;
+}
+
+int whir_ctx_set_wait_spin(whir_ctx* ctx, int32_t microseconds) {
+  WH_TRY(check_ctx(ctx));
+  WH_CHECK(microseconds >= 0 && microseconds <= 100000, "spin time out of range");
+  ctx->wait_spin_us.store(microseconds);
+  return WHIR_OK;
 }
 
 int whir_ctx_set_device_transcript(whir_ctx* ctx, int32_t enable) {

@@ -180,6 +180,9 @@ struct whir_ctx {
   // whir_ctx_set_device_transcript); off: each step round-trips to the host.
   // Atomic: a batch may switch it while its worker proves.
   std::atomic<bool> device_transcript{false};
+  // how long a wait for a device result spins before it polls with yields
+  // (whir_ctx_set_wait_spin)
+  std::atomic<int> wait_spin_us{30};
   std::vector<cudaEvent_t> event_pool;
   std::vector<std::pair<int, std::pair<cudaEvent_t, cudaEvent_t>>> stage_events;
   double stage_ms[wh::kStCount] = {};
