@@ -33,6 +33,11 @@ proof-of-work grinding), each timed alone with CUDA events on the context's
 stream and printed as one JSON line per kernel:
 
   python bench.py --micro all|eq|eval|fold|dft|merkle|grind [--steps K]
+
+The default run (N = 1) also reports, in its one JSON line: `extra` (n = 24
+with four constraints, n = 26 with one and four), `micro` (the kernel
+micro-benchmarks above, 5 timed runs each), `batched`, `served` (the rate
+sweep), `cpu_baseline`, the per-stage `rooflines` and `autotune`.
 """
 from __future__ import annotations
 
@@ -298,6 +303,15 @@ def cpu_baseline_sample() -> dict:
 
 
 def run_micro(args) -> None:
+    kinds = ["eq", "eval", "fold", "dft", "merkle", "grind"] if args.micro == "all" else [args.micro]
+    micro_lines(kinds, args.steps, args.warmup, echo=True)
+
+
+def micro_lines(kinds, steps: int, warmup: int, echo: bool = False) -> list:
+    """The kernel micro-benchmarks (eq table, evaluations and fold of 2^24
+    extension entries, the commitment LDE, the 2^21-leaf Merkle tree, an
+    18-bit proof-of-work search), each timed alone with CUDA events; one dict
+    per measurement (printed as a JSON line each with `echo`)."""
     import torch
 
     import __graft_entry__
@@ -311,10 +325,11 @@ def run_micro(args) -> None:
     hbm = float(peaks.get("hbm_gbs", 6650.0))
     flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
     rng = np.random.default_rng(7)
-    reps = max(args.steps, 1)
+    reps = max(steps, 1)
+    lines = []
 
     def timed(fn):
-        for _ in range(max(args.warmup, 1)):  # the launch-shape tuner runs here, on first use
+        for _ in range(max(warmup, 1)):  # the launch-shape tuner runs here, on first use
             fn()
         total = 0.0
         # the timed launches only, for a profiler run with --profile-from-start off
@@ -338,9 +353,10 @@ def run_micro(args) -> None:
         if units is not None:
             line[unit_name] = round(units / (ms * 1e-3), 1)
         line.update(extra or {})
-        print(json.dumps(line), flush=True)
+        lines.append(line)
+        if echo:
+            print(json.dumps(line), flush=True)
 
-    kinds = ["eq", "eval", "fold", "dft", "merkle", "grind"] if args.micro == "all" else [args.micro]
     n = 24
     N = 1 << n
     if any(k in kinds for k in ("eq", "eval", "fold")):
@@ -393,6 +409,7 @@ def run_micro(args) -> None:
              extra={"candidates_evaluated_per_call": [int(v) for v in evaluated],
                     "note": "one Poseidon2-16 permutation per evaluated candidate; expected 2^bits per search"})
     ctx.close()
+    return lines
 
 
 def batch_jobs(pkg, count: int, seed: int):
@@ -670,6 +687,10 @@ def main() -> None:
         for rate in [float(x) for x in args.rates.split(",")]:
             count = int(min(400, max(40, rate * 1.0)))
             serve.append(run_serve(pkg, ctx, local, rate, args.workers, count, 5))
+    micro = None
+    if rank == 0 and world == 1 and not args.no_extra:
+        # the kernel micro-benchmarks at their reference sizes (5 timed runs each)
+        micro = micro_lines(["eq", "eval", "fold", "dft", "merkle", "grind"], 5, 2)
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline_sample()
@@ -689,7 +710,7 @@ def main() -> None:
                 "stages_ms_per_proof": stages_ms,
                 "autotune": autotune,
                 "cpu_baseline": cpu, "clocks": clk,
-                "extra": extra, "batched": batch, "served": serve}
+                "extra": extra, "micro": micro, "batched": batch, "served": serve}
         print(json.dumps(line), flush=True)
     ctx.close()
     if dist is not None:
