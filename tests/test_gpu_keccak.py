@@ -80,3 +80,28 @@ def test_keccak_split_api_refused(pkg, gpu_ctx):
     writer = pkg.CommitmentWriter(pkg.WhirConfig(10, params))
     with pytest.raises(pkg.WhirError):
         writer.commit(gpu_ctx, pkg.DuplexChallenger(gpu_ctx), st)
+
+
+def test_keccak_in_batch_and_with_device_transcript_switch(pkg, gpu_ctx, oracle):
+    """Keccak jobs through the worker pool mixed with Poseidon2 jobs give the
+    same proofs as one at a time; the device-transcript switch, which covers
+    the duplex challenger only, leaves a Keccak proof unchanged."""
+    rng = np.random.default_rng(31)
+    jobs = []
+    for i, (n, leaf) in enumerate([(12, "keccak"), (13, "poseidon2_24"), (14, "keccak"), (12, "poseidon2_16")]):
+        params = pkg.ProtocolParameters(64, 10, pkg.FoldingFactor.constant(4), pkg.SecurityAssumption.CapacityBound,
+                                        1, 1, leaf, 4 if leaf == "keccak" else 8)
+        jobs.append((params, n, rnd(rng, 1 << n), rnd(rng, 4 * n)))
+    alone = [pkg.commit_and_prove(gpu_ctx, p, n, poly, pt)[0] for p, n, poly, pt in jobs]
+    with pkg.Batch(gpu_ctx.device, workers=3) as b:
+        reqs = [pkg.ProofRequest(p, n, poly, pt) for p, n, poly, pt in jobs]
+        b.run(reqs)
+    for r, a in zip(reqs, alone):
+        assert np.array_equal(r.proof, a)
+    gpu_ctx.set_device_transcript(True)
+    try:
+        p, n, poly, pt = jobs[2]
+        again = pkg.commit_and_prove(gpu_ctx, p, n, poly, pt)[0]
+    finally:
+        gpu_ctx.set_device_transcript(False)
+    assert np.array_equal(again, alone[2])
