@@ -388,6 +388,10 @@ def micro_lines(kinds, steps: int, warmup: int, echo: bool = False) -> list:
         ms = timed(lambda: pkg.merkle_commit(ctx, rows, log_h, words, 0, dig))
         emit("merkle 2^21 leaves x 16 (P24 leaves, P16 nodes)", ms, alg_bytes=4 * words << log_h,
              units=2 * (1 << log_h) - 1, unit_name="permutations/s")
+        # the Keccak MMCS of the reference's Keccak configuration on the same rows
+        ms = timed(lambda: pkg.merkle_commit(ctx, rows, log_h, words, 2, dig))
+        emit("merkle 2^21 leaves x 16 (Keccak MMCS)", ms, alg_bytes=4 * words << log_h,
+             units=2 * (1 << log_h) - 1, unit_name="keccak_f/s")
     if "grind" in kinds:
         bits = 18
         ch = pkg.DuplexChallenger(ctx)
