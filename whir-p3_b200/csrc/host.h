@@ -183,6 +183,16 @@ struct whir_ctx {
   // how long a wait for a device result spins before it polls with yields
   // (whir_ctx_set_wait_spin)
   std::atomic<int> wait_spin_us{30};
+  // the challenger after the domain separator, per (parameters, size): where a
+  // whir_commit_and_prove starts (observing the pattern is a few dozen host
+  // permutations, ahead of the first launch); a handful of entries, the
+  // oldest replaced
+  struct DsEntry {
+    whir_protocol_params params;
+    int32_t n;
+    wh::Chal ch;
+  };
+  std::vector<DsEntry> ds_cache;
   std::vector<cudaEvent_t> event_pool;
   std::vector<std::pair<int, std::pair<cudaEvent_t, cudaEvent_t>>> stage_events;
   double stage_ms[wh::kStCount] = {};

@@ -867,9 +867,20 @@ int whir_commit_and_prove(whir_ctx* ctx, const whir_protocol_params* params, int
   WH_TRY(wh::config_new(*params, n, &cfg));
   WH_CHECK(ctx->device >= 0, "host-only context (device -1) cannot run device work");
   wh::Chal ch;
-  if (params->leaf_hash == WHIR_LEAF_KECCAK) ch.init_keccak();
-  else ch.init();
-  for (uint32_t v : wh::domain_separator(cfg, params->ds_digest_elems)) ch.observe(ctx->hp16, kb::to_mont(v));
+  bool cached = false;
+  for (const whir_ctx::DsEntry& e : ctx->ds_cache)
+    if (e.n == n && memcmp(&e.params, params, sizeof(*params)) == 0) {
+      ch = e.ch;
+      cached = true;
+      break;
+    }
+  if (!cached) {
+    if (params->leaf_hash == WHIR_LEAF_KECCAK) ch.init_keccak();
+    else ch.init();
+    for (uint32_t v : wh::domain_separator(cfg, params->ds_digest_elems)) ch.observe(ctx->hp16, kb::to_mont(v));
+    if (ctx->ds_cache.size() >= 8) ctx->ds_cache.erase(ctx->ds_cache.begin());
+    ctx->ds_cache.push_back(whir_ctx::DsEntry{*params, n, ch});
+  }
   whir_witness* w = nullptr;
   WH_TRY(commit_with(ctx, params, n, poly, poly_on_device, user_points, num_points, user_evals_out, ch, &w));
   int s = prove_with(ctx, w, ch, proof_out, cap_words, proof_words);
