@@ -71,6 +71,12 @@ def test_keccak_proofs_with_grinding(pkg, gpu_ctx, oracle, n, pw, k, snd, rate, 
     run_keccak(pkg, gpu_ctx, oracle, n, 64, pw, k, snd, rate, rs, npts, 500 + n)
 
 
+@pytest.mark.parametrize("n,k,rs,npts", [(2, 1, 1, 1), (4, 2, 1, 0), (6, 3, 2, 2), (8, 4, 3, 1), (9, 2, 1, 3)])
+def test_keccak_small_shapes(pkg, gpu_ctx, oracle, n, k, rs, npts):
+    """Small sizes and folding factors (one-CTA trees, no four-step DFT)."""
+    run_keccak(pkg, gpu_ctx, oracle, n, 32, 4, k, 2, 1, rs, npts, 900 + 10 * n + k)
+
+
 def test_keccak_split_api_refused(pkg, gpu_ctx):
     """The split commit / prove API carries the duplex challenger's state; the
     Keccak configuration is refused there with an error, not proved wrongly."""
