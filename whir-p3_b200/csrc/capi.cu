@@ -763,7 +763,8 @@ int whir_merkle_open_ex(whir_ctx* ctx, const uint32_t* d_rows, const uint32_t* d
                         int32_t row_words, int32_t leaf_hash, uint64_t index, uint32_t* row_out,
                         uint32_t* path_out) {
   WH_TRY(check_gpu(ctx));
-  WH_CHECK(d_rows && d_digests && row_out && path_out && index < (1ull << log_height) && row_words > 0,
+  WH_CHECK(d_rows && d_digests && row_out && path_out && index < (1ull << log_height) && row_words > 0 &&
+               (leaf_hash == WHIR_LEAF_P24 || leaf_hash == WHIR_LEAF_P16 || leaf_hash == WHIR_LEAF_KECCAK),
            "bad opening arguments");
   uint64_t* d_idx = reinterpret_cast<uint64_t*>(ctx->d_arena);
   uint32_t* d_row = reinterpret_cast<uint32_t*>(d_idx + 8);
