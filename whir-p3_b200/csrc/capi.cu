@@ -254,12 +254,12 @@ int grind(whir_ctx* ctx, Chal& ch, int bits, uint32_t* witness) {
       WH_TRY_CUDA(wk::grind(ch.st, ch.in, ch.in_len, bits, kb::P, ctx->d_words, ctx->d_words + 1, ctx->d_words + 2,
                             ctx->h_mail ? ctx->d_mail : nullptr, seq, ctx->p16, ctx->stream));
   }
-  // with a mailbox the search posts its witness and the number of claims of
-  // kGrindClaim candidates it evaluated
+  // with a mailbox the search posts its witness and the number of candidates
+  // it evaluated
   uint32_t got[2] = {0u, 0u};
   WH_TRY(fetch_posted(ctx, ctx->h_mail ? seq : 0u, got, ctx->d_words, ctx->h_mail ? 8 : 4));
   const uint32_t w = got[0];
-  if (ctx->h_mail) add_stage_work(ctx, kStGrind, (uint64_t)got[1] * wk::kGrindClaim);
+  if (ctx->h_mail) add_stage_work(ctx, kStGrind, (uint64_t)got[1]);
   if (w >= kb::P) {
     set_error("proof-of-work search found no witness");
     return WHIR_ERR_NOT_FOUND;

@@ -125,7 +125,7 @@ constexpr size_t kDftTableWords = 2 * 4096;
 constexpr int kUploadGroups = 8;  // chunk groups of a pipelined polynomial upload
 // device transcript area: DevChal at word 0, the search's folded state at
 // kTrCp, the error word at kTrErr, then per sumcheck round (kTrRound words):
-// c0 and c2 (8 words), the witness and its evaluated-claim count (2), the
+// c0 and c2 (8 words), the witness and its evaluated-candidate count (2), the
 // sampled challenge (4 words, at offset 12)
 constexpr int kDevTrWords = 1024;
 constexpr int kTrCp = 40, kTrErr = 64, kTrLog = 68, kTrRound = 16;

@@ -97,7 +97,7 @@ __global__ void __launch_bounds__(KECCAK_TOP) k_keccak_top(uint32_t* __restrict_
 // so far (lanes and position in the current block). Claims of KECCAK_CLAIM
 // candidates, CTA b's first claim chunk b, later claims from the counter;
 // the smallest valid witness wins; the last CTA to stop posts the witness and
-// the counter's claims and resets the search state.
+// the candidates the counter's claims cover and resets the search state.
 constexpr int KECCAK_CLAIM = 128;
 __global__ void __launch_bounds__(KECCAK_CLAIM) k_keccak_grind(const __grid_constant__ kk::K256 in, int bits,
                                                               uint64_t limit, uint32_t* result, uint32_t* counter,
@@ -122,7 +122,7 @@ __global__ void __launch_bounds__(KECCAK_CLAIM) k_keccak_grind(const __grid_cons
       if (threadIdx.x == 0 && mail) {
         __threadfence();
         if (atomicAdd(done, 1u) == gridDim.x - 1) {
-          const uint32_t post[2] = {atomicAdd(result, 0u), atomicAdd(counter, 0u)};
+          const uint32_t post[2] = {atomicAdd(result, 0u), atomicAdd(counter, 0u) * (uint32_t)KECCAK_CLAIM};
           if (mail) mail_post(mail, post, 2, seq);
           *result = kb::P;
           *counter = 0u;

@@ -149,13 +149,14 @@ cudaError_t grind_reset(uint32_t* result, uint32_t* counter, uint32_t* done, cud
 // p2::grind_fold) is read from device memory instead of being formed from
 // `state` and `in` on the host (in_len still selects the witness position);
 // with `res_out` set, the last CTA to stop writes the witness and the number of
-// evaluated claims there (2 words) and resets the search state, and no
-// initialising launch precedes the search. A claim is kGrindClaim candidates.
+// evaluated candidates there (2 words) and resets the search state, and no
+// initialising launch precedes the search. Searches of up to kCoopGrindBits bits run the four-lane
+// permutation (lower latency per pass, more instructions per candidate).
 // With `ch` set (res_out, r_out and err too), the search's last CTA also runs
 // the transcript step after it on the device challenger: observe the witness,
 // check that sample_bits(bits) is 0, sample the round's challenge into r_out
 // (a failed check sets bit 0, no witness, or bit 1, check failed, of *err).
-constexpr int kGrindClaim = 128;
+constexpr int kCoopGrindBits = 11;
 struct DevChal;
 cudaError_t grind(const uint32_t* state, const uint32_t* in, int in_len, int bits, uint64_t limit,
                   uint32_t* result, uint32_t* counter, uint32_t* done, uint32_t* mail, uint32_t seq,

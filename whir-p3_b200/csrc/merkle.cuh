@@ -267,17 +267,21 @@ __device__ __forceinline__ void coop_ext_layer(uint32_t (&x)[4]) {
 // and that sum of products (two shuffles) runs beside the S-box; a round's
 // chain is S-box, one addition and the product by 15. ROLLED keeps the round
 // loops rolled: a kernel that permutes once or twice (the challenger steps)
-// would otherwise spend its time fetching the unrolled code.
+// would otherwise spend its time fetching the unrolled code. FROM_SBOX: x
+// already holds the first S-box inputs (the initial external layer and the
+// first round constants applied, as the proof-of-work search folds them).
 __device__ __forceinline__ uint32_t cube_m(uint32_t a) { return kb::mul(kb::mul(a, a), a); }
-template <int MAT, bool ROLLED = false>
+template <int MAT, bool ROLLED = false, bool FROM_SBOX = false>
 __device__ __forceinline__ void coop_permute16_m(uint32_t (&x)[4], int q, const P2Consts& k) {
   using namespace kb;
+  static_assert(!(ROLLED && FROM_SBOX), "the search form is unrolled");
   constexpr uint32_t k15s = (uint32_t)((15ull << 32) / P);  // Shoup constant of 15
-  coop_ext_layer<MAT>(x);
+  if (!FROM_SBOX) coop_ext_layer<MAT>(x);
 #pragma unroll(ROLLED ? 1 : p2::RF / 2)
   for (int r = 0; r < p2::RF / 2; r++) {
 #pragma unroll
-    for (int j = 0; j < 4; j++) x[j] = cube_m(add(x[j], k.ext_rc_m[r * 16 + 4 * q + j]));
+    for (int j = 0; j < 4; j++)
+      x[j] = cube_m(FROM_SBOX && r == 0 ? x[j] : add(x[j], k.ext_rc_m[r * 16 + 4 * q + j]));
     coop_ext_layer<MAT>(x);
   }
   // word 0 lives in w0 on every lane; lane 0's x[0] is not read again until
@@ -714,19 +718,23 @@ __device__ bool dc_witness_step(DevChal& c, uint32_t w, int bits, ef* r_out, uin
 // ---------------------------------------------------------------------------
 
 namespace {
-constexpr int GRIND_CTA = kGrindClaim;  // 128: one warp per SM sub-partition
+constexpr int GRIND_CTA = 128;  // one warp per SM sub-partition
 
-// Each claim is GRIND_CTA consecutive candidates, one per thread; CTA b's
-// first claim is chunk b, later claims come from the counter (chunks
-// gridDim.x, gridDim.x + 1, ...). With `ch` set (and res_out), the last CTA's
-// first warp also runs the transcript step that follows the search on the
-// device challenger (dc_witness_step).
-template <int SLOT, int MAT>
+// Each claim is CLAIM consecutive candidates: one per thread (COOP false), or
+// one per four-lane group (COOP true: the four-lane Montgomery permutation,
+// whose latency is about 40 % of a one-thread permutation's, for searches
+// small enough that one pass's latency sets their time). CTA b's first claim
+// is chunk b, later claims come from the counter (chunks gridDim.x,
+// gridDim.x + 1, ...). With `ch` set (and res_out), the last CTA's first warp
+// also runs the transcript step that follows the search on the device
+// challenger (dc_witness_step).
+template <int SLOT, int MAT, bool COOP>
 __global__ void __launch_bounds__(GRIND_CTA, 10) k_grind(const __grid_constant__ P2Consts p16, uint4 st0, uint4 st1,
                                                       uint4 st2, uint4 st3, int bits, uint64_t limit,
                                                       uint32_t* result, uint32_t* counter, uint32_t* done,
                                                       uint32_t* mail, uint32_t seq, const uint32_t* cp_dev,
                                                       uint32_t* res_out, DevChal* ch, ef* r_out, uint32_t* err) {
+  constexpr int CLAIM = COOP ? GRIND_CTA / 4 : GRIND_CTA;
   __shared__ uint64_t s_start;
   __shared__ int s_go;
   __shared__ bool s_last;
@@ -739,10 +747,23 @@ __global__ void __launch_bounds__(GRIND_CTA, 10) k_grind(const __grid_constant__
 #pragma unroll
     for (int i = 0; i < 16; i++) cp[i] = __ldcg(cp_dev + i);
   }
+  // the four-lane form: lane q's words 4q .. 4q+3 of the folded state and of
+  // the witness column, in Montgomery form
+  uint32_t cpm[4] = {0u, 0u, 0u, 0u}, colm[4] = {0u, 0u, 0u, 0u};
+  const int q = threadIdx.x & 3;
+  if constexpr (COOP) {
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+      // word 4q + j of cp, selected without indexing the array by a lane value
+      const uint32_t v = q == 0 ? cp[j] : q == 1 ? cp[4 + j] : q == 2 ? cp[8 + j] : cp[12 + j];
+      cpm[j] = kb::to_mont(v);
+      colm[j] = kb::to_mont((uint32_t)p2::ext_col16<MAT>(SLOT, 4 * q + j));
+    }
+  }
   for (bool first = true;; first = false) {
     if (threadIdx.x == 0) {
       const uint64_t chunk = first ? (uint64_t)blockIdx.x : (uint64_t)gridDim.x + atomicAdd(counter, 1u);
-      const uint64_t start = chunk * GRIND_CTA;
+      const uint64_t start = chunk * CLAIM;
       s_start = start;
       s_go = start < limit && start < (uint64_t)*(volatile uint32_t*)result;
     }
@@ -753,17 +774,17 @@ __global__ void __launch_bounds__(GRIND_CTA, 10) k_grind(const __grid_constant__
     if (!go) {
       // every atomicMin of this CTA precedes the barriers above; the last CTA
       // to stop holds the final result, posts it to the mailbox with the
-      // number of claims that were evaluated (the counter's claims: every CTA
-      // evaluated its first claim and made exactly one claim that it did not
-      // evaluate) and resets the search state for the next search (every
-      // other CTA has finished with it), which then needs no initialising
-      // launch
+      // number of candidates evaluated (the counter's claims times the claim
+      // size: every CTA evaluated its first claim and made exactly one claim
+      // that it did not evaluate) and resets the search state for the next
+      // search (every other CTA has finished with it), which then needs no
+      // initialising launch
       if (threadIdx.x == 0) {
         s_last = false;
         if (mail || res_out) {
           __threadfence();
           if (atomicAdd(done, 1u) == gridDim.x - 1) {
-            const uint32_t post[2] = {atomicAdd(result, 0u), atomicAdd(counter, 0u)};
+            const uint32_t post[2] = {atomicAdd(result, 0u), atomicAdd(counter, 0u) * (uint32_t)CLAIM};
             if (mail) mail_post(mail, post, 2, seq);
             if (res_out) {
               res_out[0] = post[0];
@@ -784,13 +805,26 @@ __global__ void __launch_bounds__(GRIND_CTA, 10) k_grind(const __grid_constant__
       if (dc_witness_step<MAT>(c, s_w, bits, r_out, err, p16)) dc_store(c, ch);
       return;
     }
-    const uint64_t w = start + threadIdx.x;
-    // a witness below this claim's first candidate makes the claim useless, so
-    // its threads may stop early; they read the same condition (up to a
-    // witness landing between their reads), and a stopped candidate is never
-    // one the smallest witness could be
-    const auto stop = [result, start] { return (uint64_t)*(volatile uint32_t*)result < start; };
-    if (w < limit && (p2::grind_word7<SLOT, MAT>((uint32_t)w, cp, p16, stop) & mask) == 0u) atomicMin(result, (uint32_t)w);
+    if constexpr (COOP) {
+      // every lane runs the permutation (its shuffles take the whole warp);
+      // word 7 of the output is lane 1's last word
+      const uint64_t w = start + (threadIdx.x >> 2);
+      const uint32_t wm = kb::to_mont(w < limit ? (uint32_t)w : 0u);
+      uint32_t x[4];
+#pragma unroll
+      for (int j = 0; j < 4; j++) x[j] = kb::add(cpm[j], kb::mul(wm, colm[j]));
+      coop_permute16_m<MAT, false, true>(x, q, p16);
+      if (q == 1 && w < limit && (kb::from_mont(x[3]) & mask) == 0u) atomicMin(result, (uint32_t)w);
+    } else {
+      const uint64_t w = start + threadIdx.x;
+      // a witness below this claim's first candidate makes the claim useless,
+      // so its threads may stop early; they read the same condition (up to a
+      // witness landing between their reads), and a stopped candidate is
+      // never one the smallest witness could be
+      const auto stop = [result, start] { return (uint64_t)*(volatile uint32_t*)result < start; };
+      if (w < limit && (p2::grind_word7<SLOT, MAT>((uint32_t)w, cp, p16, stop) & mask) == 0u)
+        atomicMin(result, (uint32_t)w);
+    }
   }
 }
 
@@ -833,9 +867,27 @@ cudaError_t grind_m(const uint32_t* state, const uint32_t* in, int in_len, int b
   // small to fill the GPU runs one CTA per SM with about 2^(bits+3)
   // candidates in flight: the first pass then holds a witness with
   // probability 1 - e^-8, and the pass costs no more than a narrower one.
+  // Searches of up to kCoopGrindBits bits (2^(bits+3) candidates in flight in
+  // at most 4 CTAs per SM) run the four-lane form: one pass is a four-lane
+  // permutation's latency instead of a one-thread permutation's.
   static const int kPerSm[7] = {1, 2, 3, 4, 6, 8, 10};
   static const double kRate[7] = {0.467, 0.703, 0.811, 0.865, 0.911, 0.948, 0.965};
   const double expect = (double)(1ull << bits);
+  const bool coop = bits <= kCoopGrindBits;
+  if (coop) {
+    const unsigned blocks = (unsigned)(((8ull << bits) + GRIND_CTA / 4 - 1) / (GRIND_CTA / 4));
+    switch (in_len) {
+#define WK_GRIND_COOP(S)                                                                                          \
+  case S:                                                                                                        \
+    k_grind<S, MAT, true><<<blocks, GRIND_CTA, 0, st>>>(p16, a, b, c, d, bits, limit, result, counter, done, mail, \
+                                                        seq, cp_dev, res_out, ch, r_out, err);                    \
+    break;
+      WK_GRIND_COOP(0) WK_GRIND_COOP(1) WK_GRIND_COOP(2) WK_GRIND_COOP(3) WK_GRIND_COOP(4) WK_GRIND_COOP(5)
+      WK_GRIND_COOP(6) WK_GRIND_COOP(7)
+#undef WK_GRIND_COOP
+    }
+    LAUNCH_DONE();
+  }
   unsigned blocks = (unsigned)(((8ull << bits) + GRIND_CTA - 1) / GRIND_CTA);
   if (blocks > (unsigned)sm_count()) {
     double best = 0.0;
@@ -853,8 +905,8 @@ cudaError_t grind_m(const uint32_t* state, const uint32_t* in, int in_len, int b
   switch (in_len) {
 #define WK_GRIND(S) \
   case S:                                                                                                      \
-    k_grind<S, MAT><<<blocks, GRIND_CTA, 0, st>>>(p16, a, b, c, d, bits, limit, result, counter, done, mail, seq, \
-                                                  cp_dev, res_out, ch, r_out, err);                             \
+    k_grind<S, MAT, false><<<blocks, GRIND_CTA, 0, st>>>(p16, a, b, c, d, bits, limit, result, counter, done, mail, \
+                                                         seq, cp_dev, res_out, ch, r_out, err);                    \
     break;
     WK_GRIND(0) WK_GRIND(1) WK_GRIND(2) WK_GRIND(3) WK_GRIND(4) WK_GRIND(5) WK_GRIND(6) WK_GRIND(7)
 #undef WK_GRIND

@@ -408,7 +408,7 @@ int sumcheck_stage_device(whir_ctx* ctx, wh::Chal& ch, Sumcheck& sd, ef* d_f, ef
     ch.observe_ef(ctx->hp16, c2);
     if (pow_bits > 0) {
       const uint32_t w = rec[8];
-      wh::add_stage_work(ctx, wh::kStGrind, (uint64_t)rec[9] * wk::kGrindClaim);
+      wh::add_stage_work(ctx, wh::kStGrind, (uint64_t)rec[9]);
       ch.observe(ctx->hp16, kb::to_mont(w));
       if (ch.sample_bits(ctx->hp16, pow_bits) != 0) return wh::set_error("device grinding returned an invalid witness"), WHIR_ERR_CUDA;
       sd.pows.push_back(w);
