@@ -91,6 +91,7 @@ int ensure_dft_tables(whir_ctx* ctx, int log_h, wk::DftTables* t) {
   t->tw_sh = reinterpret_cast<const uint2*>(ctx->tw_stage + 2048);
   t->tw_lo = ctx->tw_heights + (size_t)log_h * kDftTableWords;
   t->tw_hi = t->tw_lo + 4096;
+  t->err = ctx->d_words + 12;
   return WHIR_OK;
 }
 

@@ -8,6 +8,53 @@
 
 namespace wk {
 
+// mbarrier and bulk-copy helpers: one elected thread arms the barrier with the
+// byte count and issues the copies; the threads wait on the barrier's phase
+// with a bounded number of polls.
+namespace bulk {
+constexpr uint32_t kPolls = 1u << 22;  // bound on the polls of one wait
+__device__ __forceinline__ uint32_t saddr(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+__device__ __forceinline__ void bar_init(uint64_t* b) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(saddr(b)) : "memory");
+}
+__device__ __forceinline__ void bar_expect(uint64_t* b, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(saddr(b)), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ bool bar_test(uint64_t* b, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\tmbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, p;\n}"
+      : "=r"(ok)
+      : "r"(saddr(b)), "r"(parity)
+      : "memory");
+  return ok != 0u;
+}
+// Waits for the phase of `parity` to complete; false after kPolls polls.
+__device__ __forceinline__ bool bar_wait(uint64_t* b, uint32_t parity) {
+  for (uint32_t i = 0; i < kPolls; i++) {
+    if (bar_test(b, parity)) return true;
+    if (i >= 64) __nanosleep(128);
+  }
+  return false;
+}
+// contiguous bytes (16-byte aligned addresses, a multiple of 16 bytes)
+__device__ __forceinline__ void bulk_load(void* dst, const void* src, uint32_t bytes, uint64_t* b) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                   saddr(dst)),
+               "l"(src), "r"(bytes), "r"(saddr(b))
+               : "memory");
+}
+// one box of a three-dimensional tensor map (tile mode, no multicast) at
+// element coordinates (x, y, z); x counts elements of the innermost dimension
+__device__ __forceinline__ void tensor_load_3d(void* dst, const void* tmap, int x, int y, int z, uint64_t* b) {
+  asm volatile(
+      "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], "
+      "[%5];" ::"r"(saddr(dst)),
+      "l"(tmap), "r"(x), "r"(y), "r"(z), "r"(saddr(b))
+      : "memory");
+}
+}  // namespace bulk
+
 __device__ __forceinline__ kb::ef ld_ef(const kb::ef* p) {
   uint4 v = __ldg(reinterpret_cast<const uint4*>(p));
   return kb::ef{{v.x, v.y, v.z, v.w}};

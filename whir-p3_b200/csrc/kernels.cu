@@ -9,6 +9,9 @@
 // loops sized to the SM count; the Poseidon2 kernels keep the permutation state
 // in registers with every round constant an immediate (kernel parameters live
 // in the constant bank).
+#include <cuda.h>
+#include <cudaTypedefs.h>
+
 #include <atomic>
 #include <mutex>
 
@@ -492,19 +495,58 @@ __global__ void __launch_bounds__(1 << (LG + LT))
   }
 }
 
+namespace dftreg {
+// words of a register pass's exchange buffer, rounded up to 8 bytes, and the
+// dynamic shared memory of the TMA-staged pass 2 (the buffer, then its mbarrier)
+__host__ __device__ constexpr int xwords(int t, int vs) { return (t * vs + 1) & ~1; }
+
+// One tensor copy of this CTA's input tile into `tile`; true when every thread
+// may read it. Returns false (the caller then loads from global memory) when
+// the tile is not 128-byte aligned or the wait gives up; the latter waits once
+// more, bounded, for the copy in flight before the buffer is reused.
+__device__ __forceinline__ bool stage_tile(uint32_t* tile, uint64_t* bar, const CUtensorMap* tm, int y, int z,
+                                           uint32_t bytes, uint32_t* err) {
+  if ((bulk::saddr(tile) & 127u) != 0u) {
+    if (threadIdx.x == 0 && err) atomicOr(err, 2u);
+    return false;
+  }
+  if (threadIdx.x == 0) {
+    bulk::bar_init(bar);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    bulk::bar_expect(bar, bytes);
+    bulk::tensor_load_3d(tile, tm, 0, y, z, bar);
+  }
+  __syncthreads();
+  const bool ok = bulk::bar_wait(bar, 0);
+  if (__syncthreads_or(!ok)) {
+    if (threadIdx.x == 0) {
+      if (err) atomicOr(err, 1u);
+      bulk::bar_wait(bar, 0);
+    }
+    __syncthreads();
+    return false;
+  }
+  return true;
+}
+}  // namespace dftreg
+
 // pass 2: T = 2^LT word columns per CTA (one r1); loads with g fastest (rows
 // are contiguous in i2), outer DFTs and stores with t fastest (output rows are
 // contiguous in j). Extension data (ls = 2) runs each element's 4 words as 4
 // columns t = 4 * column + coefficient: loads take the coefficient fastest,
 // then g, and log_w counts words.
-template <int LE, int LG, int LT>
+// TMA: the CTA's input, T >> ls runs of N << ls contiguous words (one per
+// element column), arrives as one box of the tensor map `tm` (dimensions 256
+// words, (H << ls) / 256 rows of them, columns) in the exchange buffer, which
+// the threads read before they overwrite it with the exchange.
+template <int LE, int LG, int LT, bool TMA = false>
 __global__ void __launch_bounds__(1 << (LG + LT))
     k_dft_rows_reg(const uint32_t* __restrict__ y, uint32_t* __restrict__ out, int log_h1, int log_h, int log_w,
-                   int ls, const uint2* __restrict__ tw_sh) {
+                   int ls, const uint2* __restrict__ tw_sh, const __grid_constant__ CUtensorMap tm, uint32_t* err) {
   constexpr int E = 1 << LE, G = 1 << LG, T = 1 << LT, N = E * G;
   constexpr int RS = G + 1;
   constexpr int VS = dftreg::vstride<E, G>(T >= 32 ? 1 : 32 / T);
-  extern __shared__ uint32_t sm[];
+  extern __shared__ __align__(128) uint32_t sm[];
   const int r1 = blockIdx.x;
   const int j0 = blockIdx.y * T;
   {
@@ -513,9 +555,21 @@ __global__ void __launch_bounds__(1 << (LG + LT))
     const int tq = threadIdx.x >> (ls + LG);
     const int t = (tq << ls) | c;
     uint32_t a[E];
-    const uint32_t* src = y + (((((size_t)((j0 >> ls) + tq)) << log_h) + (size_t)r1 * N + g) << ls) + c;
+    bool staged = false;
+    if constexpr (TMA) {
+      uint64_t* bar = reinterpret_cast<uint64_t*>(sm + dftreg::xwords(T, VS));
+      staged = dftreg::stage_tile(sm, bar, &tm, (r1 * N << ls) >> 8, j0 >> ls, (uint32_t)(T * N * 4), err);
+    }
+    if (staged) {
+      const uint32_t* tile = sm + ((tq * N) << ls) + c;
 #pragma unroll
-    for (int e = 0; e < E; e++) a[e] = __ldg(src + ((size_t)(G * e) << ls));
+      for (int e = 0; e < E; e++) a[e] = tile[(g + G * e) << ls];
+      __syncthreads();  // the exchange below overwrites the tile
+    } else {
+      const uint32_t* src = y + (((((size_t)((j0 >> ls) + tq)) << log_h) + (size_t)r1 * N + g) << ls) + c;
+#pragma unroll
+      for (int e = 0; e < E; e++) a[e] = __ldg(src + ((size_t)(G * e) << ls));
+    }
     dftreg::dif<LE>(a);
 #pragma unroll
     for (int r = 0; r < E; r++) {
@@ -568,7 +622,8 @@ static size_t reg_smem(int m, int lt) {
 constexpr int kDftRegSmemMax = 128 * 1024;  // plans keep register-pass tiles within this
 template <typename K>
 static void raise_smem(K kernel) {
-  cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kDftRegSmemMax);
+  // the TMA-staged pass adds its mbarrier (and up to one padding word) past the tile
+  cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kDftRegSmemMax + 16);
 }
 
 template <int LE, int LG, int LT>
@@ -581,10 +636,53 @@ static void launch_cols_reg(dim3 grid, size_t smem, cudaStream_t st, const uint3
 }
 template <int LE, int LG, int LT>
 static void launch_rows_reg(dim3 grid, size_t smem, cudaStream_t st, const uint32_t* y, uint32_t* out, int log_h1,
-                            int log_h, int log_w, int ls, const DftTables& t) {
+                            int log_h, int log_w, int ls, const DftTables& t, const CUtensorMap* tm) {
+  if (tm) {
+    static std::once_flag once;
+    std::call_once(once, [] { raise_smem(k_dft_rows_reg<LE, LG, LT, true>); });
+    constexpr int E = 1 << LE, G = 1 << LG, T = 1 << LT;
+    const size_t bytes = (size_t)dftreg::xwords(T, dftreg::vstride<E, G>(T >= 32 ? 1 : 32 / T)) * 4 + 8;
+    k_dft_rows_reg<LE, LG, LT, true>
+        <<<grid, 1 << (LG + LT), bytes, st>>>(y, out, log_h1, log_h, log_w, ls, t.tw_sh, *tm, t.err);
+    return;
+  }
   static std::once_flag once;
   std::call_once(once, [] { raise_smem(k_dft_rows_reg<LE, LG, LT>); });
-  k_dft_rows_reg<LE, LG, LT><<<grid, 1 << (LG + LT), smem, st>>>(y, out, log_h1, log_h, log_w, ls, t.tw_sh);
+  k_dft_rows_reg<LE, LG, LT><<<grid, 1 << (LG + LT), smem, st>>>(y, out, log_h1, log_h, log_w, ls, t.tw_sh,
+                                                                  CUtensorMap{}, nullptr);
+}
+
+// cuTensorMapEncodeTiled from the driver, looked up once through the runtime
+// (no link-time dependency on the driver library)
+static PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
+  static std::once_flag once;
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+  std::call_once(once, [] {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPointByVersion("cuTensorMapEncodeTiled", &p, 12000, cudaEnableDefault, &q) ==
+            cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+  });
+  return fn;
+}
+
+// Tensor map of pass 2's input for the TMA-staged kernel: the scratch array
+// as `cols` element columns of H << ls words, viewed as (256 words, (H << ls)
+// / 256 rows, cols), boxes of (256, (N << ls) / 256, T >> ls). False when the
+// shape does not fit the copy engine's rules (the plain loads run instead).
+static bool rows_tensor_map(CUtensorMap* tm, const uint32_t* y, int log_h, int ls, int log_cols, int log_n,
+                            int log_t) {
+  const auto enc = tensor_map_encoder();
+  if (!enc || ((uintptr_t)y & 15u) != 0u || log_h + ls < 8 || log_n + ls < 8 || log_t < ls) return false;
+  const cuuint64_t dims[3] = {256u, (cuuint64_t)1 << (log_h + ls - 8), (cuuint64_t)1 << log_cols};
+  const cuuint64_t strides[2] = {1024u, (cuuint64_t)4 << (log_h + ls)};
+  const cuuint32_t box[3] = {256u, 1u << (log_n + ls - 8), 1u << (log_t - ls)};
+  const cuuint32_t estr[3] = {1u, 1u, 1u};
+  return enc(tm, CU_TENSOR_MAP_DATA_TYPE_UINT32, 3, const_cast<uint32_t*>(y), dims, strides, box, estr,
+             CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+             CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
 // supported (m, lt): pass 1 lt in {2, 3, 4}, pass 2 lt in {0, .., 4}
@@ -685,6 +783,7 @@ bool dft_plan_ok(const DftPlan& p, int log_chunk, int log_w, int log_blowup, int
   } else if (p.log_t1 < 0 || p.log_t1 > p.log_h2 || dft_tile_bytes(p.log_t1, log_h1, lanes) > kDftTileMax) {
     return false;
   }
+  if (p.reg2 < 0 || p.reg2 > 2 || p.reg1 < 0 || p.reg1 > 1) return false;
   if (p.reg2) {  // register pass 2: 2^8..2^12 points, 1..16 word columns per CTA (4..16 for extensions)
     if (p.log_t2 < ls || p.log_t2 > 4 || p.log_t2 > log_w + ls || p.threads2 != reg_threads(p.log_h2, p.log_t2) ||
         p.threads2 == 0 || reg_smem(p.log_h2, p.log_t2) > (size_t)kDftRegSmemMax)
@@ -753,6 +852,7 @@ void dft_candidates(int log_chunk, int log_w, int log_blowup, int lanes, DftPlan
         if (tile_ok(t2, h2)) push(DftPlan{h2, 0, 256, t2, th2, 0, 0});
     for (int t1 = 2; t1 <= 4; t1++) push(DftPlan{h2, t1, reg_threads(h1, t1), 0, 256, 1, 0});
     for (int t2 = 0; t2 <= 4; t2++) push(DftPlan{h2, 0, 256, t2, reg_threads(h2, t2), 0, 1});
+    for (int t2 = 0; t2 <= 4; t2++) push(DftPlan{h2, 0, 256, t2, reg_threads(h2, t2), 0, 2});
   }
   *count = n;
 }
@@ -814,8 +914,10 @@ cudaError_t dft_batch(const uint32_t* in, uint32_t* out, uint32_t* scratch, int 
   if ((passes & 2) && plan.reg2) {
     const int jt = 1 << plan.log_t2;
     dim3 grid(H1, (W << ls) / jt);
+    CUtensorMap tm;
+    const bool tma = plan.reg2 == 2 && rows_tensor_map(&tm, scratch, log_h, ls, log_w, log_h2, plan.log_t2);
     WK_REG_CASES(launch_rows_reg, log_h2, plan.log_t2, grid, reg_smem(log_h2, plan.log_t2), st, scratch, out,
-                 log_h1, log_h, log_w + ls, ls, t)
+                 log_h1, log_h, log_w + ls, ls, t, tma ? &tm : nullptr)
     count_launch();
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
@@ -1162,37 +1264,10 @@ constexpr uint32_t kBytes = kChunk * 4;
 constexpr int kHi = kChunk >> 8;                    // high-index entries per chunk
 constexpr uint32_t kHiBytes = kHi * 16;
 constexpr int kStageWords = kCta * 4 + kHi;         // 16-byte words per stage
-constexpr uint32_t kPolls = 1u << 22;  // bound on the polls of one wait
-__device__ __forceinline__ uint32_t saddr(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
-__device__ __forceinline__ void bar_init(uint64_t* b) {
-  asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(saddr(b)) : "memory");
-}
-__device__ __forceinline__ void bar_expect(uint64_t* b, uint32_t bytes) {
-  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(saddr(b)), "r"(bytes) : "memory");
-}
-__device__ __forceinline__ bool bar_test(uint64_t* b, uint32_t parity) {
-  uint32_t ok;
-  asm volatile(
-      "{\n\t.reg .pred p;\n\tmbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, p;\n}"
-      : "=r"(ok)
-      : "r"(saddr(b)), "r"(parity)
-      : "memory");
-  return ok != 0u;
-}
-// Waits for the phase of `parity` to complete; false after kPolls polls.
-__device__ __forceinline__ bool bar_wait(uint64_t* b, uint32_t parity) {
-  for (uint32_t i = 0; i < kPolls; i++) {
-    if (bar_test(b, parity)) return true;
-    if (i >= 64) __nanosleep(128);
-  }
-  return false;
-}
-__device__ __forceinline__ void bulk_load(void* dst, const void* src, uint32_t bytes, uint64_t* b) {
-  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
-                   saddr(dst)),
-               "l"(src), "r"(bytes), "r"(saddr(b))
-               : "memory");
-}
+using bulk::bar_expect;
+using bulk::bar_init;
+using bulk::bar_wait;
+using bulk::bulk_load;
 // chunk c of the segment and its high-index slice into stage buffer `buf`
 __device__ __forceinline__ void load_chunk(uint4* buf, const uint32_t* src, const kb::ef* hi, unsigned c, uint64_t* b) {
   bar_expect(b, kBytes + kHiBytes);

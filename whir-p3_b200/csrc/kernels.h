@@ -32,6 +32,7 @@ struct DftTables {
   const uint2* tw_sh;        // omega_{2^12}^k, k < 2^12: (canonical, Shoup constant)
   const uint32_t* tw_lo;     // omega_H^e, e < 2^12
   const uint32_t* tw_hi;     // omega_H^(e * 2^12), e < 2^12
+  uint32_t* err = nullptr;   // flags of the staged passes (bit 0: a tile wait gave up, bit 1: unaligned tile)
 };
 // words of the per-context stage table: 2^11 Montgomery twiddles, then 2^12 Shoup pairs
 constexpr int kDftStageTableWords = 2048 + 2 * 4096;
@@ -64,12 +65,13 @@ cudaError_t build_dft_tables(uint32_t* tw_stage, uint32_t* tw_lo, uint32_t* tw_h
 // 2^log_t1 length-H1 columns per CTA and pass 2 2^log_t2 length-H2 rows.
 // A pass runs either the shared-memory radix-2 kernel (threads1/threads2 per
 // CTA) or, with reg1/reg2 set, the register-resident kernel, whose CTA size
-// is fixed by the pass length and tile.
+// is fixed by the pass length and tile. reg2 = 2 runs the register pass 2 with
+// its input tile staged in shared memory by one tensor copy (TMA).
 struct DftPlan {
   int log_h2;
   int log_t1, threads1;
   int log_t2, threads2;
-  int reg1, reg2;  // pass uses the register-resident kernel (base field, 2^8..2^12 points)
+  int reg1, reg2;  // pass uses the register-resident kernel (2^8..2^12 points); reg2 2: TMA-staged tile
 };
 // the fixed plan used when tuning is off (64 KiB tiles, 256 threads)
 DftPlan dft_default_plan(int log_chunk, int log_w, int log_blowup, int lanes);
