@@ -177,6 +177,13 @@ int whir_ctx_set_device_transcript(whir_ctx* ctx, int32_t enable);
  * polls with a yield between checks. 0 yields from the start (less host CPU
  * per waiting context, e.g. many batch workers on few cores). */
 int whir_ctx_set_wait_spin(whir_ctx* ctx, int32_t microseconds);
+/* Candidates in flight of the proof-of-work searches (GrindingChallenger::grind
+ * replacement): 0 (default) sizes each search for its own latency on an
+ * otherwise idle GPU (up to 8x the expected candidates in flight for small
+ * searches); 1 sizes it for the fewest evaluated candidates (about 2x, at most
+ * one CTA per SM), for contexts whose GPU is shared with other proofs. The
+ * witness (the smallest valid one) is the same either way. */
+int whir_ctx_set_grind_window(whir_ctx* ctx, int32_t mode);
 /* Host permutation with the context's data (width taken from the state length 16 or 24). */
 int whir_poseidon2_permute(const whir_ctx* ctx, uint32_t* state, int32_t width);
 
@@ -427,6 +434,10 @@ int whir_batch_memory(whir_batch* b, uint64_t* fixed_bytes, uint64_t* pool_reser
 int whir_batch_set_device_transcript(whir_batch* b, int32_t enable);
 /* whir_ctx_set_wait_spin on every worker context */
 int whir_batch_set_wait_spin(whir_batch* b, int32_t microseconds);
+/* whir_ctx_set_grind_window on every worker context (a batch of two or more
+ * workers starts with the throughput window, a single worker with the latency
+ * window) */
+int whir_batch_set_grind_window(whir_batch* b, int32_t mode);
 /* Enqueue (non-blocking). The job and its buffers must stay valid until it is done. */
 int whir_batch_submit(whir_batch* b, whir_job* job);
 /* Wait for one job (timeout_ms < 0: no limit); returns the job's status. */

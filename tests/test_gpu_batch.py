@@ -49,6 +49,19 @@ def test_batch_matches_one_at_a_time(pkg, gpu_ctx, oracle):
     assert np.array_equal(reqs[0].proof, ref) and np.array_equal(reqs[0].checkpoint, ref_cp)
 
 
+def test_throughput_grind_window_in_batch(pkg, gpu_ctx):
+    """Workers sized for throughput (fewer grinding candidates in flight) give
+    the same proofs as one-at-a-time proving with the latency window."""
+    jobs = make_jobs(pkg, 12, 5, 10, 17)
+    reqs = [pkg.ProofRequest(p, n, poly, pts if pts.size else None) for p, n, poly, pts in jobs]
+    with pkg.Batch(0, workers=4) as b:
+        b.set_grind_window(1)
+        b.run(reqs)
+    check_against_single(pkg, gpu_ctx, jobs, reqs)
+    with pytest.raises(pkg.WhirError):
+        gpu_ctx.set_grind_window(2)
+
+
 def test_admission_budget_limits_concurrency(pkg, gpu_ctx):
     jobs = make_jobs(pkg, 8, 2, 14, 16)
     reqs = [pkg.ProofRequest(p, n, poly, pts if pts.size else None) for p, n, poly, pts in jobs]

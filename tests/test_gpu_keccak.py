@@ -71,6 +71,16 @@ def test_keccak_proofs_with_grinding(pkg, gpu_ctx, oracle, n, pw, k, snd, rate, 
     run_keccak(pkg, gpu_ctx, oracle, n, 64, pw, k, snd, rate, rs, npts, 500 + n)
 
 
+def test_keccak_grinding_throughput_window(pkg, gpu_ctx, oracle):
+    """Keccak-challenger searches with the throughput candidate window: the
+    same proof as the oracle's."""
+    gpu_ctx.set_grind_window(1)
+    try:
+        run_keccak(pkg, gpu_ctx, oracle, 14, 64, 12, 4, 0, 1, 2, 2, 514)
+    finally:
+        gpu_ctx.set_grind_window(0)
+
+
 @pytest.mark.parametrize("n,k,rs,npts", [(2, 1, 1, 1), (4, 2, 1, 0), (6, 3, 2, 2), (8, 4, 3, 1), (9, 2, 1, 3)])
 def test_keccak_small_shapes(pkg, gpu_ctx, oracle, n, k, rs, npts):
     """Small sizes and folding factors (one-CTA trees, no four-step DFT)."""

@@ -159,21 +159,29 @@ def test_svo_partial_evals(pkg, gpu_ctx, oracle, n, l):
         assert np.array_equal(parts[4 * y:4 * y + 4], oracle.eval_base(f[y * m:(y + 1) * m], z[4 * l:]))
 
 
-@pytest.mark.parametrize("bits", [1, 3, 8, 12, 16])
-def test_grind_smallest_witness(pkg, gpu_ctx, oracle, bits):
+@pytest.mark.parametrize("window", [0, 1])
+@pytest.mark.parametrize("bits", [1, 3, 8, 11, 12, 16])
+def test_grind_smallest_witness(pkg, gpu_ctx, oracle, bits, window):
+    """The smallest witness at every sponge position, with the latency and the
+    throughput candidate windows (four-lane searches up to 11 bits, one-thread
+    searches above)."""
     rng = np.random.default_rng(bits)
     ch = pkg.DuplexChallenger(gpu_ctx)
     oc = Chal()
     oracle.lib.or_chal_init(C.byref(oc))
-    for pending in range(8):  # the witness lands at position `pending` of the sponge
-        vals = rnd(rng, 8 + pending)
-        ch.observe_slice(vals)
-        for v in vals:
-            oracle.lib.or_chal_observe(C.byref(oc), C.byref(oracle.p16), int(v))
-        w = ch.grind(bits)
-        w_ref = oracle.lib.or_chal_grind(C.byref(oc), C.byref(oracle.p16), bits)
-        assert w == w_ref
-        assert list(ch.c.state) == list(oc.state)
+    gpu_ctx.set_grind_window(window)
+    try:
+        for pending in range(8):  # the witness lands at position `pending` of the sponge
+            vals = rnd(rng, 8 + pending)
+            ch.observe_slice(vals)
+            for v in vals:
+                oracle.lib.or_chal_observe(C.byref(oc), C.byref(oracle.p16), int(v))
+            w = ch.grind(bits)
+            w_ref = oracle.lib.or_chal_grind(C.byref(oc), C.byref(oracle.p16), bits)
+            assert w == w_ref
+            assert list(ch.c.state) == list(oc.state)
+    finally:
+        gpu_ctx.set_grind_window(0)
 
 
 def test_invalid_arguments_raise(pkg, gpu_ctx):

@@ -150,6 +150,8 @@ _SIGS = {
     "whir_batch_set_device_transcript": (C.c_int, [_vp, _i32]),
     "whir_batch_set_wait_spin": (C.c_int, [_vp, _i32]),
     "whir_ctx_set_wait_spin": (C.c_int, [_vp, _i32]),
+    "whir_ctx_set_grind_window": (C.c_int, [_vp, _i32]),
+    "whir_batch_set_grind_window": (C.c_int, [_vp, _i32]),
     "whir_batch_submit": (C.c_int, [_vp, C.POINTER(Job)]),
     "whir_batch_wait": (C.c_int, [_vp, C.POINTER(Job), _i32]),
     "whir_batch_wait_all": (C.c_int, [_vp]),
@@ -427,6 +429,14 @@ class Context:
     def set_wait_spin(self, microseconds: int) -> None:
         """How long a wait for a small device result spins before yielding."""
         _check(lib().whir_ctx_set_wait_spin(self.handle, int(microseconds)))
+
+    GRIND_LATENCY, GRIND_THROUGHPUT = 0, 1
+
+    def set_grind_window(self, mode: int) -> None:
+        """Candidates in flight of proof-of-work searches: GRIND_LATENCY (each search as
+        fast as possible on an idle GPU) or GRIND_THROUGHPUT (fewest evaluated candidates,
+        for a GPU shared with other proofs). The witness is the same either way."""
+        _check(lib().whir_ctx_set_grind_window(self.handle, int(mode)))
 
     def set_device_transcript(self, enable: bool) -> None:
         """Sumcheck stages with their transcript steps on the device, or with
@@ -889,6 +899,10 @@ class Batch:
     def set_wait_spin(self, microseconds: int) -> None:
         """Context.set_wait_spin on every worker."""
         _check(lib().whir_batch_set_wait_spin(self.handle, int(microseconds)))
+
+    def set_grind_window(self, mode: int) -> None:
+        """Context.set_grind_window on every worker."""
+        _check(lib().whir_batch_set_grind_window(self.handle, int(mode)))
 
     def set_device_transcript(self, enable: bool) -> None:
         """Context.set_device_transcript on every worker (jobs started later)."""

@@ -250,10 +250,11 @@ int grind(whir_ctx* ctx, Chal& ch, int bits, uint32_t* witness) {
     StageTimer t(ctx, kStGrind);
     if (ch.family == kChalKeccak)
       WH_TRY_CUDA(wk::keccak_grind(ch.kin, bits, kb::P, ctx->d_words, ctx->d_words + 1, ctx->d_words + 2,
-                                   ctx->h_mail ? ctx->d_mail : nullptr, seq, ctx->stream));
+                                   ctx->h_mail ? ctx->d_mail : nullptr, seq, ctx->stream, ctx->grind_window.load()));
     else
       WH_TRY_CUDA(wk::grind(ch.st, ch.in, ch.in_len, bits, kb::P, ctx->d_words, ctx->d_words + 1, ctx->d_words + 2,
-                            ctx->h_mail ? ctx->d_mail : nullptr, seq, ctx->p16, ctx->stream));
+                            ctx->h_mail ? ctx->d_mail : nullptr, seq, ctx->p16, ctx->stream, nullptr, nullptr,
+                            nullptr, nullptr, nullptr, ctx->grind_window.load()));
   }
   // with a mailbox the search posts its witness and the number of candidates
   // it evaluated
@@ -566,6 +567,13 @@ int whir_ctx_set_wait_spin(whir_ctx* ctx, int32_t microseconds) {
   WH_TRY(check_ctx(ctx));
   WH_CHECK(microseconds >= 0 && microseconds <= 100000, "spin time out of range");
   ctx->wait_spin_us.store(microseconds);
+  return WHIR_OK;
+}
+
+int whir_ctx_set_grind_window(whir_ctx* ctx, int32_t mode) {
+  WH_TRY(check_ctx(ctx));
+  WH_CHECK(mode == wk::kGrindLatency || mode == wk::kGrindThroughput, "grind window mode must be 0 or 1");
+  ctx->grind_window.store(mode);
   return WHIR_OK;
 }
 

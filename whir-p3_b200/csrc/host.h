@@ -184,6 +184,9 @@ struct whir_ctx {
   // how long a wait for a device result spins before it polls with yields
   // (whir_ctx_set_wait_spin)
   std::atomic<int> wait_spin_us{30};
+  // candidates in flight of proof-of-work searches (wk::kGrindLatency or
+  // wk::kGrindThroughput; whir_ctx_set_grind_window)
+  std::atomic<int> grind_window{0};
   // the challenger after the domain separator, per (parameters, size): where a
   // whir_commit_and_prove starts (observing the pattern is a few dozen host
   // permutations, ahead of the first launch); a handful of entries, the

@@ -179,15 +179,17 @@ cudaError_t keccak_upper(int log_h, uint32_t* digests, uint32_t* mail, uint32_t 
 }
 
 cudaError_t keccak_grind(const kk::K256& in, int bits, uint64_t limit, uint32_t* result, uint32_t* counter,
-                         uint32_t* done, uint32_t* mail, uint32_t seq, cudaStream_t st) {
+                         uint32_t* done, uint32_t* mail, uint32_t seq, cudaStream_t st, int window) {
   if (bits < 0 || bits > 30 || in.pos >= 136) return cudaErrorInvalidValue;
   if (limit > kb::P) limit = kb::P;
   if (!mail) {
     const cudaError_t e = grind_reset(result, counter, done, st);
     if (e != cudaSuccess) return e;
   }
-  // about 2^(bits+3) candidates in flight, at most 8 CTAs per SM
-  const unsigned blocks = blocks_for((size_t)8 << bits, KECCAK_CLAIM, 8);
+  // about 2^(bits+3) candidates in flight, at most 8 CTAs per SM (throughput
+  // window: 2^(bits+1), at most one CTA per SM)
+  const unsigned blocks = window == kGrindThroughput ? blocks_for((size_t)2 << bits, KECCAK_CLAIM, 1)
+                                                     : blocks_for((size_t)8 << bits, KECCAK_CLAIM, 8);
   k_keccak_grind<<<blocks, KECCAK_CLAIM, 0, st>>>(in, bits, limit, result, counter, done, mail, seq);
   LAUNCH_DONE();
 }

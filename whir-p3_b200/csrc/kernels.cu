@@ -978,12 +978,12 @@ cudaError_t grind_reset(uint32_t* result, uint32_t* counter, uint32_t* done, cud
 cudaError_t grind(const uint32_t* state, const uint32_t* in, int in_len, int bits, uint64_t limit,
                   uint32_t* result, uint32_t* counter, uint32_t* done, uint32_t* mail, uint32_t seq,
                   const P2Consts& p16, cudaStream_t st, const uint32_t* cp_dev, uint32_t* res_out, DevChal* ch,
-                  ef* r_out, uint32_t* err) {
+                  ef* r_out, uint32_t* err, int window) {
   if (p16.mat == (uint32_t)p2::kMatHl)
     return grind_m<p2::kMatHl>(state, in, in_len, bits, limit, result, counter, done, mail, seq, p16, st, cp_dev,
-                               res_out, ch, r_out, err);
+                               res_out, ch, r_out, err, window);
   return grind_m<p2::kMatMds>(state, in, in_len, bits, limit, result, counter, done, mail, seq, p16, st, cp_dev,
-                              res_out, ch, r_out, err);
+                              res_out, ch, r_out, err, window);
 }
 
 cudaError_t sumcheck_round_tr(ef* f, ef* w, size_t q, int fold, ef r, ef* partials, unsigned* counter, ef* out,

@@ -158,13 +158,17 @@ cudaError_t grind_reset(uint32_t* result, uint32_t* counter, uint32_t* done, cud
 // the transcript step after it on the device challenger: observe the witness,
 // check that sample_bits(bits) is 0, sample the round's challenge into r_out
 // (a failed check sets bit 0, no witness, or bit 1, check failed, of *err).
+// `window` sizes the candidates in flight: kGrindLatency for the shortest
+// search on an otherwise idle GPU, kGrindThroughput for the fewest evaluated
+// candidates when other work shares the GPU; the witness is the same.
 constexpr int kCoopGrindBits = 11;
+constexpr int kGrindLatency = 0, kGrindThroughput = 1;
 struct DevChal;
 cudaError_t grind(const uint32_t* state, const uint32_t* in, int in_len, int bits, uint64_t limit,
                   uint32_t* result, uint32_t* counter, uint32_t* done, uint32_t* mail, uint32_t seq,
                   const p2::P2Consts& p16, cudaStream_t st, const uint32_t* cp_dev = nullptr,
                   uint32_t* res_out = nullptr, DevChal* ch = nullptr, kb::ef* r_out = nullptr,
-                  uint32_t* err = nullptr);
+                  uint32_t* err = nullptr, int window = kGrindLatency);
 
 // Keccak family (keccak.cu): the Keccak MMCS's leaf digests (rows in
 // Montgomery form, hashed as canonical values) and tree levels, digests laid
@@ -175,7 +179,7 @@ cudaError_t grind(const uint32_t* state, const uint32_t* in, int in_len, int bit
 cudaError_t keccak_leaves(const uint32_t* rows, int log_h, int row_words, uint32_t* digests, cudaStream_t st);
 cudaError_t keccak_upper(int log_h, uint32_t* digests, uint32_t* mail, uint32_t seq, int* posted, cudaStream_t st);
 cudaError_t keccak_grind(const kk::K256& in, int bits, uint64_t limit, uint32_t* result, uint32_t* counter,
-                         uint32_t* done, uint32_t* mail, uint32_t seq, cudaStream_t st);
+                         uint32_t* done, uint32_t* mail, uint32_t seq, cudaStream_t st, int window = kGrindLatency);
 
 // Duplex challenger on the device (DuplexChallenger<F, Poseidon2-16, 16, 8>),
 // Montgomery words, laid out like the host's challenger: sponge state, pending
@@ -213,7 +217,7 @@ template <int MAT>
 cudaError_t grind_m(const uint32_t* state, const uint32_t* in, int in_len, int bits, uint64_t limit,
                     uint32_t* result, uint32_t* counter, uint32_t* done, uint32_t* mail, uint32_t seq,
                     const p2::P2Consts& p16, cudaStream_t st, const uint32_t* cp_dev, uint32_t* res_out,
-                    DevChal* ch, kb::ef* r_out, uint32_t* err);
+                    DevChal* ch, kb::ef* r_out, uint32_t* err, int window);
 template <int MAT>
 cudaError_t sumcheck_round_tr_m(kb::ef* f, kb::ef* w, size_t q, int fold, kb::ef r, kb::ef* partials,
                                 unsigned* counter, kb::ef* out, const kb::ef* r_dev, DevChal* ch, const DevChal* init,

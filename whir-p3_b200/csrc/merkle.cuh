@@ -834,7 +834,7 @@ template <int MAT>
 cudaError_t grind_m(const uint32_t* state, const uint32_t* in, int in_len, int bits, uint64_t limit,
                     uint32_t* result, uint32_t* counter, uint32_t* done, uint32_t* mail, uint32_t seq,
                     const P2Consts& p16, cudaStream_t st, const uint32_t* cp_dev, uint32_t* res_out, DevChal* ch,
-                    ef* r_out, uint32_t* err) {
+                    ef* r_out, uint32_t* err, int window) {
   if (in_len < 0 || in_len > 7 || bits < 0 || bits > 30) return cudaErrorInvalidValue;
   if (ch && (!res_out || !r_out || !err || bits < 1)) return cudaErrorInvalidValue;
   if (limit > kb::P) limit = kb::P;
@@ -870,12 +870,16 @@ cudaError_t grind_m(const uint32_t* state, const uint32_t* in, int in_len, int b
   // Searches of up to kCoopGrindBits bits (2^(bits+3) candidates in flight in
   // at most 4 CTAs per SM) run the four-lane form: one pass is a four-lane
   // permutation's latency instead of a one-thread permutation's.
+  // With window = kGrindThroughput (other work shares the GPU, as in a batch)
+  // the evaluated candidates count, not the search's own latency: about
+  // 2^(bits+1) in flight, at most one CTA per SM.
   static const int kPerSm[7] = {1, 2, 3, 4, 6, 8, 10};
   static const double kRate[7] = {0.467, 0.703, 0.811, 0.865, 0.911, 0.948, 0.965};
   const double expect = (double)(1ull << bits);
   const bool coop = bits <= kCoopGrindBits;
+  const int lead = window == kGrindThroughput ? 1 : 3;  // 2^(bits+lead) candidates in flight
   if (coop) {
-    const unsigned blocks = (unsigned)(((8ull << bits) + GRIND_CTA / 4 - 1) / (GRIND_CTA / 4));
+    const unsigned blocks = (unsigned)(((1ull << (bits + lead)) + GRIND_CTA / 4 - 1) / (GRIND_CTA / 4));
     switch (in_len) {
 #define WK_GRIND_COOP(S)                                                                                          \
   case S:                                                                                                        \
@@ -888,8 +892,10 @@ cudaError_t grind_m(const uint32_t* state, const uint32_t* in, int in_len, int b
     }
     LAUNCH_DONE();
   }
-  unsigned blocks = (unsigned)(((8ull << bits) + GRIND_CTA - 1) / GRIND_CTA);
-  if (blocks > (unsigned)sm_count()) {
+  unsigned blocks = (unsigned)(((1ull << (bits + lead)) + GRIND_CTA - 1) / GRIND_CTA);
+  if (window == kGrindThroughput) {
+    if (blocks > (unsigned)sm_count()) blocks = (unsigned)sm_count();
+  } else if (blocks > (unsigned)sm_count()) {
     double best = 0.0;
     unsigned pick = (unsigned)sm_count();
     for (int i = 0; i < 7; i++) {

@@ -9,7 +9,7 @@ template cudaError_t merkle_upper_m<p2::kMatHl>(int, uint32_t*, const p2::P2Cons
                                                 uint32_t, int*, cudaStream_t);
 template cudaError_t grind_m<p2::kMatHl>(const uint32_t*, const uint32_t*, int, int, uint64_t, uint32_t*, uint32_t*,
                                           uint32_t*, uint32_t*, uint32_t, const p2::P2Consts&, cudaStream_t,
-                                          const uint32_t*, uint32_t*, DevChal*, kb::ef*, uint32_t*);
+                                          const uint32_t*, uint32_t*, DevChal*, kb::ef*, uint32_t*, int);
 template cudaError_t sumcheck_round_tr_m<p2::kMatHl>(kb::ef*, kb::ef*, size_t, int, kb::ef, kb::ef*, unsigned*, kb::ef*,
                                                  const kb::ef*, DevChal*, const DevChal*, uint32_t*, int, uint32_t*,
                                                  kb::ef*, const p2::P2Consts&, cudaStream_t);

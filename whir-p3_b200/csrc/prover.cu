@@ -385,7 +385,8 @@ int sumcheck_stage_device(whir_ctx* ctx, wh::Chal& ch, Sumcheck& sd, ef* d_f, ef
       // sampled in its last CTA
       wh::StageTimer timer(ctx, wh::kStGrind);
       WH_TRY_CUDA(wk::grind(nullptr, nullptr, in_len, pow_bits, kb::P, ctx->d_words, ctx->d_words + 1,
-                            ctx->d_words + 2, nullptr, 0u, ctx->p16, ctx->stream, cp, log_w(j), dch, log_r(j), err));
+                            ctx->d_words + 2, nullptr, 0u, ctx->p16, ctx->stream, cp, log_w(j), dch, log_r(j), err,
+                            ctx->grind_window.load()));
       observed();
       sampled();
     }
