@@ -381,6 +381,12 @@ def micro_lines(kinds, steps: int, warmup: int, echo: bool = False) -> list:
         # LDE of 2^24 values is measured in the shape the prover runs it: 16 columns of 2^20 -> 2^21.
         emit("dft 16 x 2^20 -> 16 x 2^21 (commit LDE)", timed(lambda: pkg.dft_batch(ctx, x, n - 4, 4, 1, False, out)),
              alg_bytes=4 * N + 8 * N)
+        # the same transform at one fixed plan (split 2^10 x 2^11, register passes, 8 columns per CTA)
+        # with pass 2 reading its tile directly and with the tile staged by a TMA tensor copy
+        for label, reg2 in (("register pass 2", 1), ("TMA-staged register pass 2", 2)):
+            plan = (11, 3, 256, 3, 256, 1, reg2)
+            emit(f"dft commit LDE, plan {list(plan)} ({label})",
+                 timed(lambda: pkg.dft_batch_plan(ctx, x, n - 4, 4, 1, False, plan, out)), alg_bytes=4 * N + 8 * N)
     if "merkle" in kinds:
         log_h, words = 21, 16
         rows = pkg.DeviceArray.from_host(ctx, rng.integers(0, P, words << log_h, dtype=np.uint64).astype(np.uint32))
@@ -412,6 +418,15 @@ def micro_lines(kinds, steps: int, warmup: int, echo: bool = False) -> list:
         emit(f"grind {bits} bits", ms, units=float(np.mean(timed_evals)), unit_name="permutations/s",
              extra={"candidates_evaluated_per_call": [int(v) for v in evaluated],
                     "note": "one Poseidon2-16 permutation per evaluated candidate; expected 2^bits per search"})
+        # a small search (the four-lane form, latency-bound: one permutation's latency per pass)
+        bits = 10
+        evaluated.clear()
+        ctx.set_profiling(True)
+        ms = timed(grind)
+        ctx.set_profiling(False)
+        ctx.stage_times(reset=True)
+        emit(f"grind {bits} bits (four-lane form)", ms,
+             extra={"candidates_evaluated_per_call": [int(v) for v in evaluated[-reps:]]})
     ctx.close()
     return lines
 

@@ -179,10 +179,11 @@ int whir_ctx_set_device_transcript(whir_ctx* ctx, int32_t enable);
 int whir_ctx_set_wait_spin(whir_ctx* ctx, int32_t microseconds);
 /* Candidates in flight of the proof-of-work searches (GrindingChallenger::grind
  * replacement): 0 (default) sizes each search for its own latency on an
- * otherwise idle GPU (up to 8x the expected candidates in flight for small
- * searches); 1 sizes it for the fewest evaluated candidates (about 2x, at most
- * one CTA per SM), for contexts whose GPU is shared with other proofs. The
- * witness (the smallest valid one) is the same either way. */
+ * otherwise idle GPU (8x the expected candidates in flight for searches of up
+ * to 11 bits, an expected-cost model above). Bit 0 keeps 2x in flight in the
+ * small searches, bit 1 runs the larger ones with one CTA per SM: fewer
+ * evaluated candidates for a GPU shared with other work, at some latency.
+ * The witness (the smallest valid one) is the same in every mode. */
 int whir_ctx_set_grind_window(whir_ctx* ctx, int32_t mode);
 /* Host permutation with the context's data (width taken from the state length 16 or 24). */
 int whir_poseidon2_permute(const whir_ctx* ctx, uint32_t* state, int32_t width);
@@ -434,9 +435,7 @@ int whir_batch_memory(whir_batch* b, uint64_t* fixed_bytes, uint64_t* pool_reser
 int whir_batch_set_device_transcript(whir_batch* b, int32_t enable);
 /* whir_ctx_set_wait_spin on every worker context */
 int whir_batch_set_wait_spin(whir_batch* b, int32_t microseconds);
-/* whir_ctx_set_grind_window on every worker context (a batch of two or more
- * workers starts with the throughput window, a single worker with the latency
- * window) */
+/* whir_ctx_set_grind_window on every worker context */
 int whir_batch_set_grind_window(whir_batch* b, int32_t mode);
 /* Enqueue (non-blocking). The job and its buffers must stay valid until it is done. */
 int whir_batch_submit(whir_batch* b, whir_job* job);

@@ -49,17 +49,18 @@ def test_batch_matches_one_at_a_time(pkg, gpu_ctx, oracle):
     assert np.array_equal(reqs[0].proof, ref) and np.array_equal(reqs[0].checkpoint, ref_cp)
 
 
-def test_throughput_grind_window_in_batch(pkg, gpu_ctx):
-    """Workers sized for throughput (fewer grinding candidates in flight) give
-    the same proofs as one-at-a-time proving with the latency window."""
-    jobs = make_jobs(pkg, 12, 5, 10, 17)
+@pytest.mark.parametrize("mode", [1, 2, 3])
+def test_lean_grind_windows_in_batch(pkg, gpu_ctx, mode):
+    """Workers with lean grinding windows (fewer candidates in flight) give the
+    same proofs as one-at-a-time proving with the latency window."""
+    jobs = make_jobs(pkg, 12, 5 + mode, 10, 17)
     reqs = [pkg.ProofRequest(p, n, poly, pts if pts.size else None) for p, n, poly, pts in jobs]
     with pkg.Batch(0, workers=4) as b:
-        b.set_grind_window(1)
+        b.set_grind_window(mode)
         b.run(reqs)
     check_against_single(pkg, gpu_ctx, jobs, reqs)
     with pytest.raises(pkg.WhirError):
-        gpu_ctx.set_grind_window(2)
+        gpu_ctx.set_grind_window(4)
 
 
 def test_admission_budget_limits_concurrency(pkg, gpu_ctx):

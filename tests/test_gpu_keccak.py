@@ -72,9 +72,9 @@ def test_keccak_proofs_with_grinding(pkg, gpu_ctx, oracle, n, pw, k, snd, rate, 
 
 
 def test_keccak_grinding_throughput_window(pkg, gpu_ctx, oracle):
-    """Keccak-challenger searches with the throughput candidate window: the
-    same proof as the oracle's."""
-    gpu_ctx.set_grind_window(1)
+    """Keccak-challenger searches with both lean candidate windows: the same
+    proof as the oracle's."""
+    gpu_ctx.set_grind_window(3)
     try:
         run_keccak(pkg, gpu_ctx, oracle, 14, 64, 12, 4, 0, 1, 2, 2, 514)
     finally:

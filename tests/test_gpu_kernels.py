@@ -159,11 +159,11 @@ def test_svo_partial_evals(pkg, gpu_ctx, oracle, n, l):
         assert np.array_equal(parts[4 * y:4 * y + 4], oracle.eval_base(f[y * m:(y + 1) * m], z[4 * l:]))
 
 
-@pytest.mark.parametrize("window", [0, 1])
+@pytest.mark.parametrize("window", [0, 3])
 @pytest.mark.parametrize("bits", [1, 3, 8, 11, 12, 16])
 def test_grind_smallest_witness(pkg, gpu_ctx, oracle, bits, window):
-    """The smallest witness at every sponge position, with the latency and the
-    throughput candidate windows (four-lane searches up to 11 bits, one-thread
+    """The smallest witness at every sponge position, with the latency window
+    and with both lean windows (four-lane searches up to 11 bits, one-thread
     searches above)."""
     rng = np.random.default_rng(bits)
     ch = pkg.DuplexChallenger(gpu_ctx)

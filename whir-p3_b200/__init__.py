@@ -430,12 +430,13 @@ class Context:
         """How long a wait for a small device result spins before yielding."""
         _check(lib().whir_ctx_set_wait_spin(self.handle, int(microseconds)))
 
-    GRIND_LATENCY, GRIND_THROUGHPUT = 0, 1
+    GRIND_LATENCY, GRIND_LEAN_SMALL, GRIND_LEAN_LARGE = 0, 1, 2
 
     def set_grind_window(self, mode: int) -> None:
-        """Candidates in flight of proof-of-work searches: GRIND_LATENCY (each search as
-        fast as possible on an idle GPU) or GRIND_THROUGHPUT (fewest evaluated candidates,
-        for a GPU shared with other proofs). The witness is the same either way."""
+        """Candidates in flight of proof-of-work searches: GRIND_LATENCY (0, each search as
+        fast as possible on an idle GPU), or the bits GRIND_LEAN_SMALL (searches of up to 11
+        bits with 2x the expected candidates in flight instead of 8x) and GRIND_LEAN_LARGE
+        (larger searches with one CTA per SM). The witness is the same in every mode."""
         _check(lib().whir_ctx_set_grind_window(self.handle, int(mode)))
 
     def set_device_transcript(self, enable: bool) -> None:

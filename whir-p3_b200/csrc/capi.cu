@@ -572,7 +572,7 @@ int whir_ctx_set_wait_spin(whir_ctx* ctx, int32_t microseconds) {
 
 int whir_ctx_set_grind_window(whir_ctx* ctx, int32_t mode) {
   WH_TRY(check_ctx(ctx));
-  WH_CHECK(mode == wk::kGrindLatency || mode == wk::kGrindThroughput, "grind window mode must be 0 or 1");
+  WH_CHECK(mode >= 0 && mode <= (wk::kGrindLeanSmall | wk::kGrindLeanLarge), "grind window mode must be 0 to 3");
   ctx->grind_window.store(mode);
   return WHIR_OK;
 }

@@ -185,7 +185,7 @@ struct whir_ctx {
   // (whir_ctx_set_wait_spin)
   std::atomic<int> wait_spin_us{30};
   // candidates in flight of proof-of-work searches (wk::kGrindLatency or
-  // wk::kGrindThroughput; whir_ctx_set_grind_window)
+  // wk::kGrindLean* bits; whir_ctx_set_grind_window)
   std::atomic<int> grind_window{0};
   // the challenger after the domain separator, per (parameters, size): where a
   // whir_commit_and_prove starts (observing the pattern is a few dozen host

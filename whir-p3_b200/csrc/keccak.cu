@@ -186,10 +186,12 @@ cudaError_t keccak_grind(const kk::K256& in, int bits, uint64_t limit, uint32_t*
     const cudaError_t e = grind_reset(result, counter, done, st);
     if (e != cudaSuccess) return e;
   }
-  // about 2^(bits+3) candidates in flight, at most 8 CTAs per SM (throughput
-  // window: 2^(bits+1), at most one CTA per SM)
-  const unsigned blocks = window == kGrindThroughput ? blocks_for((size_t)2 << bits, KECCAK_CLAIM, 1)
-                                                     : blocks_for((size_t)8 << bits, KECCAK_CLAIM, 8);
+  // about 2^(bits+3) candidates in flight, at most 8 CTAs per SM; window bit
+  // kGrindLeanSmall: 2^(bits+1) for searches of up to kCoopGrindBits bits;
+  // kGrindLeanLarge: at most one CTA per SM for larger ones
+  const bool small = bits <= kCoopGrindBits;
+  const size_t flight = (small && (window & kGrindLeanSmall) ? (size_t)2 : (size_t)8) << bits;
+  const unsigned blocks = blocks_for(flight, KECCAK_CLAIM, !small && (window & kGrindLeanLarge) ? 1 : 8);
   k_keccak_grind<<<blocks, KECCAK_CLAIM, 0, st>>>(in, bits, limit, result, counter, done, mail, seq);
   LAUNCH_DONE();
 }

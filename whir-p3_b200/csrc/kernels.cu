@@ -672,17 +672,38 @@ static PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
 // as `cols` element columns of H << ls words, viewed as (256 words, (H << ls)
 // / 256 rows, cols), boxes of (256, (N << ls) / 256, T >> ls). False when the
 // shape does not fit the copy engine's rules (the plain loads run instead).
+// Encoding is a driver call that costs far more than a launch, so the maps of
+// the last few (address, shape) keys are kept per host thread (a context's
+// scratch array usually comes back at the same address from its pool).
 static bool rows_tensor_map(CUtensorMap* tm, const uint32_t* y, int log_h, int ls, int log_cols, int log_n,
                             int log_t) {
+  struct Entry {
+    const uint32_t* y;
+    int key;
+    CUtensorMap map;
+  };
+  constexpr int kEntries = 8;
+  thread_local Entry cache[kEntries] = {};
+  thread_local int next = 0;
+  const int key = 1 + (log_h | ls << 5 | log_cols << 7 | log_n << 12 | log_t << 16);
+  for (const Entry& e : cache)
+    if (e.key == key && e.y == y) {
+      *tm = e.map;
+      return true;
+    }
   const auto enc = tensor_map_encoder();
   if (!enc || ((uintptr_t)y & 15u) != 0u || log_h + ls < 8 || log_n + ls < 8 || log_t < ls) return false;
   const cuuint64_t dims[3] = {256u, (cuuint64_t)1 << (log_h + ls - 8), (cuuint64_t)1 << log_cols};
   const cuuint64_t strides[2] = {1024u, (cuuint64_t)4 << (log_h + ls)};
   const cuuint32_t box[3] = {256u, 1u << (log_n + ls - 8), 1u << (log_t - ls)};
   const cuuint32_t estr[3] = {1u, 1u, 1u};
-  return enc(tm, CU_TENSOR_MAP_DATA_TYPE_UINT32, 3, const_cast<uint32_t*>(y), dims, strides, box, estr,
-             CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
-             CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+  if (enc(tm, CU_TENSOR_MAP_DATA_TYPE_UINT32, 3, const_cast<uint32_t*>(y), dims, strides, box, estr,
+          CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+          CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+    return false;
+  cache[next] = Entry{y, key, *tm};
+  next = (next + 1) % kEntries;
+  return true;
 }
 
 // supported (m, lt): pass 1 lt in {2, 3, 4}, pass 2 lt in {0, .., 4}

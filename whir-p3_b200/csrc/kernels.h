@@ -158,11 +158,13 @@ cudaError_t grind_reset(uint32_t* result, uint32_t* counter, uint32_t* done, cud
 // the transcript step after it on the device challenger: observe the witness,
 // check that sample_bits(bits) is 0, sample the round's challenge into r_out
 // (a failed check sets bit 0, no witness, or bit 1, check failed, of *err).
-// `window` sizes the candidates in flight: kGrindLatency for the shortest
-// search on an otherwise idle GPU, kGrindThroughput for the fewest evaluated
-// candidates when other work shares the GPU; the witness is the same.
+// `window` sizes the candidates in flight: kGrindLatency (0) for the shortest
+// search on an otherwise idle GPU; bits kGrindLeanSmall (four-lane searches
+// with 2^(bits+1) in flight instead of 2^(bits+3)) and kGrindLeanLarge (larger
+// searches with one CTA per SM) for fewer evaluated candidates when other
+// work shares the GPU. The witness is the same.
 constexpr int kCoopGrindBits = 11;
-constexpr int kGrindLatency = 0, kGrindThroughput = 1;
+constexpr int kGrindLatency = 0, kGrindLeanSmall = 1, kGrindLeanLarge = 2;
 struct DevChal;
 cudaError_t grind(const uint32_t* state, const uint32_t* in, int in_len, int bits, uint64_t limit,
                   uint32_t* result, uint32_t* counter, uint32_t* done, uint32_t* mail, uint32_t seq,

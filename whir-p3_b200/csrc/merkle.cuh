@@ -870,14 +870,17 @@ cudaError_t grind_m(const uint32_t* state, const uint32_t* in, int in_len, int b
   // Searches of up to kCoopGrindBits bits (2^(bits+3) candidates in flight in
   // at most 4 CTAs per SM) run the four-lane form: one pass is a four-lane
   // permutation's latency instead of a one-thread permutation's.
-  // With window = kGrindThroughput (other work shares the GPU, as in a batch)
-  // the evaluated candidates count, not the search's own latency: about
-  // 2^(bits+1) in flight, at most one CTA per SM.
+  // With other work sharing the GPU (a batch), evaluated candidates count
+  // more than the search's own latency: window bit kGrindLeanSmall keeps about
+  // 2^(bits+1) candidates in flight in a four-lane search instead of
+  // 2^(bits+3); bit kGrindLeanLarge runs a larger search with one CTA per SM
+  // (the smallest window that spans the GPU, at about half the rate the cost
+  // model's window reaches on an idle GPU).
   static const int kPerSm[7] = {1, 2, 3, 4, 6, 8, 10};
   static const double kRate[7] = {0.467, 0.703, 0.811, 0.865, 0.911, 0.948, 0.965};
   const double expect = (double)(1ull << bits);
   const bool coop = bits <= kCoopGrindBits;
-  const int lead = window == kGrindThroughput ? 1 : 3;  // 2^(bits+lead) candidates in flight
+  const int lead = (window & kGrindLeanSmall) ? 1 : 3;  // 2^(bits+lead) candidates in flight
   if (coop) {
     const unsigned blocks = (unsigned)(((1ull << (bits + lead)) + GRIND_CTA / 4 - 1) / (GRIND_CTA / 4));
     switch (in_len) {
@@ -892,8 +895,8 @@ cudaError_t grind_m(const uint32_t* state, const uint32_t* in, int in_len, int b
     }
     LAUNCH_DONE();
   }
-  unsigned blocks = (unsigned)(((1ull << (bits + lead)) + GRIND_CTA - 1) / GRIND_CTA);
-  if (window == kGrindThroughput) {
+  unsigned blocks = (unsigned)(((8ull << bits) + GRIND_CTA - 1) / GRIND_CTA);
+  if (window & kGrindLeanLarge) {
     if (blocks > (unsigned)sm_count()) blocks = (unsigned)sm_count();
   } else if (blocks > (unsigned)sm_count()) {
     double best = 0.0;
