@@ -224,6 +224,13 @@ int fetch(whir_ctx* ctx, void* host, const void* dev, size_t bytes) {
 }
 
 int upload(whir_ctx* ctx, void* dev, const void* host, size_t bytes) {
+  if (bytes % 4 == 0 && bytes <= (size_t)wk::kPutWords * 4 && ((uintptr_t)dev & 3) == 0) {
+    // small data (query indices, select weights): in a launch's parameters,
+    // ordered on the stream, without waiting for the work queued before it
+    WH_TRY_CUDA(wk::put_words(static_cast<uint32_t*>(dev), static_cast<const uint32_t*>(host), (int)(bytes / 4),
+                              ctx->stream));
+    return WHIR_OK;
+  }
   if (bytes <= ctx->pinned_bytes) {
     // the staging buffer may still feed an earlier copy: wait for the stream first
     WH_TRY(sync(ctx));

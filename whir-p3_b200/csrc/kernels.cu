@@ -11,6 +11,7 @@
 // in the constant bank).
 #include <cuda.h>
 #include <cudaTypedefs.h>
+#include <string.h>
 
 #include <atomic>
 #include <mutex>
@@ -89,6 +90,23 @@ __global__ void k_publish(const uint32_t* __restrict__ src, int words, volatile 
 cudaError_t publish(const uint32_t* src, int words, uint32_t* mail, uint32_t seq, cudaStream_t st) {
   if (words < 0 || words > kMailWords) return cudaErrorInvalidValue;
   k_publish<<<1, 128, 0, st>>>(src, words, mail, seq);
+  LAUNCH_DONE();
+}
+
+struct PutBlock {
+  int words;
+  uint32_t w[kPutWords];
+};  // 4004 bytes: within the 4 KiB parameter block every launch supports
+__global__ void k_put(const __grid_constant__ PutBlock b, uint32_t* __restrict__ dst) {
+  for (int i = threadIdx.x; i < b.words; i += blockDim.x) dst[i] = b.w[i];
+}
+
+cudaError_t put_words(uint32_t* dst, const uint32_t* src, int words, cudaStream_t st) {
+  if (words < 0 || words > kPutWords) return cudaErrorInvalidValue;
+  PutBlock b;
+  b.words = words;
+  memcpy(b.w, src, (size_t)words * 4);
+  k_put<<<1, 256, 0, st>>>(b, dst);
   LAUNCH_DONE();
 }
 

@@ -43,6 +43,11 @@ constexpr int kMailWords = 512;
 // copy `words` (<= kMailWords) device words into the mailbox, then (after a
 // system-wide fence) write `seq` to the flag
 cudaError_t publish(const uint32_t* src, int words, uint32_t* mail, uint32_t seq, cudaStream_t st);
+// Small host data to device memory in stream order without a host-side
+// synchronisation: the words travel in the launch's parameter block and one
+// CTA stores them to `dst` (at most kPutWords words).
+constexpr int kPutWords = 1000;
+cudaError_t put_words(uint32_t* dst, const uint32_t* src, int words, cudaStream_t st);
 
 #ifdef __CUDACC__
 // Mailbox write by one thread: payload, a system-wide fence, then the flag.
