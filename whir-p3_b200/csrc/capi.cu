@@ -464,7 +464,11 @@ int whir_ctx_create(int32_t device, const whir_poseidon2_params* p16, const whir
     return wh::set_error("grind state initialisation failed"), fail(WHIR_ERR_CUDA);
   if (cudaHostAlloc(&c->h_pinned, kPinnedBytes, cudaHostAllocDefault) != cudaSuccess)
     return wh::set_error("pinned allocation failed"), fail(WHIR_ERR_NOMEM);
-  c->pinned_bytes = kPinnedBytes;
+  c->pinned_bytes = kPinnedBytes / 2;
+  c->h_open = static_cast<uint8_t*>(c->h_pinned) + kPinnedBytes / 2;
+  c->open_bytes = kPinnedBytes / 2;
+  if (cudaEventCreateWithFlags(&c->open_ev, cudaEventDisableTiming) != cudaSuccess)
+    return wh::set_error("event creation failed"), fail(WHIR_ERR_CUDA);
   if (cudaHostAlloc(&c->h_mail, (wk::kMailWords + 32) * 4, cudaHostAllocMapped) != cudaSuccess ||
       cudaHostGetDevicePointer(reinterpret_cast<void**>(&c->d_mail), c->h_mail, 0) != cudaSuccess)
     return wh::set_error("mapped allocation failed"), fail(WHIR_ERR_NOMEM);
@@ -512,6 +516,7 @@ int whir_ctx_destroy(whir_ctx* c) {
   }
   for (cudaEvent_t e : c->up_ev)
     if (e) cudaEventDestroy(e);
+  if (c->open_ev) cudaEventDestroy(c->open_ev);
   cudaFree(c->tw_stage);
   cudaFree(c->d_partials);
   cudaFree(c->d_small);

@@ -159,8 +159,13 @@ struct whir_ctx {
   // arena), each allocation rounded up to the driver's 2 MiB granularity
   size_t fixed_device_bytes = 0;
   size_t arena_bytes = 0;
-  void* h_pinned = nullptr;      // staging for small transfers
+  void* h_pinned = nullptr;      // staging for small transfers (the first pinned_bytes)
   size_t pinned_bytes = 0;
+  // the rest of the same pinned block: query openings copied back while the
+  // prover queues the next work (open_ev marks the copy's completion)
+  void* h_open = nullptr;
+  size_t open_bytes = 0;
+  cudaEvent_t open_ev = nullptr;
   // mailbox for small results: mapped host memory the GPU writes directly
   // (payload, then a sequence flag), polled by the host instead of a copy and
   // a stream synchronisation

@@ -246,12 +246,28 @@ int commit_matrix(whir_ctx* ctx, const uint32_t* d_src, int log_chunk, int log_w
   return WHIR_OK;
 }
 
-// Open `idx` on tree t: appends the query records to the proof and returns
-// the opened rows (Montgomery) in `rows`.
-int open_queries(whir_ctx* ctx, const Tree& t, const std::vector<uint64_t>& idx, std::vector<uint32_t>& proof,
-                 std::vector<uint32_t>& rows) {
+// Opening of `idx` on tree t in two steps. open_start queues the gather of
+// the rows and authentication paths and their copy to host memory, so the
+// prover can queue the next work (constraint weights, a sumcheck stage) before
+// it needs them: the opened values enter no challenger, only the proof and the
+// claimed sum. open_finish waits for the copy, appends the query records to
+// the proof and returns the opened rows (Montgomery) in `rows`. The gathered
+// data live in the scratch arena, which the next work overwrites; the copy is
+// ordered before it on the stream (or, when it does not fit the staging
+// block, done at once).
+struct OpenPending {
+  int q = 0;
+  size_t per = 0;
+  bool staged = false;
+  std::vector<uint32_t> tmp;
+};
+
+int open_start(whir_ctx* ctx, const Tree& t, const std::vector<uint64_t>& idx, OpenPending& op) {
   const int q = (int)idx.size();
   const size_t per = (size_t)t.row_words + (size_t)t.log_h * 8;
+  op.q = q;
+  op.per = per;
+  op.staged = false;
   WH_CHECK((size_t)q * 8 + (size_t)q * per * 4 + 64 <= ctx->arena_bytes, "too many queries for the scratch arena");
   uint64_t* d_idx = reinterpret_cast<uint64_t*>(ctx->d_arena);
   uint32_t* d_rows = reinterpret_cast<uint32_t*>(d_idx + q + 1);
@@ -262,8 +278,30 @@ int open_queries(whir_ctx* ctx, const Tree& t, const std::vector<uint64_t>& idx,
     wh::StageTimer timer(ctx, wh::kStOpen);
     WH_TRY_CUDA(wk::merkle_open(t.rows, t.digests, t.log_h, t.row_words, d_idx, q, d_rows, d_paths, ctx->stream));
   }
-  std::vector<uint32_t> tmp((size_t)q * per);
-  WH_TRY(wh::fetch(ctx, tmp.data(), d_rows, tmp.size() * 4));
+  const size_t bytes = (size_t)q * per * 4;
+  if (ctx->h_open && bytes <= ctx->open_bytes) {
+    WH_TRY_CUDA(cudaMemcpyAsync(ctx->h_open, d_rows, bytes, cudaMemcpyDeviceToHost, ctx->stream));
+    WH_TRY_CUDA(cudaEventRecord(ctx->open_ev, ctx->stream));
+    op.staged = true;
+  } else {
+    op.tmp.resize((size_t)q * per);
+    WH_TRY(wh::fetch(ctx, op.tmp.data(), d_rows, bytes));
+  }
+  return WHIR_OK;
+}
+
+int open_finish(whir_ctx* ctx, const Tree& t, OpenPending& op, std::vector<uint32_t>& proof,
+                std::vector<uint32_t>& rows) {
+  const int q = op.q;
+  const size_t per = op.per;
+  if (q == 0) return WHIR_OK;
+  if (op.staged) {
+    WH_TRY_CUDA(cudaEventSynchronize(ctx->open_ev));
+    op.tmp.resize((size_t)q * per);
+    memcpy(op.tmp.data(), ctx->h_open, (size_t)q * per * 4);
+    op.staged = false;
+  }
+  const std::vector<uint32_t>& tmp = op.tmp;
   rows.assign(tmp.begin(), tmp.begin() + (size_t)q * t.row_words);
   const uint32_t* paths = tmp.data() + (size_t)q * t.row_words;
   const int nvals = t.ext ? t.row_words / 4 : t.row_words;
@@ -615,23 +653,16 @@ int do_prove(whir_ctx* ctx, whir_witness* wit, wh::Chal& ch) {
     (void)ch.sample(ctx->hp16);
     const std::vector<uint64_t> idx = stir_queries(ctx, ch, rc.domain_size, wh::ff_at(c, round), rc.num_queries);
     pf.push_back((uint32_t)idx.size());
-    WH_TRY(open_queries(ctx, prev, idx, pf, rows));
+    // the openings are gathered and copied back while the constraint weights
+    // are queued; their values are needed for the claimed sum only
+    OpenPending op;
+    WH_TRY(open_start(ctx, prev, idx, op));
     const int kprev = wh::ff_at(c, round);
     const ef* frs = fold_rs.data() + fold_rs.size() - kprev;
     std::vector<uint32_t> svars(idx.size());
     std::vector<ef> sevs(idx.size());
     const uint32_t gen = kb::to_mont(rc.folded_domain_gen);
-    for (size_t q = 0; q < idx.size(); q++) {
-      std::vector<ef> vals((size_t)1 << kprev);
-      for (size_t v = 0; v < vals.size(); v++) {
-        if (prev.ext)
-          for (int l = 0; l < 4; l++) vals[v].c[l] = rows[q * prev.row_words + 4 * v + l];
-        else
-          vals[v] = kb::ef_from_base(rows[q * prev.row_words + v]);
-      }
-      sevs[q] = host_eval(vals, frs, kprev);
-      svars[q] = kb::pow(gen, idx[q]);
-    }
+    for (size_t q = 0; q < idx.size(); q++) svars[q] = kb::pow(gen, idx[q]);
     // Constraint::combine (constraints/mod.rs:234-248) then the sumcheck rounds
     const ef gamma = ch.sample_ef(ctx->hp16);
     std::vector<ef> gpow(opts.size());
@@ -645,10 +676,21 @@ int do_prove(whir_ctx* ctx, whir_witness* wit, wh::Chal& ch) {
     std::vector<ef> spow(idx.size());
     for (size_t q = 0; q < idx.size(); q++) {
       spow[q] = g;
-      sum = kb::ef_add(sum, kb::ef_mul(g, sevs[q]));
       g = kb::ef_mul(g, gamma);
     }
     WH_TRY(wh::add_select_vars(ctx, d_w, nv, svars, spow));
+    WH_TRY(open_finish(ctx, prev, op, pf, rows));
+    for (size_t q = 0; q < idx.size(); q++) {
+      std::vector<ef> vals((size_t)1 << kprev);
+      for (size_t v = 0; v < vals.size(); v++) {
+        if (prev.ext)
+          for (int l = 0; l < 4; l++) vals[v].c[l] = rows[q * prev.row_words + 4 * v + l];
+        else
+          vals[v] = kb::ef_from_base(rows[q * prev.row_words + v]);
+      }
+      sevs[q] = host_eval(vals, frs, kprev);
+      sum = kb::ef_add(sum, kb::ef_mul(spow[q], sevs[q]));
+    }
     Sumcheck sd;
     fold_rs.clear();
     WH_TRY(sumcheck_stage(ctx, ch, sd, d_f, d_w, nv, ffn, &sum, rc.folding_pow_bits, &fold_rs, pend));
@@ -676,14 +718,19 @@ int do_prove(whir_ctx* ctx, whir_witness* wit, wh::Chal& ch) {
     const whir_round_config fc = wh::final_round_config(c);
     const std::vector<uint64_t> idx = stir_queries(ctx, ch, fc.domain_size, wh::ff_at(c, c.n_rounds), c.final_queries);
     pf.push_back((uint32_t)idx.size());
-    WH_TRY(open_queries(ctx, prev, idx, pf, rows));
+    // the final openings go into the proof only: their copy overlaps the final
+    // sumcheck rounds, whose records follow them in the proof
+    OpenPending op;
+    WH_TRY(open_start(ctx, prev, idx, op));
     if (c.final_sumcheck_rounds > 0) {
       Sumcheck sd;
       WH_TRY(sumcheck_stage(ctx, ch, sd, d_f, d_w, nv, c.final_sumcheck_rounds, &sum, c.final_folding_pow_bits,
                             nullptr, pend));
+      WH_TRY(open_finish(ctx, prev, op, pf, rows));
       pf.push_back(1u);
       sd.emit(pf);
     } else {
+      WH_TRY(open_finish(ctx, prev, op, pf, rows));
       pf.push_back(0u);
     }
   }
