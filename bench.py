@@ -398,6 +398,19 @@ def micro_lines(kinds, steps: int, warmup: int, echo: bool = False) -> list:
         ms = timed(lambda: pkg.merkle_commit(ctx, rows, log_h, words, 2, dig))
         emit("merkle 2^21 leaves x 16 (Keccak MMCS)", ms, alg_bytes=4 * words << log_h,
              units=2 * (1 << log_h) - 1, unit_name="keccak_f/s")
+        # 64 independent trees of 2^10 .. 2^16 leaves x 16 (a batch's commitments): one call per tree
+        # (each returning its root) against one multi-instance call for all of them
+        hs = [int(h) for h in np.random.default_rng(64).integers(10, 17, 64)]
+        trows = [pkg.DeviceArray.from_host(ctx, rng.integers(0, P, words << h, dtype=np.uint64).astype(np.uint32))
+                 for h in hs]
+        tdig = [pkg.DeviceArray(ctx, (2 * (1 << h) - 1) * 8) for h in hs]
+        perms = sum(2 * (1 << h) - 1 for h in hs)
+        one = timed(lambda: [pkg.merkle_commit(ctx, r, h, words, 0, d) for r, h, d in zip(trows, hs, tdig)])
+        many = timed(lambda: pkg.merkle_commit_many(ctx, trows, hs, words, 0, tdig))
+        emit("merkle 64 trees of 2^10..2^16 leaves x 16, one call per tree", one, units=perms,
+             unit_name="permutations/s")
+        emit("merkle 64 trees of 2^10..2^16 leaves x 16, multi-instance kernels", many, units=perms,
+             unit_name="permutations/s", extra={"speedup_vs_one_call_per_tree": round(one / many, 3)})
     if "grind" in kinds:
         bits = 18
         ch = pkg.DuplexChallenger(ctx)

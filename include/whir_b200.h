@@ -280,6 +280,17 @@ int whir_dft_batch(whir_ctx* ctx, const uint32_t* d_chunks, int32_t log_chunk, i
  * canonical (Poseidon2 families) or the raw words of the Keccak digest. */
 int whir_merkle_commit(whir_ctx* ctx, const uint32_t* d_rows, int32_t log_height, int32_t row_words,
                        int32_t leaf_hash, uint32_t* d_digests, uint32_t* root);
+/* `count` (1..256) independent trees of one Poseidon2 hash family (leaf_hash
+ * WHIR_LEAF_P24 or WHIR_LEAF_P16) and row width, tree i of 2^log_heights[i]
+ * rows at d_rows[i] with its digests at d_digests[i] (laid out as for
+ * whir_merkle_commit), committed together by multi-instance kernels: one leaf
+ * launch whose CTAs claim chunks of leaves from one work queue over all trees,
+ * one launch per tree level across the trees, one root gather. roots: count x
+ * 8 words (host, canonical). Each tree equals whir_merkle_commit's. A batching
+ * entry point with no reference counterpart (the reference commits one matrix
+ * per MerkleTreeMmcs::commit_matrix call). */
+int whir_merkle_commit_many(whir_ctx* ctx, int32_t count, const uint32_t* const* d_rows, const int32_t* log_heights,
+                            int32_t row_words, int32_t leaf_hash, uint32_t* const* d_digests, uint32_t* roots);
 /* Mmcs::open_batch (prover/mod.rs:248-300): row (row_words) and sibling path
  * (log_height digests, leaf level first) for `index`, canonical, to host. */
 /* the same for a tree of hash family leaf_hash (Keccak path words are raw) */

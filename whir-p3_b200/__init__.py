@@ -123,6 +123,7 @@ _SIGS = {
     "whir_monty_decode": (C.c_int, [_vp, _vp, C.c_size_t]),
     "whir_dft_batch": (C.c_int, [_vp, _vp, _i32, _i32, _i32, _i32, _vp]),
     "whir_merkle_commit": (C.c_int, [_vp, _vp, _i32, _i32, _i32, _vp, _u32]),
+    "whir_merkle_commit_many": (C.c_int, [_vp, _i32, _vp, _vp, _i32, _i32, _vp, _vp]),
     "whir_merkle_open": (C.c_int, [_vp, _vp, _vp, _i32, _i32, C.c_uint64, _u32, _u32]),
     "whir_merkle_open_ex": (C.c_int, [_vp, _vp, _vp, _i32, _i32, _i32, C.c_uint64, _u32, _u32]),
     "whir_keccak256": (C.c_int, [C.c_char_p, C.c_size_t, _vp]),
@@ -573,6 +574,22 @@ def merkle_commit(ctx: Context, rows: DeviceArray, log_height: int, row_words: i
     root = np.zeros(8, dtype=np.uint32)
     _check(lib().whir_merkle_commit(ctx.handle, rows.ptr, log_height, row_words, leaf_hash, digests.ptr, root))
     return root
+
+
+def merkle_commit_many(ctx: Context, rows: list, log_heights, row_words: int, leaf_hash: int,
+                       digests: list) -> np.ndarray:
+    """Independent trees (DeviceArrays of rows and digests, one per tree) committed together by the
+    multi-instance kernels; returns the roots, one row of 8 canonical words per tree."""
+    n = len(rows)
+    if n != len(digests) or n != len(log_heights):
+        raise ValueError("rows, log_heights and digests must have one entry per tree")
+    rp = np.array([r.ptr for r in rows], dtype=np.uint64)
+    dp = np.array([d.ptr for d in digests], dtype=np.uint64)
+    lh = np.ascontiguousarray(log_heights, dtype=np.int32)
+    roots = np.zeros((n, 8), dtype=np.uint32)
+    _check(lib().whir_merkle_commit_many(ctx.handle, n, rp.ctypes.data, lh.ctypes.data, row_words, leaf_hash,
+                                         dp.ctypes.data, roots.ctypes.data))
+    return roots
 
 
 # ---------------------------------------------------------------------------

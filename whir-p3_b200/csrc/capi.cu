@@ -764,6 +764,53 @@ int whir_merkle_commit(whir_ctx* ctx, const uint32_t* d_rows, int32_t log_height
   return WHIR_OK;
 }
 
+int whir_merkle_commit_many(whir_ctx* ctx, int32_t count, const uint32_t* const* d_rows, const int32_t* log_heights,
+                            int32_t row_words, int32_t leaf_hash, uint32_t* const* d_digests, uint32_t* roots) {
+  WH_TRY(check_gpu(ctx));
+  WH_CHECK(count >= 1 && count <= wk::kMaxManyTrees && d_rows && log_heights && d_digests && roots && row_words > 0 &&
+               (leaf_hash == WHIR_LEAF_P24 || leaf_hash == WHIR_LEAF_P16),
+           "bad batched Merkle arguments");
+  int max_lh = 0;
+  for (int i = 0; i < count; i++) {
+    WH_CHECK(d_rows[i] && d_digests[i] && log_heights[i] >= 0 && log_heights[i] <= 30, "bad tree in the batch");
+    WH_CHECK((reinterpret_cast<uintptr_t>(d_digests[i]) & 15) == 0, "digest arrays must be 16-byte aligned");
+    max_lh = std::max(max_lh, (int)log_heights[i]);
+  }
+  // descriptors, then for every level the trees' first global nodes and the level's total
+  const size_t stride = (size_t)count + 1;
+  std::vector<wk::TreeDesc> desc((size_t)count);
+  std::vector<unsigned long long> first(stride * (size_t)(max_lh + 1));
+  std::vector<unsigned long long> totals((size_t)max_lh + 1);
+  for (int l = 0; l <= max_lh; l++) {
+    unsigned long long acc = 0;
+    for (int i = 0; i < count; i++) {
+      first[(size_t)l * stride + i] = acc;
+      if (log_heights[i] >= l) acc += 1ull << (log_heights[i] - l);
+    }
+    first[(size_t)l * stride + count] = acc;
+    totals[l] = acc;
+  }
+  for (int i = 0; i < count; i++)
+    desc[i] = wk::TreeDesc{d_rows[i], d_digests[i], first[i], log_heights[i], 0};
+  const size_t desc_bytes = desc.size() * sizeof(wk::TreeDesc), first_bytes = first.size() * 8;
+  WH_CHECK(desc_bytes + first_bytes + (size_t)count * 32 + 64 <= ctx->arena_bytes, "batch tables exceed the arena");
+  uint8_t* base = static_cast<uint8_t*>(ctx->d_arena);
+  auto* d_desc = reinterpret_cast<wk::TreeDesc*>(base);
+  auto* d_first = reinterpret_cast<unsigned long long*>(base + desc_bytes);
+  auto* d_roots = reinterpret_cast<uint32_t*>(base + desc_bytes + first_bytes);
+  WH_TRY(wh::upload(ctx, d_desc, desc.data(), desc_bytes));
+  WH_TRY(wh::upload(ctx, d_first, first.data(), first_bytes));
+  {
+    wh::StageTimer t(ctx, wh::kStLeaves);
+    WH_TRY_CUDA(wk::merkle_many(d_desc, d_first, count, max_lh, totals.data(), row_words, leaf_hash, ctx->p16,
+                                ctx->p24, reinterpret_cast<unsigned*>(ctx->d_words) + 13, d_roots, ctx->stream));
+  }
+  std::vector<uint32_t> r((size_t)count * 8);
+  WH_TRY(wh::fetch(ctx, r.data(), d_roots, r.size() * 4));
+  for (size_t k = 0; k < r.size(); k++) roots[k] = kb::from_mont(r[k]);
+  return WHIR_OK;
+}
+
 int whir_keccak256(const uint8_t* data, size_t n, uint8_t* out32) {
   WH_CHECK((data || n == 0) && out32, "null argument");
   kk::K256 k;

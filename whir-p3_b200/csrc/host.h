@@ -149,7 +149,7 @@ struct whir_ctx {
   kb::ef* d_small = nullptr;     // 256 ef
   uint32_t* d_words = nullptr;   // 16 words: grind result, claim and done counters (0-2), sumcheck round (8),
                                  // dot product (9) and tree-top (10) counters, streamed-dot wait flag (11),
-                                 // staged DFT pass flags (12)
+                                 // staged DFT pass flags (12), batched-tree work counter (13)
   void* d_arena = nullptr;       // general scratch (tables, gathers)
   // device transcript area (kDevTrWords words): the device challenger, the
   // folded state of the next search, an error word and per-round logs of a

@@ -996,6 +996,17 @@ cudaError_t merkle_leaves(const uint32_t* rows, int log_h, int row_words, int le
   return merkle_leaves_m<p2::kMatMds>(rows, log_h, row_words, leaf_hash, digests, p16, p24, leaf, st);
 }
 
+cudaError_t merkle_many(const TreeDesc* d_desc, const unsigned long long* d_level_first, int count, int max_log_h,
+                        const unsigned long long* level_totals, int row_words, int leaf_hash, const P2Consts& p16,
+                        const P2Consts& p24, unsigned* counter, uint32_t* d_roots, cudaStream_t st) {
+  if (p16.mat != p24.mat) return cudaErrorInvalidValue;
+  if (p16.mat == (uint32_t)p2::kMatHl)
+    return merkle_many_m<p2::kMatHl>(d_desc, d_level_first, count, max_log_h, level_totals, row_words, leaf_hash,
+                                     p16, p24, counter, d_roots, st);
+  return merkle_many_m<p2::kMatMds>(d_desc, d_level_first, count, max_log_h, level_totals, row_words, leaf_hash, p16,
+                                    p24, counter, d_roots, st);
+}
+
 cudaError_t merkle_upper(int log_h, uint32_t* digests, const P2Consts& p16, Shape node, unsigned* counter,
                          uint32_t* mail, uint32_t seq, int* posted, cudaStream_t st) {
   if (p16.mat == (uint32_t)p2::kMatHl)

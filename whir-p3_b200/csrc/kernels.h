@@ -211,6 +211,26 @@ cudaError_t sumcheck_round_tr(kb::ef* f, kb::ef* w, size_t q, int fold, kb::ef r
                               uint32_t* err, int grind_next, uint32_t* cp_out, kb::ef* r_out,
                               const p2::P2Consts& p16, cudaStream_t st);
 
+// Many independent Poseidon2 trees (the same row width and leaf hash, tree i
+// of 2^log_h leaves with its own digest array laid out as merkle_build's) in
+// one leaf launch, one launch per tree level and one root gather: the leaf
+// kernel's CTAs claim chunks of leaves from `counter` over all trees' leaves.
+// d_desc: the trees (leaf0 = the tree's first global leaf, increasing from
+// 0); d_level_first: for every level l in 0..max_log_h, count + 1 entries
+// (tree i's first global node of level l, then the level's total);
+// level_totals (host): those totals. The roots land in d_roots[8 * i].
+struct TreeDesc {
+  const uint32_t* rows;
+  uint32_t* digests;
+  unsigned long long leaf0;
+  int log_h;
+  int pad;
+};
+constexpr int kMaxManyTrees = 256;
+cudaError_t merkle_many(const TreeDesc* d_desc, const unsigned long long* d_level_first, int count, int max_log_h,
+                        const unsigned long long* level_totals, int row_words, int leaf_hash, const p2::P2Consts& p16,
+                        const p2::P2Consts& p24, unsigned* counter, uint32_t* d_roots, cudaStream_t st);
+
 // The Poseidon2 launchers above for one external block MAT (p2::kMatMds or
 // p2::kMatHl), each form built in its own translation unit; merkle_leaves,
 // merkle_upper and grind pick the form of their constants (P2Consts::mat).
@@ -220,6 +240,11 @@ cudaError_t merkle_leaves_m(const uint32_t* rows, int log_h, int row_words, int 
 template <int MAT>
 cudaError_t merkle_upper_m(int log_h, uint32_t* digests, const p2::P2Consts& p16, Shape node, unsigned* counter,
                            uint32_t* mail, uint32_t seq, int* posted, cudaStream_t st);
+template <int MAT>
+cudaError_t merkle_many_m(const TreeDesc* d_desc, const unsigned long long* d_level_first, int count, int max_log_h,
+                          const unsigned long long* level_totals, int row_words, int leaf_hash,
+                          const p2::P2Consts& p16, const p2::P2Consts& p24, unsigned* counter, uint32_t* d_roots,
+                          cudaStream_t st);
 template <int MAT>
 cudaError_t grind_m(const uint32_t* state, const uint32_t* in, int in_len, int bits, uint64_t limit,
                     uint32_t* result, uint32_t* counter, uint32_t* done, uint32_t* mail, uint32_t seq,

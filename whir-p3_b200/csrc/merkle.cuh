@@ -987,4 +987,152 @@ cudaError_t sumcheck_round_tr_m(ef* f, ef* w, size_t q, int fold, ef r, ef* part
   LAUNCH_DONE();
 }
 
+// ---------------------------------------------------------------------------
+// Many independent trees in few launches (merkle_many_m): one leaf launch for
+// all trees and one launch per tree level across all trees tall enough to
+// have it. The leaf kernel is persistent: its CTAs claim chunks of
+// MANY_CTA leaves from one work counter over the trees' concatenated leaves,
+// and a table of each tree's first global leaf (binary-searched in shared
+// memory) maps a claimed leaf to its tree. A level launch maps its global node
+// index to (tree, node) the same way through that level's table.
+// ---------------------------------------------------------------------------
+
+constexpr int MANY_CTA = 256;
+
+namespace {
+
+// the largest i < count with first[i] <= g (first strictly increasing, first[0] = 0)
+__device__ __forceinline__ int tree_of(const unsigned long long* first, int count, unsigned long long g) {
+  int lo = 0, hi = count - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (first[mid] <= g) lo = mid;
+    else hi = mid - 1;
+  }
+  return lo;
+}
+
+template <int T, int RP, int RATE, int MAT>
+__global__ void __launch_bounds__(MANY_CTA) k_leaves_many(const TreeDesc* __restrict__ desc, int count,
+                                                          int row_words, unsigned* __restrict__ counter,
+                                                          const __grid_constant__ P2Consts leaf) {
+  __shared__ unsigned long long s_first[kMaxManyTrees + 1];
+  __shared__ unsigned long long s_start;
+  for (int i = threadIdx.x; i <= count; i += blockDim.x)
+    s_first[i] = i < count ? desc[i].leaf0 : desc[count - 1].leaf0 + (1ull << desc[count - 1].log_h);
+  __syncthreads();
+  const unsigned long long total = s_first[count];
+  for (;;) {
+    if (threadIdx.x == 0) s_start = (unsigned long long)atomicAdd(counter, 1u) * MANY_CTA;
+    __syncthreads();
+    const unsigned long long start = s_start;
+    __syncthreads();
+    if (start >= total) break;
+    const unsigned long long g = start + threadIdx.x;
+    if (g >= total) continue;
+    const int tr = tree_of(s_first, count, g);
+    const size_t i = (size_t)(g - s_first[tr]);
+    uint32_t s[T];
+#pragma unroll
+    for (int k = 0; k < T; k++) s[k] = 0u;
+    const uint32_t* row = desc[tr].rows + i * (size_t)row_words;
+    for (int pos = 0; pos < row_words; pos += RATE) {
+      const int take = row_words - pos < RATE ? row_words - pos : RATE;
+#pragma unroll
+      for (int k = 0; k < RATE; k++)
+        if (k < take) s[k] = kb::from_mont(__ldg(row + pos + k));
+      const bool first = pos == 0, last = pos + RATE >= row_words;
+      if (first && last) p2::permute_sponge<T, RP, RATE, true, true, MAT>(s, leaf);
+      else if (first) p2::permute_sponge<T, RP, RATE, true, false, MAT>(s, leaf);
+      else if (last) p2::permute_sponge<T, RP, RATE, false, true, MAT>(s, leaf);
+      else p2::permute_sponge<T, RP, RATE, false, false, MAT>(s, leaf);
+    }
+#pragma unroll
+    for (int k = 0; k < 8; k++) s[k] = kb::to_mont(s[k]);
+    uint4* d = reinterpret_cast<uint4*>(desc[tr].digests + i * 8);
+    d[0] = make_uint4(s[0], s[1], s[2], s[3]);
+    d[1] = make_uint4(s[4], s[5], s[6], s[7]);
+  }
+}
+
+// level `level` (>= 1) of every tree with log_h >= level; first[i] is tree
+// i's first global node of this level (first[count] = all of them)
+template <int MAT>
+__global__ void __launch_bounds__(MANY_CTA) k_level_many(const TreeDesc* __restrict__ desc,
+                                                         const unsigned long long* __restrict__ first, int count,
+                                                         int level, const __grid_constant__ P2Consts comp) {
+  __shared__ unsigned long long s_first[kMaxManyTrees + 1];
+  for (int i = threadIdx.x; i <= count; i += blockDim.x) s_first[i] = first[i];
+  __syncthreads();
+  const unsigned long long total = s_first[count];
+  for (unsigned long long g = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x; g < total;
+       g += (unsigned long long)gridDim.x * blockDim.x) {
+    const int tr = tree_of(s_first, count, g);
+    const size_t j = (size_t)(g - s_first[tr]);
+    const int lh = desc[tr].log_h;
+    // level l starts at node 2h - 2^(lh - l + 1)
+    const size_t h2 = (size_t)2 << lh;
+    const size_t in_off = h2 - ((size_t)1 << (lh - level + 2)), out_off = h2 - ((size_t)1 << (lh - level + 1));
+    uint32_t* dg = desc[tr].digests;
+    uint32_t x[16];
+    const uint4* src = reinterpret_cast<const uint4*>(dg + (in_off + 2 * j) * 8);
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+      const uint4 v = src[q];
+      x[4 * q] = v.x;
+      x[4 * q + 1] = v.y;
+      x[4 * q + 2] = v.z;
+      x[4 * q + 3] = v.w;
+    }
+    compress_mont<MAT>(x, comp);
+    uint4* dst = reinterpret_cast<uint4*>(dg + (out_off + j) * 8);
+    dst[0] = make_uint4(x[0], x[1], x[2], x[3]);
+    dst[1] = make_uint4(x[4], x[5], x[6], x[7]);
+  }
+}
+
+// the roots (node 2h - 2 of every tree) gathered into roots[8 * i]
+__global__ void k_roots_many(const TreeDesc* __restrict__ desc, int count, uint32_t* __restrict__ roots) {
+  for (int k = threadIdx.x; k < count * 8; k += blockDim.x) {
+    const int i = k >> 3;
+    const size_t root = ((size_t)2 << desc[i].log_h) - 2;
+    roots[k] = desc[i].digests[root * 8 + (k & 7)];
+  }
+}
+
+}  // namespace
+
+template <int MAT>
+cudaError_t merkle_many_m(const TreeDesc* d_desc, const unsigned long long* d_level_first, int count, int max_log_h,
+                          const unsigned long long* level_totals, int row_words, int leaf_hash, const P2Consts& p16,
+                          const P2Consts& p24, unsigned* counter, uint32_t* d_roots, cudaStream_t st) {
+  if (count < 1 || count > kMaxManyTrees || row_words < 1 || max_log_h < 0 || max_log_h > 30 ||
+      (leaf_hash != 0 && leaf_hash != 1))
+    return cudaErrorInvalidValue;
+  cudaError_t e = cudaMemsetAsync(counter, 0, sizeof(unsigned), st);
+  if (e != cudaSuccess) return e;
+  const unsigned long long leaves = level_totals[0];
+  size_t blocks = (size_t)((leaves + MANY_CTA - 1) / MANY_CTA);
+  const size_t cap = (size_t)sm_count() * 4;  // resident CTAs of the leaf sponge
+  if (blocks > cap) blocks = cap;
+  if (leaf_hash == 0)
+    k_leaves_many<24, p2::RP24, 16, MAT><<<(unsigned)blocks, MANY_CTA, 0, st>>>(d_desc, count, row_words, counter, p24);
+  else
+    k_leaves_many<16, p2::RP16, 8, MAT><<<(unsigned)blocks, MANY_CTA, 0, st>>>(d_desc, count, row_words, counter, p16);
+  count_launch();
+  if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  for (int l = 1; l <= max_log_h; l++) {
+    size_t b = (size_t)((level_totals[l] + MANY_CTA - 1) / MANY_CTA);
+    const size_t lcap = (size_t)sm_count() * 8;
+    if (b > lcap) b = lcap;
+    if (b < 1) b = 1;
+    k_level_many<MAT><<<(unsigned)b, MANY_CTA, 0, st>>>(d_desc, d_level_first + (size_t)l * (count + 1), count, l,
+                                                         p16);
+    count_launch();
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  }
+  k_roots_many<<<1, 256, 0, st>>>(d_desc, count, d_roots);
+  LAUNCH_DONE();
+}
+
 }  // namespace wk

@@ -8,6 +8,9 @@ template cudaError_t merkle_leaves_m<p2::kMatMds>(const uint32_t*, int, int, int
                                                   const p2::P2Consts&, Shape, cudaStream_t);
 template cudaError_t merkle_upper_m<p2::kMatMds>(int, uint32_t*, const p2::P2Consts&, Shape, unsigned*, uint32_t*,
                                                  uint32_t, int*, cudaStream_t);
+template cudaError_t merkle_many_m<p2::kMatMds>(const TreeDesc*, const unsigned long long*, int, int,
+                                               const unsigned long long*, int, int, const p2::P2Consts&,
+                                               const p2::P2Consts&, unsigned*, uint32_t*, cudaStream_t);
 template cudaError_t grind_m<p2::kMatMds>(const uint32_t*, const uint32_t*, int, int, uint64_t, uint32_t*, uint32_t*,
                                           uint32_t*, uint32_t*, uint32_t, const p2::P2Consts&, cudaStream_t,
                                           const uint32_t*, uint32_t*, DevChal*, kb::ef*, uint32_t*, int);
