@@ -398,9 +398,8 @@ int whir_commit_and_prove(whir_ctx* ctx, const whir_protocol_params* params, int
 
 /* ---- batching and serving -------------------------------------------------
  * A pool of worker threads on one device, each with its own context and CUDA
- * stream, proves submitted jobs concurrently (the north star's batching and
- * serving patterns; no counterpart in the reference, which proves one
- * polynomial per call). A job is admitted when the device memory the pool
+ * stream, proves submitted jobs concurrently (batching and serving; no
+ * counterpart in the reference, which proves one polynomial per call). A job is admitted when the device memory the pool
  * would then hold fits the HBM budget: every worker context's fixed
  * allocations, plus per worker the larger of its stream-ordered pool's
  * reservation and its running job's charge (footprint plus one 32 MiB pool
