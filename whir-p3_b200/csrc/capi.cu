@@ -327,7 +327,32 @@ int add_eq_points(whir_ctx* ctx, ef* d_w, int n, const std::vector<std::vector<e
   WH_CHECK((H + Lc) * (size_t)m * sizeof(ef) <= ctx->arena_bytes, "too many constraints for the scratch arena");
   ef* hi = reinterpret_cast<ef*>(ctx->d_arena);
   ef* lo = hi + H * m;
-  for (int c = 0; c < m; c++) WH_TRY(split_eq_tables(ctx, pts[c].data(), n, scales[c], lo_bits, hi + H * c, lo + Lc * c));
+  // the split tables of up to four points per launch (their hi and lo tables)
+  const int hb = n - lo_bits;
+  if (hb <= wk::kEqMultiCoords) {
+    for (int c0 = 0; c0 < m; c0 += wk::kEqMultiTables / 2) {
+      wk::EqMulti em;
+      memset(&em, 0, sizeof(em));
+      for (int c = c0; c < m && c < c0 + wk::kEqMultiTables / 2; c++) {
+        const int th = em.count, tl = em.count + 1;
+        em.h[th] = hb;
+        em.zoff[th] = th * wk::kEqMultiCoords;
+        em.out[th] = hi + H * c;
+        em.scale[th] = scales[c];
+        em.h[tl] = lo_bits;
+        em.zoff[tl] = tl * wk::kEqMultiCoords;
+        em.out[tl] = lo + Lc * c;
+        em.scale[tl] = kb::ef_one();
+        for (int i = 0; i < hb; i++) em.z[em.zoff[th] + i] = pts[c][i];
+        for (int i = 0; i < lo_bits; i++) em.z[em.zoff[tl] + i] = pts[c][hb + i];
+        em.count += 2;
+      }
+      WH_TRY_CUDA(wk::eq_tables_multi(em, ctx->stream));
+    }
+  } else {
+    for (int c = 0; c < m; c++)
+      WH_TRY(split_eq_tables(ctx, pts[c].data(), n, scales[c], lo_bits, hi + H * c, lo + Lc * c));
+  }
   for (int c0 = 0; c0 < m; c0 += 16) {
     const int cnt = std::min(16, m - c0);
     WH_TRY_CUDA(wk::add_eq_batch(d_w, n, hi + H * c0, lo + Lc * c0, lo_bits, cnt, accumulate || c0 > 0, ctx->stream));

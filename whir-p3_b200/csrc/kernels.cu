@@ -1122,6 +1122,41 @@ cudaError_t eq_table_pair(const EqPoint& p1, ef* out1, const EqPoint& p2, ef* ou
   LAUNCH_DONE();
 }
 
+// several eq tables in one launch (the split tables of several points)
+__global__ void k_eq_multi(const __grid_constant__ EqMulti m) {
+  size_t total = 0;
+  for (int t = 0; t < m.count; t++) total += (size_t)1 << m.h[t];
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < total; i += (size_t)gridDim.x * blockDim.x) {
+    int t = 0;
+    size_t x = i;
+    while (x >= ((size_t)1 << m.h[t])) {
+      x -= (size_t)1 << m.h[t];
+      t++;
+    }
+    const int h = m.h[t];
+    const ef* z = m.z + m.zoff[t];
+    ef acc = m.scale[t];
+    for (int j = 0; j < h; j++) {
+      const bool bit = (x >> (h - 1 - j)) & 1;
+      acc = kb::ef_mul(acc, bit ? z[j] : kb::ef_sub(kb::ef_one(), z[j]));
+    }
+    st_ef(m.out[t] + x, acc);
+  }
+}
+
+cudaError_t eq_tables_multi(const EqMulti& m, cudaStream_t st) {
+  if (m.count < 1 || m.count > kEqMultiTables) return cudaErrorInvalidValue;
+  size_t n = 0;
+  for (int t = 0; t < m.count; t++) {
+    if (m.h[t] < 0 || m.h[t] > kEqMultiCoords || m.zoff[t] < 0 ||
+        m.zoff[t] + m.h[t] > kEqMultiTables * kEqMultiCoords || !m.out[t])
+      return cudaErrorInvalidValue;
+    n += (size_t)1 << m.h[t];
+  }
+  k_eq_multi<<<grid_for(n, 256), 256, 0, st>>>(m);
+  LAUNCH_DONE();
+}
+
 cudaError_t eq_table_small(const EqPoint& pt, ef* out, cudaStream_t st) {
   if (pt.h < 0 || pt.h > 20) return cudaErrorInvalidValue;
   const size_t n = (size_t)1 << pt.h;

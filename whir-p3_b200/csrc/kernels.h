@@ -268,6 +268,18 @@ cudaError_t eq_outer(const kb::ef* hi, const kb::ef* lo, int lo_bits, size_t n, 
 
 // both tables of a split point in one launch
 cudaError_t eq_table_pair(const EqPoint& p1, kb::ef* out1, const EqPoint& p2, kb::ef* out2, cudaStream_t st);
+// up to kEqMultiTables tables of at most kEqMultiCoords coordinates each in one
+// launch: table t is scale[t] * eq(z[zoff[t] ..], .) over 2^h[t] entries into out[t]
+constexpr int kEqMultiTables = 8, kEqMultiCoords = 16;
+struct EqMulti {
+  int count;
+  int h[kEqMultiTables];
+  int zoff[kEqMultiTables];
+  kb::ef* out[kEqMultiTables];
+  kb::ef scale[kEqMultiTables];
+  kb::ef z[kEqMultiTables * kEqMultiCoords];
+};
+cudaError_t eq_tables_multi(const EqMulti& m, cudaStream_t st);
 
 // segmented split-eq dot products:
 //   out[s] = sum_{x < M} f[s*M + x] * hi[x >> lo_bits] * lo[x & mask],  M = 2^m_bits, s < 2^seg_bits
