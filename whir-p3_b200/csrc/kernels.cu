@@ -1054,11 +1054,9 @@ cudaError_t merkle_build(const uint32_t* rows, int log_h, int row_words, int lea
 }
 
 // Mmcs::open_batch gather (src/whir/prover/mod.rs:248-300, 378-401)
-__global__ void k_merkle_open(const uint32_t* __restrict__ rows, const uint32_t* __restrict__ digests, int log_h,
-                              int row_words, const uint64_t* __restrict__ idx, uint32_t* __restrict__ rows_out,
-                              uint32_t* __restrict__ paths_out) {
-  const int q = blockIdx.x;
-  const uint64_t i = idx[q];
+__device__ __forceinline__ void open_one(const uint32_t* __restrict__ rows, const uint32_t* __restrict__ digests,
+                                         int log_h, int row_words, int q, uint64_t i, uint32_t* __restrict__ rows_out,
+                                         uint32_t* __restrict__ paths_out) {
   for (int w = threadIdx.x; w < row_words; w += blockDim.x)
     rows_out[(size_t)q * row_words + w] = rows[i * row_words + w];
   for (int k = threadIdx.x; k < log_h * 8; k += blockDim.x) {
@@ -1073,11 +1071,38 @@ __global__ void k_merkle_open(const uint32_t* __restrict__ rows, const uint32_t*
   }
 }
 
+__global__ void k_merkle_open(const uint32_t* __restrict__ rows, const uint32_t* __restrict__ digests, int log_h,
+                              int row_words, const uint64_t* __restrict__ idx, uint32_t* __restrict__ rows_out,
+                              uint32_t* __restrict__ paths_out) {
+  open_one(rows, digests, log_h, row_words, blockIdx.x, idx[blockIdx.x], rows_out, paths_out);
+}
+
+// the indices in the launch's parameter block
+struct OpenIdx {
+  uint64_t i[kOpenParamIdx];
+};
+__global__ void k_merkle_open_p(const uint32_t* __restrict__ rows, const uint32_t* __restrict__ digests, int log_h,
+                                int row_words, const __grid_constant__ OpenIdx idx, uint32_t* __restrict__ rows_out,
+                                uint32_t* __restrict__ paths_out) {
+  open_one(rows, digests, log_h, row_words, blockIdx.x, idx.i[blockIdx.x], rows_out, paths_out);
+}
+
 cudaError_t merkle_open(const uint32_t* rows, const uint32_t* digests, int log_h, int row_words,
                         const uint64_t* d_idx, int count, uint32_t* d_rows_out, uint32_t* d_paths_out,
                         cudaStream_t st) {
   if (count <= 0) return cudaSuccess;
   k_merkle_open<<<count, 128, 0, st>>>(rows, digests, log_h, row_words, d_idx, d_rows_out, d_paths_out);
+  LAUNCH_DONE();
+}
+
+cudaError_t merkle_open_host_idx(const uint32_t* rows, const uint32_t* digests, int log_h, int row_words,
+                                 const uint64_t* h_idx, int count, uint32_t* d_rows_out, uint32_t* d_paths_out,
+                                 cudaStream_t st) {
+  if (count <= 0) return cudaSuccess;
+  if (count > kOpenParamIdx) return cudaErrorInvalidValue;
+  OpenIdx ix;
+  memcpy(ix.i, h_idx, (size_t)count * 8);
+  k_merkle_open_p<<<count, 128, 0, st>>>(rows, digests, log_h, row_words, ix, d_rows_out, d_paths_out);
   LAUNCH_DONE();
 }
 

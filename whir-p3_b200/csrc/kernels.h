@@ -142,6 +142,12 @@ cudaError_t merkle_upper(int log_h, uint32_t* digests, const p2::P2Consts& p16, 
 cudaError_t merkle_open(const uint32_t* rows, const uint32_t* digests, int log_h, int row_words,
                         const uint64_t* d_idx, int count, uint32_t* d_rows_out, uint32_t* d_paths_out,
                         cudaStream_t st);
+// the same with up to kOpenParamIdx indices read from host memory into the
+// launch's parameter block (no upload of the indices)
+constexpr int kOpenParamIdx = 480;
+cudaError_t merkle_open_host_idx(const uint32_t* rows, const uint32_t* digests, int log_h, int row_words,
+                                 const uint64_t* h_idx, int count, uint32_t* d_rows_out, uint32_t* d_paths_out,
+                                 cudaStream_t st);
 
 // PoW search: smallest w in [0, limit) such that the duplex challenger whose
 // sponge state is `state` (16 words) with pending inputs in[0..in_len) samples

@@ -273,8 +273,13 @@ int open_start(whir_ctx* ctx, const Tree& t, const std::vector<uint64_t>& idx, O
   uint32_t* d_rows = reinterpret_cast<uint32_t*>(d_idx + q + 1);
   uint32_t* d_paths = d_rows + (size_t)q * t.row_words;
   if (q == 0) return WHIR_OK;
-  WH_TRY(wh::upload(ctx, d_idx, idx.data(), (size_t)q * 8));
-  {
+  if (q <= wk::kOpenParamIdx) {
+    // the indices travel in the gather kernel's parameters
+    wh::StageTimer timer(ctx, wh::kStOpen);
+    WH_TRY_CUDA(wk::merkle_open_host_idx(t.rows, t.digests, t.log_h, t.row_words, idx.data(), q, d_rows, d_paths,
+                                         ctx->stream));
+  } else {
+    WH_TRY(wh::upload(ctx, d_idx, idx.data(), (size_t)q * 8));
     wh::StageTimer timer(ctx, wh::kStOpen);
     WH_TRY_CUDA(wk::merkle_open(t.rows, t.digests, t.log_h, t.row_words, d_idx, q, d_rows, d_paths, ctx->stream));
   }
