@@ -810,7 +810,9 @@ int whir_merkle_commit_many(whir_ctx* ctx, int32_t count, const uint32_t* const*
     unsigned long long acc = 0;
     for (int i = 0; i < count; i++) {
       first[(size_t)l * stride + i] = acc;
-      if (log_heights[i] >= l) acc += 1ull << (log_heights[i] - l);
+      // level l of tree i is built by a level launch when it lies below the
+      // tree's top (its levels above 2^kManyTopLevels nodes go to one CTA)
+      if (l == 0 || log_heights[i] - l >= wk::kManyTopLevels) acc += 1ull << (log_heights[i] - l);
     }
     first[(size_t)l * stride + count] = acc;
     totals[l] = acc;

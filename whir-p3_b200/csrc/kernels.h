@@ -223,8 +223,9 @@ cudaError_t sumcheck_round_tr(kb::ef* f, kb::ef* w, size_t q, int fold, kb::ef r
 // kernel's CTAs claim chunks of leaves from `counter` over all trees' leaves.
 // d_desc: the trees (leaf0 = the tree's first global leaf, increasing from
 // 0); d_level_first: for every level l in 0..max_log_h, count + 1 entries
-// (tree i's first global node of level l, then the level's total);
-// level_totals (host): those totals. The roots land in d_roots[8 * i].
+// (tree i's first global node of level l among the trees whose level l is
+// below their top, then the level's total); level_totals (host): those
+// totals. The roots land in d_roots[8 * i].
 struct TreeDesc {
   const uint32_t* rows;
   uint32_t* digests;
@@ -233,6 +234,10 @@ struct TreeDesc {
   int pad;
 };
 constexpr int kMaxManyTrees = 256;
+// the levels of a tree's top done in one CTA: the top starts at the level of
+// 2^kManyTopLevels nodes (level log_h - kManyTopLevels), or at the leaves; the
+// level launches (d_level_first) cover levels 1 .. log_h - kManyTopLevels only
+constexpr int kManyTopLevels = 8;
 cudaError_t merkle_many(const TreeDesc* d_desc, const unsigned long long* d_level_first, int count, int max_log_h,
                         const unsigned long long* level_totals, int row_words, int leaf_hash, const p2::P2Consts& p16,
                         const p2::P2Consts& p24, unsigned* counter, uint32_t* d_roots, cudaStream_t st);

@@ -1091,6 +1091,24 @@ __global__ void __launch_bounds__(MANY_CTA) k_level_many(const TreeDesc* __restr
   }
 }
 
+// the top of every tree in one launch, one CTA per tree: the levels above
+// the tree's level of at most TOP_NODES nodes (level max(0, log_h - 8)), by
+// four-lane cooperative permutations in shared memory (coop_levels)
+template <int MAT>
+__global__ void __launch_bounds__(TOP_CTA) k_tops_many(const TreeDesc* __restrict__ desc,
+                                                       const __grid_constant__ P2Consts comp) {
+  __shared__ uint32_t sh[TOP_NODES * 8];
+  const int lh = desc[blockIdx.x].log_h;
+  if (lh == 0) return;  // a one-leaf tree: its leaf is its root
+  const int start = lh > kManyTopLevels ? lh - kManyTopLevels : 0;
+  const int cnt = 1 << (lh - start);
+  uint32_t* dg = desc[blockIdx.x].digests;
+  size_t off = ((size_t)2 << lh) - ((size_t)1 << (lh - start + 1)), lsz = (size_t)cnt;
+  for (int k = threadIdx.x; k < cnt * 8; k += blockDim.x) sh[k] = dg[off * 8 + k];
+  __syncthreads();
+  coop_levels<MAT>(sh, cnt, lh - start, 0, off, lsz, dg, comp);
+}
+
 // the roots (node 2h - 2 of every tree) gathered into roots[8 * i]
 __global__ void k_roots_many(const TreeDesc* __restrict__ desc, int count, uint32_t* __restrict__ roots) {
   for (int k = threadIdx.x; k < count * 8; k += blockDim.x) {
@@ -1121,13 +1139,19 @@ cudaError_t merkle_many_m(const TreeDesc* d_desc, const unsigned long long* d_le
     k_leaves_many<16, p2::RP16, 8, MAT><<<(unsigned)blocks, MANY_CTA, 0, st>>>(d_desc, count, row_words, counter, p16);
   count_launch();
   if ((e = cudaGetLastError()) != cudaSuccess) return e;
-  for (int l = 1; l <= max_log_h; l++) {
+  // level launches up to each tree's top, then one CTA per tree for the tops
+  for (int l = 1; l <= max_log_h - kManyTopLevels; l++) {
     size_t b = (size_t)((level_totals[l] + MANY_CTA - 1) / MANY_CTA);
     const size_t lcap = (size_t)sm_count() * 8;
     if (b > lcap) b = lcap;
     if (b < 1) b = 1;
     k_level_many<MAT><<<(unsigned)b, MANY_CTA, 0, st>>>(d_desc, d_level_first + (size_t)l * (count + 1), count, l,
                                                          p16);
+    count_launch();
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  }
+  if (max_log_h > 0) {
+    k_tops_many<MAT><<<count, TOP_CTA, 0, st>>>(d_desc, p16);
     count_launch();
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
   }
